@@ -1,0 +1,322 @@
+"""Benchmark: humanoid batched step, nworld=8192 per GPU, steps/s (one JSON line on rank 0).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--form fused|plain]
+
+Workload: the reference's humanoid (27 dof, 21 motors) with implicitfast integration, dt=0.005,
+Newton with 3 iterations and 4 line-search iterations, pyramidal condim-3 contacts; seeded
+synthetic initial states (keyframe "squat" + U(-0.05, 0.05), qvel ~ N(0, 0.01),
+ctrl ~ U(-0.4, 0.4)).  A "step" is one mjw.step over all worlds.
+
+value: world-steps/s with the state resident in HBM, one captured CUDA graph of the step replayed
+K times.  e2e: the same metric through the public API (mjw.step) with, every step, the control
+copied in from pinned host memory and qpos / qvel copied back.  Multi-GPU: one process per GPU,
+each owning its own 8192 worlds (replicas, weak scaling, no collective on the data path); time is
+the maximum over ranks of CUDA-event time between barriers.
+
+--impl reference times the reference algorithm's CPU implementation available here — the CPU
+restatement under oracle/, FP32, all host threads — on the same workload.
+"""
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+NWORLD = 8192
+MODEL = os.path.join(ROOT, "tests", "golden", "models", "humanoid.xml")
+METRIC = "humanoid nworld=8192 steps/s"
+WORKLOAD = "humanoid step, implicitfast dt=0.005, Newton 3 it / ls 4, pyramidal condim 3"
+
+
+def _model():
+  from mjx_warp_b200 import mjcf
+
+  mjm = mjcf.from_xml_path(MODEL)
+  mjm.opt.integrator, mjm.opt.timestep = 3, 0.005
+  mjm.opt.solver, mjm.opt.iterations, mjm.opt.ls_iterations = 2, 3, 4
+  return mjm
+
+
+def _state(mjm, start, count, seed=0):
+  """Seeded per-world initial states; world w gets the same state however worlds are sharded."""
+  from mjx_warp_b200.replicas import world_seeds
+
+  qpos = np.empty((count, mjm.nq))
+  qvel = np.empty((count, mjm.nv))
+  ctrl = np.empty((count, mjm.nu))
+  for i, s in enumerate(world_seeds(seed, start, count)):
+    rng = np.random.default_rng(int(s))
+    q = mjm.key_qpos[0] + rng.uniform(-0.05, 0.05, mjm.nq)
+    q[3:7] /= np.linalg.norm(q[3:7])
+    qpos[i], qvel[i], ctrl[i] = q, rng.normal(0, 0.01, mjm.nv), rng.uniform(-0.4, 0.4, mjm.nu)
+  return qpos, qvel, ctrl
+
+
+class _Clocks:
+  """Samples nvidia-smi clocks and throttle reasons during the timed region."""
+
+  FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+            "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+            "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+  def __init__(self, index):
+    self.index = index
+    self.rows = []
+    self.proc = None
+
+  def __enter__(self):
+    try:
+      self.proc = subprocess.Popen(
+        ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+         "--format=csv,noheader,nounits", "-lms", "200"],
+        stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+      threading.Thread(target=self._read, daemon=True).start()
+    except OSError:
+      self.proc = None
+    return self
+
+  def _read(self):
+    for line in self.proc.stdout:
+      self.rows.append([x.strip() for x in line.split(",")])
+
+  def __exit__(self, *a):
+    if self.proc:
+      time.sleep(0.25)
+      self.proc.terminate()
+      try:
+        self.proc.wait(timeout=2)
+      except subprocess.TimeoutExpired:
+        self.proc.kill()
+
+  def summary(self):
+    if not self.rows:
+      return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+    sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+    mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+    names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+    reasons = sorted({n for r in self.rows for n, v in zip(names, r[4:8]) if v == "Active"})
+    return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+            "reasons": reasons, "samples": len(self.rows)}
+
+
+def _bytes_of(t):
+  return t.numel() * t.element_size()
+
+
+def _algorithmic_bytes(d, mjm, ncon, nefc):
+  """HBM bytes one step must move in full-Data mode: read the state, write every Data field the
+  step produces (smooth quantities, contacts, constraint rows, solver vectors)."""
+  W = d.nworld
+  f = 4
+  nq, nv, nu, nb, nj, ng, ns = mjm.nq, mjm.nv, mjm.nu, mjm.nbody, mjm.njnt, mjm.ngeom, mjm.nsite
+  read_state = (nq + 2 * nv + nu + nv + 6 * nb) * f  # qpos, qvel, qacc_warmstart, ctrl, qfrc_applied, xfrc
+  per_world_out = (nb * (3 + 4 + 9 + 3 + 9 + 3 + 10 + 10 + 6 + 6 + 6) + nj * 6 + ng * 12 + ns * 12
+                   + nv * 6 * 2 + nv * nv * 2 + nu * (3 + nv) + nv * 14 + nq + nv * nv) * f
+  contact_bytes = ncon * (1 + 3 + 9 + 1 + 5 + 2 + 2 + 5 + 1 + 2 + 1) * f
+  efc_bytes = nefc * (nv + 10) * f
+  return W * (read_state + per_world_out) + contact_bytes + efc_bytes
+
+
+def run_ours(args):
+  import torch
+
+  import mjx_warp_b200 as mjw
+  from mjx_warp_b200 import replicas
+
+  rank, world_size, local_rank = replicas.dist_env()
+  if world_size > 1:
+    import datetime
+
+    torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+  torch.cuda.set_device(local_rank)
+  mjm = _model()
+  nworld = args.nworld
+  qpos, qvel, ctrl = _state(mjm, rank * nworld, nworld)
+  m = mjw.put_model(mjm)
+  d = mjw.make_data(mjm, nworld=nworld, nconmax=48 * nworld, njmax=80 * nworld)
+  d.qpos.copy_(torch.as_tensor(qpos, dtype=torch.float32))
+  d.qvel.copy_(torch.as_tensor(qvel, dtype=torch.float32))
+  d.ctrl.copy_(torch.as_tensor(ctrl, dtype=torch.float32))
+  fused = args.form == "fused"
+  step = lambda: mjw.step(m, d, fused=fused)  # noqa: E731
+
+  def barrier():
+    if world_size > 1:
+      torch.distributed.barrier()
+    torch.cuda.synchronize()
+
+  for _ in range(args.warmup):
+    step()
+  # device-resident: one captured graph of the step, replayed K times
+  g = torch.cuda.CUDAGraph()
+  s = torch.cuda.Stream()
+  s.wait_stream(torch.cuda.current_stream())
+  with torch.cuda.stream(s):
+    with torch.cuda.graph(g, stream=s):
+      step()
+  torch.cuda.current_stream().wait_stream(s)
+  g.replay()
+  ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+        for _ in range(args.steps)]
+  barrier()
+  with _Clocks(local_rank) as clocks:
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record()
+    for a, b in ev:
+      a.record()
+      g.replay()
+      b.record()
+    t1.record()
+    barrier()
+  elapsed = replicas.max_over_ranks(t0.elapsed_time(t1) / 1000.0, device="cuda")
+  step_ms = [a.elapsed_time(b) for a, b in ev]
+  status = mjw.world_status(d)
+  nonfinite = int(replicas.sum_over_ranks(int(np.count_nonzero(status & 0x8)), device="cuda"))
+  overflow = int(replicas.sum_over_ranks(int(np.count_nonzero(status & 0x7)), device="cuda"))
+  ncon = int(d.world_ncon.sum())
+  nefc = int(d.world_nefc.sum())
+
+  # end to end through the public API: ctrl in from pinned host memory, qpos / qvel back
+  ctrl_h = torch.as_tensor(ctrl, dtype=torch.float32).pin_memory()
+  out_h = torch.empty((nworld, mjm.nq + mjm.nv), dtype=torch.float32).pin_memory()
+  out_d = torch.empty((nworld, mjm.nq + mjm.nv), dtype=torch.float32, device="cuda")
+  for _ in range(2):
+    d.ctrl.copy_(ctrl_h, non_blocking=True)
+    step()
+  barrier()
+  e0 = torch.cuda.Event(enable_timing=True)
+  e1 = torch.cuda.Event(enable_timing=True)
+  e0.record()
+  for _ in range(args.steps):
+    d.ctrl.copy_(ctrl_h, non_blocking=True)
+    step()
+    out_d[:, :mjm.nq].copy_(d.qpos)
+    out_d[:, mjm.nq:].copy_(d.qvel)
+    out_h.copy_(out_d, non_blocking=True)
+  e1.record()
+  barrier()
+  e2e_elapsed = replicas.max_over_ranks(e0.elapsed_time(e1) / 1000.0, device="cuda")
+
+  launches_per_step = 2 if fused else 17
+  total_worlds = nworld * world_size
+  value = total_worlds * args.steps / elapsed
+  kernel_s = float(np.mean(step_ms)) / 1000.0
+  alg = _algorithmic_bytes(d, mjm, ncon, nefc)
+  peaks = {}
+  try:
+    with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+      peaks = json.load(f)
+  except OSError:
+    pass
+  hbm = float(peaks.get("hbm_gbs", 6650.0))
+  achieved = alg / kernel_s / 1e9
+  footprint = sum(_bytes_of(t) for t in list(d.arrays().values()) + list(d.contact.arrays().values())
+                  + list(d.efc.arrays().values()))
+  traffic = None
+  tpath = os.path.join(ROOT, "profiles", "traffic.json")
+  if os.path.exists(tpath):
+    with open(tpath) as f:
+      traffic = json.load(f).get(f"{args.form}_dram_bytes_per_launch")
+  line = {
+    "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world_size, "steps": args.steps,
+    "warmup": args.warmup, "ms_per_step": elapsed / args.steps * 1000.0, "higher_is_better": True,
+    "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded states)",
+    "config": {"workload": WORKLOAD, "nworld_per_gpu": nworld, "nv": mjm.nv, "form": args.form,
+               "nconmax": d.nconmax, "njmax": d.njmax,
+               "l2": f"working set {footprint / 2**20:.0f} MiB per GPU > 126 MB L2, no flush",
+               "parallelism": f"replicas x{world_size}"},
+    "e2e": {"value": total_worlds * args.steps / e2e_elapsed, "unit": "steps/s",
+            "h2d_bytes_per_step": _bytes_of(ctrl_h), "d2h_bytes_per_step": _bytes_of(out_h)},
+    "gpu_launches": launches_per_step * args.steps,
+    "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                 "frac": achieved / hbm, "traffic": traffic,
+                 "kernel": "k_step_fused" if fused else "k_stage<*> chain",
+                 "algorithmic_bytes_per_launch": alg, "peak_source": "measured" if peaks else "fallback"},
+    "clocks": clocks.summary(),
+    "status": {"nonfinite_worlds": nonfinite, "overflow_worlds": overflow,
+               "mean_contacts_per_world": ncon / nworld, "mean_efc_rows_per_world": nefc / nworld},
+  }
+  if rank == 0 and not args.no_cpu_baseline:
+    line["cpu_baseline"] = cpu_baseline(mjm, budget_s=args.cpu_seconds)
+  del g
+  if world_size > 1:
+    torch.distributed.barrier()
+    torch.distributed.destroy_process_group()
+  if rank == 0:
+    print(json.dumps(line), flush=True)
+
+
+def cpu_baseline(mjm, budget_s=10.0, nworld=1024):
+  """The CPU restatement (FP32, OpenMP over worlds, all host threads) on a bounded sample of
+  the same workload: nworld worlds stepped until about budget_s seconds have elapsed."""
+  from oracle import Oracle
+
+  qpos, qvel, ctrl = _state(mjm, 0, nworld)
+  o = Oracle(mjm, nworld, 32)
+  o.set("qpos", qpos)
+  o.set("qvel", qvel)
+  o.set("ctrl", ctrl)
+  cores = os.cpu_count() or 1
+  o.run("step", nstep=1, nthreads=cores)  # warm-up
+  steps, t0 = 0, time.perf_counter()
+  while time.perf_counter() - t0 < budget_s:
+    o.run("step", nstep=5, nthreads=cores)
+    steps += 5
+  el = time.perf_counter() - t0
+  return {"value": nworld * steps / el, "unit": "steps/s", "cores": cores, "kind": "port",
+          "sample": f"{nworld} worlds x {steps} steps ({el:.1f} s), FP32 CPU restatement"}
+
+
+def run_reference(args):
+  """Reference arm: the reference algorithm's CPU implementation (oracle/, the CPU restatement;
+  MJWarp itself needs warp-lang and MuJoCo, neither installable here), same workload."""
+  from mjx_warp_b200 import replicas
+
+  rank, world_size, _ = replicas.dist_env()
+  if rank != 0:
+    return
+  mjm = _model()
+  cpu = cpu_baseline(mjm, budget_s=max(2.0, 0.02 * (args.steps + args.warmup)), nworld=1024)
+  line = {
+    "impl": "reference", "metric": METRIC, "value": cpu["value"], "unit": "steps/s",
+    "n_gpus": world_size, "steps": args.steps, "warmup": args.warmup,
+    "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+    "data": "synthetic (seeded states)",
+    "config": {"workload": WORKLOAD, "nworld_per_gpu": args.nworld, "form": "cpu"},
+    "cpu_baseline": cpu,
+    "e2e": {"value": cpu["value"], "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+  }
+  print(json.dumps(line), flush=True)
+
+
+def main():
+  p = argparse.ArgumentParser()
+  p.add_argument("--gpus", type=int, default=1)
+  p.add_argument("--steps", type=int, default=200)
+  p.add_argument("--warmup", type=int, default=10)
+  p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+  p.add_argument("--form", default="fused", choices=["fused", "plain"])
+  p.add_argument("--nworld", type=int, default=NWORLD)
+  p.add_argument("--cpu-seconds", type=float, default=10.0)
+  p.add_argument("--no-cpu-baseline", action="store_true")
+  args = p.parse_args()
+  if args.warmup < 3:
+    args.warmup = 3
+  if args.impl == "reference":
+    run_reference(args)
+  else:
+    run_ours(args)
+
+
+if __name__ == "__main__":
+  main()

@@ -1,0 +1,190 @@
+/* mjb200.h — C ABI of the B200-native batched physics step (libmjb200.so).
+ *
+ * The library evaluates MJWarp's batched forward step (mujoco_warp 3.2.7 alpha) on one B200:
+ * every entry point below replaces one function of the reference's Python API
+ * (mujoco_warp/__init__.py:18-58) and is what a ctypes / FFI binding of that API calls.  The
+ * caller owns all device memory (PyTorch's caching allocator in the bundled Python host); the
+ * library allocates nothing on any entry point and never synchronises the stream, so a sequence
+ * of calls can be captured in a CUDA graph.
+ *
+ * Layout: every per-world array is world-major (world w's slice starts at w * <per-world size>),
+ * structured element types are flattened (vec3 = 3 floats, quat = 4 (w, x, y, z), mat33 = 9
+ * row-major, spatial vector = 6 (angular, linear), vec10 inertia = 10).  Contacts, collision pairs
+ * and constraint (efc) rows are flat arrays over nconmax / njmax entries tagged with worldid and
+ * counted by a device counter, as in the reference (types.py:615-645, 264-363); each world's
+ * entries are contiguous, and the per-world index arrays (world_*adr / world_n*) locate them.
+ *
+ * Errors: every entry point returns an MjbStatus code; launch failures are reported through
+ * cudaGetLastError as MJB_ERR_LAUNCH.  Per-world problems found on the device (capacity overflow,
+ * non-finite state) are recorded as bits in MjbData.world_status and read back with
+ * mjb_world_status.
+ */
+#ifndef MJB200_H_
+#define MJB200_H_
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MJB_ABI_VERSION 1
+
+typedef struct CUstream_st* mjbStream; /* == cudaStream_t */
+
+typedef enum MjbStatus {
+  MJB_OK = 0,
+  MJB_ERR_ARG = 1,          /* null pointer, bad size or unsupported option */
+  MJB_ERR_UNSUPPORTED = 2,  /* model feature the kernels do not implement */
+  MJB_ERR_LAUNCH = 3,       /* CUDA launch / runtime error */
+  MJB_ERR_SCRATCH = 4,      /* model too large for the kernel's on-chip scratch */
+} MjbStatus;
+
+/* per-world status bits (MjbData.world_status) */
+#define MJB_WS_CONTACT_OVERFLOW 0x1u  /* contacts beyond nconmax were dropped */
+#define MJB_WS_EFC_OVERFLOW 0x2u      /* constraint rows beyond njmax were dropped */
+#define MJB_WS_PAIR_OVERFLOW 0x4u     /* broadphase pairs beyond nconmax were dropped */
+#define MJB_WS_NONFINITE 0x8u         /* qpos / qvel / qacc not finite after the step */
+#define MJB_WS_ROWS_SPLIT 0x10u       /* a world's flat rows were not contiguous */
+
+/* Read-only model, shared by all worlds (types.py:366-612).  Device pointers. */
+typedef struct MjbModel {
+  int32_t nq, nv, na, nu, nbody, njnt, ngeom, nsite, nmocap, nM;
+  int32_t nlimit;      /* len(jnt_limited_slide_hinge_adr) */
+  int32_t nlevel;      /* BFS levels of the body tree, world included */
+  int32_t nblock;      /* dof tree blocks (one per kinematic tree) */
+  int32_t npair_cand;  /* geom pairs that pass the static filter (broadphase candidates) */
+  int32_t nlsp;        /* parallel line-search candidates */
+  /* Option (types.py:218-250) */
+  int32_t integrator, cone, solver, iterations, ls_iterations, disableflags, is_sparse,
+      ls_parallel;
+  int32_t actuator_affine_bias_gain;
+  float timestep, impratio, tolerance, ls_tolerance, meaninertia;
+  float gravity[3];
+  /* tree / level tables */
+  const int32_t *body_tree, *body_treeadr, *body_childadr, *body_childnum, *body_child,
+      *body_subtreeend;
+  const int32_t *body_parentid, *body_rootid, *body_weldid, *body_jntnum, *body_jntadr,
+      *body_dofnum, *body_dofadr;
+  const float *body_pos, *body_quat, *body_ipos, *body_iquat, *body_mass, *subtree_mass,
+      *body_inertia, *body_invweight0;
+  const int32_t *jnt_type, *jnt_qposadr, *jnt_dofadr, *jnt_bodyid, *jnt_limited,
+      *jnt_actfrclimited, *jnt_limited_slide_hinge_adr;
+  const float *jnt_solref, *jnt_solimp, *jnt_pos, *jnt_axis, *jnt_stiffness, *jnt_range,
+      *jnt_actfrcrange, *jnt_margin;
+  const int32_t *dof_bodyid, *dof_jntid, *dof_parentid, *dof_Madr;
+  const float *dof_armature, *dof_damping, *dof_invweight0;
+  const int32_t *block_adr, *block_size;
+  const int32_t *geom_type, *geom_contype, *geom_conaffinity, *geom_condim, *geom_bodyid,
+      *geom_priority;
+  const float *geom_pos, *geom_quat, *geom_size, *geom_rbound, *geom_solmix, *geom_solref,
+      *geom_solimp, *geom_friction, *geom_margin, *geom_gap;
+  const int32_t* pair_cand; /* 2 * npair_cand geom ids (g1 < g2), nxn element order */
+  const int32_t* site_bodyid;
+  const float *site_pos, *site_quat;
+  const int32_t *actuator_trntype, *actuator_dyntype, *actuator_gaintype, *actuator_biastype,
+      *actuator_trnid, *actuator_actadr, *actuator_ctrllimited, *actuator_forcelimited,
+      *actuator_actlimited;
+  const float *actuator_dynprm, *actuator_gainprm, *actuator_biasprm, *actuator_ctrlrange,
+      *actuator_forcerange, *actuator_actrange, *actuator_gear;
+  const float *qpos0, *qpos_spring;
+  const float* alpha_candidate;
+} MjbModel;
+
+/* Per-world state, intermediates, contacts and constraints (types.py:648-800).  Device
+ * pointers; fields a call does not touch may be null. */
+typedef struct MjbData {
+  int32_t nworld, nconmax, njmax;
+  /* state */
+  float *qpos, *qvel, *act, *ctrl, *qacc, *qacc_warmstart, *qfrc_applied, *xfrc_applied;
+  /* smooth dynamics */
+  float *xpos, *xquat, *xmat, *xipos, *ximat, *xanchor, *xaxis, *geom_xpos, *geom_xmat,
+      *site_xpos, *site_xmat, *subtree_com, *cinert, *crb, *cdof, *cvel, *cdof_dot, *qM, *qLD,
+      *qLDiagInv;
+  float *actuator_length, *actuator_velocity, *actuator_force, *actuator_moment;
+  float *qfrc_bias, *qfrc_spring, *qfrc_damper, *qfrc_passive, *qfrc_actuator, *qfrc_smooth,
+      *qfrc_constraint, *qacc_smooth, *act_dot, *rne_cacc, *rne_cfrc;
+  float *qfrc_integration, *qacc_integration, *qM_integration, *qLD_integration,
+      *act_vel_integration;
+  /* global counters (1 element each) */
+  int32_t *ncon, *nefc, *ncollision;
+  /* collision pairs and contacts (flat) */
+  int32_t *collision_pair, *collision_worldid;
+  float *contact_dist, *contact_pos, *contact_frame, *contact_includemargin, *contact_friction,
+      *contact_solref, *contact_solreffriction, *contact_solimp;
+  int32_t *contact_dim, *contact_geom, *contact_efc_address, *contact_worldid;
+  /* constraint rows (flat, njmax) */
+  int32_t* efc_worldid;
+  float *efc_J, *efc_pos, *efc_margin, *efc_D, *efc_aref, *efc_force, *efc_Jaref, *efc_jv,
+      *efc_quad;
+  int32_t* efc_active;
+  /* solver per world */
+  float *efc_Ma, *efc_grad, *efc_grad_dot, *efc_Mgrad, *efc_search, *efc_search_dot,
+      *efc_gauss, *efc_cost, *efc_prev_cost, *efc_gtol, *efc_mv, *efc_quad_gauss, *efc_h,
+      *efc_alpha, *efc_prev_grad, *efc_prev_Mgrad, *efc_beta;
+  int32_t* efc_solver_niter;
+  uint8_t* efc_done;
+  /* per-world index of the flat arrays and status bits */
+  int32_t *world_pairadr, *world_npair, *world_conadr, *world_ncon, *world_efcadr, *world_nefc;
+  uint32_t* world_status;
+} MjbData;
+
+/* Launch configuration for the step entry points. */
+typedef struct MjbRunCfg {
+  int32_t fused;            /* 1: fused per-world kernels (default); 0: one kernel per stage */
+  int32_t worlds_per_block; /* warps (= worlds) per CTA; 0 picks the default */
+} MjbRunCfg;
+
+int mjb_abi_version(void);
+const char* mjb_error_string(int status);
+
+/* step (forward.py:682-695): forward + Euler or implicitfast integration. */
+int mjb_step(const MjbModel* m, const MjbData* d, const MjbRunCfg* cfg, mjbStream stream);
+/* forward (forward.py:664-679). */
+int mjb_forward(const MjbModel* m, const MjbData* d, const MjbRunCfg* cfg, mjbStream stream);
+
+/* Pipeline stages (forward.py:408-661). */
+int mjb_fwd_position(const MjbModel* m, const MjbData* d, mjbStream stream);
+int mjb_fwd_velocity(const MjbModel* m, const MjbData* d, mjbStream stream);
+int mjb_fwd_actuation(const MjbModel* m, const MjbData* d, mjbStream stream);
+int mjb_fwd_acceleration(const MjbModel* m, const MjbData* d, mjbStream stream);
+int mjb_euler(const MjbModel* m, const MjbData* d, mjbStream stream);    /* forward.py:165 */
+int mjb_implicit(const MjbModel* m, const MjbData* d, mjbStream stream); /* forward.py:245 */
+
+/* Smooth dynamics (smooth.py). */
+int mjb_kinematics(const MjbModel* m, const MjbData* d, mjbStream stream);   /* :32 */
+int mjb_com_pos(const MjbModel* m, const MjbData* d, mjbStream stream);      /* :148 */
+int mjb_crb(const MjbModel* m, const MjbData* d, mjbStream stream);          /* :248 */
+int mjb_factor_m(const MjbModel* m, const MjbData* d, mjbStream stream);     /* :392 */
+int mjb_rne(const MjbModel* m, const MjbData* d, mjbStream stream);          /* :398 */
+int mjb_transmission(const MjbModel* m, const MjbData* d, mjbStream stream); /* :469 */
+int mjb_com_vel(const MjbModel* m, const MjbData* d, mjbStream stream);      /* :539 */
+int mjb_passive(const MjbModel* m, const MjbData* d, mjbStream stream);      /* passive.py:27 */
+/* x = qLD^-1 y per world (smooth.py:693-696); x and y are (nworld, nv). */
+int mjb_solve_m(const MjbModel* m, const MjbData* d, float* x, const float* y, mjbStream stream);
+
+/* Collision (collision_driver.py, collision_primitive.py). */
+int mjb_collision(const MjbModel* m, const MjbData* d, mjbStream stream);      /* :525 */
+int mjb_nxn_broadphase(const MjbModel* m, const MjbData* d, mjbStream stream); /* :458 */
+int mjb_sap_broadphase(const MjbModel* m, const MjbData* d, mjbStream stream); /* :350 */
+int mjb_primitive_narrowphase(const MjbModel* m, const MjbData* d,
+                              mjbStream stream); /* collision_primitive.py:271 */
+
+/* Constraints (constraint.py:213) and solver (solver.py:872). */
+int mjb_make_constraint(const MjbModel* m, const MjbData* d, mjbStream stream);
+int mjb_solve(const MjbModel* m, const MjbData* d, mjbStream stream);
+
+/* Support (support.py). res = M vec per world unless skip[world] (support.py:35-137). */
+int mjb_mul_m(const MjbModel* m, const MjbData* d, float* res, const float* vec,
+              const uint8_t* skip, mjbStream stream);
+/* qfrc += J^T xfrc_applied per world (support.py:140-172). */
+int mjb_xfrc_accumulate(const MjbModel* m, const MjbData* d, float* qfrc, mjbStream stream);
+
+/* Copies world_status (nworld words) to host memory; synchronises the stream. */
+int mjb_world_status(const MjbData* d, uint32_t* host_out, mjbStream stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MJB200_H_ */

@@ -1,0 +1,232 @@
+"""The reference's stage functions (mujoco_warp/__init__.py:18-58) over the CUDA kernels.
+
+Each function takes (Model, Data) like its reference counterpart, launches the corresponding
+libmjb200.so entry point on the current torch CUDA stream and returns without synchronising, so
+sequences of calls can be captured in a CUDA graph.  There is no CPU path: calling these on a
+Data whose tensors live on the CPU, or without the built library, raises.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import time as _time
+from typing import Callable, Optional, Tuple
+
+import numpy as np
+import torch
+
+from . import _abi
+from .types import Data, Model
+
+_FUSED = _abi.MjbRunCfg(1, 0)
+_PLAIN = _abi.MjbRunCfg(0, 0)
+
+
+def _call(name: str, m: Model, d: Data, *extra) -> None:
+  L = _abi.lib()
+  mv = _abi.model_view(m)
+  dv = _abi.data_view(d)
+  rc = getattr(L, "mjb_" + name)(ctypes.byref(mv), ctypes.byref(dv), *extra, _abi.stream())
+  _abi.check(rc, name)
+
+
+def _integrator_check(m: Model) -> None:
+  if m.opt.integrator == 1:
+    raise NotImplementedError(f"integrator {m.opt.integrator} not implemented.")
+  if m.opt.integrator not in (0, 3):
+    raise NotImplementedError(f"integrator {m.opt.integrator} not implemented.")
+
+
+def step(m: Model, d: Data, fused: bool = True) -> None:
+  """Advance simulation (forward.py:682-695).
+
+  fused=True runs every stage of a world inside one warp of one kernel; fused=False launches one
+  kernel per stage (the reference's stage decomposition).
+  """
+  _integrator_check(m)
+  L = _abi.lib()
+  rc = L.mjb_step(ctypes.byref(_abi.model_view(m)), ctypes.byref(_abi.data_view(d)),
+                  ctypes.byref(_FUSED if fused else _PLAIN), _abi.stream())
+  _abi.check(rc, "step")
+  d.time = d.time + m.opt.timestep
+
+
+def forward(m: Model, d: Data, fused: bool = True) -> None:
+  """Forward dynamics (forward.py:664-679)."""
+  L = _abi.lib()
+  rc = L.mjb_forward(ctypes.byref(_abi.model_view(m)), ctypes.byref(_abi.data_view(d)),
+                     ctypes.byref(_FUSED if fused else _PLAIN), _abi.stream())
+  _abi.check(rc, "forward")
+
+
+def fwd_position(m: Model, d: Data) -> None:
+  """Position-dependent computations (forward.py:408-420)."""
+  _call("fwd_position", m, d)
+
+
+def fwd_velocity(m: Model, d: Data) -> None:
+  """Velocity-dependent computations (forward.py:423-500)."""
+  _call("fwd_velocity", m, d)
+
+
+def fwd_actuation(m: Model, d: Data) -> None:
+  """Actuation-dependent computations (forward.py:503-641)."""
+  _call("fwd_actuation", m, d)
+
+
+def fwd_acceleration(m: Model, d: Data) -> None:
+  """Sum non-constraint forces and compute qacc_smooth (forward.py:644-661)."""
+  _call("fwd_acceleration", m, d)
+
+
+def euler(m: Model, d: Data) -> None:
+  """Euler integrator, semi-implicit in velocity (forward.py:165-242)."""
+  _call("euler", m, d)
+  d.time = d.time + m.opt.timestep
+
+
+def implicit(m: Model, d: Data) -> None:
+  """Implicit-in-velocity integrator, implicitfast (forward.py:245-405)."""
+  if m.opt.is_sparse:
+    raise NotImplementedError("implicit integration needs the dense mass matrix")
+  _call("implicit", m, d)
+  d.time = d.time + m.opt.timestep
+
+
+def kinematics(m: Model, d: Data) -> None:
+  """Forward kinematics (smooth.py:32-145)."""
+  _call("kinematics", m, d)
+
+
+def com_pos(m: Model, d: Data) -> None:
+  """Subtree CoM, cinert and cdof (smooth.py:148-245)."""
+  _call("com_pos", m, d)
+
+
+def crb(m: Model, d: Data) -> None:
+  """Composite rigid body inertia and qM (smooth.py:248-314)."""
+  _call("crb", m, d)
+
+
+def factor_m(m: Model, d: Data) -> None:
+  """Factorisation of qM into qLD (smooth.py:392-395)."""
+  _call("factor_m", m, d)
+
+
+def rne(m: Model, d: Data) -> None:
+  """Bias forces by recursive Newton-Euler (smooth.py:398-466)."""
+  _call("rne", m, d)
+
+
+def transmission(m: Model, d: Data):
+  """Actuator lengths and moments (smooth.py:469-536)."""
+  if not m.nu:
+    return d
+  _call("transmission", m, d)
+
+
+def com_vel(m: Model, d: Data) -> None:
+  """cvel and cdof_dot (smooth.py:539-606)."""
+  _call("com_vel", m, d)
+
+
+def passive(m: Model, d: Data) -> None:
+  """Joint springs and dampers (passive.py:27-108)."""
+  _call("passive", m, d)
+
+
+def solve_m(m: Model, d: Data, x: torch.Tensor, y: torch.Tensor) -> None:
+  """x = inv(M) y with the factor in qLD (smooth.py:693-696)."""
+  L = _abi.lib()
+  rc = L.mjb_solve_m(ctypes.byref(_abi.model_view(m)), ctypes.byref(_abi.data_view(d)),
+                     _abi._ptr(x), _abi._ptr(y), _abi.stream())
+  _abi.check(rc, "solve_m")
+
+
+def mul_m(m: Model, d: Data, res: torch.Tensor, vec: torch.Tensor, skip: Optional[torch.Tensor] = None) -> None:
+  """res = M vec for worlds not skipped (support.py:35-137)."""
+  L = _abi.lib()
+  if skip is not None and skip.dtype == torch.bool:
+    skip = skip.view(torch.uint8)
+  rc = L.mjb_mul_m(ctypes.byref(_abi.model_view(m)), ctypes.byref(_abi.data_view(d)),
+                   _abi._ptr(res), _abi._ptr(vec), _abi._ptr(skip), _abi.stream())
+  _abi.check(rc, "mul_m")
+
+
+def xfrc_accumulate(m: Model, d: Data, qfrc: torch.Tensor) -> None:
+  """qfrc += Jacobian^T xfrc_applied (support.py:140-172)."""
+  L = _abi.lib()
+  rc = L.mjb_xfrc_accumulate(ctypes.byref(_abi.model_view(m)), ctypes.byref(_abi.data_view(d)),
+                             _abi._ptr(qfrc), _abi.stream())
+  _abi.check(rc, "xfrc_accumulate")
+
+
+def collision(m: Model, d: Data) -> None:
+  """Collision detection (collision_driver.py:525-547)."""
+  _call("collision", m, d)
+
+
+def nxn_broadphase(m: Model, d: Data) -> None:
+  """All-pairs broadphase (collision_driver.py:458-512); appends to the collision_pair list."""
+  _call("nxn_broadphase", m, d)
+
+
+def sap_broadphase(m: Model, d: Data):
+  """Sweep-and-prune broadphase (collision_driver.py:350-455)."""
+  _call("sap_broadphase", m, d)
+  return d
+
+
+def primitive_narrowphase(m: Model, d: Data) -> None:
+  """Primitive narrowphase over collision_pair (collision_primitive.py:271-274)."""
+  _call("primitive_narrowphase", m, d)
+
+
+def make_constraint(m: Model, d: Data) -> None:
+  """Constraint rows for limits and pyramidal contacts (constraint.py:213-240)."""
+  _call("make_constraint", m, d)
+
+
+def solve(m: Model, d: Data) -> None:
+  """Newton / CG constraint solve (solver.py:872-1000)."""
+  _call("solve", m, d)
+
+
+def world_status(d: Data) -> np.ndarray:
+  """Per-world status bits (MJB_WS_* in include/mjb200.h); synchronises the stream."""
+  out = np.zeros(d.nworld, dtype=np.uint32)
+  rc = _abi.lib().mjb_world_status(ctypes.byref(_abi.data_view(d)), out.ctypes.data_as(ctypes.c_void_p),
+                                   _abi.stream())
+  _abi.check(rc, "world_status")
+  return out
+
+
+def benchmark(fn: Callable[[Model, Data], None], m: Model, d: Data, nstep: int = 1000,
+              graph: bool = True) -> Tuple[float, float, int]:
+  """Times nstep calls of fn(m, d) replayed from one captured CUDA graph (test_util.py:57-120).
+
+  Returns (warmup seconds, run seconds, world-steps).
+  """
+  t0 = _time.perf_counter()
+  fn(m, d)
+  fn(m, d)
+  torch.cuda.synchronize()
+  t1 = _time.perf_counter()
+  if graph:
+    g = torch.cuda.CUDAGraph()
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(s):
+      with torch.cuda.graph(g, stream=s):
+        fn(m, d)
+    torch.cuda.current_stream().wait_stream(s)
+    run = g.replay
+  else:
+    run = lambda: fn(m, d)  # noqa: E731
+  torch.cuda.synchronize()
+  t2 = _time.perf_counter()
+  for _ in range(nstep):
+    run()
+  torch.cuda.synchronize()
+  t3 = _time.perf_counter()
+  return t1 - t0, t3 - t2, d.nworld * nstep

@@ -1,0 +1,423 @@
+// libmjb200.so: kernels and the C ABI declared in include/mjb200.h.
+//
+// Two launch forms share the per-world device stages of mjb_world.cuh / mjb_collide.cuh /
+// mjb_solver.cuh:
+//  - plain: one kernel per reference stage function (mjb_kinematics, mjb_com_pos, ...), one warp
+//    per world, data passed between stages through the Data arrays in HBM; mjb_step with
+//    cfg->fused == 0 chains these, like the reference's launch sequence;
+//  - fused: mjb_step / mjb_forward with cfg->fused != 0 run every stage of a world inside one
+//    warp of a single kernel (after one tiny counter-reset kernel), with the Newton Hessian and its
+//    Cholesky factor in shared memory.
+// No entry point allocates memory or synchronises the stream (except mjb_world_status, which
+// copies results to the host).
+#include <cuda_runtime.h>
+
+#include "mjb_solver.cuh"
+
+namespace mjb {
+
+enum Stage {
+  S_KINEMATICS, S_COM_POS, S_CRB, S_FACTOR_M, S_TRANSMISSION, S_COM_VEL, S_PASSIVE, S_RNE,
+  S_FWD_VELOCITY, S_FWD_ACTUATION, S_FWD_ACCELERATION, S_NXN, S_NARROW, S_MAKE_CONSTRAINT,
+  S_SOLVE, S_EULER, S_IMPLICIT, S_QACC_SMOOTH_COPY, S_CHECK
+};
+
+constexpr int kDefaultWarps = 4;
+
+// NaN / Inf check of the integrated state (sets MJB_WS_NONFINITE)
+__device__ void check_finite(const MjbModel& m, const MjbData& d, int w, int lane) {
+  bool bad = false;
+  for (int i = lane; i < m.nq; i += 32) bad |= !isfinite(d.qpos[W(w, m.nq) + i]);
+  for (int i = lane; i < m.nv; i += 32) {
+    bad |= !isfinite(d.qvel[W(w, m.nv) + i]);
+    bad |= !isfinite(d.qacc[W(w, m.nv) + i]);
+  }
+  if (__any_sync(WARP_FULL, bad) && lane == 0 && d.world_status) atomicOr(d.world_status + w, MJB_WS_NONFINITE);
+}
+
+__device__ __forceinline__ void copy_qacc_smooth(const MjbModel& m, const MjbData& d, int w, int lane) {
+  for (int i = lane; i < m.nv; i += 32) d.qacc[W(w, m.nv) + i] = d.qacc_smooth[W(w, m.nv) + i];
+  __syncwarp();
+}
+
+template <int STAGE>
+__global__ void __launch_bounds__(128, 4) k_stage(const MjbModel m, const MjbData d, int smem_per_warp) {
+  extern __shared__ float smem[];
+  const int lane = threadIdx.x & 31;
+  const int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (w >= d.nworld) return;
+  switch (STAGE) {
+    case S_KINEMATICS: kinematics(m, d, w, lane); break;
+    case S_COM_POS: com_pos(m, d, w, lane); break;
+    case S_CRB: crb(m, d, w, lane); break;
+    case S_FACTOR_M: factor_m(m, d, w, lane); break;
+    case S_TRANSMISSION: transmission(m, d, w, lane); break;
+    case S_COM_VEL: com_vel(m, d, w, lane); break;
+    case S_PASSIVE: passive(m, d, w, lane); break;
+    case S_RNE: rne(m, d, w, lane); break;
+    case S_FWD_VELOCITY: fwd_velocity(m, d, w, lane); break;
+    case S_FWD_ACTUATION: fwd_actuation(m, d, w, lane); break;
+    case S_FWD_ACCELERATION: fwd_acceleration(m, d, w, lane); break;
+    case S_NXN: nxn_broadphase(m, d, w, lane); break;
+    case S_NARROW: primitive_narrowphase(m, d, w, lane); break;
+    case S_MAKE_CONSTRAINT: make_constraint(m, d, w, lane); break;
+    case S_SOLVE:
+      solve(m, d, w, lane, smem_per_warp ? smem + size_t(threadIdx.x >> 5) * smem_per_warp : nullptr,
+            d.efc_h + W(w, m.nv * m.nv));
+      break;
+    case S_EULER: euler(m, d, w, lane); break;
+    case S_IMPLICIT: implicit(m, d, w, lane); break;
+    case S_QACC_SMOOTH_COPY: copy_qacc_smooth(m, d, w, lane); break;
+    case S_CHECK: check_finite(m, d, w, lane); break;
+  }
+}
+
+// whole forward (+ integration) of one world per warp; dynamic shared memory holds one nv x nv
+// Hessian / factor tile per warp
+__global__ void __launch_bounds__(128, 4) k_step_fused(const MjbModel m, const MjbData d, int integrate,
+                                                    int smem_per_warp) {
+  extern __shared__ float smem[];
+  const int lane = threadIdx.x & 31;
+  const int wib = threadIdx.x >> 5;
+  const int w = blockIdx.x * (blockDim.x >> 5) + wib;
+  if (w >= d.nworld) return;
+  const int nv = m.nv;
+  float* sm = smem_per_warp ? smem + size_t(wib) * smem_per_warp : nullptr;
+  float* hs = d.efc_h + W(w, nv * nv);
+  kinematics(m, d, w, lane);
+  com_pos(m, d, w, lane);
+  crb(m, d, w, lane);
+  factor_m(m, d, w, lane);
+  collision(m, d, w, lane);
+  make_constraint(m, d, w, lane);
+  transmission(m, d, w, lane);
+  fwd_velocity(m, d, w, lane);
+  fwd_actuation(m, d, w, lane);
+  fwd_acceleration(m, d, w, lane);
+  if (d.njmax == 0) copy_qacc_smooth(m, d, w, lane);
+  else solve(m, d, w, lane, sm, hs);
+  if (integrate) {
+    if (m.integrator == 0) euler(m, d, w, lane);
+    else implicit(m, d, w, lane);
+    check_finite(m, d, w, lane);
+  }
+}
+
+// zero the flat-array counters and (optionally) the world status words
+__global__ void k_reset(int* a, int* b, int* c, uint32_t* status, int nworld) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i == 0) {
+    if (a) *a = 0;
+    if (b) *b = 0;
+    if (c) *c = 0;
+  }
+  if (status && i < nworld) status[i] = 0u;
+}
+
+// Rebuild a per-world index (first row, row count) of a flat, worldid-tagged array.
+__global__ void k_index_clear(int* adr, int* cnt, int nworld) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < nworld) {
+    adr[i] = 0x7fffffff;
+    cnt[i] = 0;
+  }
+}
+__global__ void k_index_rows(const int* worldid, const int* counter, int cap, int* adr, int* cnt,
+                             int nworld) {
+  const int n = min(*counter, cap);
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+    const int w = worldid[r];
+    if (w < 0 || w >= nworld) continue;
+    atomicMin(adr + w, r);
+    atomicAdd(cnt + w, 1);
+  }
+}
+// Checks that each world's rows are contiguous; a split world gets MJB_WS_ROWS_SPLIT and no rows.
+__global__ void k_index_fix(const int* worldid, int* adr, int* cnt, uint32_t* status, int nworld) {
+  const int lane = threadIdx.x & 31;
+  const int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (w >= nworld) return;
+  const int n = cnt[w];
+  if (n == 0) {
+    if (lane == 0) adr[w] = 0;
+    return;
+  }
+  const int a = adr[w];
+  bool bad = false;
+  for (int k = lane; k < n; k += 32) bad |= worldid[a + k] != w;
+  if (__any_sync(WARP_FULL, bad) && lane == 0) {
+    cnt[w] = 0;
+    adr[w] = 0;
+    if (status) atomicOr(status + w, MJB_WS_ROWS_SPLIT);
+  }
+}
+
+// support.py:35-137 — res = M vec per world unless skip[w]
+__global__ void k_mul_m(const MjbModel m, const MjbData d, float* res, const float* vec,
+                        const uint8_t* skip) {
+  const int lane = threadIdx.x & 31;
+  const int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (w >= d.nworld) return;
+  if (skip && skip[w]) return;
+  mul_m_world(d.qM + W(w, m.nv * m.nv), m.nv, res + W(w, m.nv), vec + W(w, m.nv), lane);
+}
+__global__ void k_solve_m(const MjbModel m, const MjbData d, float* x, const float* y) {
+  const int lane = threadIdx.x & 31;
+  const int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (w >= d.nworld) return;
+  solve_blocks(m, d.qLD + W(w, m.nv * m.nv), x + W(w, m.nv), y + W(w, m.nv), lane);
+}
+__global__ void k_xfrc(const MjbModel m, const MjbData d, float* qfrc) {
+  const int lane = threadIdx.x & 31;
+  const int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (w >= d.nworld) return;
+  xfrc_accumulate(m, d, w, qfrc + W(w, m.nv), lane);
+}
+
+}  // namespace mjb
+
+using namespace mjb;
+
+namespace {
+
+inline int grid_for(int nworld, int warps) { return (nworld + warps - 1) / warps; }
+
+inline int finish() {
+  const cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? MJB_OK : MJB_ERR_LAUNCH;
+}
+
+inline int check(const MjbModel* m, const MjbData* d) {
+  if (!m || !d) return MJB_ERR_ARG;
+  if (d->nworld <= 0) return d->nworld == 0 ? MJB_OK : MJB_ERR_ARG;
+  if (m->is_sparse) return MJB_ERR_UNSUPPORTED;
+  if (m->cone != 0) return MJB_ERR_UNSUPPORTED;
+  return MJB_OK;
+}
+
+// shared memory per warp for the solver (0 when the model needs the generic path)
+int solver_smem_per_warp(const MjbModel* m) {
+  return m->nv <= 32 ? int(solver_smem_floats(m->nv)) : 0;
+}
+
+template <int STAGE>
+int launch_stage(const MjbModel* m, const MjbData* d, cudaStream_t s) {
+  const int warps = kDefaultWarps;
+  int spw = 0;
+  size_t bytes = 0;
+  if (STAGE == S_SOLVE) {
+    spw = solver_smem_per_warp(m);
+    bytes = size_t(spw) * warps * sizeof(float);
+    static size_t configured = 0;  // opt in to > 48 KB of dynamic shared memory once per size
+    if (bytes > 48 * 1024 && bytes > configured) {
+      cudaFuncSetAttribute(k_stage<STAGE>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
+      configured = bytes;
+    }
+  }
+  k_stage<STAGE><<<grid_for(d->nworld, warps), 32 * warps, bytes, s>>>(*m, *d, spw);
+  return finish();
+}
+
+void reset_counters(const MjbData* d, bool pairs, bool contacts, bool efc, bool status,
+                    cudaStream_t s) {
+  const int n = status ? d->nworld : 1;
+  k_reset<<<(n + 255) / 256, 256, 0, s>>>(pairs ? d->ncollision : nullptr,
+                                            contacts ? d->ncon : nullptr, efc ? d->nefc : nullptr,
+                                            status ? d->world_status : nullptr, d->nworld);
+}
+
+void rebuild_index(const int* worldid, const int* counter, int cap, int* adr, int* cnt,
+                   const MjbData* d, cudaStream_t s) {
+  k_index_clear<<<(d->nworld + 255) / 256, 256, 0, s>>>(adr, cnt, d->nworld);
+  k_index_rows<<<148 * 4, 256, 0, s>>>(worldid, counter, cap, adr, cnt, d->nworld);
+  k_index_fix<<<grid_for(d->nworld, 4), 128, 0, s>>>(worldid, adr, cnt, d->world_status, d->nworld);
+}
+
+int run_forward_plain(const MjbModel* m, const MjbData* d, cudaStream_t s) {
+  int rc;
+  // fwd_position (forward.py:408-420)
+  if ((rc = launch_stage<S_KINEMATICS>(m, d, s))) return rc;
+  if ((rc = launch_stage<S_COM_POS>(m, d, s))) return rc;
+  if ((rc = launch_stage<S_CRB>(m, d, s))) return rc;
+  if ((rc = launch_stage<S_FACTOR_M>(m, d, s))) return rc;
+  reset_counters(d, true, true, true, false, s);
+  if ((rc = launch_stage<S_NXN>(m, d, s))) return rc;
+  if ((rc = launch_stage<S_NARROW>(m, d, s))) return rc;
+  if ((rc = launch_stage<S_MAKE_CONSTRAINT>(m, d, s))) return rc;
+  if ((rc = launch_stage<S_TRANSMISSION>(m, d, s))) return rc;
+  // fwd_velocity, fwd_actuation, fwd_acceleration
+  if ((rc = launch_stage<S_FWD_VELOCITY>(m, d, s))) return rc;
+  if ((rc = launch_stage<S_FWD_ACTUATION>(m, d, s))) return rc;
+  if ((rc = launch_stage<S_FWD_ACCELERATION>(m, d, s))) return rc;
+  if (d->njmax == 0) return launch_stage<S_QACC_SMOOTH_COPY>(m, d, s);
+  return launch_stage<S_SOLVE>(m, d, s);
+}
+
+int run_fused(const MjbModel* m, const MjbData* d, const MjbRunCfg* cfg, int integrate,
+              cudaStream_t s) {
+  const int warps = (cfg && cfg->worlds_per_block > 0) ? cfg->worlds_per_block : kDefaultWarps;
+  if (warps > 4) return MJB_ERR_ARG;  // __launch_bounds__(128)
+  reset_counters(d, true, true, true, true, s);
+  const int spw = solver_smem_per_warp(m);
+  const size_t smem = size_t(spw) * warps * sizeof(float);
+  static size_t configured = 0;  // opt in to > 48 KB of dynamic shared memory once per size
+  if (smem > 48 * 1024 && smem > configured) {
+    cudaFuncSetAttribute(k_step_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    configured = smem;
+  }
+  k_step_fused<<<grid_for(d->nworld, warps), 32 * warps, smem, s>>>(*m, *d, integrate, spw);
+  return finish();
+}
+
+}  // namespace
+
+extern "C" {
+
+int mjb_abi_version(void) { return MJB_ABI_VERSION; }
+
+const char* mjb_error_string(int status) {
+  switch (status) {
+    case MJB_OK: return "ok";
+    case MJB_ERR_ARG: return "invalid argument";
+    case MJB_ERR_UNSUPPORTED: return "unsupported model feature (sparse mass matrix or elliptic cone)";
+    case MJB_ERR_LAUNCH: return cudaGetErrorString(cudaGetLastError());
+    case MJB_ERR_SCRATCH: return "model too large for on-chip scratch";
+    default: return "unknown status";
+  }
+}
+
+int mjb_forward(const MjbModel* m, const MjbData* d, const MjbRunCfg* cfg, mjbStream stream) {
+  int rc = check(m, d);
+  if (rc || d->nworld == 0) return rc;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (cfg && !cfg->fused) return run_forward_plain(m, d, s);
+  return run_fused(m, d, cfg, 0, s);
+}
+
+int mjb_step(const MjbModel* m, const MjbData* d, const MjbRunCfg* cfg, mjbStream stream) {
+  int rc = check(m, d);
+  if (rc || d->nworld == 0) return rc;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (cfg && !cfg->fused) {
+    reset_counters(d, false, false, false, true, s);
+    if ((rc = run_forward_plain(m, d, s))) return rc;
+    if (m->integrator == 0) rc = launch_stage<S_EULER>(m, d, s);
+    else rc = launch_stage<S_IMPLICIT>(m, d, s);
+    if (rc) return rc;
+    return launch_stage<S_CHECK>(m, d, s);
+  }
+  return run_fused(m, d, cfg, 1, s);
+}
+
+#define MJB_STAGE_ENTRY(name, STAGE)                                           \
+  int name(const MjbModel* m, const MjbData* d, mjbStream stream) {            \
+    int rc = check(m, d);                                                      \
+    if (rc || d->nworld == 0) return rc;                                       \
+    return launch_stage<STAGE>(m, d, (cudaStream_t)stream);                    \
+  }
+
+MJB_STAGE_ENTRY(mjb_kinematics, S_KINEMATICS)
+MJB_STAGE_ENTRY(mjb_com_pos, S_COM_POS)
+MJB_STAGE_ENTRY(mjb_crb, S_CRB)
+MJB_STAGE_ENTRY(mjb_factor_m, S_FACTOR_M)
+MJB_STAGE_ENTRY(mjb_rne, S_RNE)
+MJB_STAGE_ENTRY(mjb_transmission, S_TRANSMISSION)
+MJB_STAGE_ENTRY(mjb_com_vel, S_COM_VEL)
+MJB_STAGE_ENTRY(mjb_passive, S_PASSIVE)
+MJB_STAGE_ENTRY(mjb_fwd_velocity, S_FWD_VELOCITY)
+MJB_STAGE_ENTRY(mjb_fwd_actuation, S_FWD_ACTUATION)
+MJB_STAGE_ENTRY(mjb_fwd_acceleration, S_FWD_ACCELERATION)
+MJB_STAGE_ENTRY(mjb_euler, S_EULER)
+MJB_STAGE_ENTRY(mjb_implicit, S_IMPLICIT)
+MJB_STAGE_ENTRY(mjb_nxn_broadphase, S_NXN)
+
+int mjb_fwd_position(const MjbModel* m, const MjbData* d, mjbStream stream) {
+  int rc = check(m, d);
+  if (rc || d->nworld == 0) return rc;
+  cudaStream_t s = (cudaStream_t)stream;
+  if ((rc = launch_stage<S_KINEMATICS>(m, d, s))) return rc;
+  if ((rc = launch_stage<S_COM_POS>(m, d, s))) return rc;
+  if ((rc = launch_stage<S_CRB>(m, d, s))) return rc;
+  if ((rc = launch_stage<S_FACTOR_M>(m, d, s))) return rc;
+  if ((rc = mjb_collision(m, d, stream))) return rc;
+  if ((rc = mjb_make_constraint(m, d, stream))) return rc;
+  return launch_stage<S_TRANSMISSION>(m, d, s);
+}
+
+int mjb_collision(const MjbModel* m, const MjbData* d, mjbStream stream) {
+  int rc = check(m, d);
+  if (rc || d->nworld == 0) return rc;
+  cudaStream_t s = (cudaStream_t)stream;
+  reset_counters(d, true, true, false, false, s);  // collision_driver.py:533-534
+  if ((rc = launch_stage<S_NXN>(m, d, s))) return rc;
+  return launch_stage<S_NARROW>(m, d, s);
+}
+
+// The reference uses the sweep-and-prune path only for ngeom > 100 (collision_driver.py:537-540);
+// both produce the set of candidate pairs whose bounding volumes overlap, so the pair test here is
+// the same per-world candidate sweep.
+int mjb_sap_broadphase(const MjbModel* m, const MjbData* d, mjbStream stream) {
+  return mjb_nxn_broadphase(m, d, stream);
+}
+
+int mjb_primitive_narrowphase(const MjbModel* m, const MjbData* d, mjbStream stream) {
+  int rc = check(m, d);
+  if (rc || d->nworld == 0) return rc;
+  cudaStream_t s = (cudaStream_t)stream;
+  rebuild_index(d->collision_worldid, d->ncollision, d->nconmax, d->world_pairadr, d->world_npair, d, s);
+  return launch_stage<S_NARROW>(m, d, s);
+}
+
+int mjb_make_constraint(const MjbModel* m, const MjbData* d, mjbStream stream) {
+  int rc = check(m, d);
+  if (rc || d->nworld == 0) return rc;
+  cudaStream_t s = (cudaStream_t)stream;
+  rebuild_index(d->contact_worldid, d->ncon, d->nconmax, d->world_conadr, d->world_ncon, d, s);
+  reset_counters(d, false, false, true, false, s);
+  return launch_stage<S_MAKE_CONSTRAINT>(m, d, s);
+}
+
+int mjb_solve(const MjbModel* m, const MjbData* d, mjbStream stream) {
+  int rc = check(m, d);
+  if (rc || d->nworld == 0) return rc;
+  cudaStream_t s = (cudaStream_t)stream;
+  rebuild_index(d->efc_worldid, d->nefc, d->njmax, d->world_efcadr, d->world_nefc, d, s);
+  return launch_stage<S_SOLVE>(m, d, s);
+}
+
+int mjb_solve_m(const MjbModel* m, const MjbData* d, float* x, const float* y, mjbStream stream) {
+  int rc = check(m, d);
+  if (rc || d->nworld == 0) return rc;
+  if (!x || !y) return MJB_ERR_ARG;
+  k_solve_m<<<grid_for(d->nworld, 4), 128, 0, (cudaStream_t)stream>>>(*m, *d, x, y);
+  return finish();
+}
+
+int mjb_mul_m(const MjbModel* m, const MjbData* d, float* res, const float* vec, const uint8_t* skip,
+              mjbStream stream) {
+  int rc = check(m, d);
+  if (rc || d->nworld == 0) return rc;
+  if (!res || !vec) return MJB_ERR_ARG;
+  k_mul_m<<<grid_for(d->nworld, 4), 128, 0, (cudaStream_t)stream>>>(*m, *d, res, vec, skip);
+  return finish();
+}
+
+int mjb_xfrc_accumulate(const MjbModel* m, const MjbData* d, float* qfrc, mjbStream stream) {
+  int rc = check(m, d);
+  if (rc || d->nworld == 0) return rc;
+  if (!qfrc) return MJB_ERR_ARG;
+  k_xfrc<<<grid_for(d->nworld, 4), 128, 0, (cudaStream_t)stream>>>(*m, *d, qfrc);
+  return finish();
+}
+
+int mjb_world_status(const MjbData* d, uint32_t* host_out, mjbStream stream) {
+  if (!d || !host_out || !d->world_status) return MJB_ERR_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (cudaMemcpyAsync(host_out, d->world_status, sizeof(uint32_t) * d->nworld,
+                      cudaMemcpyDeviceToHost, s) != cudaSuccess)
+    return MJB_ERR_LAUNCH;
+  if (cudaStreamSynchronize(s) != cudaSuccess) return MJB_ERR_LAUNCH;
+  return MJB_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,763 @@
+// Primal Newton / CG constraint solver (mujoco_warp/_src/solver.py:26-1000), one warp per world.
+//
+// The reference runs each solver phase as a kernel over all njmax rows or nworld*nv dofs with
+// float atomics into per-world accumulators; here one warp owns a world for the whole solve:
+// lanes stride over the world's constraint rows (contiguous in the flat efc arrays) or over its
+// dofs, per-world sums are warp reductions (identical in every lane, so control flow stays
+// uniform), and a world that is done simply leaves the iteration loop, which is what the
+// reference's per-kernel `done` early exits amount to.  The Newton Hessian
+// H = tril(qM) + sum_active D J^T J and its Cholesky factor live in the per-warp scratch `hs`
+// (nv x nv floats).
+#pragma once
+
+#include "mjb_collide.cuh"
+
+namespace mjb {
+
+struct SolverCtx {
+  const MjbModel& m;
+  const MjbData& d;
+  int w, lane, nv, adr, n;
+  float *qacc, *Ma, *grad, *Mgrad, *search, *mv, *qfrc_constraint;
+  const float *qM, *qLD, *qfrc_smooth, *qacc_smooth;
+  float* hs;
+  float cost, prev_cost, gauss, grad_dot, search_dot, gtol, alpha;
+  float qg[3];
+};
+
+__device__ __forceinline__ float safe_div(float x, float y) { return x / (y != 0.f ? y : kMinVal); }
+
+// M vec for one world (support.py:45-92; dense qM is symmetric, so rows = columns)
+__device__ __forceinline__ void mul_m_world(const float* qM, int nv, float* res, const float* vec, int lane) {
+  for (int i = lane; i < nv; i += 32) {
+    float s = 0.f;
+    for (int j = 0; j < nv; j++) s += qM[i * nv + j] * vec[j];
+    res[i] = s;
+  }
+  __syncwarp();
+}
+
+// solver.py:75-173
+__device__ void update_constraint(SolverCtx& s) {
+  const MjbData& d = s.d;
+  const int nv = s.nv;
+  s.prev_cost = s.cost;
+  float c = 0.f;
+  for (int k = s.lane; k < s.n; k += 32) {
+    const int r = s.adr + k;
+    const float Jaref = d.efc_Jaref[r], D = d.efc_D[r];
+    const int active = Jaref < 0.f;
+    d.efc_active[r] = active;
+    if (active) {
+      d.efc_force[r] = -1.f * D * Jaref;
+      c += 0.5f * D * Jaref * Jaref;
+    } else {
+      d.efc_force[r] = 0.f;
+    }
+  }
+  c = warp_sum(c);
+  __syncwarp();
+  for (int i = s.lane; i < nv; i += 32) {
+    float f = 0.f;
+    for (int k = 0; k < s.n; k++) f += d.efc_J[size_t(s.adr + k) * nv + i] * d.efc_force[s.adr + k];
+    s.qfrc_constraint[i] = f;
+  }
+  float g = 0.f;
+  for (int i = s.lane; i < nv; i += 32)
+    g += 0.5f * (s.Ma[i] - s.qfrc_smooth[i]) * (s.qacc[i] - s.qacc_smooth[i]);
+  g = warp_sum(g);
+  s.gauss = g;
+  s.cost = c + g;
+  __syncwarp();
+}
+
+// solver.py:176-312
+__device__ void update_gradient(SolverCtx& s) {
+  const MjbModel& m = s.m;
+  const MjbData& d = s.d;
+  const int nv = s.nv, lane = s.lane;
+  float gd = 0.f;
+  for (int i = lane; i < nv; i += 32) {
+    const float g = s.Ma[i] - s.qfrc_smooth[i] - s.qfrc_constraint[i];
+    s.grad[i] = g;
+    gd += g * g;
+  }
+  s.grad_dot = warp_sum(gd);
+  __syncwarp();
+  if (m.solver == 1) {  // CG: Mgrad = M^-1 grad
+    solve_blocks(m, s.qLD, s.Mgrad, s.grad, lane);
+    return;
+  }
+  // Newton: H = tril(qM) + sum_active D J^T J, then dense Cholesky solve
+  float* H = s.hs;
+  for (int e = lane; e < nv * nv; e += 32) {
+    const int i = e / nv, j = e - i * nv;
+    if (j > i) continue;
+    float h = s.qM[e];
+    for (int k = 0; k < s.n; k++) {
+      const int r = s.adr + k;
+      if (!d.efc_active[r]) continue;
+      const float D = d.efc_D[r];
+      if (D == 0.f) continue;
+      const float* J = d.efc_J + size_t(r) * nv;
+      h += J[i] * J[j] * D;
+    }
+    H[e] = h;
+  }
+  __syncwarp();
+  if (d.efc_h) {  // keep the assembled Hessian observable (lower triangle), as the reference does
+    float* out = d.efc_h + W(s.w, nv * nv);
+    if (out != H)
+      for (int e = lane; e < nv * nv; e += 32) out[e] = H[e];
+  }
+  chol_lower(H, nv, nv, lane);
+  warp_cho_solve(H, nv, nv, s.Mgrad, s.grad, lane);
+}
+
+__device__ __forceinline__ void eval_pt3(const float* q, float a, float* out) {
+  out[0] = a * a * q[2] + a * q[1] + q[0];
+  out[1] = 2.f * a * q[2] + q[1];
+  out[2] = 2.f * q[2];
+}
+__device__ __forceinline__ bool in_bracket(const float* x, const float* y) {
+  return (x[1] < y[1] && y[1] < 0.f) || (x[1] > y[1] && y[1] > 0.f);
+}
+
+// solver.py:737-869 with the iterative (:339-664) or parallel (:667-734) line search
+__device__ void linesearch(SolverCtx& s) {
+  const MjbModel& m = s.m;
+  const MjbData& d = s.d;
+  const int nv = s.nv, lane = s.lane;
+  mul_m_world(s.qM, nv, s.mv, s.search, lane);
+  float q1 = 0.f, q2 = 0.f, q0 = 0.f;
+  for (int i = lane; i < nv; i += 32) {
+    q0 += s.gauss / float(nv);
+    q1 += s.search[i] * (s.Ma[i] - s.qfrc_smooth[i]);
+    q2 += 0.5f * s.search[i] * s.mv[i];
+  }
+  s.qg[0] = warp_sum(q0);
+  s.qg[1] = warp_sum(q1);
+  s.qg[2] = warp_sum(q2);
+  for (int k = lane; k < s.n; k += 32) {
+    const int r = s.adr + k;
+    const float* J = d.efc_J + size_t(r) * nv;
+    float jv = 0.f;
+    for (int i = 0; i < nv; i++) jv += J[i] * s.search[i];
+    const float Jaref = d.efc_Jaref[r], D = d.efc_D[r];
+    d.efc_jv[r] = jv;
+    d.efc_quad[3 * r] = 0.5f * Jaref * Jaref * D;
+    d.efc_quad[3 * r + 1] = jv * Jaref * D;
+    d.efc_quad[3 * r + 2] = 0.5f * jv * jv * D;
+  }
+  __syncwarp();
+  if (m.ls_parallel) {
+    int best = 0;
+    float bestc = 0.f;
+    for (int c = 0; c < m.nlsp; c++) {
+      const float a = m.alpha_candidate[c];
+      float t0 = 0.f, t1 = 0.f, t2 = 0.f;
+      for (int k = lane; k < s.n; k += 32) {
+        const int r = s.adr + k;
+        if (d.efc_Jaref[r] + a * d.efc_jv[r] < 0.f) {
+          t0 += d.efc_quad[3 * r];
+          t1 += d.efc_quad[3 * r + 1];
+          t2 += d.efc_quad[3 * r + 2];
+        }
+      }
+      t0 = warp_sum(t0) + s.qg[0];
+      t1 = warp_sum(t1) + s.qg[1];
+      t2 = warp_sum(t2) + s.qg[2];
+      const float cost = a * a * t2 + a * t1 + t0;
+      if (c == 0 || cost < bestc) {
+        bestc = cost;
+        best = c;
+      }
+    }
+    s.alpha = m.alpha_candidate[best];
+  } else {
+    const float snorm = sqrtf(s.search_dot);
+    const float scale = m.meaninertia * float(max(1, nv));
+    s.gtol = m.tolerance * m.ls_tolerance * snorm * scale;
+    float p0[3];
+    {
+      float a0 = 0.f, a1 = 0.f, a2 = 0.f;
+      for (int k = lane; k < s.n; k += 32) {
+        const int r = s.adr + k;
+        if (d.efc_Jaref[r] >= 0.f) continue;
+        a0 += d.efc_quad[3 * r];
+        a1 += d.efc_quad[3 * r + 1];
+        a2 += 2.f * d.efc_quad[3 * r + 2];
+      }
+      p0[0] = s.qg[0] + warp_sum(a0);
+      p0[1] = s.qg[1] + warp_sum(a1);
+      p0[2] = 2.f * s.qg[2] + warp_sum(a2);
+    }
+    // evaluates the total cost polynomial at up to three step sizes at once
+    auto totals = [&](int na, const float* al, float (*out)[3]) {
+      float acc[3][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
+      for (int k = lane; k < s.n; k += 32) {
+        const int r = s.adr + k;
+        const float jaref = d.efc_Jaref[r], jv = d.efc_jv[r];
+        const float* q = d.efc_quad + 3 * r;
+        for (int t = 0; t < na; t++) {
+          if (jaref + al[t] * jv < 0.f) {
+            float p[3];
+            eval_pt3(q, al[t], p);
+            acc[t][0] += p[0];
+            acc[t][1] += p[1];
+            acc[t][2] += p[2];
+          }
+        }
+      }
+      for (int t = 0; t < na; t++) {
+        float g[3];
+        eval_pt3(s.qg, al[t], g);
+        out[t][0] = g[0] + warp_sum(acc[t][0]);
+        out[t][1] = g[1] + warp_sum(acc[t][1]);
+        out[t][2] = g[2] + warp_sum(acc[t][2]);
+      }
+    };
+    float lo_alpha = -safe_div(p0[1], p0[2]);
+    float lo[3], hi[3], hi_alpha;
+    {
+      float o[1][3];
+      totals(1, &lo_alpha, o);
+      lo[0] = o[0][0]; lo[1] = o[0][1]; lo[2] = o[0][2];
+    }
+    if (lo[1] < p0[1]) {
+      hi[0] = p0[0]; hi[1] = p0[1]; hi[2] = p0[2];
+      hi_alpha = 0.f;
+    } else {
+      hi[0] = lo[0]; hi[1] = lo[1]; hi[2] = lo[2];
+      hi_alpha = lo_alpha;
+      lo[0] = p0[0]; lo[1] = p0[1]; lo[2] = p0[2];
+      lo_alpha = 0.f;
+    }
+    bool done = false;
+    for (int it = 0; it < m.ls_iterations && !done; it++) {
+      float al[3] = {lo_alpha - safe_div(lo[1], lo[2]), hi_alpha - safe_div(hi[1], hi[2]),
+                     0.5f * (lo_alpha + hi_alpha)};
+      float o[3][3];
+      totals(3, al, o);
+      float *lon = o[0], *hin = o[1], *mid = o[2];
+      // _swap (solver.py:537-617)
+      const bool s1 = in_bracket(lo, lon);
+      if (s1) { lo[0] = lon[0]; lo[1] = lon[1]; lo[2] = lon[2]; lo_alpha = al[0]; }
+      const bool s2 = in_bracket(lo, mid);
+      if (s2) { lo[0] = mid[0]; lo[1] = mid[1]; lo[2] = mid[2]; lo_alpha = al[2]; }
+      const bool s3 = in_bracket(lo, hin);
+      if (s3) { lo[0] = hin[0]; lo[1] = hin[1]; lo[2] = hin[2]; lo_alpha = al[1]; }
+      const bool t1 = in_bracket(hi, hin);
+      if (t1) { hi[0] = hin[0]; hi[1] = hin[1]; hi[2] = hin[2]; hi_alpha = al[1]; }
+      const bool t2 = in_bracket(hi, mid);
+      if (t2) { hi[0] = mid[0]; hi[1] = mid[1]; hi[2] = mid[2]; hi_alpha = al[2]; }
+      const bool t3 = in_bracket(hi, lon);
+      if (t3) { hi[0] = lon[0]; hi[1] = lon[1]; hi[2] = lon[2]; hi_alpha = al[0]; }
+      done = (!(s1 || s2 || s3) && !(t1 || t2 || t3)) || (lo[1] < 0.f && lo[1] > -s.gtol) ||
+             (hi[1] > 0.f && hi[1] < s.gtol);
+      float alpha = 0.f;
+      const bool improved = lo[0] < p0[0] || hi[0] < p0[0];
+      const bool lo_better = lo[0] < hi[0];
+      if (improved && lo_better) alpha = lo_alpha;
+      if (improved && !lo_better) alpha = hi_alpha;
+      s.alpha = alpha;
+    }
+  }
+  // solver.py:816-841
+  for (int i = lane; i < nv; i += 32) {
+    s.qacc[i] += s.alpha * s.search[i];
+    s.Ma[i] += s.alpha * s.mv[i];
+  }
+  for (int k = lane; k < s.n; k += 32) d.efc_Jaref[s.adr + k] += s.alpha * d.efc_jv[s.adr + k];
+  __syncwarp();
+}
+
+// solver.py:872-1000, any nv; hs: per-warp scratch of nv*nv floats (Newton only)
+__device__ void solve_generic(const MjbModel& m, const MjbData& d, int w, int lane, float* hs) {
+  const int nv = m.nv;
+  SolverCtx s{m, d, w, lane, nv, d.world_efcadr[w], d.world_nefc[w]};
+  s.qacc = d.qacc + W(w, nv);
+  s.Ma = d.efc_Ma + W(w, nv);
+  s.grad = d.efc_grad + W(w, nv);
+  s.Mgrad = d.efc_Mgrad + W(w, nv);
+  s.search = d.efc_search + W(w, nv);
+  s.mv = d.efc_mv + W(w, nv);
+  s.qfrc_constraint = d.qfrc_constraint + W(w, nv);
+  s.qM = d.qM + W(w, nv * nv);
+  s.qLD = d.qLD + W(w, nv * nv);
+  s.qfrc_smooth = d.qfrc_smooth + W(w, nv);
+  s.qacc_smooth = d.qacc_smooth + W(w, nv);
+  s.hs = hs;
+  s.alpha = 0.f;
+  s.gtol = 0.f;
+  const float* ws = d.qacc_warmstart + W(w, nv);
+  for (int i = lane; i < nv; i += 32) s.qacc[i] = ws[i];
+  __syncwarp();
+  // _create_context (solver.py:26-72)
+  s.cost = __int_as_float(0x7f800000);
+  s.search_dot = 0.f;
+  bool done = false;
+  for (int k = lane; k < s.n; k += 32) {
+    const int r = s.adr + k;
+    const float* J = d.efc_J + size_t(r) * nv;
+    float v = 0.f;
+    for (int i = 0; i < nv; i++) v += J[i] * s.qacc[i];
+    d.efc_Jaref[r] = v - d.efc_aref[r];
+  }
+  mul_m_world(s.qM, nv, s.Ma, s.qacc, lane);
+  update_constraint(s);
+  update_gradient(s);
+  float sd = 0.f;
+  for (int i = lane; i < nv; i += 32) {
+    const float v = -s.Mgrad[i];
+    s.search[i] = v;
+    sd += v * v;
+  }
+  s.search_dot = warp_sum(sd);
+  __syncwarp();
+  float* prev_grad = d.efc_prev_grad ? d.efc_prev_grad + W(w, nv) : nullptr;
+  float* prev_Mgrad = d.efc_prev_Mgrad ? d.efc_prev_Mgrad + W(w, nv) : nullptr;
+  float beta = 0.f;
+  for (int it = 0; it < m.iterations && !done; it++) {
+    linesearch(s);
+    if (m.solver == 1) {
+      for (int i = lane; i < nv; i += 32) {
+        prev_grad[i] = s.grad[i];
+        prev_Mgrad[i] = s.Mgrad[i];
+      }
+      __syncwarp();
+    }
+    update_constraint(s);
+    update_gradient(s);
+    if (m.solver == 1) {  // Polak-Ribiere (solver.py:918-970)
+      float num = 0.f, den = 0.f;
+      for (int i = lane; i < nv; i += 32) {
+        num += s.grad[i] * (s.Mgrad[i] - prev_Mgrad[i]);
+        den += prev_grad[i] * prev_Mgrad[i];
+      }
+      num = warp_sum(num);
+      den = warp_sum(den);
+      beta = fmaxf(0.f, num / fmaxf(kMinVal, den));
+    }
+    sd = 0.f;
+    for (int i = lane; i < nv; i += 32) {
+      float v = -s.Mgrad[i];
+      if (m.solver == 1) v += beta * s.search[i];
+      s.search[i] = v;
+      sd += v * v;
+    }
+    s.search_dot = warp_sum(sd);
+    __syncwarp();
+    const float scale = m.meaninertia * float(max(1, nv));
+    const float improvement = (s.prev_cost - s.cost) / scale;
+    const float gradient = sqrtf(s.grad_dot) / scale;
+    done = improvement < m.tolerance || gradient < m.tolerance;
+  }
+  float* wsw = d.qacc_warmstart + W(w, nv);
+  for (int i = lane; i < nv; i += 32) wsw[i] = s.qacc[i];
+  if (lane == 0) {
+    if (d.efc_cost) d.efc_cost[w] = s.cost;
+    if (d.efc_prev_cost) d.efc_prev_cost[w] = s.prev_cost;
+    if (d.efc_gauss) d.efc_gauss[w] = s.gauss;
+    if (d.efc_grad_dot) d.efc_grad_dot[w] = s.grad_dot;
+    if (d.efc_search_dot) d.efc_search_dot[w] = s.search_dot;
+    if (d.efc_gtol) d.efc_gtol[w] = s.gtol;
+    if (d.efc_alpha) d.efc_alpha[w] = s.alpha;
+    if (d.efc_beta) d.efc_beta[w] = beta;
+    if (d.efc_done) d.efc_done[w] = done ? 1 : 0;
+    if (d.efc_solver_niter) d.efc_solver_niter[w] = 0;  // never advanced by the reference
+    if (d.efc_quad_gauss) {
+      d.efc_quad_gauss[3 * w] = s.qg[0];
+      d.efc_quad_gauss[3 * w + 1] = s.qg[1];
+      d.efc_quad_gauss[3 * w + 2] = s.qg[2];
+    }
+  }
+  __syncwarp();
+}
+
+
+// ------------------------------------------------------------------------------------------
+// Solver for nv <= 32: lane i owns dof i, so every per-dof vector (qacc, Ma, grad, Mgrad, search,
+// mv, ...) lives in one register per lane; qM, the constraint Jacobian rows (when a world has at
+// most kSolverRows rows) and the Hessian factor live in the warp's shared-memory slice; per-row
+// scalars stay in the flat efc arrays, each touched only by the lane that owns the row.
+
+constexpr int kSolverRows = 64;
+
+__host__ __device__ __forceinline__ int solver_ld(int nv) { return nv | 1; }
+__host__ __device__ __forceinline__ size_t solver_smem_floats(int nv) {
+  const int ldm = solver_ld(nv);
+  return size_t(nv) * ldm + size_t(nv) * 33 + 32 + kSolverRows + size_t(kSolverRows) * ldm;
+}
+
+struct Small {
+  const MjbModel& m;
+  const MjbData& d;
+  int w, lane, nv, ldm, adr, n, ldj;
+  bool own;
+  float *Ms, *Ls, *vs, *F;
+  const float* J;
+  // per-dof registers
+  float qacc, Ma, grad, Mgrad, search, mv, qfs, qas, qfc;
+  // per-world scalars (uniform across lanes)
+  float cost, prev_cost, gauss, grad_dot, search_dot, gtol, alpha;
+  float qg[3];
+
+  // (M v)_lane
+  __device__ __forceinline__ float mulM(float v) {
+    vs[lane] = own ? v : 0.f;
+    __syncwarp();
+    float s = 0.f;
+    if (own)
+      for (int j = 0; j < nv; j++) s += Ms[lane * ldm + j] * vs[j];
+    __syncwarp();
+    return s;
+  }
+  // publishes v for row-wise dot products; call before rowdot, __syncwarp() after the last use
+  __device__ __forceinline__ void publish(float v) {
+    vs[lane] = own ? v : 0.f;
+    __syncwarp();
+  }
+  __device__ __forceinline__ float rowdot(int k) const {
+    const float* Jr = J + size_t(k) * ldj;
+    float s = 0.f;
+    for (int j = 0; j < nv; j++) s += Jr[j] * vs[j];
+    return s;
+  }
+};
+
+// Newton step direction H^-1 grad for nv <= 32 (solver.py:234-290): lane i assembles row i of
+// H = tril(qM) + sum_k c_k J_k^T J_k in registers (c_k = D_k for active rows, 0 otherwise), stores
+// it to Ls (leading dimension 33), factors it in place and solves; returns element `lane`.
+__device__ __noinline__ float newton_direction(const float* Ms, int ldm, const float* J, int ldj,
+                                               const float* C, int n, float* Ls, int nv, float grad,
+                                               int lane) {
+  const bool own = lane < nv;
+  float h[32];
+#pragma unroll
+  for (int j = 0; j < 32; j++) h[j] = (own && j <= lane && j < nv) ? Ms[lane * ldm + j] : 0.f;
+  for (int k = 0; k < n; k++) {
+    const float c = C[k];
+    if (c == 0.f) continue;
+    const float* Jr = J + size_t(k) * ldj;
+    const float a = own ? c * Jr[lane] : 0.f;
+#pragma unroll
+    for (int j = 0; j < 32; j++)
+      if (j < nv && j <= lane) h[j] += a * Jr[j];
+  }
+  if (own) {
+#pragma unroll
+    for (int j = 0; j < 32; j++)
+      if (j <= lane && j < nv) Ls[lane * 33 + j] = h[j];
+  }
+  __syncwarp();
+  chol_lower(Ls, 33, nv, lane);
+  const float x = cho_solve_reg32(Ls, 33, nv, grad, lane);
+  return own ? x : 0.f;
+}
+
+// solver.py:75-173
+__device__ void small_update_constraint(Small& s) {
+  const MjbData& d = s.d;
+  s.prev_cost = s.cost;
+  float c = 0.f;
+  for (int k = s.lane; k < s.n; k += 32) {
+    const int r = s.adr + k;
+    const float Jaref = d.efc_Jaref[r], D = d.efc_D[r];
+    const int active = Jaref < 0.f;
+    d.efc_active[r] = active;
+    const float f = active ? -1.f * D * Jaref : 0.f;
+    d.efc_force[r] = f;
+    s.F[k] = f;
+    if (active) c += 0.5f * D * Jaref * Jaref;
+  }
+  c = warp_sum(c);
+  __syncwarp();
+  float q = 0.f;
+  if (s.own)
+    for (int k = 0; k < s.n; k++) q += s.J[size_t(k) * s.ldj + s.lane] * s.F[k];
+  s.qfc = q;
+  float g = s.own ? 0.5f * (s.Ma - s.qfs) * (s.qacc - s.qas) : 0.f;
+  g = warp_sum(g);
+  s.gauss = g;
+  s.cost = c + g;
+  __syncwarp();
+}
+
+// solver.py:176-312
+__device__ void small_update_gradient(Small& s) {
+  const MjbModel& m = s.m;
+  const MjbData& d = s.d;
+  const int nv = s.nv, lane = s.lane;
+  s.grad = s.own ? s.Ma - s.qfs - s.qfc : 0.f;
+  s.grad_dot = warp_sum(s.grad * s.grad);
+  if (m.solver == 1) {  // CG: Mgrad = M^-1 grad with the qLD factor
+    float* gg = d.efc_grad + W(s.w, nv);
+    float* mg = d.efc_Mgrad + W(s.w, nv);
+    if (s.own) gg[lane] = s.grad;
+    __syncwarp();
+    solve_blocks(m, d.qLD + W(s.w, nv * nv), mg, gg, lane);
+    s.Mgrad = s.own ? mg[lane] : 0.f;
+    __syncwarp();
+    return;
+  }
+  // coefficient of each row in J^T D J: D when active, else 0
+  for (int k = lane; k < s.n; k += 32) {
+    const int r = s.adr + k;
+    s.F[k] = d.efc_active[r] ? d.efc_D[r] : 0.f;
+  }
+  __syncwarp();
+  s.Mgrad = newton_direction(s.Ms, s.ldm, s.J, s.ldj, s.F, s.n, s.Ls, nv, s.grad, lane);
+}
+
+// solver.py:737-869
+__device__ void small_linesearch(Small& s) {
+  const MjbModel& m = s.m;
+  const MjbData& d = s.d;
+  const int nv = s.nv, lane = s.lane;
+  s.mv = s.mulM(s.search);
+  {
+    float q0 = s.own ? s.gauss / float(nv) : 0.f;
+    float q1 = s.own ? s.search * (s.Ma - s.qfs) : 0.f;
+    float q2 = s.own ? 0.5f * s.search * s.mv : 0.f;
+    s.qg[0] = warp_sum(q0);
+    s.qg[1] = warp_sum(q1);
+    s.qg[2] = warp_sum(q2);
+  }
+  s.publish(s.search);
+  for (int k = lane; k < s.n; k += 32) {
+    const int r = s.adr + k;
+    const float jv = s.rowdot(k);
+    const float Jaref = d.efc_Jaref[r], D = d.efc_D[r];
+    d.efc_jv[r] = jv;
+    d.efc_quad[3 * r] = 0.5f * Jaref * Jaref * D;
+    d.efc_quad[3 * r + 1] = jv * Jaref * D;
+    d.efc_quad[3 * r + 2] = 0.5f * jv * jv * D;
+  }
+  __syncwarp();
+  if (m.ls_parallel) {
+    int best = 0;
+    float bestc = 0.f;
+    for (int c = 0; c < m.nlsp; c++) {
+      const float a = m.alpha_candidate[c];
+      float t0 = 0.f, t1 = 0.f, t2 = 0.f;
+      for (int k = lane; k < s.n; k += 32) {
+        const int r = s.adr + k;
+        if (d.efc_Jaref[r] + a * d.efc_jv[r] < 0.f) {
+          t0 += d.efc_quad[3 * r];
+          t1 += d.efc_quad[3 * r + 1];
+          t2 += d.efc_quad[3 * r + 2];
+        }
+      }
+      t0 = warp_sum(t0) + s.qg[0];
+      t1 = warp_sum(t1) + s.qg[1];
+      t2 = warp_sum(t2) + s.qg[2];
+      const float cost = a * a * t2 + a * t1 + t0;
+      if (c == 0 || cost < bestc) {
+        bestc = cost;
+        best = c;
+      }
+    }
+    s.alpha = m.alpha_candidate[best];
+  } else {
+    const float scale = m.meaninertia * float(max(1, nv));
+    s.gtol = m.tolerance * m.ls_tolerance * sqrtf(s.search_dot) * scale;
+    float p0[3];
+    {
+      float a0 = 0.f, a1 = 0.f, a2 = 0.f;
+      for (int k = lane; k < s.n; k += 32) {
+        const int r = s.adr + k;
+        if (d.efc_Jaref[r] >= 0.f) continue;
+        a0 += d.efc_quad[3 * r];
+        a1 += d.efc_quad[3 * r + 1];
+        a2 += 2.f * d.efc_quad[3 * r + 2];
+      }
+      p0[0] = s.qg[0] + warp_sum(a0);
+      p0[1] = s.qg[1] + warp_sum(a1);
+      p0[2] = 2.f * s.qg[2] + warp_sum(a2);
+    }
+    auto totals = [&](int na, const float* al, float (*out)[3]) {
+      float acc[3][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
+      for (int k = lane; k < s.n; k += 32) {
+        const int r = s.adr + k;
+        const float jaref = d.efc_Jaref[r], jv = d.efc_jv[r];
+        const float* q = d.efc_quad + 3 * r;
+        for (int t = 0; t < na; t++) {
+          if (jaref + al[t] * jv < 0.f) {
+            float p[3];
+            eval_pt3(q, al[t], p);
+            acc[t][0] += p[0];
+            acc[t][1] += p[1];
+            acc[t][2] += p[2];
+          }
+        }
+      }
+      for (int t = 0; t < na; t++) {
+        float g[3];
+        eval_pt3(s.qg, al[t], g);
+        out[t][0] = g[0] + warp_sum(acc[t][0]);
+        out[t][1] = g[1] + warp_sum(acc[t][1]);
+        out[t][2] = g[2] + warp_sum(acc[t][2]);
+      }
+    };
+    float lo_alpha = -safe_div(p0[1], p0[2]);
+    float lo[3], hi[3], hi_alpha;
+    {
+      float o[1][3];
+      totals(1, &lo_alpha, o);
+      lo[0] = o[0][0]; lo[1] = o[0][1]; lo[2] = o[0][2];
+    }
+    if (lo[1] < p0[1]) {
+      hi[0] = p0[0]; hi[1] = p0[1]; hi[2] = p0[2];
+      hi_alpha = 0.f;
+    } else {
+      hi[0] = lo[0]; hi[1] = lo[1]; hi[2] = lo[2];
+      hi_alpha = lo_alpha;
+      lo[0] = p0[0]; lo[1] = p0[1]; lo[2] = p0[2];
+      lo_alpha = 0.f;
+    }
+    bool done = false;
+    for (int it = 0; it < m.ls_iterations && !done; it++) {
+      float al[3] = {lo_alpha - safe_div(lo[1], lo[2]), hi_alpha - safe_div(hi[1], hi[2]),
+                     0.5f * (lo_alpha + hi_alpha)};
+      float o[3][3];
+      totals(3, al, o);
+      float *lon = o[0], *hin = o[1], *mid = o[2];
+      const bool s1 = in_bracket(lo, lon);
+      if (s1) { lo[0] = lon[0]; lo[1] = lon[1]; lo[2] = lon[2]; lo_alpha = al[0]; }
+      const bool s2 = in_bracket(lo, mid);
+      if (s2) { lo[0] = mid[0]; lo[1] = mid[1]; lo[2] = mid[2]; lo_alpha = al[2]; }
+      const bool s3 = in_bracket(lo, hin);
+      if (s3) { lo[0] = hin[0]; lo[1] = hin[1]; lo[2] = hin[2]; lo_alpha = al[1]; }
+      const bool t1 = in_bracket(hi, hin);
+      if (t1) { hi[0] = hin[0]; hi[1] = hin[1]; hi[2] = hin[2]; hi_alpha = al[1]; }
+      const bool t2 = in_bracket(hi, mid);
+      if (t2) { hi[0] = mid[0]; hi[1] = mid[1]; hi[2] = mid[2]; hi_alpha = al[2]; }
+      const bool t3 = in_bracket(hi, lon);
+      if (t3) { hi[0] = lon[0]; hi[1] = lon[1]; hi[2] = lon[2]; hi_alpha = al[0]; }
+      done = (!(s1 || s2 || s3) && !(t1 || t2 || t3)) || (lo[1] < 0.f && lo[1] > -s.gtol) ||
+             (hi[1] > 0.f && hi[1] < s.gtol);
+      float alpha = 0.f;
+      const bool improved = lo[0] < p0[0] || hi[0] < p0[0];
+      const bool lo_better = lo[0] < hi[0];
+      if (improved && lo_better) alpha = lo_alpha;
+      if (improved && !lo_better) alpha = hi_alpha;
+      s.alpha = alpha;
+    }
+  }
+  if (s.own) {
+    s.qacc += s.alpha * s.search;
+    s.Ma += s.alpha * s.mv;
+  }
+  for (int k = lane; k < s.n; k += 32) d.efc_Jaref[s.adr + k] += s.alpha * d.efc_jv[s.adr + k];
+  __syncwarp();
+}
+
+// solver.py:872-1000 for nv <= 32; sm: solver_smem_floats(nv) floats of warp-private scratch
+__device__ void solve_small(const MjbModel& m, const MjbData& d, int w, int lane, float* sm) {
+  const int nv = m.nv, ldm = solver_ld(nv);
+  const int adr = d.world_efcadr[w], n = d.world_nefc[w];
+  Small s{m, d, w, lane, nv, ldm, adr, n};
+  s.own = lane < nv;
+  s.Ms = sm;
+  s.Ls = s.Ms + nv * ldm;
+  s.vs = s.Ls + nv * 33;
+  s.F = s.vs + 32;
+  float* Js = s.F + kSolverRows;
+  const float* Jg = d.efc_J + size_t(adr) * nv;
+  if (n <= kSolverRows) {
+    for (int e = lane; e < n * nv; e += 32) {
+      const int r = e / nv;
+      Js[r * ldm + (e - r * nv)] = Jg[e];
+    }
+    s.J = Js;
+    s.ldj = ldm;
+  } else {
+    s.J = Jg;
+    s.ldj = nv;
+    s.F = d.efc_force + adr;  // rows beyond the staged capacity broadcast through global memory
+  }
+  const float* qMg = d.qM + W(w, nv * nv);
+  for (int e = lane; e < nv * nv; e += 32) {
+    const int i = e / nv;
+    s.Ms[i * ldm + (e - i * nv)] = qMg[e];
+  }
+  s.qacc = s.own ? d.qacc_warmstart[W(w, nv) + lane] : 0.f;
+  s.qfs = s.own ? d.qfrc_smooth[W(w, nv) + lane] : 0.f;
+  s.qas = s.own ? d.qacc_smooth[W(w, nv) + lane] : 0.f;
+  s.alpha = 0.f;
+  s.gtol = 0.f;
+  s.qg[0] = s.qg[1] = s.qg[2] = 0.f;
+  __syncwarp();
+  // _create_context (solver.py:26-72)
+  s.cost = __int_as_float(0x7f800000);
+  s.publish(s.qacc);
+  for (int k = lane; k < n; k += 32) d.efc_Jaref[adr + k] = s.rowdot(k) - d.efc_aref[adr + k];
+  __syncwarp();
+  s.Ma = s.mulM(s.qacc);
+  small_update_constraint(s);
+  small_update_gradient(s);
+  s.search = -s.Mgrad;
+  s.search_dot = warp_sum(s.search * s.search);
+  bool done = false;
+  float beta = 0.f, prev_grad = 0.f, prev_Mgrad = 0.f;
+  for (int it = 0; it < m.iterations && !done; it++) {
+    small_linesearch(s);
+    prev_grad = s.grad;
+    prev_Mgrad = s.Mgrad;
+    small_update_constraint(s);
+    small_update_gradient(s);
+    if (m.solver == 1) {  // Polak-Ribiere (solver.py:918-970)
+      const float num = warp_sum(s.own ? s.grad * (s.Mgrad - prev_Mgrad) : 0.f);
+      const float den = warp_sum(s.own ? prev_grad * prev_Mgrad : 0.f);
+      beta = fmaxf(0.f, num / fmaxf(kMinVal, den));
+    }
+    float v = -s.Mgrad;
+    if (m.solver == 1) v += beta * s.search;
+    s.search = s.own ? v : 0.f;
+    s.search_dot = warp_sum(s.search * s.search);
+    const float scale = m.meaninertia * float(max(1, nv));
+    done = (s.prev_cost - s.cost) / scale < m.tolerance || sqrtf(s.grad_dot) / scale < m.tolerance;
+  }
+  if (s.own) {
+    const size_t o = W(w, nv) + lane;
+    d.qacc[o] = s.qacc;
+    d.qacc_warmstart[o] = s.qacc;
+    d.qfrc_constraint[o] = s.qfc;
+    d.efc_Ma[o] = s.Ma;
+    d.efc_grad[o] = s.grad;
+    d.efc_Mgrad[o] = s.Mgrad;
+    d.efc_search[o] = s.search;
+    d.efc_mv[o] = s.mv;
+    if (d.efc_prev_grad) d.efc_prev_grad[o] = prev_grad;
+    if (d.efc_prev_Mgrad) d.efc_prev_Mgrad[o] = prev_Mgrad;
+  }
+  if (lane == 0) {
+    if (d.efc_cost) d.efc_cost[w] = s.cost;
+    if (d.efc_prev_cost) d.efc_prev_cost[w] = s.prev_cost;
+    if (d.efc_gauss) d.efc_gauss[w] = s.gauss;
+    if (d.efc_grad_dot) d.efc_grad_dot[w] = s.grad_dot;
+    if (d.efc_search_dot) d.efc_search_dot[w] = s.search_dot;
+    if (d.efc_gtol) d.efc_gtol[w] = s.gtol;
+    if (d.efc_alpha) d.efc_alpha[w] = s.alpha;
+    if (d.efc_beta) d.efc_beta[w] = beta;
+    if (d.efc_done) d.efc_done[w] = done ? 1 : 0;
+    if (d.efc_solver_niter) d.efc_solver_niter[w] = 0;
+    if (d.efc_quad_gauss) {
+      d.efc_quad_gauss[3 * w] = s.qg[0];
+      d.efc_quad_gauss[3 * w + 1] = s.qg[1];
+      d.efc_quad_gauss[3 * w + 2] = s.qg[2];
+    }
+  }
+  __syncwarp();
+}
+
+// Dispatch: the register / shared-memory solver when nv <= 32 and the caller provides its scratch
+// (solver_smem_floats(nv) floats), else the generic solver with an nv x nv Hessian tile `hs`.
+__device__ __forceinline__ void solve(const MjbModel& m, const MjbData& d, int w, int lane,
+                                      float* sm, float* hs) {
+  if (m.nv <= 32 && sm) solve_small(m, d, w, lane, sm);
+  else solve_generic(m, d, w, lane, hs);
+}
+
+}  // namespace mjb

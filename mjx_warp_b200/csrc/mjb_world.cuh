@@ -1,0 +1,731 @@
+// Per-world stages of the batched step, executed by one warp per world.
+//
+// Each function evaluates one stage of the reference pipeline (mujoco_warp/_src/*.py, cited per
+// function) for world `w` with the 32 lanes of the calling warp cooperating: lanes stride over
+// the bodies of a tree level, over joints, dofs, geoms, candidate pairs, contacts or constraint
+// rows.  Tree recursions run level by level from the BFS tables (body_tree / body_treeadr) with
+// a __syncwarp() between levels; accumulations into a parent gather over that parent's children
+// (body_child tables) instead of the reference's float atomics, so every result is
+// deterministic.  All pointers are generic: the plain per-stage kernels pass global memory, the
+// fused step passes the same layout.
+#pragma once
+
+#include "../../include/mjb200.h"
+#include "mjb_math.cuh"
+
+namespace mjb {
+
+#define WARP_FULL 0xffffffffu
+
+__device__ __forceinline__ size_t W(int w, int n) { return size_t(w) * size_t(n); }
+
+// ------------------------------------------------------------------------------------------
+// smooth.py:32-145 — forward kinematics
+__device__ void kinematics(const MjbModel& m, const MjbData& d, int w, int lane) {
+  const int nb = m.nbody;
+  const float* qpos = d.qpos + W(w, m.nq);
+  float* xpos = d.xpos + W(w, 3 * nb);
+  float* xquat = d.xquat + W(w, 4 * nb);
+  float* xmat = d.xmat + W(w, 9 * nb);
+  float* xipos = d.xipos + W(w, 3 * nb);
+  float* ximat = d.ximat + W(w, 9 * nb);
+  float* xanchor = d.xanchor + W(w, 3 * m.njnt);
+  float* xaxis = d.xaxis + W(w, 3 * m.njnt);
+  if (lane == 0) {  // _root (smooth.py:37-43)
+    st3(xpos, mk3(0, 0, 0));
+    st4(xquat, q4{1, 0, 0, 0});
+    st3(xipos, mk3(0, 0, 0));
+    m33 eye{{1, 0, 0, 0, 1, 0, 0, 0, 1}};
+    st9(xmat, eye);
+    st9(ximat, eye);
+  }
+  __syncwarp();
+  for (int lvl = 1; lvl < m.nlevel; lvl++) {
+    const int beg = m.body_treeadr[lvl], end = m.body_treeadr[lvl + 1];
+    for (int n = beg + lane; n < end; n += 32) {  // _level (smooth.py:46-109)
+      const int b = m.body_tree[n];
+      const int jntadr = m.body_jntadr[b], jntnum = m.body_jntnum[b];
+      f3 pos;
+      q4 quat;
+      if (jntnum == 1 && m.jnt_type[jntadr] == JNT_FREE) {
+        const int a = m.jnt_qposadr[jntadr];
+        pos = ld3(qpos + a);
+        quat = ld4(qpos + a + 3);
+        st3(xanchor + 3 * jntadr, pos);
+        st3(xaxis + 3 * jntadr, ld3(m.jnt_axis + 3 * jntadr));
+      } else {
+        const int p = m.body_parentid[b];
+        pos = mulmv(ld9(xmat + 9 * p), ld3(m.body_pos + 3 * b)) + ld3(xpos + 3 * p);
+        quat = mul_quat(ld4(xquat + 4 * p), ld4(m.body_quat + 4 * b));
+        for (int j = jntadr; j < jntadr + jntnum; j++) {
+          const int a = m.jnt_qposadr[j];
+          const int t = m.jnt_type[j];
+          const f3 jaxis = ld3(m.jnt_axis + 3 * j), jpos = ld3(m.jnt_pos + 3 * j);
+          const f3 anchor = rot_vec_quat(jpos, quat) + pos;
+          const f3 axis = rot_vec_quat(jaxis, quat);
+          if (t == JNT_BALL) {
+            quat = mul_quat(quat, ld4(qpos + a));
+            pos = anchor - rot_vec_quat(jpos, quat);
+          } else if (t == JNT_SLIDE) {
+            pos = pos + axis * (qpos[a] - m.qpos0[a]);
+          } else if (t == JNT_HINGE) {
+            quat = mul_quat(quat, axis_angle_to_quat(jaxis, qpos[a] - m.qpos0[a]));
+            pos = anchor - rot_vec_quat(jpos, quat);
+          }
+          st3(xanchor + 3 * j, anchor);
+          st3(xaxis + 3 * j, axis);
+        }
+      }
+      st3(xpos + 3 * b, pos);
+      quat = qnormalize(quat);
+      st4(xquat + 4 * b, quat);
+      st9(xmat + 9 * b, quat_to_mat(quat));
+      st3(xipos + 3 * b, pos + rot_vec_quat(ld3(m.body_ipos + 3 * b), quat));
+      st9(ximat + 9 * b, quat_to_mat(mul_quat(quat, ld4(m.body_iquat + 4 * b))));
+    }
+    __syncwarp();
+  }
+  // geom_local_to_global / site_local_to_global (smooth.py:111-131)
+  float* gxpos = d.geom_xpos + W(w, 3 * m.ngeom);
+  float* gxmat = d.geom_xmat + W(w, 9 * m.ngeom);
+  for (int g = lane; g < m.ngeom; g += 32) {
+    const int b = m.geom_bodyid[g];
+    const q4 q = ld4(xquat + 4 * b);
+    st3(gxpos + 3 * g, ld3(xpos + 3 * b) + rot_vec_quat(ld3(m.geom_pos + 3 * g), q));
+    st9(gxmat + 9 * g, quat_to_mat(mul_quat(q, ld4(m.geom_quat + 4 * g))));
+  }
+  if (d.site_xpos) {
+    float* sxpos = d.site_xpos + W(w, 3 * m.nsite);
+    float* sxmat = d.site_xmat + W(w, 9 * m.nsite);
+    for (int s = lane; s < m.nsite; s += 32) {
+      const int b = m.site_bodyid[s];
+      const q4 q = ld4(xquat + 4 * b);
+      st3(sxpos + 3 * s, ld3(xpos + 3 * b) + rot_vec_quat(ld3(m.site_pos + 3 * s), q));
+      st9(sxmat + 9 * s, quat_to_mat(mul_quat(q, ld4(m.site_quat + 4 * s))));
+    }
+  }
+  __syncwarp();
+}
+
+// ------------------------------------------------------------------------------------------
+// smooth.py:148-245 — subtree CoM, cinert, cdof
+__device__ void com_pos(const MjbModel& m, const MjbData& d, int w, int lane) {
+  const int nb = m.nbody;
+  const float* xipos = d.xipos + W(w, 3 * nb);
+  const float* ximat = d.ximat + W(w, 9 * nb);
+  const float* xmat = d.xmat + W(w, 9 * nb);
+  const float* xanchor = d.xanchor + W(w, 3 * m.njnt);
+  const float* xaxis = d.xaxis + W(w, 3 * m.njnt);
+  float* sc = d.subtree_com + W(w, 3 * nb);
+  for (int b = lane; b < nb; b += 32) st3(sc + 3 * b, ld3(xipos + 3 * b) * m.body_mass[b]);
+  __syncwarp();
+  // bottom-up gather over children; the world also adds itself (smooth.py:238-241 runs the
+  // accumulation on level 0, where body 0 is its own parent)
+  for (int lvl = m.nlevel - 1; lvl >= 0; lvl--) {
+    const int beg = m.body_treeadr[lvl], end = m.body_treeadr[lvl + 1];
+    for (int n = beg + lane; n < end; n += 32) {
+      const int b = m.body_tree[n];
+      f3 acc = ld3(sc + 3 * b);
+      const int ca = m.body_childadr[b], cn = m.body_childnum[b];
+      for (int k = 0; k < cn; k++) acc = acc + ld3(sc + 3 * m.body_child[ca + k]);
+      if (b == 0) acc = acc + acc;
+      st3(sc + 3 * b, acc);
+    }
+    __syncwarp();
+  }
+  for (int b = lane; b < nb; b += 32) {
+    const float sm = m.subtree_mass[b];
+    f3 v = ld3(sc + 3 * b);
+    st3(sc + 3 * b, mk3(v.x / sm, v.y / sm, v.z / sm));
+  }
+  __syncwarp();
+  // cinert (smooth.py:169-201)
+  float* cinert = d.cinert + W(w, 10 * nb);
+  for (int b = lane; b < nb; b += 32) {
+    const m33 mat = ld9(ximat + 9 * b);
+    const f3 inert = ld3(m.body_inertia + 3 * b);
+    const float mass = m.body_mass[b];
+    const f3 dif = ld3(xipos + 3 * b) - ld3(sc + 3 * m.body_rootid[b]);
+    float t[6];
+    const int ij[6][2] = {{0, 0}, {1, 1}, {2, 2}, {0, 1}, {0, 2}, {1, 2}};
+#pragma unroll
+    for (int e = 0; e < 6; e++) {
+      const int i = ij[e][0], j = ij[e][1];
+      t[e] = mat.m[3 * i] * inert.x * mat.m[3 * j] + mat.m[3 * i + 1] * inert.y * mat.m[3 * j + 1] +
+             mat.m[3 * i + 2] * inert.z * mat.m[3 * j + 2];
+    }
+    float* r = cinert + 10 * b;
+    r[0] = t[0] + mass * (dif.y * dif.y + dif.z * dif.z);
+    r[1] = t[1] + mass * (dif.x * dif.x + dif.z * dif.z);
+    r[2] = t[2] + mass * (dif.x * dif.x + dif.y * dif.y);
+    r[3] = t[3] - mass * dif.x * dif.y;
+    r[4] = t[4] - mass * dif.x * dif.z;
+    r[5] = t[5] - mass * dif.y * dif.z;
+    r[6] = mass * dif.x;
+    r[7] = mass * dif.y;
+    r[8] = mass * dif.z;
+    r[9] = mass;
+  }
+  // cdof (smooth.py:203-232)
+  float* cdof = d.cdof + W(w, 6 * m.nv);
+  for (int j = lane; j < m.njnt; j += 32) {
+    const int b = m.jnt_bodyid[j], dof = m.jnt_dofadr[j], t = m.jnt_type[j];
+    const f3 off = ld3(sc + 3 * m.body_rootid[b]) - ld3(xanchor + 3 * j);
+    const m33 xm = ld9(xmat + 9 * b);
+    auto put = [&](int i, f3 a, f3 l) {
+      float* c = cdof + 6 * i;
+      c[0] = a.x; c[1] = a.y; c[2] = a.z; c[3] = l.x; c[4] = l.y; c[5] = l.z;
+    };
+    if (t == JNT_FREE) {
+      put(dof + 0, mk3(0, 0, 0), mk3(1, 0, 0));
+      put(dof + 1, mk3(0, 0, 0), mk3(0, 1, 0));
+      put(dof + 2, mk3(0, 0, 0), mk3(0, 0, 1));
+      for (int k = 0; k < 3; k++) put(dof + 3 + k, col(xm, k), cross(col(xm, k), off));
+    } else if (t == JNT_BALL) {
+      for (int k = 0; k < 3; k++) put(dof + k, col(xm, k), cross(col(xm, k), off));
+    } else if (t == JNT_SLIDE) {
+      put(dof, mk3(0, 0, 0), ld3(xaxis + 3 * j));
+    } else {
+      const f3 ax = ld3(xaxis + 3 * j);
+      put(dof, ax, cross(ax, off));
+    }
+  }
+  __syncwarp();
+}
+
+// ------------------------------------------------------------------------------------------
+// smooth.py:248-314 — composite rigid body inertia and dense qM
+__device__ void crb(const MjbModel& m, const MjbData& d, int w, int lane) {
+  const int nb = m.nbody, nv = m.nv;
+  const float* cinert = d.cinert + W(w, 10 * nb);
+  float* crb = d.crb + W(w, 10 * nb);
+  // bottom-up gather; children of the world do not add into it (smooth.py:259-260)
+  for (int lvl = m.nlevel - 1; lvl >= 0; lvl--) {
+    const int beg = m.body_treeadr[lvl], end = m.body_treeadr[lvl + 1];
+    for (int n = beg + lane; n < end; n += 32) {
+      const int b = m.body_tree[n];
+      float acc[10];
+#pragma unroll
+      for (int k = 0; k < 10; k++) acc[k] = cinert[10 * b + k];
+      if (b != 0) {
+        const int ca = m.body_childadr[b], cn = m.body_childnum[b];
+        for (int c = 0; c < cn; c++) {
+          const float* src = crb + 10 * m.body_child[ca + c];
+#pragma unroll
+          for (int k = 0; k < 10; k++) acc[k] += src[k];
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < 10; k++) crb[10 * b + k] = acc[k];
+    }
+    __syncwarp();
+  }
+  // qM_dense (smooth.py:281-302)
+  float* qM = d.qM + W(w, nv * nv);
+  const float* cdof = d.cdof + W(w, 6 * nv);
+  for (int e = lane; e < nv * nv; e += 32) qM[e] = 0.f;
+  __syncwarp();
+  for (int i = lane; i < nv; i += 32) {
+    const s6 ci = ld6(cdof + 6 * i);
+    const s6 buf = inert_vec(crb + 10 * m.dof_bodyid[i], ci);
+    qM[i * nv + i] = m.dof_armature[i] + dot6(ci, buf);
+    for (int j = m.dof_parentid[i]; j >= 0; j = m.dof_parentid[j]) {
+      const float v = dot6(ld6(cdof + 6 * j), buf);
+      qM[i * nv + j] = v;
+      qM[j * nv + i] = v;
+    }
+  }
+  __syncwarp();
+}
+
+// In-place Cholesky A = L L^T (left-looking, column by column) of the n x n SPD matrix at A with
+// leading dimension ld (shared or global memory); only the lower triangle is read and written.
+// Column k: the diagonal's dot product is split over lanes and reduced, then each lane finishes
+// the rows i = k+1+lane, k+33+lane, ... with one dot product against row k (a broadcast read).
+// Compiled once (no inlining) so every caller shares one copy of the code.
+template <typename T>
+__device__ __noinline__ void chol_lower(T* A, int ld, int n, int lane) {
+  for (int k = 0; k < n; k++) {
+    const T* Ak = A + k * ld;
+    T part = T(0);
+    for (int m = lane; m < k; m += 32) part += Ak[m] * Ak[m];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+    const T lkk = sqrt(Ak[k * 0 + k] - part);
+    const T inv = T(1) / lkk;
+    for (int i = k + 1 + lane; i < n; i += 32) {
+      T* Ai = A + i * ld;
+      T s0 = Ai[k], s1 = T(0);
+      int m = 0;
+      for (; m + 1 < k; m += 2) {
+        s0 -= Ai[m] * Ak[m];
+        s1 -= Ai[m + 1] * Ak[m + 1];
+      }
+      if (m < k) s0 -= Ai[m] * Ak[m];
+      Ai[k] = (s0 + s1) * inv;
+    }
+    __syncwarp();
+    if (lane == 0) A[k * ld + k] = lkk;
+    __syncwarp();
+  }
+}
+
+// x = (L L^T)^-1 y for a factor of size n <= 32 stored with leading dimension ldl; y given and x
+// returned per lane (lane i <-> element i).
+template <typename T>
+__device__ __forceinline__ T cho_solve_reg32(const T* L, int ldl, int n, T yi, int lane) {
+  T xi = lane < n ? yi : T(0);
+  for (int k = 0; k < n; k++) {
+    const T xk = __shfl_sync(0xffffffffu, xi, k) / L[k * ldl + k];
+    if (lane == k) xi = xk;
+    else if (lane > k && lane < n) xi -= L[lane * ldl + k] * xk;
+  }
+  for (int k = n - 1; k >= 0; k--) {
+    const T xk = __shfl_sync(0xffffffffu, xi, k) / L[k * ldl + k];
+    if (lane == k) xi = xk;
+    else if (lane < k) xi -= L[k * ldl + lane] * xk;
+  }
+  return xi;
+}
+
+// x = (L L^T)^-1 y for the n x n lower factor at L (leading dimension ld); x may alias y.
+__device__ void warp_cho_solve(const float* L, int ld, int n, float* x, const float* y, int lane) {
+  if (n <= 32) {
+    float xi = lane < n ? y[lane] : 0.f;
+    for (int k = 0; k < n; k++) {  // L z = y
+      float xk = __shfl_sync(WARP_FULL, xi, k) / L[k * ld + k];
+      if (lane == k) xi = xk;
+      else if (lane > k && lane < n) xi -= L[lane * ld + k] * xk;
+    }
+    for (int k = n - 1; k >= 0; k--) {  // L^T x = z
+      float xk = __shfl_sync(WARP_FULL, xi, k) / L[k * ld + k];
+      if (lane == k) xi = xk;
+      else if (lane < k) xi -= L[k * ld + lane] * xk;
+    }
+    __syncwarp();
+    if (lane < n) x[lane] = xi;
+    __syncwarp();
+    return;
+  }
+  for (int i = lane; i < n; i += 32) x[i] = y[i];
+  __syncwarp();
+  for (int k = 0; k < n; k++) {
+    const float xk = x[k] / L[k * ld + k];
+    __syncwarp();
+    if (lane == (k & 31)) x[k] = xk;
+    for (int i = k + 1 + lane; i < n; i += 32) x[i] -= L[i * ld + k] * xk;
+    __syncwarp();
+  }
+  for (int k = n - 1; k >= 0; k--) {
+    const float xk = x[k] / L[k * ld + k];
+    __syncwarp();
+    if (lane == (k & 31)) x[k] = xk;
+    for (int i = lane; i < k; i += 32) x[i] -= L[k * ld + i] * xk;
+    __syncwarp();
+  }
+}
+
+// Factor every tree block of the nv x nv matrix M (+ scale * diag(dadd) when dadd is given) into
+// L: dense storage, zero outside the lower block triangles.  smooth.py:353-379 (tile_cholesky per
+// qLD_tile group) and the fused damping tiles of forward.py:195-232.
+__device__ void factor_blocks(const MjbModel& m, const float* M, float* L, int lane,
+                              const float* dadd = nullptr, float scale = 0.f) {
+  const int nv = m.nv;
+  for (int e = lane; e < nv * nv; e += 32) L[e] = 0.f;
+  __syncwarp();
+  for (int blk = 0; blk < m.nblock; blk++) {
+    const int a = m.block_adr[blk], n = m.block_size[blk];
+    for (int e = lane; e < n * n; e += 32) {
+      const int i = e / n, j = e - i * n;
+      if (j <= i) {
+        float v = M[(a + i) * nv + a + j];
+        if (dadd && i == j) v += scale * dadd[a + i];
+        L[(a + i) * nv + a + j] = v;
+      }
+    }
+    __syncwarp();
+    chol_lower(L + a * nv + a, nv, n, lane);
+  }
+}
+
+// x = M^-1 y per tree block from the block factor L (smooth.py:654-681)
+__device__ void solve_blocks(const MjbModel& m, const float* L, float* x, const float* y,
+                             int lane) {
+  const int nv = m.nv;
+  for (int blk = 0; blk < m.nblock; blk++) {
+    const int a = m.block_adr[blk], n = m.block_size[blk];
+    warp_cho_solve(L + a * nv + a, nv, n, x + a, y + a, lane);
+  }
+}
+
+// smooth.py:392-395
+__device__ void factor_m(const MjbModel& m, const MjbData& d, int w, int lane) {
+  const int nv = m.nv;
+  factor_blocks(m, d.qM + W(w, nv * nv), d.qLD + W(w, nv * nv), lane);
+}
+
+// ------------------------------------------------------------------------------------------
+// smooth.py:469-536 — transmission (JOINT, JOINTINPARENT)
+__device__ void transmission(const MjbModel& m, const MjbData& d, int w, int lane) {
+  const int nv = m.nv;
+  const float* qpos = d.qpos + W(w, m.nq);
+  float* length = d.actuator_length + W(w, m.nu);
+  float* moment = d.actuator_moment + W(w, m.nu * nv);
+  for (int a = lane; a < m.nu; a += 32) {
+    const int j = m.actuator_trnid[2 * a], t = m.jnt_type[j];
+    const int qa = m.jnt_qposadr[j], va = m.jnt_dofadr[j], trn = m.actuator_trntype[a];
+    const float* gear = m.actuator_gear + 6 * a;
+    float* mom = moment + a * nv;
+    for (int i = 0; i < nv; i++) mom[i] = 0.f;
+    if (trn != 0 && trn != 1) continue;
+    if (t == JNT_FREE) {
+      length[a] = 0.f;
+      if (trn == 1) {
+        const q4 qn{qpos[qa + 3], -qpos[qa + 4], -qpos[qa + 5], -qpos[qa + 6]};
+        const f3 ga = rot_vec_quat(mk3(gear[3], gear[4], gear[5]), qn);
+        mom[va] = gear[0]; mom[va + 1] = gear[1]; mom[va + 2] = gear[2];
+        mom[va + 3] = ga.x; mom[va + 4] = ga.y; mom[va + 5] = ga.z;
+      } else {
+        for (int i = 0; i < 6; i++) mom[va + i] = gear[i];
+      }
+    } else if (t == JNT_BALL) {
+      const q4 q = ld4(qpos + qa);
+      const f3 aa = quat_to_vel(q);
+      f3 ga = mk3(gear[0], gear[1], gear[2]);
+      if (trn == 1) ga = rot_vec_quat(ga, q4{q.w, -q.x, -q.y, -q.z});
+      length[a] = dot(aa, ga);
+      mom[va] = ga.x; mom[va + 1] = ga.y; mom[va + 2] = ga.z;
+    } else {
+      length[a] = qpos[qa] * gear[0];
+      mom[va] = gear[0];
+    }
+  }
+  __syncwarp();
+}
+
+// ------------------------------------------------------------------------------------------
+// smooth.py:539-606 — cvel, cdof_dot
+__device__ void com_vel(const MjbModel& m, const MjbData& d, int w, int lane) {
+  const int nb = m.nbody, nv = m.nv;
+  float* cvel = d.cvel + W(w, 6 * nb);
+  float* cdd = d.cdof_dot + W(w, 6 * nv);
+  const float* cdof = d.cdof + W(w, 6 * nv);
+  const float* qvel = d.qvel + W(w, nv);
+  if (lane < 6) cvel[lane] = 0.f;
+  __syncwarp();
+  for (int lvl = 1; lvl < m.nlevel; lvl++) {
+    const int beg = m.body_treeadr[lvl], end = m.body_treeadr[lvl + 1];
+    for (int n = beg + lane; n < end; n += 32) {
+      const int b = m.body_tree[n];
+      s6 v = ld6(cvel + 6 * m.body_parentid[b]);
+      int dof = m.body_dofadr[b];
+      for (int j = m.body_jntadr[b]; j < m.body_jntadr[b] + m.body_jntnum[b]; j++) {
+        const int t = m.jnt_type[j];
+        const int nd = t == JNT_FREE ? 6 : (t == JNT_BALL ? 3 : 1);
+        if (t == JNT_FREE) {
+          for (int i = 0; i < 3; i++) {
+            const s6 c = ld6(cdof + 6 * (dof + i));
+            for (int k = 0; k < 6; k++) v.v[k] += c.v[k] * qvel[dof + i];
+            st6(cdd + 6 * (dof + i), s6{{0, 0, 0, 0, 0, 0}});
+          }
+          for (int i = 3; i < 6; i++) st6(cdd + 6 * (dof + i), motion_cross(v, ld6(cdof + 6 * (dof + i))));
+          for (int i = 3; i < 6; i++) {
+            const s6 c = ld6(cdof + 6 * (dof + i));
+            for (int k = 0; k < 6; k++) v.v[k] += c.v[k] * qvel[dof + i];
+          }
+        } else {
+          for (int i = 0; i < nd; i++) st6(cdd + 6 * (dof + i), motion_cross(v, ld6(cdof + 6 * (dof + i))));
+          for (int i = 0; i < nd; i++) {
+            const s6 c = ld6(cdof + 6 * (dof + i));
+            for (int k = 0; k < 6; k++) v.v[k] += c.v[k] * qvel[dof + i];
+          }
+        }
+        dof += nd;
+      }
+      st6(cvel + 6 * b, v);
+    }
+    __syncwarp();
+  }
+}
+
+// passive.py:27-108
+__device__ void passive(const MjbModel& m, const MjbData& d, int w, int lane) {
+  const int nv = m.nv;
+  float* qfrc_passive = d.qfrc_passive + W(w, nv);
+  if (m.disableflags & DSBL_PASSIVE) {
+    for (int i = lane; i < nv; i += 32) qfrc_passive[i] = 0.f;
+    __syncwarp();
+    return;
+  }
+  const float* qpos = d.qpos + W(w, m.nq);
+  const float* qvel = d.qvel + W(w, nv);
+  float* spring = d.qfrc_spring + W(w, nv);
+  float* damper = d.qfrc_damper + W(w, nv);
+  for (int i = lane; i < nv; i += 32) spring[i] = 0.f;
+  __syncwarp();
+  for (int j = lane; j < m.njnt; j += 32) {
+    const float k = m.jnt_stiffness[j];
+    if (k == 0.f) continue;
+    const int dof = m.jnt_dofadr[j], t = m.jnt_type[j], a = m.jnt_qposadr[j];
+    if (t == JNT_FREE) {
+      for (int i = 0; i < 3; i++) spring[dof + i] = -k * (qpos[a + i] - m.qpos_spring[a + i]);
+      const f3 dif = quat_sub(ld4(qpos + a + 3), ld4(m.qpos_spring + a + 3));
+      spring[dof + 3] = -k * dif.x; spring[dof + 4] = -k * dif.y; spring[dof + 5] = -k * dif.z;
+    } else if (t == JNT_BALL) {
+      const f3 dif = quat_sub(ld4(qpos + a), ld4(m.qpos_spring + a));
+      spring[dof] = -k * dif.x; spring[dof + 1] = -k * dif.y; spring[dof + 2] = -k * dif.z;
+    } else {
+      spring[dof] = -k * (qpos[a] - m.qpos_spring[a]);
+    }
+  }
+  __syncwarp();
+  for (int i = lane; i < nv; i += 32) {
+    const float dm = -m.dof_damping[i] * qvel[i];
+    damper[i] = dm;
+    qfrc_passive[i] = dm + spring[i];
+  }
+  __syncwarp();
+}
+
+// smooth.py:398-466 — recursive Newton-Euler bias forces
+__device__ void rne(const MjbModel& m, const MjbData& d, int w, int lane) {
+  const int nb = m.nbody, nv = m.nv;
+  float* cacc = d.rne_cacc + W(w, 6 * nb);
+  float* cfrc = d.rne_cfrc + W(w, 6 * nb);
+  const float* cdd = d.cdof_dot + W(w, 6 * nv);
+  const float* qvel = d.qvel + W(w, nv);
+  const float* cinert = d.cinert + W(w, 10 * nb);
+  const float* cvel = d.cvel + W(w, 6 * nb);
+  if (lane < 6) {
+    const bool grav = !(m.disableflags & DSBL_GRAVITY);
+    cacc[lane] = (lane >= 3 && grav) ? -m.gravity[lane - 3] : 0.f;
+  }
+  __syncwarp();
+  for (int lvl = 1; lvl < m.nlevel; lvl++) {
+    const int beg = m.body_treeadr[lvl], end = m.body_treeadr[lvl + 1];
+    for (int n = beg + lane; n < end; n += 32) {
+      const int b = m.body_tree[n];
+      s6 a = ld6(cacc + 6 * m.body_parentid[b]);
+      const int da = m.body_dofadr[b];
+      for (int i = 0; i < m.body_dofnum[b]; i++) {
+        const s6 c = ld6(cdd + 6 * (da + i));
+        for (int k = 0; k < 6; k++) a.v[k] += c.v[k] * qvel[da + i];
+      }
+      st6(cacc + 6 * b, a);
+    }
+    __syncwarp();
+  }
+  for (int b = lane; b < nb; b += 32) {
+    const s6 v = ld6(cvel + 6 * b);
+    const s6 f = inert_vec(cinert + 10 * b, ld6(cacc + 6 * b));
+    const s6 g = motion_cross_force(v, inert_vec(cinert + 10 * b, v));
+    s6 r;
+    for (int k = 0; k < 6; k++) r.v[k] = f.v[k] + g.v[k];
+    st6(cfrc + 6 * b, r);
+  }
+  __syncwarp();
+  // bottom-up gather; level 0 adds the world into itself as smooth.py:461-464 does
+  for (int lvl = m.nlevel - 1; lvl >= 0; lvl--) {
+    const int beg = m.body_treeadr[lvl], end = m.body_treeadr[lvl + 1];
+    for (int n = beg + lane; n < end; n += 32) {
+      const int b = m.body_tree[n];
+      s6 acc = ld6(cfrc + 6 * b);
+      const int ca = m.body_childadr[b], cn = m.body_childnum[b];
+      for (int c = 0; c < cn; c++) {
+        const s6 x = ld6(cfrc + 6 * m.body_child[ca + c]);
+        for (int k = 0; k < 6; k++) acc.v[k] += x.v[k];
+      }
+      if (b == 0)
+        for (int k = 0; k < 6; k++) acc.v[k] += acc.v[k];
+      st6(cfrc + 6 * b, acc);
+    }
+    __syncwarp();
+  }
+  const float* cdof = d.cdof + W(w, 6 * nv);
+  float* bias = d.qfrc_bias + W(w, nv);
+  for (int i = lane; i < nv; i += 32) bias[i] = dot6(ld6(cdof + 6 * i), ld6(cfrc + 6 * m.dof_bodyid[i]));
+  __syncwarp();
+}
+
+// forward.py:423-500 (dense path)
+__device__ void fwd_velocity(const MjbModel& m, const MjbData& d, int w, int lane) {
+  const int nv = m.nv;
+  const float* moment = d.actuator_moment + W(w, m.nu * nv);
+  const float* qvel = d.qvel + W(w, nv);
+  float* vel = d.actuator_velocity + W(w, m.nu);
+  for (int a = lane; a < m.nu; a += 32) {
+    float s = 0.f;
+    for (int i = 0; i < nv; i++) s += moment[a * nv + i] * qvel[i];
+    vel[a] = s;
+  }
+  __syncwarp();
+  com_vel(m, d, w, lane);
+  passive(m, d, w, lane);
+  rne(m, d, w, lane);
+}
+
+// forward.py:503-641
+__device__ void fwd_actuation(const MjbModel& m, const MjbData& d, int w, int lane) {
+  const int nv = m.nv, nu = m.nu;
+  float* qfrc = d.qfrc_actuator + W(w, nv);
+  if (!nu || (m.disableflags & DSBL_ACTUATION)) {
+    if (d.act_dot)
+      for (int i = lane; i < m.na; i += 32) d.act_dot[W(w, m.na) + i] = 0.f;
+    for (int i = lane; i < nv; i += 32) qfrc[i] = 0.f;
+    __syncwarp();
+    return;
+  }
+  const float* len = d.actuator_length + W(w, nu);
+  const float* vel = d.actuator_velocity + W(w, nu);
+  const float* ctrl = d.ctrl + W(w, nu);
+  float* force = d.actuator_force + W(w, nu);
+  for (int a = lane; a < nu; a += 32) {
+    const float* gp = m.actuator_gainprm + 10 * a;
+    const float* bp = m.actuator_biasprm + 10 * a;
+    float gain = gp[0];
+    gain += gp[1] * len[a];
+    gain += gp[2] * vel[a];
+    float bias = bp[0];
+    bias += bp[1] * len[a];
+    bias += bp[2] * vel[a];
+    float c = ctrl[a];
+    if (m.actuator_ctrllimited[a] && !(m.disableflags & DSBL_CLAMPCTRL))
+      c = fminf(fmaxf(c, m.actuator_ctrlrange[2 * a]), m.actuator_ctrlrange[2 * a + 1]);
+    force[a] = gain * c + bias;  // forcerange is not applied (forward.py:539-541)
+  }
+  __syncwarp();
+  const float* moment = d.actuator_moment + W(w, nu * nv);
+  for (int i = lane; i < nv; i += 32) {
+    float s = 0.f;
+    for (int a = 0; a < nu; a++) s += moment[a * nv + i] * force[a];
+    const int j = m.dof_jntid[i];
+    if (m.jnt_actfrclimited[j]) s = fminf(fmaxf(s, m.jnt_actfrcrange[2 * j]), m.jnt_actfrcrange[2 * j + 1]);
+    qfrc[i] = s;
+  }
+  __syncwarp();
+}
+
+// support.py:140-172 — qfrc += J^T xfrc_applied (Jacobian at each body's xipos)
+__device__ void xfrc_accumulate(const MjbModel& m, const MjbData& d, int w, float* qfrc, int lane) {
+  const int nv = m.nv, nb = m.nbody;
+  const float* cdof = d.cdof + W(w, 6 * nv);
+  const float* xipos = d.xipos + W(w, 3 * nb);
+  const float* sc = d.subtree_com + W(w, 3 * nb);
+  const float* xfrc = d.xfrc_applied + W(w, 6 * nb);
+  for (int i = lane; i < nv; i += 32) {
+    const s6 c = ld6(cdof + 6 * i);
+    const f3 rot{c.v[0], c.v[1], c.v[2]}, lin{c.v[3], c.v[4], c.v[5]};
+    const int db = m.dof_bodyid[i];
+    float acc = 0.f;
+    for (int b = db; b < m.body_subtreeend[db]; b++) {  // bodies in the subtree of db
+      const f3 off = ld3(xipos + 3 * b) - ld3(sc + 3 * m.body_rootid[b]);
+      const f3 force = ld3(xfrc + 6 * b), torque = ld3(xfrc + 6 * b + 3);
+      acc += (dot(lin, force) + dot(rot, torque)) + dot(cross(rot, off), force);
+    }
+    qfrc[i] += acc;
+  }
+  __syncwarp();
+}
+
+// forward.py:644-661
+__device__ void fwd_acceleration(const MjbModel& m, const MjbData& d, int w, int lane) {
+  const int nv = m.nv;
+  float* sm = d.qfrc_smooth + W(w, nv);
+  const float* pas = d.qfrc_passive + W(w, nv);
+  const float* bias = d.qfrc_bias + W(w, nv);
+  const float* act = d.qfrc_actuator + W(w, nv);
+  const float* app = d.qfrc_applied + W(w, nv);
+  for (int i = lane; i < nv; i += 32) sm[i] = pas[i] - bias[i] + act[i] + app[i];
+  __syncwarp();
+  xfrc_accumulate(m, d, w, sm, lane);
+  solve_blocks(m, d.qLD + W(w, nv * nv), d.qacc_smooth + W(w, nv), sm, lane);
+}
+
+// ------------------------------------------------------------------------------------------
+// forward.py:43-162 — advance velocities and positions (semi-implicit)
+__device__ void advance(const MjbModel& m, const MjbData& d, int w, const float* qacc, int lane) {
+  const int nv = m.nv;
+  const float dt = m.timestep;
+  float* qvel = d.qvel + W(w, nv);
+  float* qpos = d.qpos + W(w, m.nq);
+  for (int i = lane; i < nv; i += 32) qvel[i] = qvel[i] + qacc[i] * dt;
+  __syncwarp();
+  for (int j = lane; j < m.njnt; j += 32) {
+    const int t = m.jnt_type[j], a = m.jnt_qposadr[j], dof = m.jnt_dofadr[j];
+    if (t == JNT_FREE) {
+      for (int k = 0; k < 3; k++) qpos[a + k] = qpos[a + k] + dt * qvel[dof + k];
+      st4(qpos + a + 3, quat_integrate(ld4(qpos + a + 3), ld3(qvel + dof + 3), dt));
+    } else if (t == JNT_BALL) {
+      st4(qpos + a, quat_integrate(ld4(qpos + a), ld3(qvel + dof), dt));
+    } else {
+      qpos[a] = qpos[a] + dt * qvel[dof];
+    }
+  }
+  __syncwarp();
+}
+
+// forward.py:165-242 — Euler with implicit joint damping unless EULERDAMP is disabled
+__device__ void euler(const MjbModel& m, const MjbData& d, int w, int lane) {
+  const int nv = m.nv;
+  if (m.disableflags & DSBL_EULERDAMP) {
+    advance(m, d, w, d.qacc + W(w, nv), lane);
+    return;
+  }
+  float* L = d.qLD_integration + W(w, nv * nv);
+  float* x = d.qacc_integration + W(w, nv);
+  const float* sm = d.qfrc_smooth + W(w, nv);
+  const float* qc = d.qfrc_constraint + W(w, nv);
+  factor_blocks(m, d.qM + W(w, nv * nv), L, lane, m.dof_damping, m.timestep);
+  for (int i = lane; i < nv; i += 32) x[i] = sm[i] + qc[i];
+  __syncwarp();
+  solve_blocks(m, L, x, x, lane);
+  advance(m, d, w, x, lane);
+}
+
+// forward.py:245-405 — implicitfast (dense): (M - dt qDeriv) qacc = qfrc_smooth + qfrc_constraint
+// with qDeriv = moment^T diag(bias_vel + gain_vel * ctrl) moment - diag(damping)
+__device__ void implicit(const MjbModel& m, const MjbData& d, int w, int lane) {
+  const int nv = m.nv, nu = m.nu;
+  const bool passive_on = !(m.disableflags & DSBL_PASSIVE);
+  const bool act_on = !(m.disableflags & DSBL_ACTUATION) && m.actuator_affine_bias_gain;
+  if (!passive_on && !act_on) {
+    advance(m, d, w, d.qacc + W(w, nv), lane);
+    return;
+  }
+  float* vel = d.act_vel_integration + W(w, nu);
+  const float* moment = d.actuator_moment + W(w, nu * nv);
+  if (act_on) {  // actuator_bias_gain_vel (forward.py:277-299)
+    for (int a = lane; a < nu; a += 32) {
+      const float bv = m.actuator_biastype[a] == 1 ? m.actuator_biasprm[10 * a + 2] : 0.f;
+      const float gv = m.actuator_gaintype[a] == 1 ? m.actuator_gainprm[10 * a + 2] : 0.f;
+      const float c = m.actuator_dyntype[a] != 0 ? d.act[W(w, m.na) + a] : d.ctrl[W(w, nu) + a];
+      vel[a] = bv + gv * c;
+    }
+    __syncwarp();
+  }
+  const float* qM = d.qM + W(w, nv * nv);
+  float* Mi = d.qM_integration + W(w, nv * nv);
+  for (int blk = 0; blk < m.nblock; blk++) {  // qderiv_actuator_fused_kernel, per tree tile
+    const int a0 = m.block_adr[blk], n = m.block_size[blk];
+    for (int e = lane; e < n * n; e += 32) {
+      const int i = a0 + e / n, j = a0 + e % n;
+      float qd = 0.f;
+      if (act_on)
+        for (int a = 0; a < nu; a++) qd += moment[a * nv + i] * vel[a] * moment[a * nv + j];
+      if (passive_on && i == j) qd -= m.dof_damping[i];
+      Mi[i * nv + j] = qM[i * nv + j] - qd * m.timestep;
+    }
+  }
+  float* f = d.qfrc_integration + W(w, nv);
+  const float* sm = d.qfrc_smooth + W(w, nv);
+  const float* qc = d.qfrc_constraint + W(w, nv);
+  for (int i = lane; i < nv; i += 32) f[i] = sm[i] + qc[i];
+  __syncwarp();
+  float* L = d.qLD_integration + W(w, nv * nv);
+  float* x = d.qacc_integration + W(w, nv);
+  factor_blocks(m, Mi, L, lane);
+  solve_blocks(m, L, x, f, lane);
+  advance(m, d, w, x, lane);
+}
+
+}  // namespace mjb

@@ -1,0 +1,183 @@
+"""Integrators and whole steps on the GPU (forward_test.py), determinism, graphs, status bits."""
+
+import numpy as np
+import pytest
+import torch
+
+import mjx_warp_b200 as mjw
+from helpers import (assert_close, dev, device_data, generic_state, humanoid, humanoid_state, load,
+                     oracle, rel_err)
+from mjx_warp_b200 import mjcf
+
+pytestmark = pytest.mark.gpu
+
+
+def test_euler_eulerdamp():
+  """forward_test.py:95-128: Euler with implicit damping on the pendula."""
+  mjm = load("pendula.xml")
+  qpos, _, ctrl = generic_state(mjm, 4, 1)
+  qvel = np.ones((4, mjm.nv))
+  m = mjw.put_model(mjm)
+  d = device_data(mjm, qpos, qvel, ctrl)
+  mjw.forward(m, d)
+  mjw.euler(m, d)
+  o = oracle(mjm, qpos, qvel, ctrl, 64)
+  o.run("forward")
+  o.run("euler")
+  torch.cuda.synchronize()
+  assert_close(dev(d.qpos), o.get("qpos"), "qpos")
+  assert_close(dev(d.qvel), o.get("qvel"), "qvel")
+
+
+def test_disable_eulerdamp():
+  """forward_test.py:130-145: qvel = 1 + dt exactly when eulerdamp is disabled and qacc = 1."""
+  mjm = load("pendula.xml")
+  mjm.opt.disableflags |= int(mjw.DisableBit.EULERDAMP)
+  m = mjw.put_model(mjm)
+  d = mjw.make_data(mjm, nworld=1)
+  d.qvel.fill_(1.0)
+  d.qacc.fill_(1.0)
+  mjw.euler(m, d)
+  np.testing.assert_allclose(d.qvel.numpy()[0], 1 + mjm.opt.timestep, rtol=1e-6)
+
+
+@pytest.mark.parametrize("flags", [0, int(mjw.DisableBit.PASSIVE), int(mjw.DisableBit.ACTUATION),
+                                   int(mjw.DisableBit.PASSIVE | mjw.DisableBit.ACTUATION)])
+def test_implicit(flags):
+  """forward_test.py:148-196: implicitfast with affine actuators under disable flags."""
+  rng = np.random.default_rng(0)
+  mjm = load("pendula.xml", integrator=3)
+  mjm.opt.disableflags |= flags
+  mjm.actuator_gainprm[:, 2] = rng.normal(scale=10, size=mjm.nu)
+  mjm.actuator_gaintype[3] = 1
+  mjm.actuator_gaintype[6] = 1
+  mjm.actuator_biastype[0:3] = 1
+  mjm.actuator_biastype[4:6] = 1
+  mjm.actuator_biasprm[0:3, 2] = -1
+  mjm.actuator_biasprm[4:6, 2] = -1
+  mjm.actuator_ctrlrange[3:7] = 10.0
+  mjm.actuator_gear[:] = 1.0
+  qpos, _, _ = generic_state(mjm, 4, 2)
+  qvel = rng.uniform(-0.01, 0.01, (4, mjm.nv))
+  ctrl = rng.normal(scale=10, size=(4, mjm.nu))
+  m = mjw.put_model(mjm)
+  d = device_data(mjm, qpos, qvel, ctrl)
+  mjw.forward(m, d)
+  mjw.implicit(m, d)
+  o = oracle(mjm, qpos, qvel, ctrl, 64)
+  o.run("forward")
+  o.run("implicit")
+  torch.cuda.synchronize()
+  assert_close(dev(d.qpos), o.get("qpos"), "qpos")
+  assert_close(dev(d.qvel), o.get("qvel"), "qvel", rtol=2e-3, atol=2e-3)
+
+
+def test_humanoid_steps_converged_vs_fp64():
+  """Ten implicitfast steps with a converged solver track the FP64 oracle step by step."""
+  mjm = humanoid(iterations=10, ls_iterations=20)
+  qpos, qvel, ctrl = humanoid_state(mjm, 64, seed=8)
+  m = mjw.put_model(mjm)
+  d = device_data(mjm, qpos, qvel, ctrl)
+  o = oracle(mjm, qpos, qvel, ctrl, 64)
+  for _ in range(10):
+    mjw.step(m, d)
+    o.run("step")
+  torch.cuda.synchronize()
+  assert np.median(rel_err(dev(d.qvel), o.get("qvel"))) < 1e-4
+  assert np.quantile(rel_err(dev(d.qpos), o.get("qpos")), 0.9) < 1e-4
+  assert d.time == pytest.approx(10 * mjm.opt.timestep)
+
+
+def test_sphere_chain_long_rollout():
+  """Config 1 (sphere + 5-link chain, Euler with eulerdamp): 1000 steps stay finite and track
+  the FP64 oracle closely for the first 50 steps."""
+  mjm = load("sphere_chain.xml")
+  rng = np.random.default_rng(0)
+  nworld = 32
+  qpos = np.tile(mjm.qpos0, (nworld, 1))
+  qpos[:, 7:] = rng.uniform(-0.1, 0.1, (nworld, 5))
+  qvel = rng.normal(0, 0.1, (nworld, mjm.nv))
+  ctrl = rng.uniform(-1, 1, (nworld, mjm.nu))
+  m = mjw.put_model(mjm)
+  d = device_data(mjm, qpos, qvel, ctrl)
+  o = oracle(mjm, qpos, qvel, ctrl, 64)
+  for _ in range(50):
+    mjw.step(m, d)
+  o.run("step", nstep=50)
+  torch.cuda.synchronize()
+  assert rel_err(dev(d.qpos), o.get("qpos")).max() < 1e-4
+  for _ in range(950):
+    mjw.step(m, d)
+  assert np.all(np.isfinite(d.qpos.cpu().numpy()))
+  assert np.all(mjw.world_status(d) == 0)
+  assert float(d.qpos[:, 2].min()) > 0.05  # the ball rests on the floor
+
+
+def test_fused_plain_agree_and_deterministic():
+  mjm = humanoid()
+  qpos, qvel, ctrl = humanoid_state(mjm, 64, seed=9)
+  m = mjw.put_model(mjm)
+  outs = []
+  for fused in (True, True, False, False):
+    d = device_data(mjm, qpos, qvel, ctrl)
+    mjw.step(m, d, fused=fused)
+    outs.append((d.qpos.clone(), d.qvel.clone(), d.qacc_smooth.clone()))
+  for a, b in zip(outs[0], outs[1]):
+    assert torch.equal(a, b)
+  for a, b in zip(outs[2], outs[3]):
+    assert torch.equal(a, b)
+  assert_close(dev(outs[0][2]), dev(outs[2][2]), "qacc_smooth fused vs plain", rtol=1e-4, atol=1e-4)
+
+
+def test_cuda_graph_replay_matches_eager():
+  mjm = humanoid()
+  qpos, qvel, ctrl = humanoid_state(mjm, 64, seed=10)
+  m = mjw.put_model(mjm)
+  de = device_data(mjm, qpos, qvel, ctrl)
+  dg = device_data(mjm, qpos, qvel, ctrl)
+  mjw.step(m, de)
+  mjw.step(m, dg)  # warm-up outside capture
+  g = torch.cuda.CUDAGraph()
+  s = torch.cuda.Stream()
+  s.wait_stream(torch.cuda.current_stream())
+  with torch.cuda.stream(s):
+    with torch.cuda.graph(g, stream=s):
+      mjw.step(m, dg)
+  torch.cuda.current_stream().wait_stream(s)
+  for _ in range(3):
+    g.replay()
+    mjw.step(m, de)
+  torch.cuda.synchronize()
+  assert torch.equal(de.qpos, dg.qpos) and torch.equal(de.qvel, dg.qvel)
+
+
+def test_nonfinite_world_is_flagged_and_isolated():
+  """Fault injection on the host: a NaN in one world's qpos flags only that world."""
+  mjm = humanoid()
+  qpos, qvel, ctrl = humanoid_state(mjm, 8, seed=12)
+  qpos[3, 10] = np.nan
+  m = mjw.put_model(mjm)
+  d = device_data(mjm, qpos, qvel, ctrl)
+  mjw.step(m, d)
+  st = mjw.world_status(d)
+  assert st[3] & 0x8
+  assert np.all(st[np.arange(8) != 3] == 0)
+  q = d.qpos.cpu().numpy()
+  assert np.all(np.isfinite(np.delete(q, 3, axis=0)))
+
+
+def test_get_data_into_roundtrip():
+  """io.py:728-831: one world read back into a host MjData."""
+  mjm = load("sphere_chain.xml")
+  mjd = mjcf.MjData(mjm)
+  mjd.qpos[2] = 0.09
+  m = mjw.put_model(mjm)
+  d = mjw.put_data(mjm, mjd)
+  mjw.forward(m, d)
+  out = mjcf.MjData(mjm)
+  mjw.get_data_into(out, mjm, d)
+  np.testing.assert_allclose(out.xpos, d.xpos.numpy()[0], rtol=1e-6)
+  assert out.ncon == int(d.ncon.numpy()[0]) and out.ncon > 0
+  assert out.efc_J.shape == (out.nefc, mjm.nv)
+  d2 = mjw.put_data(mjm, out)
+  np.testing.assert_allclose(d2.qacc.numpy(), d.qacc.numpy(), rtol=1e-6)
