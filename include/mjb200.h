@@ -22,6 +22,7 @@
 #ifndef MJB200_H_
 #define MJB200_H_
 
+#include <stddef.h>
 #include <stdint.h>
 
 #ifdef __cplusplus
@@ -182,6 +183,22 @@ int mjb_xfrc_accumulate(const MjbModel* m, const MjbData* d, float* qfrc, mjbStr
 
 /* Copies world_status (nworld words) to host memory; synchronises the stream. */
 int mjb_world_status(const MjbData* d, uint32_t* host_out, mjbStream stream);
+
+/* Allocation-free variant of mjb_implicit, with no counterpart in the reference.  For callers
+ * that may not allocate device memory when they step (a plugin that receives only its operand
+ * buffers, a control loop that cannot afford cudaMalloc's synchronisation): the integrator's
+ * three per-world work arrays (qM_integration, qLD_integration, qfrc_integration) come from a
+ * 64 MiB array compiled into the library instead of from MjbData, so those three fields may be
+ * null.  Inputs and outputs are as for mjb_implicit: qM, qfrc_smooth, qfrc_constraint,
+ * actuator_moment, ctrl / act are read; qpos, qvel are advanced; qacc_integration is written.
+ * Limit: nworld * (2 * nv * nv + nv) * 4 bytes <= mjb_implicit_noalloc_max_bytes() (64 MiB,
+ * e.g. 11298 humanoid worlds at nv = 27); larger requests return MJB_ERR_SCRATCH.  The first call
+ * on each device resolves the array's device address (cudaGetSymbolAddress), so make one call per
+ * device before capturing a CUDA graph.  All calls share the one array: calls that overlap on the
+ * GPU (different streams, or graphs replayed concurrently) race on it.  Nothing in it needs to
+ * start at zero: every call writes each element before reading it. */
+int mjb_implicit_noalloc(const MjbModel* m, const MjbData* d, mjbStream stream);
+size_t mjb_implicit_noalloc_max_bytes(void);
 
 #ifdef __cplusplus
 }

@@ -421,3 +421,56 @@ int mjb_world_status(const MjbData* d, uint32_t* host_out, mjbStream stream) {
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------------------------------------------
+// Allocation-free implicitfast integration.
+//
+// Some callers cannot allocate device memory at the point where they step the simulation: a
+// host framework that hands a plugin nothing but its operand buffers (an XLA / JAX custom call
+// without a workspace, for instance), or a real-time control loop that must never pay for
+// cudaMalloc's implicit device synchronisation after start-up.  mjb_implicit needs three
+// per-world work arrays (the damped mass matrix, its Cholesky factor and the right-hand side);
+// this variant takes them from a fixed array that lives in the library itself, so the caller only
+// provides the inputs and outputs it already has: qM, qfrc_smooth, qfrc_constraint, the actuator
+// moments and controls (read), qpos and qvel (advanced in place) and qacc_integration (written).
+namespace {
+
+constexpr size_t kNoallocScratchBytes = size_t(64) << 20;  // 64 MiB, held by every GPU that loads
+                                                             // the library until the process exits
+__device__ __align__(256) float g_noalloc_scratch[kNoallocScratchBytes / sizeof(float)];
+
+constexpr int kMaxDevices = 64;
+float* g_noalloc_ptr[kMaxDevices] = {};
+
+// Device address of the scratch array on the current device, resolved once per device (the name
+// g_noalloc_scratch in host code is only a host-side stand-in and must never be passed to a kernel).
+int noalloc_scratch(float** out) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return MJB_ERR_LAUNCH;
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return MJB_ERR_LAUNCH;
+    g_noalloc_ptr[dev] = static_cast<float*>(p);
+  }
+  *out = g_noalloc_ptr[dev];
+  return MJB_OK;
+}
+
+}  // namespace
+
+extern "C" size_t mjb_implicit_noalloc_max_bytes(void) { return kNoallocScratchBytes; }
+
+extern "C" int mjb_implicit_noalloc(const MjbModel* m, const MjbData* d, mjbStream stream) {
+  int rc = check(m, d);
+  if (rc || d->nworld == 0) return rc;
+  const size_t nv = size_t(m->nv);
+  const size_t need = size_t(d->nworld) * (2 * nv * nv + nv) * sizeof(float);
+  if (need > kNoallocScratchBytes) return MJB_ERR_SCRATCH;
+  float* scratch = nullptr;
+  if ((rc = noalloc_scratch(&scratch))) return rc;
+  MjbData dd = *d;  // same inputs and outputs, work arrays redirected into the static scratch
+  dd.qM_integration = scratch;
+  dd.qLD_integration = scratch + size_t(d->nworld) * nv * nv;
+  dd.qfrc_integration = scratch + 2 * size_t(d->nworld) * nv * nv;
+  return launch_stage<S_IMPLICIT>(m, &dd, (cudaStream_t)stream);
+}
