@@ -14,7 +14,8 @@ from typing import Optional
 import torch
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libmjb200.so")
+# MJX_WARP_B200_LIB selects another build of the library (e.g. one compiled with other options)
+LIB_PATH = os.environ.get("MJX_WARP_B200_LIB") or os.path.join(_HERE, "libmjb200.so")
 
 MODEL_INTS = ("nq", "nv", "na", "nu", "nbody", "njnt", "ngeom", "nsite", "nmocap", "nM", "nlimit",
               "nlevel", "nblock", "npair_cand", "nlsp", "integrator", "cone", "solver",

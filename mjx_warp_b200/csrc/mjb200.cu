@@ -14,6 +14,11 @@
 
 #include "mjb_solver.cuh"
 
+// minimum resident CTAs per SM requested from the compiler (caps registers per thread)
+#ifndef MJB_MINB
+#define MJB_MINB 4
+#endif
+
 namespace mjb {
 
 enum Stage {
@@ -41,7 +46,7 @@ __device__ __forceinline__ void copy_qacc_smooth(const MjbModel& m, const MjbDat
 }
 
 template <int STAGE>
-__global__ void __launch_bounds__(128, 4) k_stage(const MjbModel m, const MjbData d, int smem_per_warp) {
+__global__ void __launch_bounds__(128, MJB_MINB) k_stage(const MjbModel m, const MjbData d, int smem_per_warp) {
   extern __shared__ float smem[];
   const int lane = threadIdx.x & 31;
   const int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
@@ -74,7 +79,7 @@ __global__ void __launch_bounds__(128, 4) k_stage(const MjbModel m, const MjbDat
 
 // whole forward (+ integration) of one world per warp; dynamic shared memory holds one nv x nv
 // Hessian / factor tile per warp
-__global__ void __launch_bounds__(128, 4) k_step_fused(const MjbModel m, const MjbData d, int integrate,
+__global__ void __launch_bounds__(128, MJB_MINB) k_step_fused(const MjbModel m, const MjbData d, int integrate,
                                                     int smem_per_warp) {
   extern __shared__ float smem[];
   const int lane = threadIdx.x & 31;

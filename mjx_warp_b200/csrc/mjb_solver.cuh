@@ -382,12 +382,20 @@ __device__ void solve_generic(const MjbModel& m, const MjbData& d, int w, int la
 // most kSolverRows rows) and the Hessian factor live in the warp's shared-memory slice; per-row
 // scalars stay in the flat efc arrays, each touched only by the lane that owns the row.
 
-constexpr int kSolverRows = 64;
+#ifndef MJB_JROWS
+#define MJB_JROWS 32
+#endif
+constexpr int kSolverRows = MJB_JROWS;
+constexpr int kJld = 36;  // staged Jacobian rows: 32 columns (zero padded) + 4, float4-aligned
 
 __host__ __device__ __forceinline__ int solver_ld(int nv) { return nv | 1; }
+__host__ __device__ __forceinline__ int round4(int x) { return (x + 3) & ~3; }
+// per-warp layout: Ms (nv x ld) | Ls (nv x 33) | vs (32) | F (kSolverRows) | Js (kSolverRows x kJld)
+__host__ __device__ __forceinline__ int solver_js_offset(int nv) {
+  return round4(nv * solver_ld(nv) + nv * 33 + 32 + kSolverRows);
+}
 __host__ __device__ __forceinline__ size_t solver_smem_floats(int nv) {
-  const int ldm = solver_ld(nv);
-  return size_t(nv) * ldm + size_t(nv) * 33 + 32 + kSolverRows + size_t(kSolverRows) * ldm;
+  return size_t(solver_js_offset(nv)) + size_t(kSolverRows) * kJld;
 }
 
 struct Small {
@@ -395,6 +403,8 @@ struct Small {
   const MjbData& d;
   int w, lane, nv, ldm, adr, n, ldj;
   bool own;
+  bool factored = false;        // Ls holds the factor of H for the active set factored_mask
+  unsigned factored_mask = 0u;
   float *Ms, *Ls, *vs, *F;
   const float* J;
   // per-dof registers
@@ -426,33 +436,52 @@ struct Small {
   }
 };
 
-// Newton step direction H^-1 grad for nv <= 32 (solver.py:234-290): lane i assembles row i of
-// H = tril(qM) + sum_k c_k J_k^T J_k in registers (c_k = D_k for active rows, 0 otherwise), stores
-// it to Ls (leading dimension 33), factors it in place and solves; returns element `lane`.
+// Newton step direction H^-1 grad for nv <= 32 (solver.py:234-290).  When `refactor` is set,
+// lane i assembles row i of H = tril(qM) + sum_k c_k J_k^T J_k in registers (c_k = D_k for active
+// rows, 0 otherwise; inactive rows are skipped), stores it to Ls (leading dimension 33) and factors
+// it in place; otherwise Ls already holds the factor of the same H.  The coefficients come from C
+// (staged rows) or, when C is null, from the rows' active flags and D.  Returns element `lane` of the
+// solution.  Staged Jacobian rows (ldj == kJld) are read as float4 broadcasts.
 __device__ __noinline__ float newton_direction(const float* Ms, int ldm, const float* J, int ldj,
-                                               const float* C, int n, float* Ls, int nv, float grad,
-                                               int lane) {
+                                               const float* C, const int* act, const float* D,
+                                               int n, float* Ls, int nv, float grad, int lane,
+                                               bool refactor) {
   const bool own = lane < nv;
-  float h[32];
+  if (refactor) {
+    float h[32];
 #pragma unroll
-  for (int j = 0; j < 32; j++) h[j] = (own && j <= lane && j < nv) ? Ms[lane * ldm + j] : 0.f;
-  for (int k = 0; k < n; k++) {
-    const float c = C[k];
-    if (c == 0.f) continue;
-    const float* Jr = J + size_t(k) * ldj;
-    const float a = own ? c * Jr[lane] : 0.f;
+    for (int j = 0; j < 32; j++) h[j] = (own && j <= lane && j < nv) ? Ms[lane * ldm + j] : 0.f;
+    for (int k = 0; k < n; k++) {
+      const float c = C ? C[k] : (act[k] ? D[k] : 0.f);
+      if (c == 0.f) continue;
+      const float* Jr = J + size_t(k) * ldj;
+      const float a = own ? c * Jr[lane] : 0.f;
+      if (ldj == kJld) {  // zero-padded to 32 columns, 16-byte aligned rows
+        const float4* J4 = reinterpret_cast<const float4*>(Jr);
 #pragma unroll
-    for (int j = 0; j < 32; j++)
-      if (j < nv && j <= lane) h[j] += a * Jr[j];
+        for (int q = 0; q < 8; q++) {
+          const float4 v = J4[q];
+          h[4 * q] += a * v.x;
+          h[4 * q + 1] += a * v.y;
+          h[4 * q + 2] += a * v.z;
+          h[4 * q + 3] += a * v.w;
+        }
+      } else {
+#pragma unroll
+        for (int j = 0; j < 32; j++)
+          if (j < nv) h[j] += a * Jr[j];
+      }
+    }
+    if (own) {
+#pragma unroll
+      for (int j = 0; j < 32; j++)
+        if (j <= lane) Ls[lane * 33 + j] = h[j];
+    }
+    __syncwarp();
+    chol_lower(Ls, 33, nv, lane);
   }
-  if (own) {
-#pragma unroll
-    for (int j = 0; j < 32; j++)
-      if (j <= lane && j < nv) Ls[lane * 33 + j] = h[j];
-  }
-  __syncwarp();
-  chol_lower(Ls, 33, nv, lane);
-  const float x = cho_solve_reg32(Ls, 33, nv, grad, lane);
+  const float invd = own ? __frcp_rn(Ls[lane * 33 + lane]) : 0.f;
+  const float x = cho_solve32(Ls, 33, nv, invd, grad, lane);
   return own ? x : 0.f;
 }
 
@@ -501,13 +530,23 @@ __device__ void small_update_gradient(Small& s) {
     __syncwarp();
     return;
   }
-  // coefficient of each row in J^T D J: D when active, else 0
-  for (int k = lane; k < s.n; k += 32) {
-    const int r = s.adr + k;
-    s.F[k] = d.efc_active[r] ? d.efc_D[r] : 0.f;
+  // H depends on the solve's inputs only through the active set, so the factor of the previous
+  // call is reused (bit-identical) while the set of active rows is unchanged; rows past the
+  // first 32 are not tracked, so such worlds refactor every time
+  const unsigned mask = __ballot_sync(WARP_FULL, lane < s.n && d.efc_active[s.adr + lane]);
+  const bool refactor = !s.factored || s.n > 32 || mask != s.factored_mask;
+  const bool staged = s.ldj == kJld;  // unstaged rows keep F in efc_force, which must survive
+  if (refactor && staged) {  // coefficient of each row in J^T D J: D when active, else 0
+    for (int k = lane; k < s.n; k += 32) {
+      const int r = s.adr + k;
+      s.F[k] = d.efc_active[r] ? d.efc_D[r] : 0.f;
+    }
+    __syncwarp();
   }
-  __syncwarp();
-  s.Mgrad = newton_direction(s.Ms, s.ldm, s.J, s.ldj, s.F, s.n, s.Ls, nv, s.grad, lane);
+  s.Mgrad = newton_direction(s.Ms, s.ldm, s.J, s.ldj, staged ? s.F : nullptr, d.efc_active + s.adr,
+                             d.efc_D + s.adr, s.n, s.Ls, nv, s.grad, lane, refactor);
+  s.factored = true;
+  s.factored_mask = mask;
 }
 
 // solver.py:737-869
@@ -663,25 +702,23 @@ __device__ void solve_small(const MjbModel& m, const MjbData& d, int w, int lane
   s.Ls = s.Ms + nv * ldm;
   s.vs = s.Ls + nv * 33;
   s.F = s.vs + 32;
-  float* Js = s.F + kSolverRows;
+  float* Js = sm + solver_js_offset(nv);
   const float* Jg = d.efc_J + size_t(adr) * nv;
   if (n <= kSolverRows) {
-    for (int e = lane; e < n * nv; e += 32) {
-      const int r = e / nv;
-      Js[r * ldm + (e - r * nv)] = Jg[e];
+    for (int r = 0; r < n; r++) {  // rows padded with zeros to 32 columns for float4 reads
+      const float v = lane < nv ? Jg[size_t(r) * nv + lane] : 0.f;
+      Js[r * kJld + lane] = v;
     }
     s.J = Js;
-    s.ldj = ldm;
+    s.ldj = kJld;
   } else {
     s.J = Jg;
     s.ldj = nv;
     s.F = d.efc_force + adr;  // rows beyond the staged capacity broadcast through global memory
   }
   const float* qMg = d.qM + W(w, nv * nv);
-  for (int e = lane; e < nv * nv; e += 32) {
-    const int i = e / nv;
-    s.Ms[i * ldm + (e - i * nv)] = qMg[e];
-  }
+  if (lane < nv)
+    for (int i = 0; i < nv; i++) s.Ms[i * ldm + lane] = qMg[i * nv + lane];
   s.qacc = s.own ? d.qacc_warmstart[W(w, nv) + lane] : 0.f;
   s.qfs = s.own ? d.qfrc_smooth[W(w, nv) + lane] : 0.f;
   s.qas = s.own ? d.qacc_smooth[W(w, nv) + lane] : 0.f;

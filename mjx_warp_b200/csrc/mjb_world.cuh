@@ -13,6 +13,11 @@
 #include "../../include/mjb200.h"
 #include "mjb_math.cuh"
 
+// Cholesky for n <= 32 blocks: 0 = memory rows (chol_lower, the faster one measured), 1 = register rows (chol32)
+#ifndef MJB_CHOL
+#define MJB_CHOL 0
+#endif
+
 namespace mjb {
 
 #define WARP_FULL 0xffffffffu
@@ -240,53 +245,132 @@ __device__ void crb(const MjbModel& m, const MjbData& d, int w, int lane) {
 
 // In-place Cholesky A = L L^T (left-looking, column by column) of the n x n SPD matrix at A with
 // leading dimension ld (shared or global memory); only the lower triangle is read and written.
-// Column k: the diagonal's dot product is split over lanes and reduced, then each lane finishes
-// the rows i = k+1+lane, k+33+lane, ... with one dot product against row k (a broadcast read).
+// Column k: lane j takes row k + j (+ 32 t) and forms the dot product of that row with row k over
+// the finished columns (four independent partial sums); lane 0's row is row k itself, so its
+// result is the pivot, which is broadcast by shuffle before every lane scales its entry.
 // Compiled once (no inlining) so every caller shares one copy of the code.
+// correctly rounded reciprocal (the value of 1 / x)
+__device__ __forceinline__ float rcp_rn(float x) { return __frcp_rn(x); }
+__device__ __forceinline__ double rcp_rn(double x) { return __drcp_rn(x); }
+
+template <typename T>
+__device__ __forceinline__ T chol_dot(const T* a, const T* b, int k) {
+  T s0 = T(0), s1 = T(0), s2 = T(0), s3 = T(0);
+  int m = 0;
+  for (; m + 3 < k; m += 4) {
+    s0 += a[m] * b[m];
+    s1 += a[m + 1] * b[m + 1];
+    s2 += a[m + 2] * b[m + 2];
+    s3 += a[m + 3] * b[m + 3];
+  }
+  for (; m < k; m++) s0 += a[m] * b[m];
+  return (s0 + s1) + (s2 + s3);
+}
+
 template <typename T>
 __device__ __noinline__ void chol_lower(T* A, int ld, int n, int lane) {
   for (int k = 0; k < n; k++) {
     const T* Ak = A + k * ld;
-    T part = T(0);
-    for (int m = lane; m < k; m += 32) part += Ak[m] * Ak[m];
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
-    const T lkk = sqrt(Ak[k * 0 + k] - part);
-    const T inv = T(1) / lkk;
-    for (int i = k + 1 + lane; i < n; i += 32) {
-      T* Ai = A + i * ld;
-      T s0 = Ai[k], s1 = T(0);
-      int m = 0;
-      for (; m + 1 < k; m += 2) {
-        s0 -= Ai[m] * Ak[m];
-        s1 -= Ai[m + 1] * Ak[m + 1];
+    if (n - k <= 32) {  // one row per lane: the pivot and the column in a single pass
+      const int i = k + lane;
+      T s = T(0);
+      if (i < n) s = A[i * ld + k] - chol_dot(A + i * ld, Ak, k);
+      const T lkk = sqrt(__shfl_sync(0xffffffffu, s, 0));
+      const T inv = rcp_rn(lkk);
+      __syncwarp();
+      if (lane == 0) A[k * ld + k] = lkk;
+      else if (i < n) A[i * ld + k] = s * inv;
+    } else {
+      T s = T(0);
+      if (lane == 0) s = Ak[k] - chol_dot(Ak, Ak, k);
+      const T lkk = sqrt(__shfl_sync(0xffffffffu, s, 0));
+      const T inv = rcp_rn(lkk);
+      for (int i = k + 1 + lane; i < n; i += 32) {
+        T* Ai = A + i * ld;
+        Ai[k] = (Ai[k] - chol_dot(Ai, Ak, k)) * inv;
       }
-      if (m < k) s0 -= Ai[m] * Ak[m];
-      Ai[k] = (s0 + s1) * inv;
+      __syncwarp();
+      if (lane == 0) A[k * ld + k] = lkk;
     }
-    __syncwarp();
-    if (lane == 0) A[k * ld + k] = lkk;
     __syncwarp();
   }
 }
 
-// x = (L L^T)^-1 y for a factor of size n <= 32 stored with leading dimension ldl; y given and x
-// returned per lane (lane i <-> element i).
-template <typename T>
-__device__ __forceinline__ T cho_solve_reg32(const T* L, int ldl, int n, T yi, int lane) {
-  T xi = lane < n ? yi : T(0);
-  for (int k = 0; k < n; k++) {
-    const T xk = __shfl_sync(0xffffffffu, xi, k) / L[k * ldl + k];
-    if (lane == k) xi = xk;
-    else if (lane > k && lane < n) xi -= L[lane * ldl + k] * xk;
+// Cholesky of an n x n (n <= 32) SPD matrix, in place, with the forward substitution of one
+// right-hand side folded in.  The lower triangle is read from L (leading dimension ldl, shared or
+// global memory); lane i keeps row i in registers.  Right-looking: at column k every lane takes
+// the updated diagonal from lane k by shuffle, scales its entry L[i][k], publishes it to a 32-float
+// per-warp buffer and subtracts L[i][k] * L[j][k] from the rest of its row — independent FMAs fed
+// by broadcast reads.  On exit L holds the factor; the return value is (1 / L[i][i], z_i) with
+// z = L^-1 y for the lane's y_i (0 for lanes >= n).  Blocks of up to 4 warps (one buffer each).
+__device__ __noinline__ float2 chol32(float* L, int ldl, int n, int lane, float y) {
+  __shared__ float colbuf[4][32];
+  float* col = colbuf[(threadIdx.x >> 5) & 3];
+  float r[32];
+#pragma unroll
+  for (int j = 0; j < 32; j++) r[j] = (lane < n && j <= lane) ? L[lane * ldl + j] : 0.f;
+  float z = lane < n ? y : 0.f, invd = 0.f;
+  __syncwarp();
+#pragma unroll
+  for (int k = 0; k < 32; k++) {
+    if (k >= n) break;
+    const float lkk = sqrtf(__shfl_sync(0xffffffffu, r[k], k));
+    const float inv = 1.f / lkk;
+    const float zk = __shfl_sync(0xffffffffu, z, k) * inv;
+    if (lane == k) {
+      r[k] = lkk;
+      invd = inv;
+      z = zk;
+    } else if (lane > k) {
+      r[k] *= inv;
+      z -= r[k] * zk;
+    }
+    col[lane] = r[k];
+    __syncwarp();
+    if (lane > k && lane < n) {
+      const float lik = r[k];
+#pragma unroll
+      for (int j = k + 1; j < 32; j++)
+        if (j <= lane) r[j] -= lik * col[j];
+    }
+    __syncwarp();
   }
-  for (int k = n - 1; k >= 0; k--) {
-    const T xk = __shfl_sync(0xffffffffu, xi, k) / L[k * ldl + k];
-    if (lane == k) xi = xk;
-    else if (lane < k) xi -= L[k * ldl + lane] * xk;
+  if (lane < n) {
+#pragma unroll
+    for (int j = 0; j < 32; j++)
+      if (j <= lane) L[lane * ldl + j] = r[j];
   }
-  return xi;
+  __syncwarp();
+  return make_float2(invd, z);
 }
+
+// Back substitution x = L^-T z for a chol32 factor; lane i holds z_i and 1 / L_ii, returns x_i.
+__device__ __forceinline__ float cho_back32(const float* L, int ldl, int n, float invd, float z,
+                                            int lane) {
+  float x = lane < n ? z : 0.f;
+  for (int k = n - 1; k >= 0; k--) {
+    const float lk = lane < k ? L[k * ldl + lane] : 0.f;
+    const float xk = __shfl_sync(0xffffffffu, x, k) * __shfl_sync(0xffffffffu, invd, k);
+    if (lane == k) x = xk;
+    else if (lane < k) x -= lk * xk;
+  }
+  return x;
+}
+
+// x = (L L^T)^-1 y for a chol32 factor (n <= 32) with lane i holding y_i and invd_i = 1/L_ii;
+// returns x_i.  No divisions: the reciprocal diagonal is broadcast by shuffle.
+__device__ __forceinline__ float cho_solve32(const float* L, int ldl, int n, float invd, float y,
+                                             int lane) {
+  float z = lane < n ? y : 0.f;
+  for (int k = 0; k < n; k++) {
+    const float lk = (lane > k && lane < n) ? L[lane * ldl + k] : 0.f;
+    const float zk = __shfl_sync(0xffffffffu, z, k) * __shfl_sync(0xffffffffu, invd, k);
+    if (lane == k) z = zk;
+    else if (lane > k && lane < n) z -= lk * zk;
+  }
+  return cho_back32(L, ldl, n, invd, z, lane);
+}
+
 
 // x = (L L^T)^-1 y for the n x n lower factor at L (leading dimension ld); x may alias y.
 __device__ void warp_cho_solve(const float* L, int ld, int n, float* x, const float* y, int lane) {
@@ -335,26 +419,39 @@ __device__ void factor_blocks(const MjbModel& m, const float* M, float* L, int l
   __syncwarp();
   for (int blk = 0; blk < m.nblock; blk++) {
     const int a = m.block_adr[blk], n = m.block_size[blk];
-    for (int e = lane; e < n * n; e += 32) {
-      const int i = e / n, j = e - i * n;
-      if (j <= i) {
-        float v = M[(a + i) * nv + a + j];
-        if (dadd && i == j) v += scale * dadd[a + i];
-        L[(a + i) * nv + a + j] = v;
-      }
+    for (int i = lane; i < n; i += 32) {  // row i of the block's lower triangle (+ damping on the diagonal)
+      const float* src = M + (a + i) * nv + a;
+      float* dst = L + (a + i) * nv + a;
+      for (int j = 0; j < i; j++) dst[j] = src[j];
+      dst[i] = src[i] + (dadd ? scale * dadd[a + i] : 0.f);
     }
     __syncwarp();
+#if MJB_CHOL == 1
+    if (n <= 32) chol32(L + a * nv + a, nv, n, lane, 0.f);
+    else chol_lower(L + a * nv + a, nv, n, lane);
+#else
     chol_lower(L + a * nv + a, nv, n, lane);
+#endif
   }
 }
 
-// x = M^-1 y per tree block from the block factor L (smooth.py:654-681)
+// x = M^-1 y per tree block from the block factor L (smooth.py:654-681); x may alias y
 __device__ void solve_blocks(const MjbModel& m, const float* L, float* x, const float* y,
                              int lane) {
   const int nv = m.nv;
   for (int blk = 0; blk < m.nblock; blk++) {
     const int a = m.block_adr[blk], n = m.block_size[blk];
-    warp_cho_solve(L + a * nv + a, nv, n, x + a, y + a, lane);
+    if (n <= 32) {
+      const float* Lb = L + a * nv + a;
+      const float invd = lane < n ? 1.f / Lb[lane * nv + lane] : 0.f;
+      const float yi = lane < n ? y[a + lane] : 0.f;
+      const float xi = cho_solve32(Lb, nv, n, invd, yi, lane);
+      __syncwarp();
+      if (lane < n) x[a + lane] = xi;
+      __syncwarp();
+    } else {
+      warp_cho_solve(L + a * nv + a, nv, n, x + a, y + a, lane);
+    }
   }
 }
 
@@ -707,13 +804,15 @@ __device__ void implicit(const MjbModel& m, const MjbData& d, int w, int lane) {
   float* Mi = d.qM_integration + W(w, nv * nv);
   for (int blk = 0; blk < m.nblock; blk++) {  // qderiv_actuator_fused_kernel, per tree tile
     const int a0 = m.block_adr[blk], n = m.block_size[blk];
-    for (int e = lane; e < n * n; e += 32) {
-      const int i = a0 + e / n, j = a0 + e % n;
-      float qd = 0.f;
-      if (act_on)
-        for (int a = 0; a < nu; a++) qd += moment[a * nv + i] * vel[a] * moment[a * nv + j];
-      if (passive_on && i == j) qd -= m.dof_damping[i];
-      Mi[i * nv + j] = qM[i * nv + j] - qd * m.timestep;
+    for (int ii = lane; ii < n; ii += 32) {
+      const int i = a0 + ii;
+      for (int j = a0; j < a0 + n; j++) {
+        float qd = 0.f;
+        if (act_on)
+          for (int a = 0; a < nu; a++) qd += moment[a * nv + i] * vel[a] * moment[a * nv + j];
+        if (passive_on && i == j) qd -= m.dof_damping[i];
+        Mi[i * nv + j] = qM[i * nv + j] - qd * m.timestep;
+      }
     }
   }
   float* f = d.qfrc_integration + W(w, nv);

@@ -13,7 +13,8 @@ import pytest
 import torch
 
 import mjx_warp_b200 as mjw
-from helpers import assert_close, dev, device_data, humanoid, humanoid_state, oracle, rel_err, world_rows
+from helpers import (assert_close, dev, device_data, generic_state, humanoid, humanoid_state, load,
+                     oracle, rel_err, world_rows)
 
 pytestmark = pytest.mark.gpu
 
@@ -101,3 +102,40 @@ def test_solve_standalone_matches_forward():
   e = rel_err(dev(d.qacc), dev(qacc))
   assert e.max() < 1e-3
   del ws
+
+
+_MANY_ROWS = """
+<mujoco model="footprint">
+  <option timestep="0.002" solver="Newton" iterations="30" ls_iterations="30" tolerance="1e-10"/>
+  <worldbody>
+    <geom type="plane" size="0 0 1"/>
+    <body pos="0 0 0.045">
+      <freejoint/>
+      {spheres}
+    </body>
+  </worldbody>
+</mujoco>
+"""
+
+
+def test_many_rows_past_the_staged_capacity():
+  """One body resting on 12 spheres: 48 pyramid rows in one world, more than the solver stages in
+  shared memory, so the rows are read from global memory; forces must still match the oracle."""
+  spheres = "\n".join(f'<geom type="sphere" size="0.05" pos="{0.1 * np.cos(a):.4f} {0.1 * np.sin(a):.4f} 0"/>'
+                      for a in np.linspace(0, 2 * np.pi, 12, endpoint=False))
+  mjm = load(_MANY_ROWS.format(spheres=spheres))
+  qpos, qvel, ctrl = generic_state(mjm, 16, seed=7, qscale=0.003, vscale=0.01)
+  m = mjw.put_model(mjm)
+  d = device_data(mjm, qpos, qvel, ctrl)
+  mjw.forward(m, d)
+  o = oracle(mjm, qpos, qvel, ctrl, 64)
+  o.run("forward")
+  torch.cuda.synchronize()
+  n, idx = world_rows(d, "efc")
+  cnt, f = o.rows("efc_force")
+  np.testing.assert_array_equal(n, cnt)
+  assert n.min() > 32, n
+  e = rel_err(dev(d.qacc), o.get("qacc"))
+  assert e.max() < 1e-3, e.max()
+  ef = d.efc.force.cpu().numpy()[idx]
+  np.testing.assert_allclose(ef, f.ravel(), rtol=1e-3, atol=1e-3 * np.abs(f).max())
