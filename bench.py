@@ -1,6 +1,7 @@
 """Benchmark: humanoid batched step, nworld=8192 per GPU, steps/s (one JSON line on rank 0).
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--form fused|plain]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--form chosen|plain|single]
 
 Workload: the reference's humanoid (27 dof, 21 motors) with implicitfast integration, dt=0.005,
 Newton with 3 iterations and 4 line-search iterations, pyramidal condim-3 contacts; seeded
@@ -8,8 +9,12 @@ synthetic initial states (keyframe "squat" + U(-0.05, 0.05), qvel ~ N(0, 0.01),
 ctrl ~ U(-0.4, 0.4)).  A "step" is one mjw.step over all worlds.
 
 value: world-steps/s with the state resident in HBM, one captured CUDA graph of the step replayed
-K times.  e2e: the same metric through the public API (mjw.step) with, every step, the control
-copied in from pinned host memory and qpos / qvel copied back.  Multi-GPU: one process per GPU,
+K times, in the chosen launch form (reset + k_smooth + k_solve + k_integrate); `forms` gives the
+same number for the plain one-kernel-per-stage form (the reference's launch sequence and
+algorithm) and the single-kernel form, measured in the same run.  e2e: the metric through the
+public API (mjw.step) with, every step, the control copied in from pinned host memory and
+qpos / qvel copied back.  roofline: the dominant kernel (the solver) timed with CUDA events
+around its own launch (mjw.step_phase) over K steps.  Multi-GPU: one process per GPU,
 each owning its own 8192 worlds (replicas, weak scaling, no collective on the data path); time is
 the maximum over ranks of CUDA-event time between barriers.
 
@@ -126,6 +131,46 @@ def _algorithmic_bytes(d, mjm, ncon, nefc):
   return W * (read_state + per_world_out) + contact_bytes + efc_bytes
 
 
+FORMS = {"plain": 0, "chosen": 1, "single": 2}
+LAUNCHES = {"plain": 16, "chosen": 4, "single": 2}  # kernels per step (mjb200.cu run_* paths)
+
+
+def _solver_bytes(mjm, nworld, nefc):
+  """HBM bytes the solver must move: read qM, qfrc_smooth, qacc_smooth, qacc_warmstart and each
+  row's J, D, aref; write qacc, qacc_warmstart, qfrc_constraint and the solver vectors (Ma, grad,
+  Mgrad, search, mv, prev_grad, prev_Mgrad), per-world scalars (16) and each row's force, Jaref,
+  active, jv and quad (3)."""
+  nv = mjm.nv
+  per_world = (nv * nv + 3 * nv) + (10 * nv + 16)
+  per_row = (nv + 2) + 7
+  return 4 * (nworld * per_world + nefc * per_row)
+
+
+STATE = ("qpos", "qvel", "act", "ctrl", "qacc_warmstart")
+
+
+def _graph_steps_per_s(torch, step, nworld, steps, barrier, restore):
+  g = torch.cuda.CUDAGraph()
+  s = torch.cuda.Stream()
+  s.wait_stream(torch.cuda.current_stream())
+  with torch.cuda.stream(s):
+    with torch.cuda.graph(g, stream=s):
+      step()
+  torch.cuda.current_stream().wait_stream(s)
+  restore()
+  barrier()
+  t0 = torch.cuda.Event(enable_timing=True)
+  t1 = torch.cuda.Event(enable_timing=True)
+  t0.record()
+  for _ in range(steps):
+    g.replay()
+  t1.record()
+  barrier()
+  el = t0.elapsed_time(t1) / 1000.0
+  del g
+  return el
+
+
 def run_ours(args):
   import torch
 
@@ -146,8 +191,8 @@ def run_ours(args):
   d.qpos.copy_(torch.as_tensor(qpos, dtype=torch.float32))
   d.qvel.copy_(torch.as_tensor(qvel, dtype=torch.float32))
   d.ctrl.copy_(torch.as_tensor(ctrl, dtype=torch.float32))
-  fused = args.form == "fused"
-  step = lambda: mjw.step(m, d, fused=fused)  # noqa: E731
+  form = FORMS[args.form]
+  step = lambda: mjw.step(m, d, fused=form)  # noqa: E731
 
   def barrier():
     if world_size > 1:
@@ -156,6 +201,15 @@ def run_ours(args):
 
   for _ in range(args.warmup):
     step()
+  # every measurement below starts from the state after the warm-up steps, so each times the
+  # same K steps of the same trajectories
+  barrier()
+  snap = {k: getattr(d, k).clone() for k in STATE}
+
+  def restore():
+    for k, v in snap.items():
+      getattr(d, k).copy_(v)
+
   # device-resident: one captured graph of the step, replayed K times
   g = torch.cuda.CUDAGraph()
   s = torch.cuda.Stream()
@@ -165,21 +219,17 @@ def run_ours(args):
       step()
   torch.cuda.current_stream().wait_stream(s)
   g.replay()
-  ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-        for _ in range(args.steps)]
+  restore()
   barrier()
   with _Clocks(local_rank) as clocks:
     t0 = torch.cuda.Event(enable_timing=True)
     t1 = torch.cuda.Event(enable_timing=True)
     t0.record()
-    for a, b in ev:
-      a.record()
+    for _ in range(args.steps):
       g.replay()
-      b.record()
     t1.record()
     barrier()
   elapsed = replicas.max_over_ranks(t0.elapsed_time(t1) / 1000.0, device="cuda")
-  step_ms = [a.elapsed_time(b) for a, b in ev]
   status = mjw.world_status(d)
   nonfinite = int(replicas.sum_over_ranks(int(np.count_nonzero(status & 0x8)), device="cuda"))
   overflow = int(replicas.sum_over_ranks(int(np.count_nonzero(status & 0x7)), device="cuda"))
@@ -190,9 +240,7 @@ def run_ours(args):
   ctrl_h = torch.as_tensor(ctrl, dtype=torch.float32).pin_memory()
   out_h = torch.empty((nworld, mjm.nq + mjm.nv), dtype=torch.float32).pin_memory()
   out_d = torch.empty((nworld, mjm.nq + mjm.nv), dtype=torch.float32, device="cuda")
-  for _ in range(2):
-    d.ctrl.copy_(ctrl_h, non_blocking=True)
-    step()
+  restore()
   barrier()
   e0 = torch.cuda.Event(enable_timing=True)
   e1 = torch.cuda.Event(enable_timing=True)
@@ -207,11 +255,47 @@ def run_ours(args):
   barrier()
   e2e_elapsed = replicas.max_over_ranks(e0.elapsed_time(e1) / 1000.0, device="cuda")
 
-  launches_per_step = 2 if fused else 17
+  # the dominant kernel (the solver) timed around its own launch, same stream, K steps
+  solve_ms = []
+  if args.form == "plain":
+    pre = lambda: (mjw.fwd_position(m, d), mjw.fwd_velocity(m, d), mjw.fwd_actuation(m, d),  # noqa: E731
+                   mjw.fwd_acceleration(m, d))
+    solve = lambda: mjw.solve(m, d)  # noqa: E731
+    post = lambda: mjw.implicit(m, d)  # noqa: E731
+  else:
+    pre = lambda: mjw.step_phase(m, d, 0)  # noqa: E731
+    solve = lambda: mjw.step_phase(m, d, 1)  # noqa: E731
+    post = lambda: mjw.step_phase(m, d, 2)  # noqa: E731
+  restore()
+  barrier()
+  for _ in range(args.steps):
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    pre()
+    a.record()
+    solve()
+    b.record()
+    post()
+    solve_ms.append((a, b))
+  barrier()
+  solve_s = replicas.max_over_ranks(float(np.mean([a.elapsed_time(b) for a, b in solve_ms])) / 1000.0,
+                                    device="cuda")
+  nefc_solve = int(d.world_nefc.sum())
+
+  # the other launch forms on the same worlds, for the chosen-vs-plain comparison
+  forms = {}
+  for name, f in FORMS.items():
+    if name == args.form:
+      continue
+    el = _graph_steps_per_s(torch, lambda: mjw.step(m, d, fused=f), nworld, args.steps, barrier,
+                            restore)
+    el = replicas.max_over_ranks(el, device="cuda")
+    forms[name] = {"value": nworld * world_size * args.steps / el, "ms_per_step": el / args.steps * 1e3}
+
+  launches_per_step = LAUNCHES[args.form]
   total_worlds = nworld * world_size
   value = total_worlds * args.steps / elapsed
-  kernel_s = float(np.mean(step_ms)) / 1000.0
-  alg = _algorithmic_bytes(d, mjm, ncon, nefc)
+  alg = _solver_bytes(mjm, nworld, nefc_solve)
+  step_alg = _algorithmic_bytes(d, mjm, ncon, nefc)
   peaks = {}
   try:
     with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -219,19 +303,20 @@ def run_ours(args):
   except OSError:
     pass
   hbm = float(peaks.get("hbm_gbs", 6650.0))
-  achieved = alg / kernel_s / 1e9
+  achieved = alg / solve_s / 1e9
   footprint = sum(_bytes_of(t) for t in list(d.arrays().values()) + list(d.contact.arrays().values())
                   + list(d.efc.arrays().values()))
   traffic = None
   tpath = os.path.join(ROOT, "profiles", "traffic.json")
   if os.path.exists(tpath):
     with open(tpath) as f:
-      traffic = json.load(f).get(f"{args.form}_dram_bytes_per_launch")
+      traffic = json.load(f).get(args.form, {}).get("dram_bytes_per_launch")
   line = {
     "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world_size, "steps": args.steps,
     "warmup": args.warmup, "ms_per_step": elapsed / args.steps * 1000.0, "higher_is_better": True,
     "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded states)",
     "config": {"workload": WORKLOAD, "nworld_per_gpu": nworld, "nv": mjm.nv, "form": args.form,
+               "solver_reuses_factor": args.form != "plain",
                "nconmax": d.nconmax, "njmax": d.njmax,
                "l2": f"working set {footprint / 2**20:.0f} MiB per GPU > 126 MB L2, no flush",
                "parallelism": f"replicas x{world_size}"},
@@ -240,8 +325,12 @@ def run_ours(args):
     "gpu_launches": launches_per_step * args.steps,
     "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                  "frac": achieved / hbm, "traffic": traffic,
-                 "kernel": "k_step_fused" if fused else "k_stage<*> chain",
-                 "algorithmic_bytes_per_launch": alg, "peak_source": "measured" if peaks else "fallback"},
+                 "kernel": "k_stage<S_SOLVE> (plain)" if args.form == "plain" else "k_solve",
+                 "kernel_ms": solve_s * 1e3, "kernel_share_of_step": solve_s / (elapsed / args.steps),
+                 "algorithmic_bytes_per_launch": alg, "peak_source": "measured" if peaks else "fallback",
+                 "step_algorithmic_bytes": step_alg,
+                 "step_achieved_gbs": step_alg / (elapsed / args.steps) / 1e9},
+    "forms": forms,
     "clocks": clocks.summary(),
     "status": {"nonfinite_worlds": nonfinite, "overflow_worlds": overflow,
                "mean_contacts_per_world": ncon / nworld, "mean_efc_rows_per_world": nefc / nworld},
@@ -305,7 +394,7 @@ def main():
   p.add_argument("--steps", type=int, default=200)
   p.add_argument("--warmup", type=int, default=10)
   p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-  p.add_argument("--form", default="fused", choices=["fused", "plain"])
+  p.add_argument("--form", default="chosen", choices=list(FORMS))
   p.add_argument("--nworld", type=int, default=NWORLD)
   p.add_argument("--cpu-seconds", type=float, default=10.0)
   p.add_argument("--no-cpu-baseline", action="store_true")

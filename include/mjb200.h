@@ -131,9 +131,14 @@ typedef struct MjbData {
 } MjbData;
 
 /* Launch configuration for the step entry points. */
+/* Launch forms of mjb_step / mjb_forward (MjbRunCfg.fused; a null cfg selects MJB_FORM_CHOSEN). */
+#define MJB_FORM_PLAIN 0  /* one kernel per reference stage; Hessian refactored every iteration */
+#define MJB_FORM_CHOSEN 1 /* reset + smooth/collision/constraint kernel + solver + integrator */
+#define MJB_FORM_SINGLE 2 /* the whole step of a world in one warp of one kernel */
+
 typedef struct MjbRunCfg {
-  int32_t fused;            /* 1: fused per-world kernels (default); 0: one kernel per stage */
-  int32_t worlds_per_block; /* warps (= worlds) per CTA; 0 picks the default */
+  int32_t fused;            /* launch form, MJB_FORM_* */
+  int32_t worlds_per_block; /* MJB_FORM_SINGLE: warps (= worlds) per CTA, at most 4; 0 = 4 */
 } MjbRunCfg;
 
 int mjb_abi_version(void);
@@ -143,6 +148,11 @@ const char* mjb_error_string(int status);
 int mjb_step(const MjbModel* m, const MjbData* d, const MjbRunCfg* cfg, mjbStream stream);
 /* forward (forward.py:664-679). */
 int mjb_forward(const MjbModel* m, const MjbData* d, const MjbRunCfg* cfg, mjbStream stream);
+/* One phase of MJB_FORM_CHOSEN's step (no counterpart in the reference, whose step is one call):
+   0 = counter reset + fwd_position .. fwd_acceleration, 1 = the constraint solver, 2 = Euler /
+   implicitfast integration + the finiteness check.  Phases 0, 1, 2 in order equal mjb_step; they
+   let a caller time the kernels separately or act between forward and integration. */
+int mjb_step_phase(const MjbModel* m, const MjbData* d, int phase, mjbStream stream);
 
 /* Pipeline stages (forward.py:408-661). */
 int mjb_fwd_position(const MjbModel* m, const MjbData* d, mjbStream stream);

@@ -38,6 +38,7 @@ from ._api import sap_broadphase as sap_broadphase
 from ._api import solve as solve
 from ._api import solve_m as solve_m
 from ._api import step as step
+from ._api import step_phase as step_phase
 from ._api import transmission as transmission
 from ._api import world_status as world_status
 from ._api import xfrc_accumulate as xfrc_accumulate

@@ -150,6 +150,8 @@ def lib() -> ctypes.CDLL:
   L.mjb_mul_m.argtypes = [pm, pd, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
   L.mjb_xfrc_accumulate.restype = ctypes.c_int
   L.mjb_xfrc_accumulate.argtypes = [pm, pd, ctypes.c_void_p, ctypes.c_void_p]
+  L.mjb_step_phase.restype = ctypes.c_int
+  L.mjb_step_phase.argtypes = [pm, pd, ctypes.c_int, ctypes.c_void_p]
   L.mjb_world_status.restype = ctypes.c_int
   L.mjb_world_status.argtypes = [pd, ctypes.c_void_p, ctypes.c_void_p]
   if L.mjb_abi_version() != 1:

@@ -18,8 +18,16 @@ import torch
 from . import _abi
 from .types import Data, Model
 
-_FUSED = _abi.MjbRunCfg(1, 0)
-_PLAIN = _abi.MjbRunCfg(0, 0)
+# launch forms (include/mjb200.h MJB_FORM_*): True / 1 the chosen form, False / 0 the plain
+# one-kernel-per-stage form, 2 the single-kernel form
+_FORMS = {0: _abi.MjbRunCfg(0, 0), 1: _abi.MjbRunCfg(1, 0), 2: _abi.MjbRunCfg(2, 0)}
+
+
+def _form(fused) -> "_abi.MjbRunCfg":
+  try:
+    return _FORMS[int(fused)]
+  except (KeyError, TypeError, ValueError):
+    raise ValueError(f"unknown launch form {fused!r} (True/1 chosen, False/0 plain, 2 single)") from None
 
 
 def _call(name: str, m: Model, d: Data, *extra) -> None:
@@ -37,25 +45,38 @@ def _integrator_check(m: Model) -> None:
     raise NotImplementedError(f"integrator {m.opt.integrator} not implemented.")
 
 
-def step(m: Model, d: Data, fused: bool = True) -> None:
+def step(m: Model, d: Data, fused=True) -> None:
   """Advance simulation (forward.py:682-695).
 
-  fused=True runs every stage of a world inside one warp of one kernel; fused=False launches one
-  kernel per stage (the reference's stage decomposition).
+  fused=True (or 1) runs the chosen form: one kernel for fwd_position .. fwd_acceleration, one
+  for the solver (keeping the Newton Hessian's factor while the active set is unchanged) and one
+  for the integrator; fused=False (or 0) launches one kernel per reference stage and refactors
+  the Hessian in every iteration, as the reference does; fused=2 runs the whole step of a world
+  in one warp of a single kernel.
   """
   _integrator_check(m)
   L = _abi.lib()
   rc = L.mjb_step(ctypes.byref(_abi.model_view(m)), ctypes.byref(_abi.data_view(d)),
-                  ctypes.byref(_FUSED if fused else _PLAIN), _abi.stream())
+                  ctypes.byref(_form(fused)), _abi.stream())
   _abi.check(rc, "step")
   d.time = d.time + m.opt.timestep
 
 
-def forward(m: Model, d: Data, fused: bool = True) -> None:
-  """Forward dynamics (forward.py:664-679)."""
+def step_phase(m: Model, d: Data, phase: int) -> None:
+  """One phase of the chosen form's step (not in the reference): 0 = fwd_position ..
+  fwd_acceleration, 1 = the constraint solver, 2 = integration.  Phases 0, 1, 2 in order equal
+  step(m, d) except for d.time, which only step() advances."""
+  L = _abi.lib()
+  rc = L.mjb_step_phase(ctypes.byref(_abi.model_view(m)), ctypes.byref(_abi.data_view(d)),
+                        int(phase), _abi.stream())
+  _abi.check(rc, "step_phase")
+
+
+def forward(m: Model, d: Data, fused=True) -> None:
+  """Forward dynamics (forward.py:664-679); `fused` selects the launch form as in step()."""
   L = _abi.lib()
   rc = L.mjb_forward(ctypes.byref(_abi.model_view(m)), ctypes.byref(_abi.data_view(d)),
-                     ctypes.byref(_FUSED if fused else _PLAIN), _abi.stream())
+                     ctypes.byref(_form(fused)), _abi.stream())
   _abi.check(rc, "forward")
 
 

@@ -1,13 +1,15 @@
 // libmjb200.so: kernels and the C ABI declared in include/mjb200.h.
 //
-// Two launch forms share the per-world device stages of mjb_world.cuh / mjb_collide.cuh /
-// mjb_solver.cuh:
-//  - plain: one kernel per reference stage function (mjb_kinematics, mjb_com_pos, ...), one warp
-//    per world, data passed between stages through the Data arrays in HBM; mjb_step with
-//    cfg->fused == 0 chains these, like the reference's launch sequence;
-//  - fused: mjb_step / mjb_forward with cfg->fused != 0 run every stage of a world inside one
-//    warp of a single kernel (after one tiny counter-reset kernel), with the Newton Hessian and its
-//    Cholesky factor in shared memory.
+// Three launch forms share the per-world device stages of mjb_world.cuh / mjb_collide.cuh /
+// mjb_solver.cuh (one warp per world everywhere):
+//  - plain (MJB_FORM_PLAIN): one kernel per reference stage function (mjb_kinematics,
+//    mjb_com_pos, ...), data passed between stages through the Data arrays in HBM, the Newton
+//    Hessian refactored in every iteration: the reference's launch sequence and algorithm;
+//  - chosen (MJB_FORM_CHOSEN, the default): a counter reset, then three kernels sized for their
+//    own register and shared-memory needs: k_smooth (fwd_position .. fwd_acceleration, 64
+//    registers, one factor tile per warp), k_solve (the solver, keeping the Hessian factor while
+//    the active set is unchanged) and k_integrate (Euler / implicitfast + the finiteness check);
+//  - single (MJB_FORM_SINGLE): every stage of a world inside one warp of one kernel.
 // No entry point allocates memory or synchronises the stream (except mjb_world_status, which
 // copies results to the host).
 #include <cuda_runtime.h>
@@ -45,43 +47,44 @@ __device__ __forceinline__ void copy_qacc_smooth(const MjbModel& m, const MjbDat
   __syncwarp();
 }
 
+// the solver needs up to 128 registers; every other stage is held to 64 for occupancy
 template <int STAGE>
-__global__ void __launch_bounds__(128, MJB_MINB) k_stage(const MjbModel m, const MjbData d, int smem_per_warp) {
-  extern __shared__ float smem[];
+__global__ void __launch_bounds__(128, STAGE == S_SOLVE ? MJB_MINB : 8)
+    k_stage(const MjbModel m, const MjbData d, int smem_per_warp) {
+  extern __shared__ __align__(16) float smem[];
   const int lane = threadIdx.x & 31;
   const int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   if (w >= d.nworld) return;
+  float* sm = smem_per_warp ? smem + size_t(threadIdx.x >> 5) * smem_per_warp : nullptr;
   switch (STAGE) {
     case S_KINEMATICS: kinematics(m, d, w, lane); break;
     case S_COM_POS: com_pos(m, d, w, lane); break;
     case S_CRB: crb(m, d, w, lane); break;
-    case S_FACTOR_M: factor_m(m, d, w, lane); break;
+    case S_FACTOR_M: factor_m(m, d, w, lane, sm); break;
     case S_TRANSMISSION: transmission(m, d, w, lane); break;
     case S_COM_VEL: com_vel(m, d, w, lane); break;
     case S_PASSIVE: passive(m, d, w, lane); break;
     case S_RNE: rne(m, d, w, lane); break;
     case S_FWD_VELOCITY: fwd_velocity(m, d, w, lane); break;
     case S_FWD_ACTUATION: fwd_actuation(m, d, w, lane); break;
-    case S_FWD_ACCELERATION: fwd_acceleration(m, d, w, lane); break;
+    case S_FWD_ACCELERATION: fwd_acceleration(m, d, w, lane, sm); break;
     case S_NXN: nxn_broadphase(m, d, w, lane); break;
     case S_NARROW: primitive_narrowphase(m, d, w, lane); break;
     case S_MAKE_CONSTRAINT: make_constraint(m, d, w, lane); break;
-    case S_SOLVE:
-      solve(m, d, w, lane, smem_per_warp ? smem + size_t(threadIdx.x >> 5) * smem_per_warp : nullptr,
-            d.efc_h + W(w, m.nv * m.nv));
-      break;
-    case S_EULER: euler(m, d, w, lane); break;
-    case S_IMPLICIT: implicit(m, d, w, lane); break;
+    case S_SOLVE: solve(m, d, w, lane, sm, d.efc_h + W(w, m.nv * m.nv)); break;
+    case S_EULER: euler(m, d, w, lane, sm); break;
+    case S_IMPLICIT: implicit(m, d, w, lane, sm); break;
     case S_QACC_SMOOTH_COPY: copy_qacc_smooth(m, d, w, lane); break;
     case S_CHECK: check_finite(m, d, w, lane); break;
   }
 }
 
-// whole forward (+ integration) of one world per warp; dynamic shared memory holds one nv x nv
-// Hessian / factor tile per warp
+// whole forward (+ integration) of one world per warp; each warp's slice of dynamic shared memory
+// holds the solver's workspace, whose leading factor tile also serves the mass-matrix
+// factorisations (factor_m, then the integrator)
 __global__ void __launch_bounds__(128, MJB_MINB) k_step_fused(const MjbModel m, const MjbData d, int integrate,
                                                     int smem_per_warp) {
-  extern __shared__ float smem[];
+  extern __shared__ __align__(16) float smem[];
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
   const int w = blockIdx.x * (blockDim.x >> 5) + wib;
@@ -92,20 +95,63 @@ __global__ void __launch_bounds__(128, MJB_MINB) k_step_fused(const MjbModel m, 
   kinematics(m, d, w, lane);
   com_pos(m, d, w, lane);
   crb(m, d, w, lane);
-  factor_m(m, d, w, lane);
+  factor_m(m, d, w, lane, sm);
   collision(m, d, w, lane);
   make_constraint(m, d, w, lane);
   transmission(m, d, w, lane);
   fwd_velocity(m, d, w, lane);
   fwd_actuation(m, d, w, lane);
-  fwd_acceleration(m, d, w, lane);
+  fwd_acceleration(m, d, w, lane, sm, true);  // the tile still holds factor_m's factor
   if (d.njmax == 0) copy_qacc_smooth(m, d, w, lane);
-  else solve(m, d, w, lane, sm, hs);
+  else solve(m, d, w, lane, sm, hs, true);
   if (integrate) {
-    if (m.integrator == 0) euler(m, d, w, lane);
-    else implicit(m, d, w, lane);
+    if (m.integrator == 0) euler(m, d, w, lane, sm);
+    else implicit(m, d, w, lane, sm);
     check_finite(m, d, w, lane);
   }
+}
+
+// chosen form, kernel 1: fwd_position .. fwd_acceleration (forward.py:408-661) of one world per
+// warp; the warp's factor tile holds factor_m's factor until fwd_acceleration's solve
+__global__ void __launch_bounds__(128, 8) k_smooth(const MjbModel m, const MjbData d, int tile_per_warp) {
+  extern __shared__ __align__(16) float smem[];
+  const int lane = threadIdx.x & 31;
+  const int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (w >= d.nworld) return;
+  float* tile = smem + size_t(threadIdx.x >> 5) * tile_per_warp;
+  kinematics(m, d, w, lane);
+  com_pos(m, d, w, lane);
+  crb(m, d, w, lane);
+  factor_m(m, d, w, lane, tile);
+  collision(m, d, w, lane);
+  make_constraint(m, d, w, lane);
+  transmission(m, d, w, lane);
+  fwd_velocity(m, d, w, lane);
+  fwd_actuation(m, d, w, lane);
+  fwd_acceleration(m, d, w, lane, tile, true);
+  if (d.njmax == 0) copy_qacc_smooth(m, d, w, lane);
+}
+
+// chosen form, kernel 2: the constraint solver with the Hessian factor kept across iterations
+__global__ void __launch_bounds__(128, MJB_MINB) k_solve(const MjbModel m, const MjbData d, int smem_per_warp) {
+  extern __shared__ __align__(16) float smem[];
+  const int lane = threadIdx.x & 31;
+  const int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (w >= d.nworld) return;
+  float* sm = smem_per_warp ? smem + size_t(threadIdx.x >> 5) * smem_per_warp : nullptr;
+  solve(m, d, w, lane, sm, d.efc_h + W(w, m.nv * m.nv), true);
+}
+
+// chosen form, kernel 3: integration (forward.py:165-405) and the finiteness check
+__global__ void __launch_bounds__(128, 8) k_integrate(const MjbModel m, const MjbData d, int tile_per_warp) {
+  extern __shared__ __align__(16) float smem[];
+  const int lane = threadIdx.x & 31;
+  const int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (w >= d.nworld) return;
+  float* tile = smem + size_t(threadIdx.x >> 5) * tile_per_warp;
+  if (m.integrator == 0) euler(m, d, w, lane, tile);
+  else implicit(m, d, w, lane, tile);
+  check_finite(m, d, w, lane);
 }
 
 // zero the flat-array counters and (optionally) the world status words
@@ -200,9 +246,23 @@ inline int check(const MjbModel* m, const MjbData* d) {
   return MJB_OK;
 }
 
-// shared memory per warp for the solver (0 when the model needs the generic path)
+// shared memory per warp (floats) for the solver workspace when nv <= 32, else a factor tile for
+// the tree blocks of up to 32 dofs (the generic solver keeps its Hessian in efc_h)
 int solver_smem_per_warp(const MjbModel* m) {
-  return m->nv <= 32 ? int(solver_smem_floats(m->nv)) : 0;
+  return m->nv <= 32 ? int(solver_smem_floats(m->nv)) : tile_floats(m->nv);
+}
+
+// opts a kernel in to more than 48 KB of dynamic shared memory (once per kernel, device and size)
+constexpr int kSmemDevices = 64;
+template <typename K>
+void allow_smem(K kernel, size_t bytes, size_t (&configured)[kSmemDevices]) {
+  if (bytes <= 48 * 1024) return;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= kSmemDevices || bytes > configured[dev]) {
+    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
+    if (dev >= 0 && dev < kSmemDevices) configured[dev] = bytes;
+  }
 }
 
 template <int STAGE>
@@ -210,14 +270,13 @@ int launch_stage(const MjbModel* m, const MjbData* d, cudaStream_t s) {
   const int warps = kDefaultWarps;
   int spw = 0;
   size_t bytes = 0;
-  if (STAGE == S_SOLVE) {
-    spw = solver_smem_per_warp(m);
+  if (STAGE == S_SOLVE) spw = m->nv <= 32 ? int(solver_smem_floats(m->nv)) : 0;
+  if (STAGE == S_FACTOR_M || STAGE == S_FWD_ACCELERATION || STAGE == S_EULER || STAGE == S_IMPLICIT)
+    spw = tile_floats(m->nv);
+  if (spw) {
     bytes = size_t(spw) * warps * sizeof(float);
-    static size_t configured = 0;  // opt in to > 48 KB of dynamic shared memory once per size
-    if (bytes > 48 * 1024 && bytes > configured) {
-      cudaFuncSetAttribute(k_stage<STAGE>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
-      configured = bytes;
-    }
+    static size_t configured[kSmemDevices];
+    allow_smem(k_stage<STAGE>, bytes, configured);
   }
   k_stage<STAGE><<<grid_for(d->nworld, warps), 32 * warps, bytes, s>>>(*m, *d, spw);
   return finish();
@@ -258,6 +317,40 @@ int run_forward_plain(const MjbModel* m, const MjbData* d, cudaStream_t s) {
   return launch_stage<S_SOLVE>(m, d, s);
 }
 
+// the chosen form's phases: 0 = counter reset + k_smooth, 1 = k_solve, 2 = k_integrate
+int run_chosen_phase(const MjbModel* m, const MjbData* d, int phase, cudaStream_t s) {
+  const int warps = kDefaultWarps;
+  const int grid = grid_for(d->nworld, warps);
+  const int tpw = tile_floats(m->nv);
+  const size_t tile_bytes = size_t(tpw) * warps * sizeof(float);
+  static size_t conf_smooth[kSmemDevices], conf_solve[kSmemDevices], conf_int[kSmemDevices];
+  if (phase == 0) {
+    reset_counters(d, true, true, true, true, s);
+    allow_smem(k_smooth, tile_bytes, conf_smooth);
+    k_smooth<<<grid, 32 * warps, tile_bytes, s>>>(*m, *d, tpw);
+  } else if (phase == 1) {
+    if (d->njmax > 0) {
+      const int spw = m->nv <= 32 ? int(solver_smem_floats(m->nv)) : 0;
+      const size_t bytes = size_t(spw) * warps * sizeof(float);
+      allow_smem(k_solve, bytes, conf_solve);
+      k_solve<<<grid, 32 * warps, bytes, s>>>(*m, *d, spw);
+    }
+  } else if (phase == 2) {
+    allow_smem(k_integrate, tile_bytes, conf_int);
+    k_integrate<<<grid, 32 * warps, tile_bytes, s>>>(*m, *d, tpw);
+  } else {
+    return MJB_ERR_ARG;
+  }
+  return finish();
+}
+
+int run_chosen(const MjbModel* m, const MjbData* d, int integrate, cudaStream_t s) {
+  int rc;
+  if ((rc = run_chosen_phase(m, d, 0, s))) return rc;
+  if ((rc = run_chosen_phase(m, d, 1, s))) return rc;
+  return integrate ? run_chosen_phase(m, d, 2, s) : MJB_OK;
+}
+
 int run_fused(const MjbModel* m, const MjbData* d, const MjbRunCfg* cfg, int integrate,
               cudaStream_t s) {
   const int warps = (cfg && cfg->worlds_per_block > 0) ? cfg->worlds_per_block : kDefaultWarps;
@@ -265,11 +358,8 @@ int run_fused(const MjbModel* m, const MjbData* d, const MjbRunCfg* cfg, int int
   reset_counters(d, true, true, true, true, s);
   const int spw = solver_smem_per_warp(m);
   const size_t smem = size_t(spw) * warps * sizeof(float);
-  static size_t configured = 0;  // opt in to > 48 KB of dynamic shared memory once per size
-  if (smem > 48 * 1024 && smem > configured) {
-    cudaFuncSetAttribute(k_step_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-    configured = smem;
-  }
+  static size_t configured[kSmemDevices];
+  allow_smem(k_step_fused, smem, configured);
   k_step_fused<<<grid_for(d->nworld, warps), 32 * warps, smem, s>>>(*m, *d, integrate, spw);
   return finish();
 }
@@ -295,15 +385,19 @@ int mjb_forward(const MjbModel* m, const MjbData* d, const MjbRunCfg* cfg, mjbSt
   int rc = check(m, d);
   if (rc || d->nworld == 0) return rc;
   cudaStream_t s = (cudaStream_t)stream;
-  if (cfg && !cfg->fused) return run_forward_plain(m, d, s);
-  return run_fused(m, d, cfg, 0, s);
+  const int form = cfg ? cfg->fused : MJB_FORM_CHOSEN;
+  if (form == MJB_FORM_PLAIN) return run_forward_plain(m, d, s);
+  if (form == MJB_FORM_SINGLE) return run_fused(m, d, cfg, 0, s);
+  if (form != MJB_FORM_CHOSEN) return MJB_ERR_ARG;
+  return run_chosen(m, d, 0, s);
 }
 
 int mjb_step(const MjbModel* m, const MjbData* d, const MjbRunCfg* cfg, mjbStream stream) {
   int rc = check(m, d);
   if (rc || d->nworld == 0) return rc;
   cudaStream_t s = (cudaStream_t)stream;
-  if (cfg && !cfg->fused) {
+  const int form = cfg ? cfg->fused : MJB_FORM_CHOSEN;
+  if (form == MJB_FORM_PLAIN) {
     reset_counters(d, false, false, false, true, s);
     if ((rc = run_forward_plain(m, d, s))) return rc;
     if (m->integrator == 0) rc = launch_stage<S_EULER>(m, d, s);
@@ -311,7 +405,15 @@ int mjb_step(const MjbModel* m, const MjbData* d, const MjbRunCfg* cfg, mjbStrea
     if (rc) return rc;
     return launch_stage<S_CHECK>(m, d, s);
   }
-  return run_fused(m, d, cfg, 1, s);
+  if (form == MJB_FORM_SINGLE) return run_fused(m, d, cfg, 1, s);
+  if (form != MJB_FORM_CHOSEN) return MJB_ERR_ARG;
+  return run_chosen(m, d, 1, s);
+}
+
+int mjb_step_phase(const MjbModel* m, const MjbData* d, int phase, mjbStream stream) {
+  int rc = check(m, d);
+  if (rc || d->nworld == 0) return rc;
+  return run_chosen_phase(m, d, phase, (cudaStream_t)stream);
 }
 
 #define MJB_STAGE_ENTRY(name, STAGE)                                           \

@@ -273,7 +273,7 @@ __device__ void linesearch(SolverCtx& s) {
 }
 
 // solver.py:872-1000, any nv; hs: per-warp scratch of nv*nv floats (Newton only)
-__device__ void solve_generic(const MjbModel& m, const MjbData& d, int w, int lane, float* hs) {
+__device__ __noinline__ void solve_generic(const MjbModel& m, const MjbData& d, int w, int lane, float* hs) {
   const int nv = m.nv;
   SolverCtx s{m, d, w, lane, nv, d.world_efcadr[w], d.world_nefc[w]};
   s.qacc = d.qacc + W(w, nv);
@@ -388,21 +388,38 @@ __device__ void solve_generic(const MjbModel& m, const MjbData& d, int w, int la
 constexpr int kSolverRows = MJB_JROWS;
 constexpr int kJld = 36;  // staged Jacobian rows: 32 columns (zero padded) + 4, float4-aligned
 
-__host__ __device__ __forceinline__ int solver_ld(int nv) { return nv | 1; }
 __host__ __device__ __forceinline__ int round4(int x) { return (x + 3) & ~3; }
-// per-warp layout: Ms (nv x ld) | Ls (nv x 33) | vs (32) | F (kSolverRows) | Js (kSolverRows x kJld)
-__host__ __device__ __forceinline__ int solver_js_offset(int nv) {
-  return round4(nv * solver_ld(nv) + nv * 33 + 32 + kSolverRows);
-}
+// per-warp layout, every part 16-byte aligned and every matrix row kTileLd = kJld = 36 floats (32
+// columns, zero padded past nv, + 4): Ls (the factor tile, nv rows) | Js (kSolverRows rows) |
+// Ms (qM, nv rows) | vs (32) | F (kSolverRows).  The tile comes first so the fused step can use
+// it for the mass-matrix factorisations too.  A lane reading its own row as float4 (8 lanes of a
+// quarter warp start 4 banks apart) has no bank conflict.
 __host__ __device__ __forceinline__ size_t solver_smem_floats(int nv) {
-  return size_t(solver_js_offset(nv)) + size_t(kSolverRows) * kJld;
+  return size_t(round4(tile_floats(nv) + kSolverRows * kJld + tile_floats(nv) + 32 + kSolverRows));
+}
+
+// sum_j a_j b_j over 32 columns of two 16-byte aligned rows (four partial sums)
+__device__ __forceinline__ float dot32(const float* a, const float* b) {
+  const float4* a4 = reinterpret_cast<const float4*>(a);
+  const float4* b4 = reinterpret_cast<const float4*>(b);
+  float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f;
+#pragma unroll
+  for (int q = 0; q < 8; q++) {
+    const float4 x = a4[q], y = b4[q];
+    s0 += x.x * y.x;
+    s1 += x.y * y.y;
+    s2 += x.z * y.z;
+    s3 += x.w * y.w;
+  }
+  return (s0 + s1) + (s2 + s3);
 }
 
 struct Small {
   const MjbModel& m;
   const MjbData& d;
-  int w, lane, nv, ldm, adr, n, ldj;
+  int w, lane, nv, adr, n, ldj;
   bool own;
+  bool reuse = false;           // keep the factor of H while the active set is unchanged
   bool factored = false;        // Ls holds the factor of H for the active set factored_mask
   unsigned factored_mask = 0u;
   float *Ms, *Ls, *vs, *F;
@@ -417,9 +434,7 @@ struct Small {
   __device__ __forceinline__ float mulM(float v) {
     vs[lane] = own ? v : 0.f;
     __syncwarp();
-    float s = 0.f;
-    if (own)
-      for (int j = 0; j < nv; j++) s += Ms[lane * ldm + j] * vs[j];
+    const float s = own ? dot32(Ms + lane * kTileLd, vs) : 0.f;
     __syncwarp();
     return s;
   }
@@ -430,6 +445,7 @@ struct Small {
   }
   __device__ __forceinline__ float rowdot(int k) const {
     const float* Jr = J + size_t(k) * ldj;
+    if (ldj == kJld) return dot32(Jr, vs);  // staged rows
     float s = 0.f;
     for (int j = 0; j < nv; j++) s += Jr[j] * vs[j];
     return s;
@@ -438,19 +454,26 @@ struct Small {
 
 // Newton step direction H^-1 grad for nv <= 32 (solver.py:234-290).  When `refactor` is set,
 // lane i assembles row i of H = tril(qM) + sum_k c_k J_k^T J_k in registers (c_k = D_k for active
-// rows, 0 otherwise; inactive rows are skipped), stores it to Ls (leading dimension 33) and factors
-// it in place; otherwise Ls already holds the factor of the same H.  The coefficients come from C
+// rows, 0 otherwise; inactive rows are skipped), stores it to the tile Ls and factors it in place;
+// otherwise Ls already holds the factor of the same H.  The coefficients come from C
 // (staged rows) or, when C is null, from the rows' active flags and D.  Returns element `lane` of the
 // solution.  Staged Jacobian rows (ldj == kJld) are read as float4 broadcasts.
-__device__ __noinline__ float newton_direction(const float* Ms, int ldm, const float* J, int ldj,
+__device__ __noinline__ float newton_direction(const float* Ms, const float* J, int ldj,
                                                const float* C, const int* act, const float* D,
                                                int n, float* Ls, int nv, float grad, int lane,
                                                bool refactor) {
   const bool own = lane < nv;
   if (refactor) {
-    float h[32];
+    float h[32];  // row `lane` of qM (columns past nv are zero; entries above the diagonal unused)
+    const float4* M4 = reinterpret_cast<const float4*>(Ms + min(lane, nv - 1) * kTileLd);
 #pragma unroll
-    for (int j = 0; j < 32; j++) h[j] = (own && j <= lane && j < nv) ? Ms[lane * ldm + j] : 0.f;
+    for (int q = 0; q < 8; q++) {
+      const float4 v = M4[q];
+      h[4 * q] = v.x;
+      h[4 * q + 1] = v.y;
+      h[4 * q + 2] = v.z;
+      h[4 * q + 3] = v.w;
+    }
     for (int k = 0; k < n; k++) {
       const float c = C ? C[k] : (act[k] ? D[k] : 0.f);
       if (c == 0.f) continue;
@@ -472,17 +495,15 @@ __device__ __noinline__ float newton_direction(const float* Ms, int ldm, const f
           if (j < nv) h[j] += a * Jr[j];
       }
     }
-    if (own) {
+    if (own) {  // the whole row (entries above the diagonal are never read)
+      float4* row = reinterpret_cast<float4*>(Ls + lane * kTileLd);
 #pragma unroll
-      for (int j = 0; j < 32; j++)
-        if (j <= lane) Ls[lane * 33 + j] = h[j];
+      for (int q = 0; q < 8; q++) row[q] = make_float4(h[4 * q], h[4 * q + 1], h[4 * q + 2], h[4 * q + 3]);
     }
     __syncwarp();
-    chol_lower(Ls, 33, nv, lane);
+    chol_tile(Ls, nv, lane);
   }
-  const float invd = own ? __frcp_rn(Ls[lane * 33 + lane]) : 0.f;
-  const float x = cho_solve32(Ls, 33, nv, invd, grad, lane);
-  return own ? x : 0.f;
+  return cho_solve_tile(Ls, nv, grad, lane);
 }
 
 // solver.py:75-173
@@ -530,11 +551,12 @@ __device__ void small_update_gradient(Small& s) {
     __syncwarp();
     return;
   }
-  // H depends on the solve's inputs only through the active set, so the factor of the previous
-  // call is reused (bit-identical) while the set of active rows is unchanged; rows past the
-  // first 32 are not tracked, so such worlds refactor every time
+  // H depends on the solve's inputs only through the active set, so with s.reuse the factor of
+  // the previous call is kept (bit-identical) while the set of active rows is unchanged; rows
+  // past the first 32 are not tracked, so such worlds refactor every time.  Without s.reuse every
+  // call refactors, as the reference does.
   const unsigned mask = __ballot_sync(WARP_FULL, lane < s.n && d.efc_active[s.adr + lane]);
-  const bool refactor = !s.factored || s.n > 32 || mask != s.factored_mask;
+  const bool refactor = !s.reuse || !s.factored || s.n > 32 || mask != s.factored_mask;
   const bool staged = s.ldj == kJld;  // unstaged rows keep F in efc_force, which must survive
   if (refactor && staged) {  // coefficient of each row in J^T D J: D when active, else 0
     for (int k = lane; k < s.n; k += 32) {
@@ -543,7 +565,7 @@ __device__ void small_update_gradient(Small& s) {
     }
     __syncwarp();
   }
-  s.Mgrad = newton_direction(s.Ms, s.ldm, s.J, s.ldj, staged ? s.F : nullptr, d.efc_active + s.adr,
+  s.Mgrad = newton_direction(s.Ms, s.J, s.ldj, staged ? s.F : nullptr, d.efc_active + s.adr,
                              d.efc_D + s.adr, s.n, s.Ls, nv, s.grad, lane, refactor);
   s.factored = true;
   s.factored_mask = mask;
@@ -693,16 +715,18 @@ __device__ void small_linesearch(Small& s) {
 }
 
 // solver.py:872-1000 for nv <= 32; sm: solver_smem_floats(nv) floats of warp-private scratch
-__device__ void solve_small(const MjbModel& m, const MjbData& d, int w, int lane, float* sm) {
-  const int nv = m.nv, ldm = solver_ld(nv);
+__device__ void solve_small(const MjbModel& m, const MjbData& d, int w, int lane, float* sm,
+                            bool reuse) {
+  const int nv = m.nv;
   const int adr = d.world_efcadr[w], n = d.world_nefc[w];
-  Small s{m, d, w, lane, nv, ldm, adr, n};
+  Small s{m, d, w, lane, nv, adr, n};
   s.own = lane < nv;
-  s.Ms = sm;
-  s.Ls = s.Ms + nv * ldm;
-  s.vs = s.Ls + nv * 33;
+  s.reuse = reuse;
+  s.Ls = sm;
+  float* Js = sm + tile_floats(nv);
+  s.Ms = Js + kSolverRows * kJld;
+  s.vs = s.Ms + tile_floats(nv);
   s.F = s.vs + 32;
-  float* Js = sm + solver_js_offset(nv);
   const float* Jg = d.efc_J + size_t(adr) * nv;
   if (n <= kSolverRows) {
     for (int r = 0; r < n; r++) {  // rows padded with zeros to 32 columns for float4 reads
@@ -717,8 +741,7 @@ __device__ void solve_small(const MjbModel& m, const MjbData& d, int w, int lane
     s.F = d.efc_force + adr;  // rows beyond the staged capacity broadcast through global memory
   }
   const float* qMg = d.qM + W(w, nv * nv);
-  if (lane < nv)
-    for (int i = 0; i < nv; i++) s.Ms[i * ldm + lane] = qMg[i * nv + lane];
+  for (int i = 0; i < nv; i++) s.Ms[i * kTileLd + lane] = lane < nv ? qMg[i * nv + lane] : 0.f;
   s.qacc = s.own ? d.qacc_warmstart[W(w, nv) + lane] : 0.f;
   s.qfs = s.own ? d.qfrc_smooth[W(w, nv) + lane] : 0.f;
   s.qas = s.own ? d.qacc_smooth[W(w, nv) + lane] : 0.f;
@@ -791,9 +814,10 @@ __device__ void solve_small(const MjbModel& m, const MjbData& d, int w, int lane
 
 // Dispatch: the register / shared-memory solver when nv <= 32 and the caller provides its scratch
 // (solver_smem_floats(nv) floats), else the generic solver with an nv x nv Hessian tile `hs`.
+// reuse: keep the Newton Hessian's factor across iterations with an unchanged active set.
 __device__ __forceinline__ void solve(const MjbModel& m, const MjbData& d, int w, int lane,
-                                      float* sm, float* hs) {
-  if (m.nv <= 32 && sm) solve_small(m, d, w, lane, sm);
+                                      float* sm, float* hs, bool reuse = false) {
+  if (m.nv <= 32 && sm) solve_small(m, d, w, lane, sm, reuse);
   else solve_generic(m, d, w, lane, hs);
 }
 

@@ -17,6 +17,15 @@
 #ifndef MJB_CHOL
 #define MJB_CHOL 0
 #endif
+// the shared-memory factor / solve routines: called (1) or inlined into each caller (0)
+#ifndef MJB_TILE_CALL
+#define MJB_TILE_CALL 1
+#endif
+#if MJB_TILE_CALL
+#define MJB_TILE_FN __noinline__
+#else
+#define MJB_TILE_FN __forceinline__
+#endif
 
 namespace mjb {
 
@@ -372,6 +381,79 @@ __device__ __forceinline__ float cho_solve32(const float* L, int ldl, int n, flo
 }
 
 
+// Per-warp factor tiles for blocks of n <= 32: rows of kTileLd floats in shared memory, 16-byte
+// aligned, so a lane reads its own row as float4 with no bank conflict (the 8 lanes of a quarter
+// warp start 4 banks apart); entries above the diagonal are never read.
+constexpr int kTileLd = 36;
+
+__host__ __device__ __forceinline__ int tile_floats(int nv) { return (nv < 32 ? nv : 32) * kTileLd; }
+
+// In-place Cholesky of an n x n (n <= 32) SPD tile (lower triangle): the arithmetic of chol_lower
+// (same partial sums, pivot and reciprocal) with float4 row reads.
+__device__ MJB_TILE_FN void chol_tile(float* A, int n, int lane) {
+  for (int k = 0; k < n; k++) {
+    const float* Ai = A + min(k + lane, n - 1) * kTileLd;  // lanes past the last row reuse it
+    const float* Ak = A + k * kTileLd;
+    float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f;
+    int m = 0;
+    for (; m + 3 < k; m += 4) {
+      const float4 a = *reinterpret_cast<const float4*>(Ai + m);
+      const float4 b = *reinterpret_cast<const float4*>(Ak + m);
+      s0 += a.x * b.x;
+      s1 += a.y * b.y;
+      s2 += a.z * b.z;
+      s3 += a.w * b.w;
+    }
+    for (; m < k; m++) s0 += Ai[m] * Ak[m];
+    const float s = Ai[k] - ((s0 + s1) + (s2 + s3));
+    const float lkk = sqrtf(__shfl_sync(WARP_FULL, s, 0));
+    const float inv = __frcp_rn(lkk);
+    __syncwarp();
+    if (lane == 0) A[k * kTileLd + k] = lkk;
+    else if (k + lane < n) A[(k + lane) * kTileLd + k] = s * inv;
+    __syncwarp();
+  }
+}
+
+// x = (L L^T)^-1 y for an n <= 32 tile factor; lane i holds y_i and returns x_i (the arithmetic of
+// cho_solve32).  The forward pass reads the lane's own row four columns at a time, the backward
+// pass row k across the lanes; neither load depends on the substitution chain.
+__device__ MJB_TILE_FN float cho_solve_tile(const float* L, int n, float y, int lane) {
+  const bool own = lane < n;
+  const float* Li = L + min(lane, n - 1) * kTileLd;
+  const float invd = own ? __frcp_rn(Li[lane]) : 0.f;
+  float z = own ? y : 0.f;
+  for (int q = 0; 4 * q < n; q++) {  // the lane's row, four columns per float4 read
+    const float4 l4 = *reinterpret_cast<const float4*>(Li + 4 * q);
+    const float lq[4] = {l4.x, l4.y, l4.z, l4.w};
+#pragma unroll
+    for (int t = 0; t < 4; t++) {
+      const int k = 4 * q + t;
+      if (k < n) {
+        const float zk = __shfl_sync(WARP_FULL, z, k) * __shfl_sync(WARP_FULL, invd, k);
+        if (lane == k) z = zk;
+        else if (lane > k && own) z -= lq[t] * zk;
+      }
+    }
+  }
+  float x = z;
+#pragma unroll 4
+  for (int k = n - 1; k >= 0; k--) {
+    const float lk = L[k * kTileLd + (lane < k ? lane : 0)];
+    const float xk = __shfl_sync(WARP_FULL, x, k) * __shfl_sync(WARP_FULL, invd, k);
+    if (lane == k) x = xk;
+    else if (lane < k) x -= lk * xk;
+  }
+  return own ? x : 0.f;
+}
+
+// Copies the lower triangle of an n <= 32 tile to L (leading dimension ld) with zeros above the
+// diagonal, one coalesced row at a time.
+__device__ __forceinline__ void tile_store_lower(const float* T, int n, float* L, int ld, int lane) {
+  for (int r = 0; r < n; r++)
+    if (lane < n) L[r * ld + lane] = lane <= r ? T[r * kTileLd + lane] : 0.f;
+}
+
 // x = (L L^T)^-1 y for the n x n lower factor at L (leading dimension ld); x may alias y.
 __device__ void warp_cho_solve(const float* L, int ld, int n, float* x, const float* y, int lane) {
   if (n <= 32) {
@@ -412,13 +494,29 @@ __device__ void warp_cho_solve(const float* L, int ld, int n, float* x, const fl
 // Factor every tree block of the nv x nv matrix M (+ scale * diag(dadd) when dadd is given) into
 // L: dense storage, zero outside the lower block triangles.  smooth.py:353-379 (tile_cholesky per
 // qLD_tile group) and the fused damping tiles of forward.py:195-232.
+// Dense Cholesky of each tree block of the inertia-like matrix M (+ scale * dadd on the diagonal)
+// into L (smooth.py:353-379, qLD_tile semantics; zeros outside the blocks' lower triangles).  With
+// a per-warp tile, blocks of n <= 32 are factored in shared memory and written back row by row;
+// the tile then holds the factor of the last block.
 __device__ void factor_blocks(const MjbModel& m, const float* M, float* L, int lane,
-                              const float* dadd = nullptr, float scale = 0.f) {
+                              const float* dadd = nullptr, float scale = 0.f, float* tile = nullptr) {
   const int nv = m.nv;
   for (int e = lane; e < nv * nv; e += 32) L[e] = 0.f;
   __syncwarp();
   for (int blk = 0; blk < m.nblock; blk++) {
     const int a = m.block_adr[blk], n = m.block_size[blk];
+    if (tile && n <= 32) {
+      for (int r = 0; r < n; r++) {  // coalesced row reads of the block
+        float v = lane < n ? M[(a + r) * nv + a + lane] : 0.f;
+        if (dadd && lane == r) v += scale * dadd[a + r];
+        tile[r * kTileLd + lane] = v;
+      }
+      __syncwarp();
+      chol_tile(tile, n, lane);
+      tile_store_lower(tile, n, L + a * nv + a, nv, lane);
+      __syncwarp();
+      continue;
+    }
     for (int i = lane; i < n; i += 32) {  // row i of the block's lower triangle (+ damping on the diagonal)
       const float* src = M + (a + i) * nv + a;
       float* dst = L + (a + i) * nv + a;
@@ -435,17 +533,29 @@ __device__ void factor_blocks(const MjbModel& m, const float* M, float* L, int l
   }
 }
 
-// x = M^-1 y per tree block from the block factor L (smooth.py:654-681); x may alias y
+// x = M^-1 y per tree block from the block factor L (smooth.py:654-681); x may alias y.  With a
+// tile, blocks of n <= 32 are staged into it row by row first, unless tile_has_factor says that
+// the tile already holds the factor of the model's only block.
 __device__ void solve_blocks(const MjbModel& m, const float* L, float* x, const float* y,
-                             int lane) {
+                             int lane, float* tile = nullptr, bool tile_has_factor = false) {
   const int nv = m.nv;
   for (int blk = 0; blk < m.nblock; blk++) {
     const int a = m.block_adr[blk], n = m.block_size[blk];
     if (n <= 32) {
-      const float* Lb = L + a * nv + a;
-      const float invd = lane < n ? 1.f / Lb[lane * nv + lane] : 0.f;
       const float yi = lane < n ? y[a + lane] : 0.f;
-      const float xi = cho_solve32(Lb, nv, n, invd, yi, lane);
+      float xi;
+      if (tile) {
+        if (!(tile_has_factor && m.nblock == 1)) {
+          for (int r = 0; r < n; r++)
+            if (lane < n) tile[r * kTileLd + lane] = L[(a + r) * nv + a + lane];
+          __syncwarp();
+        }
+        xi = cho_solve_tile(tile, n, yi, lane);
+      } else {
+        const float* Lb = L + a * nv + a;
+        const float invd = lane < n ? 1.f / Lb[lane * nv + lane] : 0.f;
+        xi = cho_solve32(Lb, nv, n, invd, yi, lane);
+      }
       __syncwarp();
       if (lane < n) x[a + lane] = xi;
       __syncwarp();
@@ -456,9 +566,9 @@ __device__ void solve_blocks(const MjbModel& m, const float* L, float* x, const 
 }
 
 // smooth.py:392-395
-__device__ void factor_m(const MjbModel& m, const MjbData& d, int w, int lane) {
+__device__ void factor_m(const MjbModel& m, const MjbData& d, int w, int lane, float* tile = nullptr) {
   const int nv = m.nv;
-  factor_blocks(m, d.qM + W(w, nv * nv), d.qLD + W(w, nv * nv), lane);
+  factor_blocks(m, d.qM + W(w, nv * nv), d.qLD + W(w, nv * nv), lane, nullptr, 0.f, tile);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -468,12 +578,13 @@ __device__ void transmission(const MjbModel& m, const MjbData& d, int w, int lan
   const float* qpos = d.qpos + W(w, m.nq);
   float* length = d.actuator_length + W(w, m.nu);
   float* moment = d.actuator_moment + W(w, m.nu * nv);
+  for (int e = lane; e < m.nu * nv; e += 32) moment[e] = 0.f;  // coalesced; then the nonzeros
+  __syncwarp();
   for (int a = lane; a < m.nu; a += 32) {
     const int j = m.actuator_trnid[2 * a], t = m.jnt_type[j];
     const int qa = m.jnt_qposadr[j], va = m.jnt_dofadr[j], trn = m.actuator_trntype[a];
     const float* gear = m.actuator_gear + 6 * a;
     float* mom = moment + a * nv;
-    for (int i = 0; i < nv; i++) mom[i] = 0.f;
     if (trn != 0 && trn != 1) continue;
     if (t == JNT_FREE) {
       length[a] = 0.f;
@@ -725,7 +836,9 @@ __device__ void xfrc_accumulate(const MjbModel& m, const MjbData& d, int w, floa
 }
 
 // forward.py:644-661
-__device__ void fwd_acceleration(const MjbModel& m, const MjbData& d, int w, int lane) {
+// tile_has_qLD: the per-warp tile still holds the factor left by factor_m
+__device__ void fwd_acceleration(const MjbModel& m, const MjbData& d, int w, int lane,
+                                 float* tile = nullptr, bool tile_has_qLD = false) {
   const int nv = m.nv;
   float* sm = d.qfrc_smooth + W(w, nv);
   const float* pas = d.qfrc_passive + W(w, nv);
@@ -735,7 +848,7 @@ __device__ void fwd_acceleration(const MjbModel& m, const MjbData& d, int w, int
   for (int i = lane; i < nv; i += 32) sm[i] = pas[i] - bias[i] + act[i] + app[i];
   __syncwarp();
   xfrc_accumulate(m, d, w, sm, lane);
-  solve_blocks(m, d.qLD + W(w, nv * nv), d.qacc_smooth + W(w, nv), sm, lane);
+  solve_blocks(m, d.qLD + W(w, nv * nv), d.qacc_smooth + W(w, nv), sm, lane, tile, tile_has_qLD);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -762,7 +875,7 @@ __device__ void advance(const MjbModel& m, const MjbData& d, int w, const float*
 }
 
 // forward.py:165-242 — Euler with implicit joint damping unless EULERDAMP is disabled
-__device__ void euler(const MjbModel& m, const MjbData& d, int w, int lane) {
+__device__ void euler(const MjbModel& m, const MjbData& d, int w, int lane, float* tile = nullptr) {
   const int nv = m.nv;
   if (m.disableflags & DSBL_EULERDAMP) {
     advance(m, d, w, d.qacc + W(w, nv), lane);
@@ -772,16 +885,16 @@ __device__ void euler(const MjbModel& m, const MjbData& d, int w, int lane) {
   float* x = d.qacc_integration + W(w, nv);
   const float* sm = d.qfrc_smooth + W(w, nv);
   const float* qc = d.qfrc_constraint + W(w, nv);
-  factor_blocks(m, d.qM + W(w, nv * nv), L, lane, m.dof_damping, m.timestep);
+  factor_blocks(m, d.qM + W(w, nv * nv), L, lane, m.dof_damping, m.timestep, tile);
   for (int i = lane; i < nv; i += 32) x[i] = sm[i] + qc[i];
   __syncwarp();
-  solve_blocks(m, L, x, x, lane);
+  solve_blocks(m, L, x, x, lane, tile, true);
   advance(m, d, w, x, lane);
 }
 
 // forward.py:245-405 — implicitfast (dense): (M - dt qDeriv) qacc = qfrc_smooth + qfrc_constraint
 // with qDeriv = moment^T diag(bias_vel + gain_vel * ctrl) moment - diag(damping)
-__device__ void implicit(const MjbModel& m, const MjbData& d, int w, int lane) {
+__device__ void implicit(const MjbModel& m, const MjbData& d, int w, int lane, float* tile = nullptr) {
   const int nv = m.nv, nu = m.nu;
   const bool passive_on = !(m.disableflags & DSBL_PASSIVE);
   const bool act_on = !(m.disableflags & DSBL_ACTUATION) && m.actuator_affine_bias_gain;
@@ -800,30 +913,49 @@ __device__ void implicit(const MjbModel& m, const MjbData& d, int w, int lane) {
     }
     __syncwarp();
   }
+  bool tiled = tile != nullptr;  // every block small enough for the tile
+  for (int blk = 0; blk < m.nblock; blk++) tiled &= m.block_size[blk] <= 32;
   const float* qM = d.qM + W(w, nv * nv);
   float* Mi = d.qM_integration + W(w, nv * nv);
-  for (int blk = 0; blk < m.nblock; blk++) {  // qderiv_actuator_fused_kernel, per tree tile
+  float* f = d.qfrc_integration + W(w, nv);
+  const float* sm = d.qfrc_smooth + W(w, nv);
+  const float* qc = d.qfrc_constraint + W(w, nv);
+  float* L = d.qLD_integration + W(w, nv * nv);
+  float* x = d.qacc_integration + W(w, nv);
+  for (int i = lane; i < nv; i += 32) f[i] = sm[i] + qc[i];
+  if (tiled)
+    for (int e = lane; e < nv * nv; e += 32) L[e] = 0.f;
+  __syncwarp();
+  // qderiv_actuator_fused_kernel, per tree tile: Mi = qM - dt qDeriv, one coalesced row at a time
+  for (int blk = 0; blk < m.nblock; blk++) {
     const int a0 = m.block_adr[blk], n = m.block_size[blk];
-    for (int ii = lane; ii < n; ii += 32) {
-      const int i = a0 + ii;
-      for (int j = a0; j < a0 + n; j++) {
+    for (int r = 0; r < n; r++) {
+      const int i = a0 + r;
+      for (int jj = lane; jj < n; jj += 32) {
+        const int j = a0 + jj;
         float qd = 0.f;
         if (act_on)
           for (int a = 0; a < nu; a++) qd += moment[a * nv + i] * vel[a] * moment[a * nv + j];
         if (passive_on && i == j) qd -= m.dof_damping[i];
-        Mi[i * nv + j] = qM[i * nv + j] - qd * m.timestep;
+        const float v = qM[i * nv + j] - qd * m.timestep;
+        Mi[i * nv + j] = v;
+        if (tiled) tile[r * kTileLd + jj] = v;
       }
     }
+    __syncwarp();
+    if (tiled) {  // factor and solve this block in the tile
+      chol_tile(tile, n, lane);
+      tile_store_lower(tile, n, L + a0 * nv + a0, nv, lane);
+      const float xi = cho_solve_tile(tile, n, lane < n ? f[a0 + lane] : 0.f, lane);
+      __syncwarp();
+      if (lane < n) x[a0 + lane] = xi;
+      __syncwarp();
+    }
   }
-  float* f = d.qfrc_integration + W(w, nv);
-  const float* sm = d.qfrc_smooth + W(w, nv);
-  const float* qc = d.qfrc_constraint + W(w, nv);
-  for (int i = lane; i < nv; i += 32) f[i] = sm[i] + qc[i];
-  __syncwarp();
-  float* L = d.qLD_integration + W(w, nv * nv);
-  float* x = d.qacc_integration + W(w, nv);
-  factor_blocks(m, Mi, L, lane);
-  solve_blocks(m, L, x, f, lane);
+  if (!tiled) {
+    factor_blocks(m, Mi, L, lane);
+    solve_blocks(m, L, x, f, lane);
+  }
   advance(m, d, w, x, lane);
 }
 

@@ -167,21 +167,28 @@ class Statistic:
   meaninertia: float = 1.0
 
 
+# Data scalars copied into the cached C-ABI view (every other non-tensor field is host-only)
+_VIEW_SCALARS = frozenset(("nworld", "nconmax", "njmax"))
+
+
 class _Struct:
   """Attribute bag whose array fields are torch tensors.
 
-  Assigning a field bumps ``_version`` so the cached C-ABI view of the owning Model/Data is
-  rebuilt before the next kernel launch (callers may swap arrays, as solver_test.py:251-258
-  does with the reference's Data).
+  Assigning an array field (or a capacity) drops the cached C-ABI view of the owning Model/Data
+  so it is rebuilt before the next kernel launch (callers may swap arrays, as
+  solver_test.py:251-258 does with the reference's Data); host scalars such as ``time`` do not.
   """
 
   def __init__(self, owner=None):
     object.__setattr__(self, "_owner", owner)
 
   def __setattr__(self, name, value):
-    if isinstance(value, torch.Tensor) and not isinstance(value, DeviceArray):
+    is_tensor = isinstance(value, torch.Tensor)
+    if is_tensor and not isinstance(value, DeviceArray):
       value = as_device_array(value)
     object.__setattr__(self, name, value)
+    if not is_tensor and name not in _VIEW_SCALARS:
+      return  # host scalars such as time do not enter the C-ABI view
     owner = self.__dict__.get("_owner")
     if owner is not None:
       owner._invalidate()

@@ -134,7 +134,7 @@ def test_humanoid_forward_all_fields():
   mjm = humanoid()
   qpos, qvel, ctrl = humanoid_state(mjm, 64, seed=5)
   m = mjw.put_model(mjm)
-  for fused in (True, False):
+  for fused in (1, 0, 2):
     d = device_data(mjm, qpos, qvel, ctrl)
     mjw.forward(m, d, fused=fused)
     o = oracle(mjm, qpos, qvel, ctrl, 64)

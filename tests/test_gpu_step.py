@@ -113,20 +113,26 @@ def test_sphere_chain_long_rollout():
   assert float(d.qpos[:, 2].min()) > 0.05  # the ball rests on the floor
 
 
-def test_fused_plain_agree_and_deterministic():
+def test_launch_forms_agree_and_deterministic():
+  """Chosen (1), plain (0) and single-kernel (2) forms: each bit-reproducible run to run, and the
+  smooth accelerations of all three within 1e-4 of each other."""
   mjm = humanoid()
   qpos, qvel, ctrl = humanoid_state(mjm, 64, seed=9)
   m = mjw.put_model(mjm)
-  outs = []
-  for fused in (True, True, False, False):
-    d = device_data(mjm, qpos, qvel, ctrl)
-    mjw.step(m, d, fused=fused)
-    outs.append((d.qpos.clone(), d.qvel.clone(), d.qacc_smooth.clone()))
-  for a, b in zip(outs[0], outs[1]):
-    assert torch.equal(a, b)
-  for a, b in zip(outs[2], outs[3]):
-    assert torch.equal(a, b)
-  assert_close(dev(outs[0][2]), dev(outs[2][2]), "qacc_smooth fused vs plain", rtol=1e-4, atol=1e-4)
+  outs = {}
+  for form in (1, 0, 2):
+    runs = []
+    for _ in range(2):
+      d = device_data(mjm, qpos, qvel, ctrl)
+      mjw.step(m, d, fused=form)
+      runs.append((d.qpos.clone(), d.qvel.clone(), d.qacc_smooth.clone()))
+    for a, b in zip(*runs):
+      assert torch.equal(a, b), form
+    outs[form] = runs[0]
+  for form in (0, 2):
+    assert_close(dev(outs[1][2]), dev(outs[form][2]), f"qacc_smooth chosen vs form {form}", rtol=1e-4, atol=1e-4)
+  with pytest.raises(ValueError):
+    mjw.step(m, device_data(mjm, qpos, qvel, ctrl), fused=3)
 
 
 def test_cuda_graph_replay_matches_eager():
