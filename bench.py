@@ -132,7 +132,7 @@ def _algorithmic_bytes(d, mjm, ncon, nefc):
 
 
 FORMS = {"plain": 0, "chosen": 1, "single": 2}
-LAUNCHES = {"plain": 16, "chosen": 4, "single": 2}  # kernels per step (mjb200.cu run_* paths)
+LAUNCHES = {"plain": 16, "chosen": 15, "single": 2}  # kernels per step (mjb200.cu run_* paths)
 
 
 def _solver_bytes(mjm, nworld, nefc):

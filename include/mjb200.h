@@ -133,7 +133,7 @@ typedef struct MjbData {
 /* Launch configuration for the step entry points. */
 /* Launch forms of mjb_step / mjb_forward (MjbRunCfg.fused; a null cfg selects MJB_FORM_CHOSEN). */
 #define MJB_FORM_PLAIN 0  /* one kernel per reference stage; Hessian refactored every iteration */
-#define MJB_FORM_CHOSEN 1 /* reset + smooth/collision/constraint kernel + solver + integrator */
+#define MJB_FORM_CHOSEN 1 /* stage kernels to fwd_acceleration + solver reusing its factor + integrator */
 #define MJB_FORM_SINGLE 2 /* the whole step of a world in one warp of one kernel */
 
 typedef struct MjbRunCfg {

@@ -5,10 +5,11 @@
 //  - plain (MJB_FORM_PLAIN): one kernel per reference stage function (mjb_kinematics,
 //    mjb_com_pos, ...), data passed between stages through the Data arrays in HBM, the Newton
 //    Hessian refactored in every iteration: the reference's launch sequence and algorithm;
-//  - chosen (MJB_FORM_CHOSEN, the default): a counter reset, then three kernels sized for their
-//    own register and shared-memory needs: k_smooth (fwd_position .. fwd_acceleration, 64
-//    registers, one factor tile per warp), k_solve (the solver, keeping the Hessian factor while
-//    the active set is unchanged) and k_integrate (Euler / implicitfast + the finiteness check);
+//  - chosen (MJB_FORM_CHOSEN, the default): the plain form's stage kernels up to
+//    fwd_acceleration (fusing them into one kernel measured slower: the fused collision and
+//    constraint stages cost more than the launches they save), then k_solve (the solver, keeping
+//    the Hessian factor while the active set is unchanged) and k_integrate (Euler / implicitfast
+//    and the finiteness check in one kernel);
 //  - single (MJB_FORM_SINGLE): every stage of a world inside one warp of one kernel.
 // No entry point allocates memory or synchronises the stream (except mjb_world_status, which
 // copies results to the host).
@@ -16,9 +17,10 @@
 
 #include "mjb_solver.cuh"
 
-// minimum resident CTAs per SM requested from the compiler (caps registers per thread)
+// minimum resident CTAs per SM requested for the solver kernels (caps registers per thread at
+// 65536 / (128 * MJB_MINB)); 5 measured fastest: 4 leaves occupancy on the table, 6 spills
 #ifndef MJB_MINB
-#define MJB_MINB 4
+#define MJB_MINB 5
 #endif
 
 namespace mjb {
@@ -111,28 +113,7 @@ __global__ void __launch_bounds__(128, MJB_MINB) k_step_fused(const MjbModel m, 
   }
 }
 
-// chosen form, kernel 1: fwd_position .. fwd_acceleration (forward.py:408-661) of one world per
-// warp; the warp's factor tile holds factor_m's factor until fwd_acceleration's solve
-__global__ void __launch_bounds__(128, 8) k_smooth(const MjbModel m, const MjbData d, int tile_per_warp) {
-  extern __shared__ __align__(16) float smem[];
-  const int lane = threadIdx.x & 31;
-  const int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  if (w >= d.nworld) return;
-  float* tile = smem + size_t(threadIdx.x >> 5) * tile_per_warp;
-  kinematics(m, d, w, lane);
-  com_pos(m, d, w, lane);
-  crb(m, d, w, lane);
-  factor_m(m, d, w, lane, tile);
-  collision(m, d, w, lane);
-  make_constraint(m, d, w, lane);
-  transmission(m, d, w, lane);
-  fwd_velocity(m, d, w, lane);
-  fwd_actuation(m, d, w, lane);
-  fwd_acceleration(m, d, w, lane, tile, true);
-  if (d.njmax == 0) copy_qacc_smooth(m, d, w, lane);
-}
-
-// chosen form, kernel 2: the constraint solver with the Hessian factor kept across iterations
+// chosen form: the constraint solver with the Hessian factor kept across iterations
 __global__ void __launch_bounds__(128, MJB_MINB) k_solve(const MjbModel m, const MjbData d, int smem_per_warp) {
   extern __shared__ __align__(16) float smem[];
   const int lane = threadIdx.x & 31;
@@ -142,7 +123,7 @@ __global__ void __launch_bounds__(128, MJB_MINB) k_solve(const MjbModel m, const
   solve(m, d, w, lane, sm, d.efc_h + W(w, m.nv * m.nv), true);
 }
 
-// chosen form, kernel 3: integration (forward.py:165-405) and the finiteness check
+// chosen form: integration (forward.py:165-405) and the finiteness check
 __global__ void __launch_bounds__(128, 8) k_integrate(const MjbModel m, const MjbData d, int tile_per_warp) {
   extern __shared__ __align__(16) float smem[];
   const int lane = threadIdx.x & 31;
@@ -297,9 +278,8 @@ void rebuild_index(const int* worldid, const int* counter, int cap, int* adr, in
   k_index_fix<<<grid_for(d->nworld, 4), 128, 0, s>>>(worldid, adr, cnt, d->world_status, d->nworld);
 }
 
-int run_forward_plain(const MjbModel* m, const MjbData* d, cudaStream_t s) {
+int run_forward_plain_nosolve(const MjbModel* m, const MjbData* d, cudaStream_t s) {
   int rc;
-  // fwd_position (forward.py:408-420)
   if ((rc = launch_stage<S_KINEMATICS>(m, d, s))) return rc;
   if ((rc = launch_stage<S_COM_POS>(m, d, s))) return rc;
   if ((rc = launch_stage<S_CRB>(m, d, s))) return rc;
@@ -309,25 +289,31 @@ int run_forward_plain(const MjbModel* m, const MjbData* d, cudaStream_t s) {
   if ((rc = launch_stage<S_NARROW>(m, d, s))) return rc;
   if ((rc = launch_stage<S_MAKE_CONSTRAINT>(m, d, s))) return rc;
   if ((rc = launch_stage<S_TRANSMISSION>(m, d, s))) return rc;
-  // fwd_velocity, fwd_actuation, fwd_acceleration
   if ((rc = launch_stage<S_FWD_VELOCITY>(m, d, s))) return rc;
   if ((rc = launch_stage<S_FWD_ACTUATION>(m, d, s))) return rc;
   if ((rc = launch_stage<S_FWD_ACCELERATION>(m, d, s))) return rc;
   if (d->njmax == 0) return launch_stage<S_QACC_SMOOTH_COPY>(m, d, s);
-  return launch_stage<S_SOLVE>(m, d, s);
+  return MJB_OK;
 }
 
-// the chosen form's phases: 0 = counter reset + k_smooth, 1 = k_solve, 2 = k_integrate
+int run_forward_plain(const MjbModel* m, const MjbData* d, cudaStream_t s) {
+  int rc;
+  if ((rc = run_forward_plain_nosolve(m, d, s))) return rc;
+  return d->njmax == 0 ? MJB_OK : launch_stage<S_SOLVE>(m, d, s);
+}
+
+// the chosen form's phases: 0 = status reset + the stage kernels up to fwd_acceleration,
+// 1 = k_solve, 2 = k_integrate
 int run_chosen_phase(const MjbModel* m, const MjbData* d, int phase, cudaStream_t s) {
   const int warps = kDefaultWarps;
   const int grid = grid_for(d->nworld, warps);
   const int tpw = tile_floats(m->nv);
   const size_t tile_bytes = size_t(tpw) * warps * sizeof(float);
-  static size_t conf_smooth[kSmemDevices], conf_solve[kSmemDevices], conf_int[kSmemDevices];
+  static size_t conf_solve[kSmemDevices], conf_int[kSmemDevices];
   if (phase == 0) {
-    reset_counters(d, true, true, true, true, s);
-    allow_smem(k_smooth, tile_bytes, conf_smooth);
-    k_smooth<<<grid, 32 * warps, tile_bytes, s>>>(*m, *d, tpw);
+    reset_counters(d, false, false, false, true, s);
+    int rc = run_forward_plain_nosolve(m, d, s);
+    if (rc) return rc;
   } else if (phase == 1) {
     if (d->njmax > 0) {
       const int spw = m->nv <= 32 ? int(solver_smem_floats(m->nv)) : 0;

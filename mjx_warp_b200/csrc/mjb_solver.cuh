@@ -386,30 +386,31 @@ __device__ __noinline__ void solve_generic(const MjbModel& m, const MjbData& d, 
 #define MJB_JROWS 32
 #endif
 constexpr int kSolverRows = MJB_JROWS;
-constexpr int kJld = 36;  // staged Jacobian rows: 32 columns (zero padded) + 4, float4-aligned
 
 __host__ __device__ __forceinline__ int round4(int x) { return (x + 3) & ~3; }
-// per-warp layout, every part 16-byte aligned and every matrix row kTileLd = kJld = 36 floats (32
-// columns, zero padded past nv, + 4): Ls (the factor tile, nv rows) | Js (kSolverRows rows) |
-// Ms (qM, nv rows) | vs (32) | F (kSolverRows).  The tile comes first so the fused step can use
-// it for the mass-matrix factorisations too.  A lane reading its own row as float4 (8 lanes of a
-// quarter warp start 4 banks apart) has no bank conflict.
+// Per-warp layout, every part 16-byte aligned, every matrix row tile_ld(nv) floats with the
+// columns from nv to the next multiple of 4 zero: Ls (the factor tile, nv rows) | Js (kSolverRows
+// rows) | Ms (qM, nv rows) | vs (32) | F (kSolverRows).  The tile comes first so the fused step can
+// use it for the mass-matrix factorisations too.  Lanes read their own rows as float4 without bank
+// conflicts (see tile_ld).
 __host__ __device__ __forceinline__ size_t solver_smem_floats(int nv) {
-  return size_t(round4(tile_floats(nv) + kSolverRows * kJld + tile_floats(nv) + 32 + kSolverRows));
+  return size_t(round4(2 * tile_floats(nv) + kSolverRows * tile_ld(nv) + 32 + kSolverRows));
 }
 
-// sum_j a_j b_j over 32 columns of two 16-byte aligned rows (four partial sums)
-__device__ __forceinline__ float dot32(const float* a, const float* b) {
+// sum_j a_j b_j over the first 4 * nq columns of two 16-byte aligned rows (four partial sums)
+__device__ __forceinline__ float dotq(const float* a, const float* b, int nq) {
   const float4* a4 = reinterpret_cast<const float4*>(a);
   const float4* b4 = reinterpret_cast<const float4*>(b);
   float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f;
 #pragma unroll
   for (int q = 0; q < 8; q++) {
-    const float4 x = a4[q], y = b4[q];
-    s0 += x.x * y.x;
-    s1 += x.y * y.y;
-    s2 += x.z * y.z;
-    s3 += x.w * y.w;
+    if (q < nq) {
+      const float4 x = a4[q], y = b4[q];
+      s0 += x.x * y.x;
+      s1 += x.y * y.y;
+      s2 += x.z * y.z;
+      s3 += x.w * y.w;
+    }
   }
   return (s0 + s1) + (s2 + s3);
 }
@@ -418,6 +419,8 @@ struct Small {
   const MjbModel& m;
   const MjbData& d;
   int w, lane, nv, adr, n, ldj;
+  int ld, nq;                   // staged row stride and float4 count per row (4 * nq >= nv)
+  bool staged;                  // J rows copied to shared memory (else read from efc_J)
   bool own;
   bool reuse = false;           // keep the factor of H while the active set is unchanged
   bool factored = false;        // Ls holds the factor of H for the active set factored_mask
@@ -434,7 +437,7 @@ struct Small {
   __device__ __forceinline__ float mulM(float v) {
     vs[lane] = own ? v : 0.f;
     __syncwarp();
-    const float s = own ? dot32(Ms + lane * kTileLd, vs) : 0.f;
+    const float s = own ? dotq(Ms + lane * ld, vs, nq) : 0.f;
     __syncwarp();
     return s;
   }
@@ -445,7 +448,7 @@ struct Small {
   }
   __device__ __forceinline__ float rowdot(int k) const {
     const float* Jr = J + size_t(k) * ldj;
-    if (ldj == kJld) return dot32(Jr, vs);  // staged rows
+    if (staged) return dotq(Jr, vs, nq);
     float s = 0.f;
     for (int j = 0; j < nv; j++) s += Jr[j] * vs[j];
     return s;
@@ -457,18 +460,19 @@ struct Small {
 // rows, 0 otherwise; inactive rows are skipped), stores it to the tile Ls and factors it in place;
 // otherwise Ls already holds the factor of the same H.  The coefficients come from C
 // (staged rows) or, when C is null, from the rows' active flags and D.  Returns element `lane` of the
-// solution.  Staged Jacobian rows (ldj == kJld) are read as float4 broadcasts.
-__device__ __noinline__ float newton_direction(const float* Ms, const float* J, int ldj,
-                                               const float* C, const int* act, const float* D,
-                                               int n, float* Ls, int nv, float grad, int lane,
-                                               bool refactor) {
+// solution.  Staged Jacobian rows are read as float4 broadcasts.
+__device__ __noinline__ float newton_direction(const float* Ms, int ld, const float* J, int ldj,
+                                               bool staged, const float* C, const int* act,
+                                               const float* D, int n, float* Ls, int nv,
+                                               float grad, int lane, bool refactor) {
+  const int nq = (nv + 3) >> 2;
   const bool own = lane < nv;
   if (refactor) {
     float h[32];  // row `lane` of qM (columns past nv are zero; entries above the diagonal unused)
-    const float4* M4 = reinterpret_cast<const float4*>(Ms + min(lane, nv - 1) * kTileLd);
+    const float4* M4 = reinterpret_cast<const float4*>(Ms + min(lane, nv - 1) * ld);
 #pragma unroll
     for (int q = 0; q < 8; q++) {
-      const float4 v = M4[q];
+      const float4 v = q < nq ? M4[q] : make_float4(0.f, 0.f, 0.f, 0.f);
       h[4 * q] = v.x;
       h[4 * q + 1] = v.y;
       h[4 * q + 2] = v.z;
@@ -479,11 +483,11 @@ __device__ __noinline__ float newton_direction(const float* Ms, const float* J, 
       if (c == 0.f) continue;
       const float* Jr = J + size_t(k) * ldj;
       const float a = own ? c * Jr[lane] : 0.f;
-      if (ldj == kJld) {  // zero-padded to 32 columns, 16-byte aligned rows
+      if (staged) {  // zero-padded, 16-byte aligned rows
         const float4* J4 = reinterpret_cast<const float4*>(Jr);
 #pragma unroll
         for (int q = 0; q < 8; q++) {
-          const float4 v = J4[q];
+          const float4 v = q < nq ? J4[q] : make_float4(0.f, 0.f, 0.f, 0.f);
           h[4 * q] += a * v.x;
           h[4 * q + 1] += a * v.y;
           h[4 * q + 2] += a * v.z;
@@ -496,14 +500,15 @@ __device__ __noinline__ float newton_direction(const float* Ms, const float* J, 
       }
     }
     if (own) {  // the whole row (entries above the diagonal are never read)
-      float4* row = reinterpret_cast<float4*>(Ls + lane * kTileLd);
+      float4* row = reinterpret_cast<float4*>(Ls + lane * ld);
 #pragma unroll
-      for (int q = 0; q < 8; q++) row[q] = make_float4(h[4 * q], h[4 * q + 1], h[4 * q + 2], h[4 * q + 3]);
+      for (int q = 0; q < 8; q++)
+        if (q < nq) row[q] = make_float4(h[4 * q], h[4 * q + 1], h[4 * q + 2], h[4 * q + 3]);
     }
     __syncwarp();
-    chol_tile(Ls, nv, lane);
+    chol_tile(Ls, ld, nv, lane);
   }
-  return cho_solve_tile(Ls, nv, grad, lane);
+  return cho_solve_tile(Ls, ld, nv, grad, lane);
 }
 
 // solver.py:75-173
@@ -557,7 +562,7 @@ __device__ void small_update_gradient(Small& s) {
   // call refactors, as the reference does.
   const unsigned mask = __ballot_sync(WARP_FULL, lane < s.n && d.efc_active[s.adr + lane]);
   const bool refactor = !s.reuse || !s.factored || s.n > 32 || mask != s.factored_mask;
-  const bool staged = s.ldj == kJld;  // unstaged rows keep F in efc_force, which must survive
+  const bool staged = s.staged;  // unstaged rows keep F in efc_force, which must survive
   if (refactor && staged) {  // coefficient of each row in J^T D J: D when active, else 0
     for (int k = lane; k < s.n; k += 32) {
       const int r = s.adr + k;
@@ -565,8 +570,9 @@ __device__ void small_update_gradient(Small& s) {
     }
     __syncwarp();
   }
-  s.Mgrad = newton_direction(s.Ms, s.J, s.ldj, staged ? s.F : nullptr, d.efc_active + s.adr,
-                             d.efc_D + s.adr, s.n, s.Ls, nv, s.grad, lane, refactor);
+  s.Mgrad = newton_direction(s.Ms, s.ld, s.J, s.ldj, staged, staged ? s.F : nullptr,
+                             d.efc_active + s.adr, d.efc_D + s.adr, s.n, s.Ls, nv, s.grad, lane,
+                             refactor);
   s.factored = true;
   s.factored_mask = mask;
 }
@@ -722,26 +728,30 @@ __device__ void solve_small(const MjbModel& m, const MjbData& d, int w, int lane
   Small s{m, d, w, lane, nv, adr, n};
   s.own = lane < nv;
   s.reuse = reuse;
+  s.ld = tile_ld(nv);
+  s.nq = (nv + 3) >> 2;
   s.Ls = sm;
   float* Js = sm + tile_floats(nv);
-  s.Ms = Js + kSolverRows * kJld;
+  s.Ms = Js + kSolverRows * s.ld;
   s.vs = s.Ms + tile_floats(nv);
   s.F = s.vs + 32;
+  const int ncol = 4 * s.nq;  // staged columns: nv, zero padded to a multiple of 4
   const float* Jg = d.efc_J + size_t(adr) * nv;
   if (n <= kSolverRows) {
-    for (int r = 0; r < n; r++) {  // rows padded with zeros to 32 columns for float4 reads
-      const float v = lane < nv ? Jg[size_t(r) * nv + lane] : 0.f;
-      Js[r * kJld + lane] = v;
-    }
+    for (int r = 0; r < n; r++)  // rows zero padded for float4 reads
+      if (lane < ncol) Js[r * s.ld + lane] = lane < nv ? Jg[size_t(r) * nv + lane] : 0.f;
     s.J = Js;
-    s.ldj = kJld;
+    s.ldj = s.ld;
+    s.staged = true;
   } else {
     s.J = Jg;
     s.ldj = nv;
+    s.staged = false;
     s.F = d.efc_force + adr;  // rows beyond the staged capacity broadcast through global memory
   }
   const float* qMg = d.qM + W(w, nv * nv);
-  for (int i = 0; i < nv; i++) s.Ms[i * kTileLd + lane] = lane < nv ? qMg[i * nv + lane] : 0.f;
+  for (int i = 0; i < nv; i++)
+    if (lane < ncol) s.Ms[i * s.ld + lane] = lane < nv ? qMg[i * nv + lane] : 0.f;
   s.qacc = s.own ? d.qacc_warmstart[W(w, nv) + lane] : 0.f;
   s.qfs = s.own ? d.qfrc_smooth[W(w, nv) + lane] : 0.f;
   s.qas = s.own ? d.qacc_smooth[W(w, nv) + lane] : 0.f;

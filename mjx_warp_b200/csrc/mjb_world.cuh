@@ -381,21 +381,27 @@ __device__ __forceinline__ float cho_solve32(const float* L, int ldl, int n, flo
 }
 
 
-// Per-warp factor tiles for blocks of n <= 32: rows of kTileLd floats in shared memory, 16-byte
-// aligned, so a lane reads its own row as float4 with no bank conflict (the 8 lanes of a quarter
-// warp start 4 banks apart); entries above the diagonal are never read.
-constexpr int kTileLd = 36;
+// Per-warp factor tiles for blocks of n <= 32 in shared memory.  Rows are tile_ld(nv) floats:
+// the padded width 4 * ceil(n / 4) rounded so that ld / 4 is odd, which keeps rows 16-byte
+// aligned and lets the 8 lanes of a quarter warp read their own rows as float4 from 8 distinct
+// groups of 4 banks (no conflict); entries above the diagonal are never read.
+__host__ __device__ __forceinline__ int tile_ld(int nv) {
+  const int r = ((nv < 32 ? nv : 32) + 3) & ~3;
+  return (r & 4) ? r : r + 4;
+}
+__host__ __device__ __forceinline__ int tile_floats(int nv) {
+  return (nv < 32 ? nv : 32) * tile_ld(nv);
+}
 
-__host__ __device__ __forceinline__ int tile_floats(int nv) { return (nv < 32 ? nv : 32) * kTileLd; }
-
-// In-place Cholesky of an n x n (n <= 32) SPD tile (lower triangle): the arithmetic of chol_lower
-// (same partial sums, pivot and reciprocal) with float4 row reads.
-__device__ MJB_TILE_FN void chol_tile(float* A, int n, int lane) {
+// In-place Cholesky of an n x n (n <= 32) SPD tile with row stride ld (lower triangle): the
+// arithmetic of chol_lower (same partial sums, pivot and reciprocal) with float4 row reads.
+__device__ MJB_TILE_FN void chol_tile(float* A, int ld, int n, int lane) {
   for (int k = 0; k < n; k++) {
-    const float* Ai = A + min(k + lane, n - 1) * kTileLd;  // lanes past the last row reuse it
-    const float* Ak = A + k * kTileLd;
+    const float* Ai = A + min(k + lane, n - 1) * ld;  // lanes past the last row reuse it
+    const float* Ak = A + k * ld;
     float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f;
     int m = 0;
+#pragma unroll 4
     for (; m + 3 < k; m += 4) {
       const float4 a = *reinterpret_cast<const float4*>(Ai + m);
       const float4 b = *reinterpret_cast<const float4*>(Ak + m);
@@ -409,8 +415,8 @@ __device__ MJB_TILE_FN void chol_tile(float* A, int n, int lane) {
     const float lkk = sqrtf(__shfl_sync(WARP_FULL, s, 0));
     const float inv = __frcp_rn(lkk);
     __syncwarp();
-    if (lane == 0) A[k * kTileLd + k] = lkk;
-    else if (k + lane < n) A[(k + lane) * kTileLd + k] = s * inv;
+    if (lane == 0) A[k * ld + k] = lkk;
+    else if (k + lane < n) A[(k + lane) * ld + k] = s * inv;
     __syncwarp();
   }
 }
@@ -418,9 +424,9 @@ __device__ MJB_TILE_FN void chol_tile(float* A, int n, int lane) {
 // x = (L L^T)^-1 y for an n <= 32 tile factor; lane i holds y_i and returns x_i (the arithmetic of
 // cho_solve32).  The forward pass reads the lane's own row four columns at a time, the backward
 // pass row k across the lanes; neither load depends on the substitution chain.
-__device__ MJB_TILE_FN float cho_solve_tile(const float* L, int n, float y, int lane) {
+__device__ MJB_TILE_FN float cho_solve_tile(const float* L, int ld, int n, float y, int lane) {
   const bool own = lane < n;
-  const float* Li = L + min(lane, n - 1) * kTileLd;
+  const float* Li = L + min(lane, n - 1) * ld;
   const float invd = own ? __frcp_rn(Li[lane]) : 0.f;
   float z = own ? y : 0.f;
   for (int q = 0; 4 * q < n; q++) {  // the lane's row, four columns per float4 read
@@ -439,7 +445,7 @@ __device__ MJB_TILE_FN float cho_solve_tile(const float* L, int n, float y, int 
   float x = z;
 #pragma unroll 4
   for (int k = n - 1; k >= 0; k--) {
-    const float lk = L[k * kTileLd + (lane < k ? lane : 0)];
+    const float lk = L[k * ld + (lane < k ? lane : 0)];
     const float xk = __shfl_sync(WARP_FULL, x, k) * __shfl_sync(WARP_FULL, invd, k);
     if (lane == k) x = xk;
     else if (lane < k) x -= lk * xk;
@@ -449,9 +455,9 @@ __device__ MJB_TILE_FN float cho_solve_tile(const float* L, int n, float y, int 
 
 // Copies the lower triangle of an n <= 32 tile to L (leading dimension ld) with zeros above the
 // diagonal, one coalesced row at a time.
-__device__ __forceinline__ void tile_store_lower(const float* T, int n, float* L, int ld, int lane) {
+__device__ __forceinline__ void tile_store_lower(const float* T, int tld, int n, float* L, int ld, int lane) {
   for (int r = 0; r < n; r++)
-    if (lane < n) L[r * ld + lane] = lane <= r ? T[r * kTileLd + lane] : 0.f;
+    if (lane < n) L[r * ld + lane] = lane <= r ? T[r * tld + lane] : 0.f;
 }
 
 // x = (L L^T)^-1 y for the n x n lower factor at L (leading dimension ld); x may alias y.
@@ -506,14 +512,17 @@ __device__ void factor_blocks(const MjbModel& m, const float* M, float* L, int l
   for (int blk = 0; blk < m.nblock; blk++) {
     const int a = m.block_adr[blk], n = m.block_size[blk];
     if (tile && n <= 32) {
+      const int tld = tile_ld(nv);
       for (int r = 0; r < n; r++) {  // coalesced row reads of the block
-        float v = lane < n ? M[(a + r) * nv + a + lane] : 0.f;
-        if (dadd && lane == r) v += scale * dadd[a + r];
-        tile[r * kTileLd + lane] = v;
+        if (lane < n) {
+          float v = M[(a + r) * nv + a + lane];
+          if (dadd && lane == r) v += scale * dadd[a + r];
+          tile[r * tld + lane] = v;
+        }
       }
       __syncwarp();
-      chol_tile(tile, n, lane);
-      tile_store_lower(tile, n, L + a * nv + a, nv, lane);
+      chol_tile(tile, tld, n, lane);
+      tile_store_lower(tile, tld, n, L + a * nv + a, nv, lane);
       __syncwarp();
       continue;
     }
@@ -545,12 +554,13 @@ __device__ void solve_blocks(const MjbModel& m, const float* L, float* x, const 
       const float yi = lane < n ? y[a + lane] : 0.f;
       float xi;
       if (tile) {
+        const int tld = tile_ld(nv);
         if (!(tile_has_factor && m.nblock == 1)) {
           for (int r = 0; r < n; r++)
-            if (lane < n) tile[r * kTileLd + lane] = L[(a + r) * nv + a + lane];
+            if (lane < n) tile[r * tld + lane] = L[(a + r) * nv + a + lane];
           __syncwarp();
         }
-        xi = cho_solve_tile(tile, n, yi, lane);
+        xi = cho_solve_tile(tile, tld, n, yi, lane);
       } else {
         const float* Lb = L + a * nv + a;
         const float invd = lane < n ? 1.f / Lb[lane * nv + lane] : 0.f;
@@ -939,14 +949,15 @@ __device__ void implicit(const MjbModel& m, const MjbData& d, int w, int lane, f
         if (passive_on && i == j) qd -= m.dof_damping[i];
         const float v = qM[i * nv + j] - qd * m.timestep;
         Mi[i * nv + j] = v;
-        if (tiled) tile[r * kTileLd + jj] = v;
+        if (tiled) tile[r * tile_ld(nv) + jj] = v;
       }
     }
     __syncwarp();
     if (tiled) {  // factor and solve this block in the tile
-      chol_tile(tile, n, lane);
-      tile_store_lower(tile, n, L + a0 * nv + a0, nv, lane);
-      const float xi = cho_solve_tile(tile, n, lane < n ? f[a0 + lane] : 0.f, lane);
+      const int tld = tile_ld(nv);
+      chol_tile(tile, tld, n, lane);
+      tile_store_lower(tile, tld, n, L + a0 * nv + a0, nv, lane);
+      const float xi = cho_solve_tile(tile, tld, n, lane < n ? f[a0 + lane] : 0.f, lane);
       __syncwarp();
       if (lane < n) x[a0 + lane] = xi;
       __syncwarp();
