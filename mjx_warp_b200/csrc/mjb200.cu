@@ -33,6 +33,10 @@ enum Stage {
 
 constexpr int kDefaultWarps = 4;
 
+// Kernels take the Model / Data views by value as __grid_constant__ parameters: the stages receive
+// them by reference, and without the qualifier every thread would copy both structs (~1.6 KB)
+// into its local memory whenever a reference reaches a function that is not inlined.
+
 // NaN / Inf check of the integrated state (sets MJB_WS_NONFINITE)
 __device__ void check_finite(const MjbModel& m, const MjbData& d, int w, int lane) {
   bool bad = false;
@@ -52,7 +56,7 @@ __device__ __forceinline__ void copy_qacc_smooth(const MjbModel& m, const MjbDat
 // the solver needs up to 128 registers; every other stage is held to 64 for occupancy
 template <int STAGE>
 __global__ void __launch_bounds__(128, STAGE == S_SOLVE ? MJB_MINB : 8)
-    k_stage(const MjbModel m, const MjbData d, int smem_per_warp) {
+    k_stage(const __grid_constant__ MjbModel m, const __grid_constant__ MjbData d, int smem_per_warp) {
   extern __shared__ __align__(16) float smem[];
   const int lane = threadIdx.x & 31;
   const int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
@@ -84,7 +88,7 @@ __global__ void __launch_bounds__(128, STAGE == S_SOLVE ? MJB_MINB : 8)
 // whole forward (+ integration) of one world per warp; each warp's slice of dynamic shared memory
 // holds the solver's workspace, whose leading factor tile also serves the mass-matrix
 // factorisations (factor_m, then the integrator)
-__global__ void __launch_bounds__(128, MJB_MINB) k_step_fused(const MjbModel m, const MjbData d, int integrate,
+__global__ void __launch_bounds__(128, MJB_MINB) k_step_fused(const __grid_constant__ MjbModel m, const __grid_constant__ MjbData d, int integrate,
                                                     int smem_per_warp) {
   extern __shared__ __align__(16) float smem[];
   const int lane = threadIdx.x & 31;
@@ -114,7 +118,7 @@ __global__ void __launch_bounds__(128, MJB_MINB) k_step_fused(const MjbModel m, 
 }
 
 // chosen form: the constraint solver with the Hessian factor kept across iterations
-__global__ void __launch_bounds__(128, MJB_MINB) k_solve(const MjbModel m, const MjbData d, int smem_per_warp) {
+__global__ void __launch_bounds__(128, MJB_MINB) k_solve(const __grid_constant__ MjbModel m, const __grid_constant__ MjbData d, int smem_per_warp) {
   extern __shared__ __align__(16) float smem[];
   const int lane = threadIdx.x & 31;
   const int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
@@ -124,7 +128,7 @@ __global__ void __launch_bounds__(128, MJB_MINB) k_solve(const MjbModel m, const
 }
 
 // chosen form: integration (forward.py:165-405) and the finiteness check
-__global__ void __launch_bounds__(128, 8) k_integrate(const MjbModel m, const MjbData d, int tile_per_warp) {
+__global__ void __launch_bounds__(128, 8) k_integrate(const __grid_constant__ MjbModel m, const __grid_constant__ MjbData d, int tile_per_warp) {
   extern __shared__ __align__(16) float smem[];
   const int lane = threadIdx.x & 31;
   const int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
@@ -185,7 +189,7 @@ __global__ void k_index_fix(const int* worldid, int* adr, int* cnt, uint32_t* st
 }
 
 // support.py:35-137 — res = M vec per world unless skip[w]
-__global__ void k_mul_m(const MjbModel m, const MjbData d, float* res, const float* vec,
+__global__ void k_mul_m(const __grid_constant__ MjbModel m, const __grid_constant__ MjbData d, float* res, const float* vec,
                         const uint8_t* skip) {
   const int lane = threadIdx.x & 31;
   const int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
@@ -193,13 +197,13 @@ __global__ void k_mul_m(const MjbModel m, const MjbData d, float* res, const flo
   if (skip && skip[w]) return;
   mul_m_world(d.qM + W(w, m.nv * m.nv), m.nv, res + W(w, m.nv), vec + W(w, m.nv), lane);
 }
-__global__ void k_solve_m(const MjbModel m, const MjbData d, float* x, const float* y) {
+__global__ void k_solve_m(const __grid_constant__ MjbModel m, const __grid_constant__ MjbData d, float* x, const float* y) {
   const int lane = threadIdx.x & 31;
   const int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   if (w >= d.nworld) return;
   solve_blocks(m, d.qLD + W(w, m.nv * m.nv), x + W(w, m.nv), y + W(w, m.nv), lane);
 }
-__global__ void k_xfrc(const MjbModel m, const MjbData d, float* qfrc) {
+__global__ void k_xfrc(const __grid_constant__ MjbModel m, const __grid_constant__ MjbData d, float* qfrc) {
   const int lane = threadIdx.x & 31;
   const int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   if (w >= d.nworld) return;
