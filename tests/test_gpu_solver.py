@@ -139,3 +139,23 @@ def test_many_rows_past_the_staged_capacity():
   assert e.max() < 1e-3, e.max()
   ef = d.efc.force.cpu().numpy()[idx]
   np.testing.assert_allclose(ef, f.ravel(), rtol=1e-3, atol=1e-3 * np.abs(f).max())
+
+
+def test_reused_factor_matches_refactoring():
+  """The chosen form keeps the Newton factor across iterations while the active set is unchanged;
+  with a converged solve it must agree with the plain form, which refactors H in every iteration
+  as the reference does."""
+  mjm = humanoid(iterations=15, ls_iterations=20)
+  qpos, qvel, ctrl = humanoid_state(mjm, 256, seed=11)
+  m = mjw.put_model(mjm)
+  out = []
+  for form in (0, 1):
+    d = device_data(mjm, qpos, qvel, ctrl)
+    for _ in range(5):  # into contact, so the active sets change between iterations
+      mjw.step(m, d, fused=0)
+    mjw.forward(m, d, fused=form)
+    torch.cuda.synchronize()
+    out.append((dev(d.qacc), d.efc.cost.cpu().numpy()))
+  e = rel_err(out[1][0], out[0][0])
+  assert np.median(e) < 1e-5 and e.max() < 1e-3, (np.median(e), e.max())
+  np.testing.assert_allclose(out[1][1], out[0][1], rtol=1e-4, atol=1e-4)
