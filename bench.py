@@ -18,6 +18,9 @@ around its own launch (mjw.step_phase) over K steps.  Multi-GPU: one process per
 each owning its own 8192 worlds (replicas, weak scaling, no collective on the data path); time is
 the maximum over ranks of CUDA-event time between barriers.
 
+qacc_err (rank 0): one forward from the bench state in every launch form, checked against the
+FP64 CPU restatement (the oracle, used only as the checker) on the first 256 worlds.
+
 --impl reference times the reference algorithm's CPU implementation available here — the CPU
 restatement under oracle/, FP32, all host threads — on the same workload.
 """
@@ -147,6 +150,37 @@ def _solver_bytes(mjm, nworld, nefc):
 
 
 STATE = ("qpos", "qvel", "act", "ctrl", "qacc_warmstart")
+
+
+def _qacc_error(mjm, m, d, mjw, torch, restore, forms, sample=256):
+  """qacc of one forward from the bench state (after the warm-up steps), per launch form, against
+  the FP64 CPU restatement with the same solver settings on the first `sample` worlds:
+  per-world ||qacc - qacc_fp64|| / max(||qacc_fp64||, 1)."""
+  from oracle import Oracle
+
+  restore()
+  torch.cuda.synchronize()
+  s = min(sample, d.nworld)
+  host = {k: getattr(d, k)[:s].double().cpu().numpy() for k in ("qpos", "qvel", "ctrl",
+                                                                "qacc_warmstart")}
+  o = Oracle(mjm, s, 64)
+  for k, v in host.items():
+    o.set(k, v)
+  o.run("forward", nthreads=os.cpu_count() or 1)
+  ref = o.get("qacc")
+  finite = np.all(np.isfinite(ref), axis=1)
+  out = {"vs": "FP64 CPU restatement, same solver settings (3 Newton it / ls 4)",
+         "worlds": int(finite.sum())}
+  for name, f in forms.items():
+    restore()
+    mjw.forward(m, d, fused=f)
+    q = d.qacc[:s].double().cpu().numpy()
+    e = (np.linalg.norm(q - ref, axis=1) / np.maximum(np.linalg.norm(ref, axis=1), 1.0))[finite]
+    e = np.where(np.isfinite(e), e, np.inf)
+    out[name] = {"median": float(np.median(e)), "p90": float(np.quantile(e, 0.9)),
+                 "max": float(e.max()), "frac_le_1e-4": float(np.mean(e <= 1e-4))}
+  restore()
+  return out
 
 
 def _graph_steps_per_s(torch, step, nworld, steps, barrier, restore):
@@ -291,6 +325,10 @@ def run_ours(args):
     el = replicas.max_over_ranks(el, device="cuda")
     forms[name] = {"value": nworld * world_size * args.steps / el, "ms_per_step": el / args.steps * 1e3}
 
+  accuracy = None
+  if rank == 0 and not args.no_accuracy:
+    accuracy = _qacc_error(mjm, m, d, mjw, torch, restore, FORMS)
+
   launches_per_step = LAUNCHES[args.form]
   total_worlds = nworld * world_size
   value = total_worlds * args.steps / elapsed
@@ -335,6 +373,8 @@ def run_ours(args):
     "status": {"nonfinite_worlds": nonfinite, "overflow_worlds": overflow,
                "mean_contacts_per_world": ncon / nworld, "mean_efc_rows_per_world": nefc / nworld},
   }
+  if accuracy is not None:
+    line["qacc_err"] = accuracy
   if rank == 0 and not args.no_cpu_baseline:
     line["cpu_baseline"] = cpu_baseline(mjm, budget_s=args.cpu_seconds)
   del g
@@ -398,6 +438,7 @@ def main():
   p.add_argument("--nworld", type=int, default=NWORLD)
   p.add_argument("--cpu-seconds", type=float, default=10.0)
   p.add_argument("--no-cpu-baseline", action="store_true")
+  p.add_argument("--no-accuracy", action="store_true")
   args = p.parse_args()
   if args.warmup < 3:
     args.warmup = 3
