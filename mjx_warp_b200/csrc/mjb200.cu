@@ -15,6 +15,8 @@
 // copies results to the host).
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "mjb_solver.cuh"
 
 // minimum resident CTAs per SM requested for the solver kernels (caps registers per thread at
@@ -28,7 +30,7 @@ namespace mjb {
 enum Stage {
   S_KINEMATICS, S_COM_POS, S_CRB, S_FACTOR_M, S_TRANSMISSION, S_COM_VEL, S_PASSIVE, S_RNE,
   S_FWD_VELOCITY, S_FWD_ACTUATION, S_FWD_ACCELERATION, S_NXN, S_NARROW, S_MAKE_CONSTRAINT,
-  S_SOLVE, S_EULER, S_IMPLICIT, S_QACC_SMOOTH_COPY, S_CHECK
+  S_SOLVE, S_EULER, S_IMPLICIT, S_QACC_SMOOTH_COPY, S_CHECK, S_SAP
 };
 
 constexpr int kDefaultWarps = 4;
@@ -75,6 +77,7 @@ __global__ void __launch_bounds__(128, STAGE == S_SOLVE ? MJB_MINB : 8)
     case S_FWD_ACTUATION: fwd_actuation(m, d, w, lane); break;
     case S_FWD_ACCELERATION: fwd_acceleration(m, d, w, lane, sm); break;
     case S_NXN: nxn_broadphase(m, d, w, lane); break;
+    case S_SAP: sap_broadphase(m, d, w, lane, sm); break;
     case S_NARROW: primitive_narrowphase(m, d, w, lane); break;
     case S_MAKE_CONSTRAINT: make_constraint(m, d, w, lane); break;
     case S_SOLVE: solve(m, d, w, lane, sm, d.efc_h + W(w, m.nv * m.nv)); break;
@@ -102,7 +105,7 @@ __global__ void __launch_bounds__(128, MJB_MINB) k_step_fused(const __grid_const
   com_pos(m, d, w, lane);
   crb(m, d, w, lane);
   factor_m(m, d, w, lane, sm);
-  collision(m, d, w, lane);
+  collision(m, d, w, lane, sm);
   make_constraint(m, d, w, lane);
   transmission(m, d, w, lane);
   fwd_velocity(m, d, w, lane);
@@ -237,6 +240,15 @@ int solver_smem_per_warp(const MjbModel* m) {
   return m->nv <= 32 ? int(solver_smem_floats(m->nv)) : tile_floats(m->nv);
 }
 
+// the single form's warp slice also serves the sweep-and-prune broadphase (ngeom > 100)
+int fused_smem_per_warp(const MjbModel* m) {
+  const int spw = solver_smem_per_warp(m);
+  return m->ngeom > 100 ? std::max(spw, sap_smem_floats(m->ngeom)) : spw;
+}
+
+// dynamic shared memory a CTA of kDefaultWarps warps may use (the opt-in limit of sm_100)
+constexpr size_t kMaxSmemPerCta = 227 * 1024;
+
 // opts a kernel in to more than 48 KB of dynamic shared memory (once per kernel, device and size)
 constexpr int kSmemDevices = 64;
 template <typename K>
@@ -258,13 +270,20 @@ int launch_stage(const MjbModel* m, const MjbData* d, cudaStream_t s) {
   if (STAGE == S_SOLVE) spw = m->nv <= 32 ? int(solver_smem_floats(m->nv)) : 0;
   if (STAGE == S_FACTOR_M || STAGE == S_FWD_ACCELERATION || STAGE == S_EULER || STAGE == S_IMPLICIT)
     spw = tile_floats(m->nv);
+  if (STAGE == S_SAP) spw = sap_smem_floats(m->ngeom);
   if (spw) {
     bytes = size_t(spw) * warps * sizeof(float);
+    if (bytes > kMaxSmemPerCta) return MJB_ERR_SCRATCH;
     static size_t configured[kSmemDevices];
     allow_smem(k_stage<STAGE>, bytes, configured);
   }
   k_stage<STAGE><<<grid_for(d->nworld, warps), 32 * warps, bytes, s>>>(*m, *d, spw);
   return finish();
+}
+
+// the reference's broadphase choice (collision_driver.py:537-540)
+int launch_broadphase(const MjbModel* m, const MjbData* d, cudaStream_t s) {
+  return m->ngeom > 100 ? launch_stage<S_SAP>(m, d, s) : launch_stage<S_NXN>(m, d, s);
 }
 
 void reset_counters(const MjbData* d, bool pairs, bool contacts, bool efc, bool status,
@@ -289,7 +308,7 @@ int run_forward_plain_nosolve(const MjbModel* m, const MjbData* d, cudaStream_t 
   if ((rc = launch_stage<S_CRB>(m, d, s))) return rc;
   if ((rc = launch_stage<S_FACTOR_M>(m, d, s))) return rc;
   reset_counters(d, true, true, true, false, s);
-  if ((rc = launch_stage<S_NXN>(m, d, s))) return rc;
+  if ((rc = launch_broadphase(m, d, s))) return rc;
   if ((rc = launch_stage<S_NARROW>(m, d, s))) return rc;
   if ((rc = launch_stage<S_MAKE_CONSTRAINT>(m, d, s))) return rc;
   if ((rc = launch_stage<S_TRANSMISSION>(m, d, s))) return rc;
@@ -346,8 +365,9 @@ int run_fused(const MjbModel* m, const MjbData* d, const MjbRunCfg* cfg, int int
   const int warps = (cfg && cfg->worlds_per_block > 0) ? cfg->worlds_per_block : kDefaultWarps;
   if (warps > 4) return MJB_ERR_ARG;  // __launch_bounds__(128)
   reset_counters(d, true, true, true, true, s);
-  const int spw = solver_smem_per_warp(m);
+  const int spw = fused_smem_per_warp(m);
   const size_t smem = size_t(spw) * warps * sizeof(float);
+  if (smem > kMaxSmemPerCta) return MJB_ERR_SCRATCH;
   static size_t configured[kSmemDevices];
   allow_smem(k_step_fused, smem, configured);
   k_step_fused<<<grid_for(d->nworld, warps), 32 * warps, smem, s>>>(*m, *d, integrate, spw);
@@ -446,16 +466,11 @@ int mjb_collision(const MjbModel* m, const MjbData* d, mjbStream stream) {
   if (rc || d->nworld == 0) return rc;
   cudaStream_t s = (cudaStream_t)stream;
   reset_counters(d, true, true, false, false, s);  // collision_driver.py:533-534
-  if ((rc = launch_stage<S_NXN>(m, d, s))) return rc;
+  if ((rc = launch_broadphase(m, d, s))) return rc;
   return launch_stage<S_NARROW>(m, d, s);
 }
 
-// The reference uses the sweep-and-prune path only for ngeom > 100 (collision_driver.py:537-540);
-// both produce the set of candidate pairs whose bounding volumes overlap, so the pair test here is
-// the same per-world candidate sweep.
-int mjb_sap_broadphase(const MjbModel* m, const MjbData* d, mjbStream stream) {
-  return mjb_nxn_broadphase(m, d, stream);
-}
+MJB_STAGE_ENTRY(mjb_sap_broadphase, S_SAP)
 
 int mjb_primitive_narrowphase(const MjbModel* m, const MjbData* d, mjbStream stream) {
   int rc = check(m, d);

@@ -93,6 +93,216 @@ __device__ void nxn_broadphase(const MjbModel& m, const MjbData& d, int w, int l
   __syncwarp();
 }
 
+// ------------------------------------------------------------------------------------------
+// Sweep-and-prune broadphase (collision_driver.py:71-301, 350-455), one warp per world.
+//
+// Each geom's bounding sphere (rbound + margin; planes get radius 1e9) is projected on the fixed
+// sweep direction normalize(0.5935, 0.7790, 0.1235); the lower bounds are sorted with their geom
+// ids (a bitonic sort of the world's keys in the warp's shared memory, ties in geom-id order as a
+// stable radix sort leaves them); sorted position i is then tested against positions
+// i+1 .. limit, limit = min(ngeom - 1, first position whose lower bound exceeds i's upper bound)
+// (a binary search; the reference's range includes that first position), with the model filter
+// (_geom_filter, :27-49) and the reference's overlap test on the sorted spheres and encoded planes
+// (:163-184).  Pairs are written in sweep order (position i ascending, then j), with the
+// type-ordering swap of _add_geom_pair; the reference appends them with an atomic counter.
+//
+// encode_plane / decode_plane are restated as the reference evaluates them, including
+// decode_plane taking the length of the whole 4-vector (the w code -2 or -3 included) as the
+// plane offset's magnitude; for planes through the origin (code -1) the offset is 0.
+//
+// Shared memory per warp (sap_smem_floats): sorted spheres / planes (float4, ngeom), sorted lower
+// bounds and geom ids (padded to a power of two), upper bounds by geom id, per-position counts.
+
+__host__ __device__ __forceinline__ int sap_pow2(int n) {
+  int p = 32;
+  while (p < n) p <<= 1;
+  return p;
+}
+// a multiple of 4 floats, so every warp's slice (and its float4 array) stays 16-byte aligned
+__host__ __device__ __forceinline__ int sap_smem_floats(int ngeom) {
+  return (4 * ngeom + 2 * sap_pow2(ngeom) + 2 * ngeom + 3) & ~3;
+}
+
+// collision_driver.py:27-49
+__device__ __forceinline__ bool geom_filter(const MjbModel& m, int g1, int g2, bool filterparent) {
+  const int b1 = m.geom_bodyid[g1], b2 = m.geom_bodyid[g2];
+  const int w1 = m.body_weldid[b1], w2 = m.body_weldid[b2];
+  const int wp1 = m.body_weldid[m.body_parentid[w1]], wp2 = m.body_weldid[m.body_parentid[w2]];
+  const bool self = w1 == w2;
+  const bool pc = filterparent && w1 != 0 && w2 != 0 && (w1 == wp2 || w2 == wp1);
+  const bool mask = (m.geom_contype[g1] & m.geom_conaffinity[g2]) ||
+                    (m.geom_contype[g2] & m.geom_conaffinity[g1]);
+  return mask && !self && !pc;
+}
+
+// wp.normalize: the vector divided by its length
+__device__ __forceinline__ void sap_normalize(float& x, float& y, float& z) {
+  const float l = __fsqrt_rn(rdot3(x, y, z, x, y, z));
+  if (l > 0.f) {
+    x = __fdiv_rn(x, l);
+    y = __fdiv_rn(y, l);
+    z = __fdiv_rn(z, l);
+  }
+}
+
+// collision_driver.py:98-118
+__device__ __forceinline__ float4 sap_encode_plane(float nx, float ny, float nz, float px, float py,
+                                                   float pz, float margin) {
+  sap_normalize(nx, ny, nz);
+  const float off = -rdot3(nx, ny, nz, __fadd_rn(px, __fmul_rn(nx, margin)),
+                           __fadd_rn(py, __fmul_rn(ny, margin)), __fadd_rn(pz, __fmul_rn(nz, margin)));
+  const float scale = fabsf(off);
+  if (fabsf(off) < 1e-6f) return make_float4(nx, ny, nz, -1.f);
+  return make_float4(__fmul_rn(scale, nx), __fmul_rn(scale, ny), __fmul_rn(scale, nz),
+                     off < 0.f ? -2.f : -3.f);
+}
+
+// collision_driver.py:121-130 (normal, offset)
+__device__ __forceinline__ float4 sap_decode_plane(float4 e) {
+  const float mag = __fsqrt_rn(__fadd_rn(rdot3(e.x, e.y, e.z, e.x, e.y, e.z), __fmul_rn(e.w, e.w)));
+  float nx = e.x, ny = e.y, nz = e.z;
+  sap_normalize(nx, ny, nz);
+  const float off = e.w == -1.f ? 0.f : (e.w == -2.f ? -mag : mag);
+  return make_float4(nx, ny, nz, off);
+}
+
+// collision_driver.py:163-184
+__device__ __forceinline__ bool sap_overlap(float4 a, float4 b) {
+  if (a.w < 0.f && b.w < 0.f) return false;
+  if (a.w < 0.f || b.w < 0.f) {
+    if (b.w < 0.f) {
+      const float4 t = a;
+      a = b;
+      b = t;
+    }
+    const float4 p = sap_decode_plane(a);
+    const float dist = __fadd_rn(rdot3(b.x, b.y, b.z, p.x, p.y, p.z), p.w);
+    return dist <= b.w;
+  }
+  const float dx = __fsub_rn(a.x, b.x), dy = __fsub_rn(a.y, b.y), dz = __fsub_rn(a.z, b.z);
+  const float r = __fadd_rn(a.w, b.w);
+  return rdot3(dx, dy, dz, dx, dy, dz) <= __fmul_rn(r, r);
+}
+
+__device__ void sap_broadphase(const MjbModel& m, const MjbData& d, int w, int lane, float* sm) {
+  const int ng = m.ngeom, P = sap_pow2(ng);
+  float4* S = reinterpret_cast<float4*>(sm);
+  float* lo = sm + 4 * ng;
+  int* idx = reinterpret_cast<int*>(lo + P);
+  float* up = lo + 2 * P;
+  int* cnt = reinterpret_cast<int*>(up + ng);
+  const float* gxpos = d.geom_xpos + W(w, 3 * ng);
+  const float* gxmat = d.geom_xmat + W(w, 9 * ng);
+  float dx = 0.5935f, dy = 0.7790f, dz = 0.1235f;
+  sap_normalize(dx, dy, dz);
+  // broadphase_project_spheres_onto_sweep_direction_kernel (:72-92)
+  for (int g = lane; g < P; g += 32) {
+    if (g < ng) {
+      float r = m.geom_rbound[g];
+      if (r == 0.f) r = 1e9f;
+      const float sr = __fadd_rn(r, m.geom_margin[g]);
+      const float c = rdot3(dx, dy, dz, gxpos[3 * g], gxpos[3 * g + 1], gxpos[3 * g + 2]);
+      lo[g] = __fsub_rn(c, sr);
+      up[g] = __fadd_rn(c, sr);
+      idx[g] = g;
+    } else {
+      lo[g] = __int_as_float(0x7f800000);
+      idx[g] = g;
+    }
+  }
+  __syncwarp();
+  // sort (lower bound, geom id) ascending
+  for (int k = 2; k <= P; k <<= 1) {
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int t = lane; t < P / 2; t += 32) {
+        const int a = 2 * j * (t / j) + (t % j), b = a + j;
+        const float ka = lo[a], kb = lo[b];
+        const int ia = idx[a], ib = idx[b];
+        const bool gt = ka > kb || (ka == kb && ia > ib);
+        if (gt == ((a & k) == 0)) {
+          lo[a] = kb;
+          lo[b] = ka;
+          idx[a] = ib;
+          idx[b] = ia;
+        }
+      }
+      __syncwarp();
+    }
+  }
+  // reorder_bounding_spheres_kernel (:134-156)
+  for (int i = lane; i < ng; i += 32) {
+    const int g = idx[i];
+    const float* c = gxpos + 3 * g;
+    const float r = m.geom_rbound[g], margin = m.geom_margin[g];
+    if (r == 0.f) {
+      const float* x = gxmat + 9 * g;
+      S[i] = sap_encode_plane(x[2], x[5], x[8], c[0], c[1], c[2], margin);
+    } else {
+      S[i] = make_float4(c[0], c[1], c[2], __fadd_rn(r, margin));
+    }
+  }
+  __syncwarp();
+  const bool filterparent = !(m.disableflags & DSBL_FILTERPARENT);
+  // sap_broadphase_prepare_kernel (:219-236) + sap_broadphase_kernel (:272-300), per position i
+  auto sweep = [&](int i, int out) {
+    const int g1 = idx[i];
+    const float end = up[g1];
+    int a = i + 1, b = ng;
+    while (a < b) {
+      const int mid = (a + b) >> 1;
+      if (lo[mid] > end) b = mid;
+      else a = mid + 1;
+    }
+    const int limit = min(ng - 1, a);
+    int n = 0;
+    for (int j = i + 1; j <= limit; j++) {
+      const int g2 = idx[j];
+      if (!geom_filter(m, g1, g2, filterparent) || !sap_overlap(S[i], S[j])) continue;
+      if (out >= 0) {
+        const int k = out + n;
+        const bool swap = m.geom_type[g1] > m.geom_type[g2];
+        d.collision_pair[2 * k] = swap ? g2 : g1;
+        d.collision_pair[2 * k + 1] = swap ? g1 : g2;
+        d.collision_worldid[k] = w;
+      }
+      n++;
+    }
+    return n;
+  };
+  int total = 0;
+  for (int i = lane; i < ng; i += 32) {
+    cnt[i] = sweep(i, -1);
+    total += cnt[i];
+  }
+  total = warp_sum_i(total);
+  const int adr = reserve(d.ncollision, total, d.nconmax, d.world_status ? d.world_status + w : nullptr,
+                          MJB_WS_PAIR_OVERFLOW, lane);
+  if (adr < 0) total = 0;
+  if (total > 0) {
+    int run = adr;
+    for (int base = 0; base < ng; base += 32) {
+      const int i = base + lane;
+      const int c = i < ng ? cnt[i] : 0;
+      int incl = c;
+      for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(WARP_FULL, incl, o);
+        if (lane >= o) incl += v;
+      }
+      if (c > 0) sweep(i, run + incl - c);
+      run += __shfl_sync(WARP_FULL, incl, 31);
+    }
+  }
+  if (lane == 0) {
+    d.world_pairadr[w] = adr < 0 ? 0 : adr;
+    d.world_npair[w] = total;
+  }
+  __syncwarp();
+}
+
+// The reference's broadphase choice (collision_driver.py:537-540): nxn for ngeom <= 100, else
+// sweep-and-prune (which needs sap_smem_floats(ngeom) floats of warp scratch `sm`).
+__device__ __forceinline__ bool use_sap(const MjbModel& m) { return m.ngeom > 100; }
+
 struct ContactOut {
   const MjbModel* m;
   const MjbData* d;
@@ -274,8 +484,10 @@ __device__ void primitive_narrowphase(const MjbModel& m, const MjbData& d, int w
 
 // collision_driver.py:525-547 (ngeom <= 100 path; larger models go through sap_broadphase, whose
 // pair set is the same set of overlapping candidates)
-__device__ void collision(const MjbModel& m, const MjbData& d, int w, int lane) {
-  nxn_broadphase(m, d, w, lane);
+// sm: sap_smem_floats(ngeom) floats of warp scratch when use_sap(m)
+__device__ void collision(const MjbModel& m, const MjbData& d, int w, int lane, float* sm) {
+  if (use_sap(m)) sap_broadphase(m, d, w, lane, sm);
+  else nxn_broadphase(m, d, w, lane);
   primitive_narrowphase(m, d, w, lane);
 }
 

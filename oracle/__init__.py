@@ -24,7 +24,7 @@ STAGES = {
   "fwd_acceleration": 5, "kinematics": 6, "com_pos": 7, "crb": 8, "factor_m": 9,
   "collision": 10, "nxn_broadphase": 11, "narrowphase": 12, "make_constraint": 13,
   "transmission": 14, "com_vel": 15, "passive": 16, "rne": 17, "solve": 18, "euler": 19,
-  "implicit": 20, "forward_nosolve": 21,
+  "implicit": 20, "forward_nosolve": 21, "sap_broadphase": 22,
 }
 
 

@@ -881,6 +881,103 @@ void nxn_broadphase(const Model<T>& m, World<T>& w) {
   }
 }
 
+// collision_driver.py:350-455 — sweep-and-prune: project bounding spheres on the fixed direction
+// (:72-92), stable sort of the lower bounds (the segmented radix sort, :373-378), reorder into
+// spheres / encoded planes (:134-156), then every sorted position i against positions
+// i+1 .. min(ngeom-1, first position whose lower bound exceeds i's upper bound) (:219-236), with
+// the filter and the overlap test (:163-184, 272-300).  encode_plane / decode_plane (:98-130) as
+// the reference evaluates them: the decoded offset magnitude is the length of the whole 4-vector,
+// w code included.  Pairs in sweep order.
+template <typename T>
+V3<T> sap_normalize(V3<T> v) {
+  T l = std::sqrt(dot(v, v));
+  return l > T(0) ? V3<T>(v[0] / l, v[1] / l, v[2] / l) : v;
+}
+
+template <typename T>
+void sap_encode_plane(V3<T> normal, V3<T> point, T margin, T out[4]) {
+  V3<T> n = sap_normalize(normal);
+  V3<T> q(point[0] + n[0] * margin, point[1] + n[1] * margin, point[2] + n[2] * margin);
+  T off = -dot(n, q);
+  T scale = std::fabs(off);
+  if (std::fabs(off) < T(1e-6)) {
+    out[0] = n[0]; out[1] = n[1]; out[2] = n[2]; out[3] = T(-1);
+  } else {
+    out[0] = scale * n[0]; out[1] = scale * n[1]; out[2] = scale * n[2];
+    out[3] = off < T(0) ? T(-2) : T(-3);
+  }
+}
+
+template <typename T>
+bool sap_overlap(const T* a, const T* b) {
+  if (a[3] < T(0) && b[3] < T(0)) return false;
+  if (a[3] < T(0) || b[3] < T(0)) {
+    if (b[3] < T(0)) std::swap(a, b);
+    V3<T> e(a[0], a[1], a[2]);
+    T mag = std::sqrt(dot(e, e) + a[3] * a[3]);
+    V3<T> n = sap_normalize(e);
+    T off = a[3] == T(-1) ? T(0) : (a[3] == T(-2) ? -mag : mag);
+    T dist = dot(V3<T>(b[0], b[1], b[2]), n) + off;
+    return dist <= b[3];
+  }
+  V3<T> dlt(a[0] - b[0], a[1] - b[1], a[2] - b[2]);
+  T r = a[3] + b[3];
+  return dot(dlt, dlt) <= r * r;
+}
+
+template <typename T>
+void sap_broadphase(const Model<T>& m, World<T>& w) {
+  w.pair.clear();
+  const int ng = m.ngeom;
+  bool filterparent = !(m.disableflags & DSBL_FILTERPARENT);
+  V3<T> dir = sap_normalize(V3<T>(T(0.5935f), T(0.7790f), T(0.1235f)));
+  std::vector<T> lo(ng), up(ng), S(4 * ng);
+  std::vector<int> idx(ng);
+  for (int g = 0; g < ng; g++) {
+    T r = m.geom_rbound[g];
+    if (r == T(0)) r = T(1e9f);
+    T sr = r + m.geom_margin[g];
+    T c = dot(dir, V3<T>(w.geom_xpos[3 * g], w.geom_xpos[3 * g + 1], w.geom_xpos[3 * g + 2]));
+    lo[g] = c - sr;
+    up[g] = c + sr;
+    idx[g] = g;
+  }
+  std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return lo[a] < lo[b]; });
+  std::vector<T> los(ng);
+  for (int i = 0; i < ng; i++) los[i] = lo[idx[i]];
+  for (int i = 0; i < ng; i++) {
+    int g = idx[i];
+    V3<T> c(w.geom_xpos[3 * g], w.geom_xpos[3 * g + 1], w.geom_xpos[3 * g + 2]);
+    T r = m.geom_rbound[g], margin = m.geom_margin[g];
+    if (r == T(0)) {
+      const T* x = &w.geom_xmat[9 * g];
+      sap_encode_plane(V3<T>(x[2], x[5], x[8]), c, margin, &S[4 * i]);
+    } else {
+      S[4 * i] = c[0]; S[4 * i + 1] = c[1]; S[4 * i + 2] = c[2]; S[4 * i + 3] = r + margin;
+    }
+  }
+  for (int i = 0; i < ng; i++) {
+    int g1 = idx[i];
+    T end = up[g1];
+    int a = i + 1, b = ng;
+    while (a < b) {
+      int mid = (a + b) >> 1;
+      if (los[mid] > end) b = mid;
+      else a = mid + 1;
+    }
+    int limit = std::min(ng - 1, a);
+    for (int j = i + 1; j <= limit; j++) {
+      int g2 = idx[j];
+      if (!geom_filter(m, g1, g2, filterparent) || !sap_overlap(&S[4 * i], &S[4 * j])) continue;
+      if (m.geom_type[g1] > m.geom_type[g2]) {
+        w.pair.push_back(g2); w.pair.push_back(g1);
+      } else {
+        w.pair.push_back(g1); w.pair.push_back(g2);
+      }
+    }
+  }
+}
+
 template <typename T>
 void write_contact(World<T>& w, T dist, V3<T> pos, const M3<T>& frame, T margin, int g1, int g2) {
   // collision_primitive.py:52-70
@@ -1009,7 +1106,8 @@ void narrowphase(const Model<T>& m, World<T>& w) {
 
 template <typename T>
 void collision(const Model<T>& m, World<T>& w) {
-  nxn_broadphase(m, w);
+  if (m.ngeom > 100) sap_broadphase(m, w);  // collision_driver.py:537-540
+  else nxn_broadphase(m, w);
   narrowphase(m, w);
 }
 
@@ -1570,7 +1668,7 @@ enum Stage {
   ST_STEP = 0, ST_FORWARD, ST_FWD_POSITION, ST_FWD_VELOCITY, ST_FWD_ACTUATION,
   ST_FWD_ACCELERATION, ST_KINEMATICS, ST_COM_POS, ST_CRB, ST_FACTOR_M, ST_COLLISION,
   ST_NXN_BROADPHASE, ST_NARROWPHASE, ST_MAKE_CONSTRAINT, ST_TRANSMISSION, ST_COM_VEL, ST_PASSIVE,
-  ST_RNE, ST_SOLVE, ST_EULER, ST_IMPLICIT, ST_FORWARD_NOSOLVE
+  ST_RNE, ST_SOLVE, ST_EULER, ST_IMPLICIT, ST_FORWARD_NOSOLVE, ST_SAP_BROADPHASE
 };
 
 template <typename T>
@@ -1588,6 +1686,7 @@ void run_stage(const Model<T>& m, World<T>& w, int stage, bool njmax_zero) {
     case ST_FACTOR_M: factor_m(m, w); break;
     case ST_COLLISION: collision(m, w); break;
     case ST_NXN_BROADPHASE: nxn_broadphase(m, w); break;
+    case ST_SAP_BROADPHASE: sap_broadphase(m, w); break;
     case ST_NARROWPHASE: narrowphase(m, w); break;
     case ST_MAKE_CONSTRAINT: make_constraint(m, w); break;
     case ST_TRANSMISSION: transmission(m, w); break;

@@ -81,6 +81,68 @@ def test_sap_model_expected_pairs():
   assert got == {tuple(p) for p in f["sap_expected_pairs"]}
 
 
+def _spheres_xml(n):
+  """Project-written: a floor, two wall planes off the origin (x = +-0.5) and n free spheres of
+  radius 0.05, so ngeom = n + 3."""
+  bodies = "".join(f'<body pos="0 0 {0.2 + 0.1 * i}"><freejoint/><geom type="sphere" size="0.05"/></body>'
+                   for i in range(n))
+  return ('<mujoco><worldbody><geom type="plane" size="0 0 0.05"/>'
+          '<geom type="plane" pos="0.5 0 0" zaxis="-1 0 0" size="0 0 0.05"/>'
+          '<geom type="plane" pos="-0.5 0 0" zaxis="1 0 0" size="0 0 0.05"/>'
+          f'{bodies}</worldbody></mujoco>')
+
+
+def _scatter(mjm, nworld, seed, half=0.45, zmax=0.4):
+  """Free bodies at x, y ~ U(-half, half), z ~ U(0.02, zmax), random orientations."""
+  rng = np.random.default_rng(seed)
+  qpos = np.tile(mjm.qpos0, (nworld, 1))
+  for b in range(mjm.nq // 7):
+    a = 7 * b
+    qpos[:, a:a + 2] = rng.uniform(-half, half, (nworld, 2))
+    qpos[:, a + 2] = rng.uniform(0.02, zmax, nworld)
+    q = rng.normal(size=(nworld, 4))
+    qpos[:, a + 3:a + 7] = q / np.linalg.norm(q, axis=1, keepdims=True)
+  return qpos, np.zeros((nworld, mjm.nv)), np.zeros((nworld, 0))
+
+
+@pytest.mark.parametrize("name", ["bin.xml", "spheres120"])
+def test_sap_pair_lists_bit_exact(name):
+  """Sweep-and-prune (collision_driver.py:350-455) on the device vs the oracle's restatement given
+  the device's geom poses: identical pair lists, in the same sweep order, in every world.
+  bin.xml (69 geoms, walls off the origin) calls sap_broadphase directly; the 123-geom model goes
+  through collision(), which selects sweep-and-prune for ngeom > 100 as the reference does, and
+  its contacts are compared too.  (Both models are large enough for the reference's automatic
+  sparse mass matrix; jacobian = 0 selects the dense one the kernels implement.)"""
+  mjm = load("bin.xml", jacobian=0) if name == "bin.xml" else load(_spheres_xml(120), jacobian=0)
+  nworld = 64
+  qpos, qvel, ctrl = _scatter(mjm, nworld, seed=5)
+  m = mjw.put_model(mjm)
+  d = device_data(mjm, qpos, qvel, ctrl, nconmax=4096 * nworld // 8, njmax=64 * nworld)
+  mjw.kinematics(m, d)
+  if name == "bin.xml":
+    mjw.sap_broadphase(m, d)
+  else:
+    assert mjm.ngeom > 100
+    mjw.collision(m, d)
+  torch.cuda.synchronize()
+  assert np.all(mjw.world_status(d) == 0)
+  o = oracle(mjm, qpos, qvel, ctrl, 32)
+  o.set("geom_xpos", dev(d.geom_xpos))
+  o.set("geom_xmat", dev(d.geom_xmat))
+  o.run("sap_broadphase")
+  cnt, opairs = o.rows("pair")
+  n, pairs = _device_rows(d, "pair", d.collision_pair, 2)
+  assert cnt.sum() > nworld
+  np.testing.assert_array_equal(n, cnt)
+  np.testing.assert_array_equal(pairs, opairs.astype(np.int32))
+  if name != "bin.xml":
+    o.run("narrowphase")
+    ccnt, _ = o.rows("contact_dist")
+    nc, geoms = _device_rows(d, "contact", d.contact.geom, 2)
+    np.testing.assert_array_equal(nc, ccnt)
+    np.testing.assert_array_equal(geoms, o.rows("contact_geom")[1].astype(np.int32))
+
+
 @pytest.mark.parametrize("name", ["humanoid.xml", "collision.xml"])
 def test_pair_sets_bit_exact(name):
   """Given the device's geom poses, the oracle's FP32 nxn test selects the identical pair list,

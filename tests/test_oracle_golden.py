@@ -24,24 +24,39 @@ def test_closest_segment_points(precision):
                                    err_msg=f"{case['name']} {e['var']}")
 
 
-def _pairs_at(mjm, qpos, nworld=1):
+def _pairs_at(mjm, qpos, nworld=1, stage="nxn_broadphase"):
   o = Oracle(mjm, nworld, 32)
   o.set("qpos", qpos)
   o.run("kinematics")
-  o.run("nxn_broadphase")
+  o.run(stage)
   cnt, pairs = o.rows("pair")
   return cnt, pairs.astype(int)
 
 
-def test_sap_model_pairs():
-  """broad_phase_test.py:42-118: the 19 overlapping box / plane pairs at qpos0."""
+@pytest.mark.parametrize("stage", ["nxn_broadphase", "sap_broadphase"])
+def test_sap_model_pairs(stage):
+  """broad_phase_test.py:42-118: the 19 overlapping box / plane pairs at qpos0 (the reference
+  checks its sweep-and-prune result against this brute-force list)."""
   f = fixtures()
   mjm = load(f["sap_model"])
-  cnt, pairs = _pairs_at(mjm, mjm.qpos0)
+  cnt, pairs = _pairs_at(mjm, mjm.qpos0, stage=stage)
   expected = {tuple(p) for p in f["sap_expected_pairs"]}
   got = {tuple(sorted(p)) for p in pairs}
   assert cnt[0] == len(expected)
   assert got == expected
+
+
+def test_sap_matches_nxn_without_margins_or_offset_planes():
+  """With zero margins and no planes, the sweep-and-prune overlap test is the nxn bounding test:
+  the same pair set in every keyframe world of the nxn model (broad_phase_test.py:124-185)."""
+  mjm = load(fixtures()["nxn_model"])
+  qpos = np.stack([mjm.key_qpos[k] for k in range(mjm.key_qpos.shape[0])])
+  cn, pn = _pairs_at(mjm, qpos, nworld=qpos.shape[0])
+  cs, ps = _pairs_at(mjm, qpos, nworld=qpos.shape[0], stage="sap_broadphase")
+  np.testing.assert_array_equal(cn, cs)
+  off = np.concatenate([[0], np.cumsum(cn)])
+  for w in range(len(cn)):
+    assert {tuple(p) for p in pn[off[w]:off[w + 1]]} == {tuple(p) for p in ps[off[w]:off[w + 1]]}
 
 
 def test_nxn_keyframes():
