@@ -21,6 +21,12 @@ the maximum over ranks of CUDA-event time between barriers.
 qacc_err (rank 0): one forward from the bench state in every launch form, checked against the
 FP64 CPU restatement (the oracle, used only as the checker) on the first 256 worlds.
 
+grad (rank 0): grad-steps/s of the differentiation workload — the same humanoid with the Newton
+solve run to convergence (10 iterations), nworld=1024, a 32-step rollout, loss = ||root_pos_T - target||^2 + 1e-3 sum ||ctrl||^2, gradients w.r.t. the
+control sequence (32 x 21), qpos0 and qvel0, checkpoints every 8 steps — through
+mjx_warp_b200.derivative (GPU finite-difference transition Jacobians, centered, eps 1e-3, and
+the reverse recursion); one forward + backward timed with CUDA events after one warm-up.
+
 --impl reference times the reference algorithm's CPU implementation available here — the CPU
 restatement under oracle/, FP32, all host threads — on the same workload.
 """
@@ -183,6 +189,60 @@ def _qacc_error(mjm, m, d, mjw, torch, restore, forms, sample=256):
   return out
 
 
+def _grad_rate(mjw, torch, nworld=1024, horizon=32, checkpoint=8, reps=2):
+  """grad-steps/s of a differentiated rollout (see the module docstring).  The Newton solve runs
+  to convergence (10 iterations, 10 line-search iterations): the 3-iteration iterate of the
+  steps/s workload is discontinuous in its inputs, and differences across those jumps make the
+  products of 32 transition Jacobians explode (measured: median max |dL/du| ~1e16 at 3
+  iterations, ~6e-3 at 10 or 30)."""
+  mjm = _model()
+  mjm.opt.iterations, mjm.opt.ls_iterations = 10, 10
+  qpos, qvel, ctrl0 = _state(mjm, 0, nworld, seed=1)
+  m = mjw.put_model(mjm)
+  roll = mjw.derivative.Rollout(mjm, m, nworld, checkpoint=checkpoint, eps=1e-3, centered=True,
+                                nconmax=48, njmax=80)
+  rng = np.random.default_rng(2)
+  ctrl = np.repeat(ctrl0[None], horizon, axis=0) + rng.normal(0.0, 0.05, (horizon, nworld, mjm.nu))
+  q0 = torch.tensor(qpos, dtype=torch.float32, device="cuda")
+  v0 = torch.tensor(qvel, dtype=torch.float32, device="cuda")
+  u0 = torch.tensor(ctrl, dtype=torch.float32, device="cuda")
+  target = q0[:, :3] + torch.tensor([0.05, 0.0, 0.0], device="cuda")
+
+  def once():
+    q, v, u = (t.clone().requires_grad_(True) for t in (q0, v0, u0))
+    e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    e0.record()
+    qT, _ = roll(q, v, u)
+    loss = ((qT[:, :3] - target) ** 2).sum() + 1e-3 * (u ** 2).sum()
+    e1.record()
+    loss.backward()
+    e2.record()
+    torch.cuda.synchronize()
+    ok = torch.isfinite(u.grad).all(2).all(0) & torch.isfinite(q.grad).all(1) & torch.isfinite(v.grad).all(1)
+    gmax = u.grad.abs().amax(dim=(0, 2))[ok]
+    return e0.elapsed_time(e1) * 1e-3, e1.elapsed_time(e2) * 1e-3, ok, gmax
+
+  once()
+  fwd = bwd = 0.0
+  for _ in range(reps):
+    f, b, ok, gmax = once()
+    fwd, bwd = fwd + f / reps, bwd + b / reps
+  t = fwd + bwd
+  flags = mjw.world_status(roll.fd.pert)
+  q = np.quantile(gmax.cpu().numpy(), [0.5, 0.99]) if gmax.numel() else [None, None]
+  return {"value": nworld * horizon / t, "unit": "grad-steps/s",
+          "config": {"nworld": nworld, "horizon": horizon, "checkpoint": checkpoint,
+                     "wrt": "ctrl (32x21), qpos0, qvel0",
+                     "method": "GPU finite-difference transition Jacobians (centered, eps 1e-3, "
+                               f"{roll.fd.K} world-steps per world-step) + reverse recursion"},
+          "solver": "Newton 10 it / ls 10 (converged)",
+          "forward_ms": fwd * 1e3, "backward_ms": bwd * 1e3,
+          "rollout_steps_per_s": nworld * horizon / fwd, "cost_vs_forward": t / fwd,
+          "worlds_with_finite_grads": int(ok.sum()), "perturbed_worlds_flagged": int((flags != 0).sum()),
+          "max_abs_dL_du_per_world": {"median": float(q[0]) if q[0] is not None else None,
+                                      "p99": float(q[1]) if q[1] is not None else None}}
+
+
 def _graph_steps_per_s(torch, step, nworld, steps, barrier, restore):
   g = torch.cuda.CUDAGraph()
   s = torch.cuda.Stream()
@@ -328,6 +388,9 @@ def run_ours(args):
   accuracy = None
   if rank == 0 and not args.no_accuracy:
     accuracy = _qacc_error(mjm, m, d, mjw, torch, restore, FORMS)
+  grad = None
+  if rank == 0 and not args.no_grad:
+    grad = _grad_rate(mjw, torch)
 
   launches_per_step = LAUNCHES[args.form]
   total_worlds = nworld * world_size
@@ -375,6 +438,8 @@ def run_ours(args):
   }
   if accuracy is not None:
     line["qacc_err"] = accuracy
+  if grad is not None:
+    line["grad"] = grad
   if rank == 0 and not args.no_cpu_baseline:
     line["cpu_baseline"] = cpu_baseline(mjm, budget_s=args.cpu_seconds)
   del g
@@ -439,6 +504,7 @@ def main():
   p.add_argument("--cpu-seconds", type=float, default=10.0)
   p.add_argument("--no-cpu-baseline", action="store_true")
   p.add_argument("--no-accuracy", action="store_true")
+  p.add_argument("--no-grad", action="store_true")
   args = p.parse_args()
   if args.warmup < 3:
     args.warmup = 3

@@ -194,6 +194,24 @@ int mjb_xfrc_accumulate(const MjbModel* m, const MjbData* d, float* qfrc, mjbStr
 /* Copies world_status (nworld words) to host memory; synchronises the stream. */
 int mjb_world_status(const MjbData* d, uint32_t* host_out, mjbStream stream);
 
+/* Finite-difference transition Jacobians, no counterpart in the reference (whose API has no
+ * derivatives); the scheme is MuJoCo's mjd_transitionFD, batched over worlds.  State
+ * x = (qpos in the tangent space, qvel, act), nx = 2 nv + na; input u = ctrl.  `pert` is a Data
+ * of nworld * K worlds, K = 1 + ncol (forward differences) or 1 + 2 ncol (centered),
+ * ncol = nx + nu.  mjb_fd_perturb copies every base world's state into its K slots and perturbs
+ * one column per slot by eps (tangent-space rotations for quaternions); the caller then steps
+ * `pert` (mjb_step); mjb_fd_jacobian differences the next states into A (nworld x nx x nx) and
+ * B (nworld x nx x nu), row-major per world: A[w][i][j] = d x'_i / d x_j.  eps > 0; in FP32 a
+ * value near 1e-3 balances truncation and rounding. */
+int mjb_fd_perturb(const MjbModel* m, const MjbData* base, const MjbData* pert, float eps,
+                   int centered, mjbStream stream);
+int mjb_fd_jacobian(const MjbModel* m, const MjbData* pert, int nworld, float eps, int centered,
+                    float* A, float* B, mjbStream stream);
+/* Reverse step of a rollout adjoint, per world: lam_out = A^T lam, grad_ctrl = B^T lam
+ * (B / grad_ctrl may be null); lam and lam_out are nworld x nx and must not alias. */
+int mjb_transition_vjp(const MjbModel* m, int nworld, const float* A, const float* B,
+                       const float* lam, float* lam_out, float* grad_ctrl, mjbStream stream);
+
 /* Allocation-free variant of mjb_implicit, with no counterpart in the reference.  For callers
  * that may not allocate device memory when they step (a plugin that receives only its operand
  * buffers, a control loop that cannot afford cudaMalloc's synchronisation): the integrator's

@@ -13,6 +13,7 @@ stage functions launch the hand-written sm_100a kernels of libmjb200.so through 
 (include/mjb200.h).
 """
 
+from . import derivative as derivative
 from . import mjcf as mjcf
 from ._api import benchmark as benchmark
 from ._api import collision as collision

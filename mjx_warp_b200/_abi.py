@@ -154,6 +154,13 @@ def lib() -> ctypes.CDLL:
   L.mjb_step_phase.argtypes = [pm, pd, ctypes.c_int, ctypes.c_void_p]
   L.mjb_world_status.restype = ctypes.c_int
   L.mjb_world_status.argtypes = [pd, ctypes.c_void_p, ctypes.c_void_p]
+  vp, ci, cf = ctypes.c_void_p, ctypes.c_int, ctypes.c_float
+  L.mjb_fd_perturb.restype = ctypes.c_int
+  L.mjb_fd_perturb.argtypes = [pm, pd, pd, cf, ci, vp]
+  L.mjb_fd_jacobian.restype = ctypes.c_int
+  L.mjb_fd_jacobian.argtypes = [pm, pd, ci, cf, ci, vp, vp, vp]
+  L.mjb_transition_vjp.restype = ctypes.c_int
+  L.mjb_transition_vjp.argtypes = [pm, ci, vp, vp, vp, vp, vp, vp]
   if L.mjb_abi_version() != 1:
     raise RuntimeError("libmjb200.so ABI version mismatch")
   _lib = L

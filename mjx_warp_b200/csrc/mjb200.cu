@@ -17,6 +17,7 @@
 
 #include <algorithm>
 
+#include "mjb_deriv.cuh"
 #include "mjb_solver.cuh"
 
 // minimum resident CTAs per SM requested for the solver kernels (caps registers per thread at
@@ -140,6 +141,36 @@ __global__ void __launch_bounds__(128, 8) k_integrate(const __grid_constant__ Mj
   if (m.integrator == 0) euler(m, d, w, lane, tile);
   else implicit(m, d, w, lane, tile);
   check_finite(m, d, w, lane);
+}
+
+// finite-difference transition Jacobians (mjb_deriv.cuh): one warp per perturbed slot
+__global__ void k_fd_perturb(const __grid_constant__ MjbModel m, const __grid_constant__ MjbData b,
+                             const __grid_constant__ MjbData p, float eps, int centered) {
+  const int lane = threadIdx.x & 31;
+  const int pw = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (pw >= p.nworld) return;
+  const int K = fd_slots(m, centered), w = pw / K, k = pw - w * K;
+  const int col = k == 0 ? -1 : (centered ? (k - 1) >> 1 : k - 1);
+  const float delta = (centered && ((k - 1) & 1)) ? -eps : eps;
+  fd_perturb_world(m, b, p, w, pw, col, delta, lane);
+}
+// one warp per (base world, column)
+__global__ void k_fd_jacobian(const __grid_constant__ MjbModel m, const __grid_constant__ MjbData p,
+                              int nworld, float eps, int centered, float* A, float* B) {
+  const int lane = threadIdx.x & 31;
+  const long long t = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int ncol = fd_ncol(m);
+  if (t >= (long long)nworld * ncol) return;
+  const int w = int(t / ncol), col = int(t - (long long)w * ncol);
+  fd_column(m, p, w, col, centered, eps, A, B, lane);
+}
+// one warp per world
+__global__ void k_transition_vjp(const __grid_constant__ MjbModel m, int nworld, const float* A,
+                                 const float* B, const float* lam, float* lam_out, float* grad_ctrl) {
+  const int lane = threadIdx.x & 31;
+  const int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (w >= nworld) return;
+  transition_vjp_world(m, A, B, lam, lam_out, grad_ctrl, w, lane);
 }
 
 // zero the flat-array counters and (optionally) the world status words
@@ -585,4 +616,43 @@ extern "C" int mjb_implicit_noalloc(const MjbModel* m, const MjbData* d, mjbStre
   dd.qLD_integration = scratch + size_t(d->nworld) * nv * nv;
   dd.qfrc_integration = scratch + 2 * size_t(d->nworld) * nv * nv;
   return launch_stage<S_IMPLICIT>(m, &dd, (cudaStream_t)stream);
+}
+
+// ------------------------------------------------------------------------------------------
+// Finite-difference transition Jacobians (mjb_deriv.cuh).
+
+extern "C" int mjb_fd_perturb(const MjbModel* m, const MjbData* base, const MjbData* pert,
+                              float eps, int centered, mjbStream stream) {
+  int rc = check(m, base);
+  if (rc || base->nworld == 0) return rc;
+  if (!pert || !(eps > 0.f)) return MJB_ERR_ARG;
+  if ((long long)pert->nworld != (long long)base->nworld * fd_slots(*m, centered)) return MJB_ERR_ARG;
+  if (!pert->qpos || !pert->qvel || !base->qpos || !base->qvel) return MJB_ERR_ARG;
+  if ((m->na && (!pert->act || !base->act)) || (m->nu && (!pert->ctrl || !base->ctrl)))
+    return MJB_ERR_ARG;
+  k_fd_perturb<<<grid_for(pert->nworld, 4), 128, 0, (cudaStream_t)stream>>>(*m, *base, *pert, eps,
+                                                                            centered);
+  return finish();
+}
+
+extern "C" int mjb_fd_jacobian(const MjbModel* m, const MjbData* pert, int nworld, float eps,
+                               int centered, float* A, float* B, mjbStream stream) {
+  int rc = check(m, pert);
+  if (rc || nworld == 0) return rc;
+  if (nworld < 0 || !A || (m->nu && !B) || !(eps > 0.f)) return MJB_ERR_ARG;
+  if ((long long)pert->nworld != (long long)nworld * fd_slots(*m, centered)) return MJB_ERR_ARG;
+  const long long warps = (long long)nworld * fd_ncol(*m);
+  k_fd_jacobian<<<int((warps + 3) / 4), 128, 0, (cudaStream_t)stream>>>(*m, *pert, nworld, eps,
+                                                                       centered, A, B);
+  return finish();
+}
+
+extern "C" int mjb_transition_vjp(const MjbModel* m, int nworld, const float* A, const float* B,
+                                  const float* lam, float* lam_out, float* grad_ctrl,
+                                  mjbStream stream) {
+  if (!m || nworld < 0 || !A || !lam || !lam_out || lam == lam_out) return MJB_ERR_ARG;
+  if (nworld == 0) return MJB_OK;
+  k_transition_vjp<<<grid_for(nworld, 4), 128, 0, (cudaStream_t)stream>>>(*m, nworld, A, B, lam,
+                                                                          lam_out, grad_ctrl);
+  return finish();
 }

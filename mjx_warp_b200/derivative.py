@@ -1,0 +1,264 @@
+"""Derivatives of the batched step: finite-difference transition Jacobians on the GPU and a
+rollout adjoint behind torch.autograd.
+
+The reference (mujoco_warp 3.2.7) has no derivative API.  ``TransitionFD`` follows MuJoCo's
+mjd_transitionFD scheme for a whole batch at once: every world's state is copied into
+1 + ncol (forward differences) or 1 + 2 ncol (centered) slots of a second Data, one column per
+slot is perturbed (``mjb_fd_perturb``), the slots advance by one step in a single launch
+sequence, and the differences of their next states give, per world,
+
+  A = dx'/dx  (nx x nx),  B = dx'/du  (nx x nu),  x = (qpos tangent, qvel, act), u = ctrl,
+
+with nx = 2 nv + na and positions in the tangent space (free and ball joints rotate about local
+axes, as mj_integratePos / mj_differentiatePos do).  ``rollout`` runs T steps forward, keeping
+checkpoints every ``checkpoint`` steps, and its backward pass recomputes each segment's states
+from its checkpoint and applies lam <- A^T lam, dL/du_t = B^T lam (``mjb_transition_vjp``) from
+the last step to the first.  qacc_warmstart is part of each step's saved state but is not
+differentiated (it is held fixed in every perturbed slot, as mjd_transitionFD does).
+
+These are finite-difference derivatives, not an analytic adjoint: their cost is ncol (or
+2 ncol) extra world-steps per world-step, and across a contact or active-set switch they
+describe the secant of the switch.  They need a step that is (piecewise) smooth in its inputs:
+a Newton solve stopped after 1-3 iterations returns an iterate that jumps when the active set
+seen by an early iteration changes, and differences across those jumps make products of
+transition Jacobians explode; run the solver to convergence (e.g. 10 iterations) when
+differentiating.
+"""
+
+from __future__ import annotations
+
+import ctypes
+from typing import Optional, Tuple
+
+import numpy as np
+import torch
+
+from . import _abi
+from ._api import step
+from .io import make_data
+from .types import Data, Model
+
+JNT_FREE, JNT_BALL = 0, 1
+
+
+def _sizes(m: Model) -> Tuple[int, int]:
+  nx = 2 * m.nv + m.na
+  return nx, nx + m.nu
+
+
+class TransitionFD:
+  """Workspace for the transition Jacobians of `nworld` worlds of model `mjm` / `m`.
+
+  Allocates a Data of nworld * K worlds (K = 1 + ncol, or 1 + 2 ncol when centered) once, with
+  per-world pair / contact / constraint capacities `nconmax` / `njmax` (defaults: 64 and 128
+  per world), and the output tensors A (nworld, nx, nx) and B (nworld, nx, nu).  eps is the
+  perturbation size; in FP32 a value near 1e-3 balances truncation against rounding.
+  """
+
+  def __init__(self, mjm, m: Model, nworld: int, eps: float = 1e-3, centered: bool = True,
+               nconmax: int = 64, njmax: int = 128, fused=True):
+    self.m, self.nworld, self.eps, self.centered, self.fused = m, nworld, float(eps), centered, fused
+    self.nx, self.ncol = _sizes(m)
+    self.K = 1 + self.ncol * (2 if centered else 1)
+    n = nworld * self.K
+    self.pert = make_data(mjm, n, nconmax=nconmax * n, njmax=njmax * n)
+    dev = self.pert.qpos.device
+    self.A = torch.zeros((nworld, self.nx, self.nx), dtype=torch.float32, device=dev)
+    self.B = torch.zeros((nworld, self.nx, m.nu), dtype=torch.float32, device=dev)
+
+  def __call__(self, d: Data) -> Tuple[torch.Tensor, torch.Tensor]:
+    """Jacobians at d's current state and controls (d itself is not modified)."""
+    if d.nworld != self.nworld:
+      raise ValueError(f"workspace is for {self.nworld} worlds, Data has {d.nworld}")
+    L = _abi.lib()
+    mv = _abi.model_view(self.m)
+    rc = L.mjb_fd_perturb(ctypes.byref(mv), ctypes.byref(_abi.data_view(d)),
+                          ctypes.byref(_abi.data_view(self.pert)), self.eps, int(self.centered),
+                          _abi.stream())
+    _abi.check(rc, "fd_perturb")
+    step(self.m, self.pert, fused=self.fused)
+    rc = L.mjb_fd_jacobian(ctypes.byref(mv), ctypes.byref(_abi.data_view(self.pert)), self.nworld,
+                           self.eps, int(self.centered), _abi._ptr(self.A), _abi._ptr(self.B),
+                           _abi.stream())
+    _abi.check(rc, "fd_jacobian")
+    return self.A, self.B
+
+
+def transition_vjp(m: Model, A: torch.Tensor, B: Optional[torch.Tensor], lam: torch.Tensor
+                   ) -> Tuple[torch.Tensor, Optional[torch.Tensor]]:
+  """(A^T lam, B^T lam) per world, on the device."""
+  nworld, nx = lam.shape
+  out = torch.empty_like(lam)
+  gu = torch.empty((nworld, m.nu), dtype=lam.dtype, device=lam.device) if B is not None else None
+  rc = _abi.lib().mjb_transition_vjp(ctypes.byref(_abi.model_view(m)), nworld, _abi._ptr(A),
+                                     _abi._ptr(B) if B is not None else None,
+                                     _abi._ptr(lam.contiguous()), _abi._ptr(out),
+                                     _abi._ptr(gu) if gu is not None else None, _abi.stream())
+  _abi.check(rc, "transition_vjp")
+  return out, gu
+
+
+def _quat_joints(m: Model):
+  """(qpos address of each free / ball joint's quaternion, its first rotational dof)."""
+  cache = m.__dict__.get("_quat_joint_cache")
+  if cache is None:
+    t = m.jnt_type.cpu().numpy()
+    qa = m.jnt_qposadr.cpu().numpy()
+    da = m.jnt_dofadr.cpu().numpy()
+    adr, dof = [], []
+    for j in range(t.shape[0]):
+      if t[j] == JNT_FREE:
+        adr.append(qa[j] + 3)
+        dof.append(da[j] + 3)
+      elif t[j] == JNT_BALL:
+        adr.append(qa[j])
+        dof.append(da[j])
+    dev = m.jnt_type.device
+    cache = (torch.as_tensor(adr, dtype=torch.long, device=dev),
+             torch.as_tensor(dof, dtype=torch.long, device=dev))
+    object.__setattr__(m, "_quat_joint_cache", cache)
+  return cache
+
+
+def _qpos_dof_map(m: Model) -> torch.Tensor:
+  """For every non-quaternion qpos coordinate its dof (qpos and dof coordinates coincide there);
+  -1 for quaternion coordinates."""
+  cache = m.__dict__.get("_qpos_dof_cache")
+  if cache is None:
+    t = m.jnt_type.cpu().numpy()
+    qa = m.jnt_qposadr.cpu().numpy()
+    da = m.jnt_dofadr.cpu().numpy()
+    mp = -np.ones(m.nq, dtype=np.int64)
+    for j in range(t.shape[0]):
+      if t[j] == JNT_FREE:
+        mp[qa[j]:qa[j] + 3] = np.arange(da[j], da[j] + 3)
+      elif t[j] != JNT_BALL:
+        mp[qa[j]] = da[j]
+    cache = torch.as_tensor(mp, device=m.jnt_type.device)
+    object.__setattr__(m, "_qpos_dof_cache", cache)
+  return cache
+
+
+def _quat_basis(q: torch.Tensor) -> torch.Tensor:
+  """q (..., 4) -> (..., 3, 4): q (x) (0, e_k) for k = x, y, z, the tangent directions at q."""
+  w, x, y, z = q.unbind(-1)
+  return torch.stack([torch.stack([-x, w, z, -y], -1),
+                      torch.stack([-y, -z, w, x], -1),
+                      torch.stack([-z, y, -x, w], -1)], -2)
+
+
+def qpos_grad_to_tangent(m: Model, qpos: torch.Tensor, g: torch.Tensor) -> torch.Tensor:
+  """dL/d(qpos coordinates) (nworld, nq) -> dL/d(tangent) (nworld, nv) at qpos: a quaternion's
+  rotation delta about local axis k moves it by 0.5 q (x) (0, e_k)."""
+  out = torch.zeros((g.shape[0], m.nv), dtype=g.dtype, device=g.device)
+  mp = _qpos_dof_map(m)
+  lin = mp >= 0
+  out[:, mp[lin]] = g[:, lin]
+  adr, dof = _quat_joints(m)
+  for a, k in zip(adr.tolist(), dof.tolist()):
+    basis = _quat_basis(qpos[:, a:a + 4])  # (nworld, 3, 4)
+    out[:, k:k + 3] = 0.5 * torch.einsum("wkc,wc->wk", basis, g[:, a:a + 4])
+  return out
+
+
+def tangent_grad_to_qpos(m: Model, qpos: torch.Tensor, lam: torch.Tensor) -> torch.Tensor:
+  """dL/d(tangent) (nworld, nv) -> dL/d(qpos coordinates) (nworld, nq) at unit quaternions: the
+  tangent delta of a coordinate change dq is 2 vec(q* (x) dq), whose rows are q (x) (0, e_k)."""
+  out = torch.zeros((lam.shape[0], m.nq), dtype=lam.dtype, device=lam.device)
+  mp = _qpos_dof_map(m)
+  lin = mp >= 0
+  out[:, lin] = lam[:, mp[lin]]
+  adr, dof = _quat_joints(m)
+  for a, k in zip(adr.tolist(), dof.tolist()):
+    basis = _quat_basis(qpos[:, a:a + 4])
+    out[:, a:a + 4] = 2.0 * torch.einsum("wkc,wk->wc", basis, lam[:, k:k + 3])
+  return out
+
+
+_STATE = ("qpos", "qvel", "act", "qacc_warmstart")
+
+
+def _snapshot(d: Data):
+  return tuple(getattr(d, k).clone() for k in _STATE)
+
+
+def _restore(d: Data, s) -> None:
+  for k, v in zip(_STATE, s):
+    getattr(d, k).copy_(v)
+
+
+class _Rollout(torch.autograd.Function):
+  @staticmethod
+  def forward(ctx, qpos0, qvel0, ctrl, r):
+    d, m = r.d, r.m
+    T = ctrl.shape[0]
+    d.qpos.copy_(qpos0)
+    d.qvel.copy_(qvel0)
+    d.act.zero_()
+    d.qacc_warmstart.zero_()
+    ckpts = []
+    for t in range(T):
+      if t % r.checkpoint == 0:
+        ckpts.append(_snapshot(d))
+      d.ctrl.copy_(ctrl[t])
+      step(m, d, fused=r.fused)
+    ctx.r, ctx.ckpts, ctx.qpos0, ctx.qpos_T = r, ckpts, qpos0.detach(), d.qpos.clone()
+    ctx.save_for_backward(ctrl)
+    return d.qpos.clone(), d.qvel.clone()
+
+  @staticmethod
+  def backward(ctx, gq, gv):
+    (ctrl,) = ctx.saved_tensors
+    r, m, d = ctx.r, ctx.r.m, ctx.r.d
+    T, nworld = ctrl.shape[0], ctrl.shape[1]
+    nv, na = m.nv, m.na
+    lam = torch.zeros((nworld, 2 * nv + na), dtype=torch.float32, device=ctrl.device)
+    if gq is not None:
+      lam[:, :nv] = qpos_grad_to_tangent(m, ctx.qpos_T, gq.float())
+    if gv is not None:
+      lam[:, nv:2 * nv] = gv.float()
+    grad_ctrl = torch.zeros_like(ctrl)
+    for seg in reversed(range(len(ctx.ckpts))):
+      t0, t1 = seg * r.checkpoint, min(T, (seg + 1) * r.checkpoint)
+      _restore(d, ctx.ckpts[seg])
+      states = []
+      for t in range(t0, t1):  # recompute the segment's states from its checkpoint
+        states.append(_snapshot(d))
+        d.ctrl.copy_(ctrl[t])
+        step(m, d, fused=r.fused)
+      for t in reversed(range(t0, t1)):
+        _restore(d, states[t - t0])
+        d.ctrl.copy_(ctrl[t])
+        A, B = r.fd(d)
+        lam, gu = transition_vjp(m, A, B, lam)
+        grad_ctrl[t] = gu
+    grad_qpos0 = tangent_grad_to_qpos(m, ctx.qpos0, lam[:, :nv])
+    grad_qvel0 = lam[:, nv:2 * nv].clone()
+    return grad_qpos0, grad_qvel0, grad_ctrl, None
+
+
+class Rollout:
+  """Differentiable T-step rollout of `nworld` worlds from (qpos0, qvel0) under ctrl (T, nworld, nu).
+
+  Calling it returns (qpos_T, qvel_T); gradients flow to qpos0 (per qpos coordinate), qvel0 and
+  ctrl through finite-difference transition Jacobians (TransitionFD), with the forward states
+  checkpointed every `checkpoint` steps and recomputed segment by segment in the backward pass.
+  Each rollout starts from zero act and qacc_warmstart.
+  """
+
+  def __init__(self, mjm, m: Model, nworld: int, checkpoint: int = 8, eps: float = 1e-3,
+               centered: bool = True, nconmax: int = 64, njmax: int = 128, fused=True):
+    self.m, self.checkpoint, self.fused = m, int(checkpoint), fused
+    self.d = make_data(mjm, nworld, nconmax=nconmax * nworld, njmax=njmax * nworld)
+    self.fd = TransitionFD(mjm, m, nworld, eps=eps, centered=centered, nconmax=nconmax,
+                           njmax=njmax, fused=fused)
+
+  def __call__(self, qpos0: torch.Tensor, qvel0: torch.Tensor, ctrl: torch.Tensor):
+    return _Rollout.apply(qpos0, qvel0, ctrl, self)
+
+
+def rollout(mjm, m: Model, qpos0, qvel0, ctrl, checkpoint: int = 8, eps: float = 1e-3,
+            centered: bool = True):
+  """One-shot form of Rollout (allocates its workspaces)."""
+  return Rollout(mjm, m, qpos0.shape[0], checkpoint=checkpoint, eps=eps, centered=centered)(
+      qpos0, qvel0, ctrl)

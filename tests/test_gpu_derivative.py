@@ -1,0 +1,197 @@
+"""Finite-difference transition Jacobians and the rollout adjoint on the GPU vs FP64 finite
+differences of the oracle (the reference has no derivative API; the scheme is MuJoCo's
+mjd_transitionFD).  Models: pendula.xml (free, ball, slide and hinge joints, motors, no contacts)
+and the humanoid lifted 1 m above the floor (no contacts within the tested steps)."""
+
+import numpy as np
+import pytest
+import torch
+
+import mjx_warp_b200 as mjw
+from helpers import device_data, generic_state, humanoid, humanoid_state, load, oracle
+
+pytestmark = pytest.mark.gpu
+
+
+# quaternion helpers (math.py:118-152): rotation about a local axis and the rotation-vector
+# difference, for the oracle-side perturbations
+def _qmul(u, v):
+  return np.array([u[0] * v[0] - u[1] * v[1] - u[2] * v[2] - u[3] * v[3],
+                   u[0] * v[1] + u[1] * v[0] + u[2] * v[3] - u[3] * v[2],
+                   u[0] * v[2] - u[1] * v[3] + u[2] * v[0] + u[3] * v[1],
+                   u[0] * v[3] + u[1] * v[2] - u[2] * v[1] + u[3] * v[0]])
+
+
+def _qrot(q, axis, ang):
+  r = np.concatenate([[np.cos(0.5 * ang)], np.sin(0.5 * ang) * np.asarray(axis, float)])
+  out = _qmul(q, r)
+  return out / np.linalg.norm(out)
+
+
+def _qsub(qa, qb):
+  dq = _qmul(np.array([qb[0], -qb[1], -qb[2], -qb[3]]), qa)
+  if dq[0] < 0:
+    dq = -dq
+  s = np.linalg.norm(dq[1:])
+  ang = 2.0 * np.arctan2(s, dq[0])
+  return dq[1:] * (ang / s) if s > 0 else np.zeros(3)
+
+
+def _tangent_diff(mjm, qa, qb):
+  out = np.zeros(mjm.nv)
+  for j in range(mjm.njnt):
+    t, a, v = mjm.jnt_type[j], mjm.jnt_qposadr[j], mjm.jnt_dofadr[j]
+    if t == 0:
+      out[v:v + 3] = qa[a:a + 3] - qb[a:a + 3]
+      out[v + 3:v + 6] = _qsub(qa[a + 3:a + 7], qb[a + 3:a + 7])
+    elif t == 1:
+      out[v:v + 3] = _qsub(qa[a:a + 4], qb[a:a + 4])
+    else:
+      out[v] = qa[a] - qb[a]
+  return out
+
+
+def _perturb(mjm, qpos, qvel, ctrl, col, delta):
+  qpos, qvel, ctrl = qpos.copy(), qvel.copy(), ctrl.copy()
+  nv = mjm.nv
+  if col < nv:
+    j = mjm.dof_jntid[col]
+    t, a, r = mjm.jnt_type[j], mjm.jnt_qposadr[j], col - mjm.jnt_dofadr[j]
+    if t == 0 and r < 3:
+      qpos[a + r] += delta
+    elif t in (0, 1):
+      qa = a + 3 if t == 0 else a
+      k = r - 3 if t == 0 else r
+      qpos[qa:qa + 4] = _qrot(qpos[qa:qa + 4], np.eye(3)[k], delta)
+    else:
+      qpos[a] += delta
+  elif col < 2 * nv:
+    qvel[col - nv] += delta
+  else:
+    ctrl[col - 2 * nv] += delta
+  return qpos, qvel, ctrl
+
+
+def _oracle_fd(mjm, qpos, qvel, ctrl, eps=1e-6):
+  """Centered FP64 finite differences of one oracle step, per world (na = 0 here)."""
+  nworld, nv, nu = qpos.shape[0], mjm.nv, mjm.nu
+  nx, ncol = 2 * nv, 2 * nv + nu
+  A = np.zeros((nworld, nx, nx))
+  B = np.zeros((nworld, nx, nu))
+  for c in range(ncol):
+    nxt = []
+    for sgn in (1.0, -1.0):
+      st = [_perturb(mjm, qpos[w], qvel[w], ctrl[w], c, sgn * eps) for w in range(nworld)]
+      o = oracle(mjm, np.stack([s[0] for s in st]), np.stack([s[1] for s in st]),
+                 np.stack([s[2] for s in st]), 64)
+      o.run("step")
+      nxt.append((o.get("qpos"), o.get("qvel")))
+    for w in range(nworld):
+      col = np.concatenate([_tangent_diff(mjm, nxt[0][0][w], nxt[1][0][w]),
+                            nxt[0][1][w] - nxt[1][1][w]]) / (2 * eps)
+      if c < nx:
+        A[w, :, c] = col
+      else:
+        B[w, :, c - nx] = col
+  return A, B
+
+
+def _mid_range(mjm, qpos):
+  """Moves every limited slide / hinge joint to the middle of its range (+ the state's offset
+  from qpos0), away from the limit switch that finite differences would straddle."""
+  qpos = qpos.copy()
+  for j in range(mjm.njnt):
+    if mjm.jnt_type[j] in (2, 3) and mjm.jnt_limited[j]:
+      a = mjm.jnt_qposadr[j]
+      lo, hi = mjm.jnt_range[j]
+      qpos[:, a] += 0.5 * (lo + hi) - mjm.qpos0[a]
+  return qpos
+
+
+def _lifted_humanoid(mjm, nworld, seed):
+  qpos, qvel, ctrl = humanoid_state(mjm, nworld, seed=seed)
+  qpos[:, 2] += 1.0
+  return qpos, qvel, ctrl
+
+
+@pytest.mark.parametrize("name", ["pendula.xml", "humanoid"])
+def test_transition_jacobians_vs_fp64_fd(name):
+  if name == "humanoid":
+    mjm = humanoid()
+    qpos, qvel, ctrl = _lifted_humanoid(mjm, 3, seed=2)
+  else:
+    mjm = load(name)
+    qpos, qvel, ctrl = generic_state(mjm, 3, seed=2, qscale=0.05, vscale=0.05)
+    qpos = _mid_range(mjm, qpos)
+  m = mjw.put_model(mjm)
+  d = device_data(mjm, qpos, qvel, ctrl)
+  fd = mjw.derivative.TransitionFD(mjm, m, 3, eps=1e-3, centered=True)
+  A, B = fd(d)
+  torch.cuda.synchronize()
+  assert np.allclose(d.qpos.cpu().numpy(), qpos.astype(np.float32))  # base Data untouched
+  Ar, Br = _oracle_fd(mjm, qpos, qvel, ctrl)
+  A, B = A.cpu().numpy().astype(float), B.cpu().numpy().astype(float)
+  for w in range(3):
+    ea = np.linalg.norm(A[w] - Ar[w]) / np.linalg.norm(Ar[w])
+    eb = np.linalg.norm(B[w] - Br[w]) / max(np.linalg.norm(Br[w]), 1e-12)
+    assert ea < 2e-3 and eb < 2e-3, (w, ea, eb)
+
+
+def test_forward_and_centered_differences_agree():
+  mjm = load("pendula.xml")
+  qpos, qvel, ctrl = generic_state(mjm, 4, seed=3, qscale=0.05, vscale=0.05)
+  qpos = _mid_range(mjm, qpos)
+  m = mjw.put_model(mjm)
+  d = device_data(mjm, qpos, qvel, ctrl)
+  Ac, Bc = (t.clone() for t in mjw.derivative.TransitionFD(mjm, m, 4, eps=1e-3, centered=True)(d))
+  Af, Bf = mjw.derivative.TransitionFD(mjm, m, 4, eps=1e-3, centered=False)(d)
+  assert torch.linalg.norm(Af - Ac) / torch.linalg.norm(Ac) < 2e-2
+  assert torch.linalg.norm(Bf - Bc) / torch.linalg.norm(Bc) < 2e-2
+
+
+def test_rollout_gradient_vs_fp64_central_fd():
+  """d/d(ctrl, qvel0, qpos0) of ||root_pos_T - target||^2 + 1e-3 ||ctrl||^2 over an 8-step
+  rollout (checkpoints every 4 steps) vs central FP64 differences of the oracle's loss."""
+  mjm = humanoid()
+  nworld, T = 2, 8
+  qpos, qvel, _ = _lifted_humanoid(mjm, nworld, seed=4)
+  rng = np.random.default_rng(5)
+  ctrl = rng.uniform(-0.4, 0.4, (T, nworld, mjm.nu))
+  target = np.array([0.1, -0.1, 2.0])
+  m = mjw.put_model(mjm)
+  roll = mjw.derivative.Rollout(mjm, m, nworld, checkpoint=4)
+  q0 = torch.tensor(qpos, dtype=torch.float32, device="cuda", requires_grad=True)
+  v0 = torch.tensor(qvel, dtype=torch.float32, device="cuda", requires_grad=True)
+  u = torch.tensor(ctrl, dtype=torch.float32, device="cuda", requires_grad=True)
+  qT, _ = roll(q0, v0, u)
+  tgt = torch.tensor(target, dtype=torch.float32, device="cuda")
+  loss = ((qT[:, :3] - tgt) ** 2).sum() + 1e-3 * (u ** 2).sum()
+  loss.backward()
+
+  def loss64(qp, qv, cu):
+    o = oracle(mjm, qp, qv, cu[0], 64)
+    for t in range(T):
+      o.set("ctrl", cu[t])
+      o.run("step")
+    return float(((o.get("qpos")[:, :3] - target) ** 2).sum() + 1e-3 * (cu ** 2).sum())
+
+  h = 1e-5
+  checks = []
+  for (t, w, a) in [(0, 0, 3), (3, 1, 10), (7, 0, 20), (5, 1, 0)]:
+    cp, cm = ctrl.copy(), ctrl.copy()
+    cp[t, w, a] += h
+    cm[t, w, a] -= h
+    checks.append((u.grad[t, w, a].item(), (loss64(qpos, qvel, cp) - loss64(qpos, qvel, cm)) / (2 * h)))
+  for (w, i) in [(0, 2), (1, 8), (0, 20)]:
+    vp, vm = qvel.copy(), qvel.copy()
+    vp[w, i] += h
+    vm[w, i] -= h
+    checks.append((v0.grad[w, i].item(), (loss64(qpos, vp, ctrl) - loss64(qpos, vm, ctrl)) / (2 * h)))
+  for (w, i) in [(1, 0), (0, 2), (1, 10)]:  # root x, root z, a hinge
+    pp, pm = qpos.copy(), qpos.copy()
+    pp[w, i] += h
+    pm[w, i] -= h
+    checks.append((q0.grad[w, i].item(), (loss64(pp, qvel, ctrl) - loss64(pm, qvel, ctrl)) / (2 * h)))
+  scale = max(abs(c[1]) for c in checks)
+  for g, f in checks:
+    assert abs(g - f) <= 1e-2 * abs(f) + 2e-3 * scale, checks
