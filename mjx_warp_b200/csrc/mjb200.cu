@@ -268,7 +268,8 @@ inline int check(const MjbModel* m, const MjbData* d) {
 // shared memory per warp (floats) for the solver workspace when nv <= 32, else a factor tile for
 // the tree blocks of up to 32 dofs (the generic solver keeps its Hessian in efc_h)
 int solver_smem_per_warp(const MjbModel* m) {
-  return m->nv <= 32 ? int(solver_smem_floats(m->nv)) : tile_floats(m->nv);
+  return m->nv <= 32 ? int(solver_smem_floats(m->nv))
+                     : std::max(tile_floats(m->nv), generic_nz_floats(m->nv));
 }
 
 // the single form's warp slice also serves the sweep-and-prune broadphase (ngeom > 100)
@@ -298,7 +299,7 @@ int launch_stage(const MjbModel* m, const MjbData* d, cudaStream_t s) {
   const int warps = kDefaultWarps;
   int spw = 0;
   size_t bytes = 0;
-  if (STAGE == S_SOLVE) spw = m->nv <= 32 ? int(solver_smem_floats(m->nv)) : 0;
+  if (STAGE == S_SOLVE) spw = m->nv <= 32 ? int(solver_smem_floats(m->nv)) : generic_nz_floats(m->nv);
   if (STAGE == S_FACTOR_M || STAGE == S_FWD_ACCELERATION || STAGE == S_EULER || STAGE == S_IMPLICIT)
     spw = tile_floats(m->nv);
   if (STAGE == S_SAP) spw = sap_smem_floats(m->ngeom);
@@ -370,7 +371,7 @@ int run_chosen_phase(const MjbModel* m, const MjbData* d, int phase, cudaStream_
     if (rc) return rc;
   } else if (phase == 1) {
     if (d->njmax > 0) {
-      const int spw = m->nv <= 32 ? int(solver_smem_floats(m->nv)) : 0;
+      const int spw = m->nv <= 32 ? int(solver_smem_floats(m->nv)) : generic_nz_floats(m->nv);
       const size_t bytes = size_t(spw) * warps * sizeof(float);
       allow_smem(k_solve, bytes, conf_solve);
       k_solve<<<grid, 32 * warps, bytes, s>>>(*m, *d, spw);

@@ -21,9 +21,20 @@ struct SolverCtx {
   float *qacc, *Ma, *grad, *Mgrad, *search, *mv, *qfrc_constraint;
   const float *qM, *qLD, *qfrc_smooth, *qacc_smooth;
   float* hs;
+  float* nz;                 // warp scratch of generic_nz_floats(nv) floats, or null
+  bool reuse = false;        // keep the Hessian factor while the active set is unchanged
+  bool factored = false;     // hs holds the factor of the current active set's Hessian
+  bool changed = true;       // the last update_constraint changed an active flag
   float cost, prev_cost, gauss, grad_dot, search_dot, gtol, alpha;
   float qg[3];
 };
+
+__host__ __device__ __forceinline__ int round4i(int x) { return (x + 3) & ~3; }
+// warp scratch of the generic (nv > 32) solver: a constraint row's nonzero columns and values
+// during the Hessian assembly, then the blocked Cholesky's 32 x 36 tile
+__host__ __device__ __forceinline__ int generic_nz_floats(int nv) {
+  return 2 * round4i(nv) > 32 * 36 ? 2 * round4i(nv) : 32 * 36;
+}
 
 __device__ __forceinline__ float safe_div(float x, float y) { return x / (y != 0.f ? y : kMinVal); }
 
@@ -43,10 +54,12 @@ __device__ void update_constraint(SolverCtx& s) {
   const int nv = s.nv;
   s.prev_cost = s.cost;
   float c = 0.f;
+  bool changed = false;
   for (int k = s.lane; k < s.n; k += 32) {
     const int r = s.adr + k;
     const float Jaref = d.efc_Jaref[r], D = d.efc_D[r];
     const int active = Jaref < 0.f;
+    changed |= d.efc_active[r] != active;
     d.efc_active[r] = active;
     if (active) {
       d.efc_force[r] = -1.f * D * Jaref;
@@ -55,6 +68,7 @@ __device__ void update_constraint(SolverCtx& s) {
       d.efc_force[r] = 0.f;
     }
   }
+  s.changed = __any_sync(WARP_FULL, changed);
   c = warp_sum(c);
   __syncwarp();
   for (int i = s.lane; i < nv; i += 32) {
@@ -88,29 +102,76 @@ __device__ void update_gradient(SolverCtx& s) {
     solve_blocks(m, s.qLD, s.Mgrad, s.grad, lane);
     return;
   }
-  // Newton: H = tril(qM) + sum_active D J^T J, then dense Cholesky solve
+  // Newton: H = tril(qM) + sum_active D J^T J, then dense Cholesky solve.  With s.reuse the
+  // factor of the previous call is kept while no active flag changed (the same H, the same bits).
   float* H = s.hs;
-  for (int e = lane; e < nv * nv; e += 32) {
-    const int i = e / nv, j = e - i * nv;
-    if (j > i) continue;
-    float h = s.qM[e];
-    for (int k = 0; k < s.n; k++) {
-      const int r = s.adr + k;
-      if (!d.efc_active[r]) continue;
-      const float D = d.efc_D[r];
-      if (D == 0.f) continue;
-      const float* J = d.efc_J + size_t(r) * nv;
-      h += J[i] * J[j] * D;
+  if (!(s.reuse && s.factored && !s.changed)) {
+    if (s.nz) {
+      // Each row's outer product touches only the row's nonzero columns (a contact row has the
+      // dofs of two kinematic chains): the columns are compacted in order into the warp's
+      // scratch and the lower-triangle pairs updated, row by row, with the per-entry arithmetic
+      // of the dense form (h += J_i * J_j * D in row order; zero terms are skipped).
+      for (int e = lane; e < nv * nv; e += 32) {
+        const int i = e / nv, j = e - i * nv;
+        if (j <= i) H[e] = s.qM[e];
+      }
+      __syncwarp();
+      int* nzi = reinterpret_cast<int*>(s.nz);
+      float* nzv = s.nz + round4i(nv);
+      for (int k = 0; k < s.n; k++) {
+        const int r = s.adr + k;
+        if (!d.efc_active[r]) continue;
+        const float D = d.efc_D[r];
+        if (D == 0.f) continue;
+        const float* J = d.efc_J + size_t(r) * nv;
+        int cnt = 0;
+        for (int base = 0; base < nv; base += 32) {
+          const int c = base + lane;
+          const float v = c < nv ? J[c] : 0.f;
+          const unsigned mk = __ballot_sync(WARP_FULL, v != 0.f);
+          if (v != 0.f) {
+            const int p = cnt + __popc(mk & ((1u << lane) - 1u));
+            nzi[p] = c;
+            nzv[p] = v;
+          }
+          cnt += __popc(mk);
+        }
+        __syncwarp();
+        const int npair = cnt * (cnt + 1) / 2;
+        for (int t = lane; t < npair; t += 32) {  // pair t = (a, b), b <= a, in triangle order
+          int a = int((sqrtf(8.f * float(t) + 1.f) - 1.f) * 0.5f);
+          while (a * (a + 1) / 2 > t) a--;
+          while ((a + 1) * (a + 2) / 2 <= t) a++;
+          const int b = t - a * (a + 1) / 2;
+          H[nzi[a] * nv + nzi[b]] += nzv[a] * nzv[b] * D;
+        }
+        __syncwarp();
+      }
+    } else {
+      for (int e = lane; e < nv * nv; e += 32) {
+        const int i = e / nv, j = e - i * nv;
+        if (j > i) continue;
+        float h = s.qM[e];
+        for (int k = 0; k < s.n; k++) {
+          const int r = s.adr + k;
+          if (!d.efc_active[r]) continue;
+          const float D = d.efc_D[r];
+          if (D == 0.f) continue;
+          const float* J = d.efc_J + size_t(r) * nv;
+          h += J[i] * J[j] * D;
+        }
+        H[e] = h;
+      }
+      __syncwarp();
     }
-    H[e] = h;
+    if (d.efc_h) {  // keep the assembled Hessian observable (lower triangle), as the reference does
+      float* out = d.efc_h + W(s.w, nv * nv);
+      if (out != H)
+        for (int e = lane; e < nv * nv; e += 32) out[e] = H[e];
+    }
+    chol_any(H, nv, nv, lane, s.nz);
+    s.factored = true;
   }
-  __syncwarp();
-  if (d.efc_h) {  // keep the assembled Hessian observable (lower triangle), as the reference does
-    float* out = d.efc_h + W(s.w, nv * nv);
-    if (out != H)
-      for (int e = lane; e < nv * nv; e += 32) out[e] = H[e];
-  }
-  chol_lower(H, nv, nv, lane);
   warp_cho_solve(H, nv, nv, s.Mgrad, s.grad, lane);
 }
 
@@ -272,10 +333,15 @@ __device__ void linesearch(SolverCtx& s) {
   __syncwarp();
 }
 
-// solver.py:872-1000, any nv; hs: per-warp scratch of nv*nv floats (Newton only)
-__device__ __noinline__ void solve_generic(const MjbModel& m, const MjbData& d, int w, int lane, float* hs) {
+// solver.py:872-1000, any nv; hs: per-world nv*nv floats (the Newton Hessian and its factor);
+// nz: null or generic_nz_floats(nv) floats of warp scratch for the sparse-row Hessian assembly;
+// reuse: keep the factor while the active set is unchanged
+__device__ __noinline__ void solve_generic(const MjbModel& m, const MjbData& d, int w, int lane,
+                                           float* hs, float* nz, bool reuse) {
   const int nv = m.nv;
   SolverCtx s{m, d, w, lane, nv, d.world_efcadr[w], d.world_nefc[w]};
+  s.nz = nz;
+  s.reuse = reuse;
   s.qacc = d.qacc + W(w, nv);
   s.Ma = d.efc_Ma + W(w, nv);
   s.grad = d.efc_grad + W(w, nv);
@@ -825,10 +891,11 @@ __device__ void solve_small(const MjbModel& m, const MjbData& d, int w, int lane
 // Dispatch: the register / shared-memory solver when nv <= 32 and the caller provides its scratch
 // (solver_smem_floats(nv) floats), else the generic solver with an nv x nv Hessian tile `hs`.
 // reuse: keep the Newton Hessian's factor across iterations with an unchanged active set.
+// For nv > 32, sm (when given) is the generic solver's scratch of generic_nz_floats(nv) floats.
 __device__ __forceinline__ void solve(const MjbModel& m, const MjbData& d, int w, int lane,
                                       float* sm, float* hs, bool reuse = false) {
   if (m.nv <= 32 && sm) solve_small(m, d, w, lane, sm, reuse);
-  else solve_generic(m, d, w, lane, hs);
+  else solve_generic(m, d, w, lane, hs, m.nv > 32 ? sm : nullptr, reuse);
 }
 
 }  // namespace mjb

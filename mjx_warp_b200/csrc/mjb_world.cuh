@@ -460,6 +460,86 @@ __device__ __forceinline__ void tile_store_lower(const float* T, int tld, int n,
     if (lane < n) L[r * ld + lane] = lane <= r ? T[r * tld + lane] : 0.f;
 }
 
+// Right-looking blocked Cholesky of the n x n SPD lower triangle of A (row stride ld, shared or
+// global memory) in panels of 32 columns, with a warp scratch tile T of 32 x 36 floats (16-byte
+// aligned).  Per panel: (a) the diagonal block is staged in T, factored by chol_tile and written
+// back; (b) every row below it solves L_i = A_i L_pp^-T against the factored block (lane per row,
+// the row's 32 panel entries in registers, the block and its reciprocal diagonal read from T by
+// broadcast); (c) the trailing lower triangle is updated, A_ij -= L_i . L_j over the panel, one
+// chunk of 32 rows j at a time staged in T, lane per row i, float4 broadcast reads.  The column
+// dot products are accumulated panel by panel, so the bits differ from chol_lower's.
+__device__ __noinline__ void chol_blocked(float* A, int ld, int n, int lane, float* T) {
+  constexpr int TL = 36;
+  for (int p0 = 0; p0 < n; p0 += 32) {
+    const int pn = min(32, n - p0);
+    // (a)
+    for (int r = 0; r < pn; r++)
+      if (lane < pn) T[r * TL + lane] = lane <= r ? A[size_t(p0 + r) * ld + p0 + lane] : 0.f;
+    __syncwarp();
+    chol_tile(T, TL, pn, lane);
+    for (int r = 0; r < pn; r++)
+      if (lane <= r) A[size_t(p0 + r) * ld + p0 + lane] = T[r * TL + lane];
+    if (lane < pn) T[lane * TL + 32] = __frcp_rn(T[lane * TL + lane]);
+    __syncwarp();
+    // (b)
+    for (int i = p0 + pn + lane; i < n; i += 32) {
+      float* Ai = A + size_t(i) * ld + p0;
+      float x[32];
+#pragma unroll
+      for (int c = 0; c < 32; c++) x[c] = c < pn ? Ai[c] : 0.f;
+#pragma unroll
+      for (int c = 0; c < 32; c++) {
+        if (c < pn) {
+          float v = x[c];
+#pragma unroll
+          for (int q = 0; q < c; q++) v -= x[q] * T[c * TL + q];
+          x[c] = v * T[c * TL + 32];
+        }
+      }
+#pragma unroll
+      for (int c = 0; c < 32; c++)
+        if (c < pn) Ai[c] = x[c];
+    }
+    __syncwarp();
+    // (c)
+    for (int j0 = p0 + pn; j0 < n; j0 += 32) {
+      const int jn = min(32, n - j0);
+      for (int jj = 0; jj < jn; jj++)
+        T[jj * TL + lane] = lane < pn ? A[size_t(j0 + jj) * ld + p0 + lane] : 0.f;
+      __syncwarp();
+      for (int i = j0 + lane; i < n; i += 32) {
+        const float* Li = A + size_t(i) * ld + p0;
+        float x[32];
+#pragma unroll
+        for (int c = 0; c < 32; c++) x[c] = c < pn ? Li[c] : 0.f;
+        float* Ai = A + size_t(i) * ld + j0;
+        const int jm = min(jn, i - j0 + 1);
+        for (int jj = 0; jj < jm; jj++) {
+          const float4* P4 = reinterpret_cast<const float4*>(T + jj * TL);
+          float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f;
+#pragma unroll
+          for (int q = 0; q < 8; q++) {
+            const float4 pv = P4[q];
+            s0 += x[4 * q] * pv.x;
+            s1 += x[4 * q + 1] * pv.y;
+            s2 += x[4 * q + 2] * pv.z;
+            s3 += x[4 * q + 3] * pv.w;
+          }
+          Ai[jj] -= (s0 + s1) + (s2 + s3);
+        }
+      }
+      __syncwarp();
+    }
+  }
+}
+
+// Cholesky of an n x n SPD block: blocked (chol_blocked) when n > 32 and a 32 x 36 warp scratch
+// tile is given, else chol_lower.
+__device__ __forceinline__ void chol_any(float* A, int ld, int n, int lane, float* tile) {
+  if (n > 32 && tile) chol_blocked(A, ld, n, lane, tile);
+  else chol_lower(A, ld, n, lane);
+}
+
 // x = (L L^T)^-1 y for the n x n lower factor at L (leading dimension ld); x may alias y.
 __device__ void warp_cho_solve(const float* L, int ld, int n, float* x, const float* y, int lane) {
   if (n <= 32) {
@@ -535,9 +615,9 @@ __device__ void factor_blocks(const MjbModel& m, const float* M, float* L, int l
     __syncwarp();
 #if MJB_CHOL == 1
     if (n <= 32) chol32(L + a * nv + a, nv, n, lane, 0.f);
-    else chol_lower(L + a * nv + a, nv, n, lane);
+    else chol_any(L + a * nv + a, nv, n, lane, tile);
 #else
-    chol_lower(L + a * nv + a, nv, n, lane);
+    chol_any(L + a * nv + a, nv, n, lane, tile);
 #endif
   }
 }
@@ -964,7 +1044,7 @@ __device__ void implicit(const MjbModel& m, const MjbData& d, int w, int lane, f
     }
   }
   if (!tiled) {
-    factor_blocks(m, Mi, L, lane);
+    factor_blocks(m, Mi, L, lane, nullptr, 0.f, tile);
     solve_blocks(m, L, x, f, lane);
   }
   advance(m, d, w, x, lane);
