@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define MJB_ABI_VERSION 1
+#define MJB_ABI_VERSION 2
 
 typedef struct CUstream_st* mjbStream; /* == cudaStream_t */
 
@@ -128,6 +128,10 @@ typedef struct MjbData {
   /* per-world index of the flat arrays and status bits */
   int32_t *world_pairadr, *world_npair, *world_conadr, *world_ncon, *world_efcadr, *world_nefc;
   uint32_t* world_status;
+  /* the chosen form's solver schedule (may be null: worlds are then solved in index order):
+     world_order (nworld) receives the worlds sorted by constraint rows, largest first, and
+     work_queue (1) is the persistent solver's next-world counter */
+  int32_t *world_order, *work_queue;
 } MjbData;
 
 /* Launch configuration for the step entry points. */

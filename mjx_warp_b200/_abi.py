@@ -97,6 +97,7 @@ DATA_PTRS = (
   ("world_conadr", "world_conadr"), ("world_ncon", "world_ncon"),
   ("world_efcadr", "world_efcadr"), ("world_nefc", "world_nefc"),
   ("world_status", "world_status"),
+  ("world_order", "world_order"), ("work_queue", "work_queue"),
 )
 
 
@@ -161,7 +162,7 @@ def lib() -> ctypes.CDLL:
   L.mjb_fd_jacobian.argtypes = [pm, pd, ci, cf, ci, vp, vp, vp]
   L.mjb_transition_vjp.restype = ctypes.c_int
   L.mjb_transition_vjp.argtypes = [pm, ci, vp, vp, vp, vp, vp, vp]
-  if L.mjb_abi_version() != 1:
+  if L.mjb_abi_version() != 2:
     raise RuntimeError("libmjb200.so ABI version mismatch")
   _lib = L
   return L

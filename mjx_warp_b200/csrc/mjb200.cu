@@ -131,6 +131,49 @@ __global__ void __launch_bounds__(128, MJB_MINB) k_solve(const __grid_constant__
   solve(m, d, w, lane, sm, d.efc_h + W(w, m.nv * m.nv), true);
 }
 
+// The chosen form's solver schedule.  k_order_worlds sorts the worlds by their constraint row
+// count, largest first (a counting sort over buckets min(nefc, 255) in one CTA), and resets the
+// work queue; k_solve_queue is persistent — as many CTAs as fit on the GPU at once — and each of
+// its warps takes the next world in that order from the queue until none is left, so the longest
+// solves start first and the last ones to finish are short (longest-processing-time-first).
+// Each world's result does not depend on which warp solves it or when.
+constexpr int kOrderBuckets = 256;
+__global__ void __launch_bounds__(1024) k_order_worlds(const int* nefc, int* order, int* queue,
+                                                      int nworld) {
+  __shared__ int cnt[kOrderBuckets];
+  for (int b = threadIdx.x; b < kOrderBuckets; b += blockDim.x) cnt[b] = 0;
+  __syncthreads();
+  for (int w = threadIdx.x; w < nworld; w += blockDim.x)
+    atomicAdd(&cnt[min(max(nefc[w], 0), kOrderBuckets - 1)], 1);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int run = 0;
+    for (int b = kOrderBuckets - 1; b >= 0; b--) {
+      const int c = cnt[b];
+      cnt[b] = run;
+      run += c;
+    }
+    *queue = 0;
+  }
+  __syncthreads();
+  for (int w = threadIdx.x; w < nworld; w += blockDim.x)
+    order[atomicAdd(&cnt[min(max(nefc[w], 0), kOrderBuckets - 1)], 1)] = w;
+}
+
+__global__ void __launch_bounds__(128, MJB_MINB) k_solve_queue(const __grid_constant__ MjbModel m, const __grid_constant__ MjbData d, int smem_per_warp) {
+  extern __shared__ __align__(16) float smem[];
+  const int lane = threadIdx.x & 31;
+  float* sm = smem_per_warp ? smem + size_t(threadIdx.x >> 5) * smem_per_warp : nullptr;
+  for (;;) {
+    int idx = 0;
+    if (lane == 0) idx = atomicAdd(d.work_queue, 1);
+    idx = __shfl_sync(WARP_FULL, idx, 0);
+    if (idx >= d.nworld) break;
+    const int w = d.world_order[idx];
+    solve(m, d, w, lane, sm, d.efc_h + W(w, m.nv * m.nv), true);
+  }
+}
+
 // chosen form: integration (forward.py:165-405) and the finiteness check
 __global__ void __launch_bounds__(128, 8) k_integrate(const __grid_constant__ MjbModel m, const __grid_constant__ MjbData d, int tile_per_warp) {
   extern __shared__ __align__(16) float smem[];
@@ -294,6 +337,27 @@ void allow_smem(K kernel, size_t bytes, size_t (&configured)[kSmemDevices]) {
   }
 }
 
+// CTAs of `kernel` resident on the whole GPU at once for blocks of `threads` threads and `smem`
+// bytes, queried once per device and shared-memory size (the block size is fixed per kernel)
+template <typename K>
+int resident_ctas(K kernel, int threads, size_t smem) {
+  static int cached[kSmemDevices];
+  static size_t cached_smem[kSmemDevices];
+  int dev = 0;
+  cudaGetDevice(&dev);
+  const bool slot = dev >= 0 && dev < kSmemDevices;
+  if (slot && cached[dev] > 0 && cached_smem[dev] == smem) return cached[dev];
+  int sms = 0, per_sm = 0;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem);
+  const int n = std::max(1, sms * std::max(1, per_sm));
+  if (slot) {
+    cached[dev] = n;
+    cached_smem[dev] = smem;
+  }
+  return n;
+}
+
 template <int STAGE>
 int launch_stage(const MjbModel* m, const MjbData* d, cudaStream_t s) {
   const int warps = kDefaultWarps;
@@ -373,8 +437,16 @@ int run_chosen_phase(const MjbModel* m, const MjbData* d, int phase, cudaStream_
     if (d->njmax > 0) {
       const int spw = m->nv <= 32 ? int(solver_smem_floats(m->nv)) : generic_nz_floats(m->nv);
       const size_t bytes = size_t(spw) * warps * sizeof(float);
-      allow_smem(k_solve, bytes, conf_solve);
-      k_solve<<<grid, 32 * warps, bytes, s>>>(*m, *d, spw);
+      if (d->world_order && d->work_queue && d->world_nefc) {
+        static size_t conf_queue[kSmemDevices];
+        allow_smem(k_solve_queue, bytes, conf_queue);
+        const int ctas = resident_ctas(k_solve_queue, 32 * warps, bytes);
+        k_order_worlds<<<1, 1024, 0, s>>>(d->world_nefc, d->world_order, d->work_queue, d->nworld);
+        k_solve_queue<<<std::min(ctas, grid), 32 * warps, bytes, s>>>(*m, *d, spw);
+      } else {
+        allow_smem(k_solve, bytes, conf_solve);
+        k_solve<<<grid, 32 * warps, bytes, s>>>(*m, *d, spw);
+      }
     }
   } else if (phase == 2) {
     allow_smem(k_integrate, tile_bytes, conf_int);

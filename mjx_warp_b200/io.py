@@ -273,6 +273,7 @@ def _data_arrays(mjm, nworld, nconmax, njmax, dev):
     "ncon": i(1), "nefc": i(1),
     "world_pairadr": i(W), "world_npair": i(W), "world_conadr": i(W), "world_ncon": i(W),
     "world_efcadr": i(W), "world_nefc": i(W), "world_status": torch.zeros(W, dtype=torch.int32, device=dev),
+    "world_order": i(W), "work_queue": i(1),
   }
   contact = {
     "dist": f(nconmax), "pos": f(nconmax, 3), "frame": f(nconmax, 3, 3),
