@@ -9,7 +9,8 @@ synthetic initial states (keyframe "squat" + U(-0.05, 0.05), qvel ~ N(0, 0.01),
 ctrl ~ U(-0.4, 0.4)).  A "step" is one mjw.step over all worlds.
 
 value: world-steps/s with the state resident in HBM, one captured CUDA graph of the step replayed
-K times, in the chosen launch form (reset + k_smooth + k_solve + k_integrate); `forms` gives the
+K times, in the chosen launch form (the stage kernels to fwd_acceleration, the solver's world
+ordering + persistent k_solve_queue, k_integrate); `forms` gives the
 same number for the plain one-kernel-per-stage form (the reference's launch sequence and
 algorithm) and the single-kernel form, measured in the same run.  e2e: the metric through the
 public API (mjw.step) with, every step, the control copied in from pinned host memory and
@@ -141,7 +142,7 @@ def _algorithmic_bytes(d, mjm, ncon, nefc):
 
 
 FORMS = {"plain": 0, "chosen": 1, "single": 2}
-LAUNCHES = {"plain": 16, "chosen": 15, "single": 2}  # kernels per step (mjb200.cu run_* paths)
+LAUNCHES = {"plain": 16, "chosen": 16, "single": 2}  # kernels per step (mjb200.cu run_* paths)
 
 
 def _solver_bytes(mjm, nworld, nefc):
@@ -426,7 +427,8 @@ def run_ours(args):
     "gpu_launches": launches_per_step * args.steps,
     "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                  "frac": achieved / hbm, "traffic": traffic,
-                 "kernel": "k_stage<S_SOLVE> (plain)" if args.form == "plain" else "k_solve",
+                 "kernel": "k_stage<S_SOLVE> (plain)" if args.form == "plain"
+                           else "k_solve_queue (+ k_order_worlds)",
                  "kernel_ms": solve_s * 1e3, "kernel_share_of_step": solve_s / (elapsed / args.steps),
                  "algorithmic_bytes_per_launch": alg, "peak_source": "measured" if peaks else "fallback",
                  "step_algorithmic_bytes": step_alg,
