@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <mutex>
 
 #include "mjb_deriv.cuh"
 #include "mjb_solver.cuh"
@@ -415,6 +416,60 @@ int run_forward_plain_nosolve(const MjbModel* m, const MjbData* d, cudaStream_t 
   return MJB_OK;
 }
 
+// The chosen form's fwd_position .. fwd_acceleration as a fork-join over three chains that share
+// no outputs: after kinematics and com_pos on the caller's stream, crb -> factor_m and
+// transmission -> fwd_velocity -> fwd_actuation run on two auxiliary streams while collision and
+// make_constraint continue on the caller's stream; fwd_acceleration joins them.  Each chain's
+// kernels fill the tails of the others'.  The auxiliary streams and events are created once per
+// device (no memory is allocated) and the enqueue sequence is serialised by a mutex; inside a
+// stream capture the fork and join become graph edges.
+struct StageFork {
+  cudaStream_t aux[2] = {nullptr, nullptr};
+  cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+  bool ready = false;
+};
+std::mutex g_fork_mutex;
+StageFork g_fork[kSmemDevices];
+
+int run_forward_fork(const MjbModel* m, const MjbData* d, cudaStream_t s) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kSmemDevices)
+    return run_forward_plain_nosolve(m, d, s);
+  std::lock_guard<std::mutex> lock(g_fork_mutex);
+  StageFork& f = g_fork[dev];
+  if (!f.ready) {
+    for (auto& a : f.aux)
+      if (cudaStreamCreateWithFlags(&a, cudaStreamNonBlocking) != cudaSuccess) return MJB_ERR_LAUNCH;
+    for (auto& e : f.ev)
+      if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return MJB_ERR_LAUNCH;
+    f.ready = true;
+  }
+  int rc;
+  if ((rc = launch_stage<S_KINEMATICS>(m, d, s))) return rc;
+  if ((rc = launch_stage<S_COM_POS>(m, d, s))) return rc;
+  if (cudaEventRecord(f.ev[0], s) != cudaSuccess) return MJB_ERR_LAUNCH;
+  for (auto& a : f.aux)
+    if (cudaStreamWaitEvent(a, f.ev[0], 0) != cudaSuccess) return MJB_ERR_LAUNCH;
+  int rc0 = launch_stage<S_CRB>(m, d, f.aux[0]);
+  if (!rc0) rc0 = launch_stage<S_FACTOR_M>(m, d, f.aux[0]);
+  int rc1 = launch_stage<S_TRANSMISSION>(m, d, f.aux[1]);
+  if (!rc1) rc1 = launch_stage<S_FWD_VELOCITY>(m, d, f.aux[1]);
+  if (!rc1) rc1 = launch_stage<S_FWD_ACTUATION>(m, d, f.aux[1]);
+  reset_counters(d, true, true, true, false, s);
+  int rc2 = launch_broadphase(m, d, s);
+  if (!rc2) rc2 = launch_stage<S_NARROW>(m, d, s);
+  if (!rc2) rc2 = launch_stage<S_MAKE_CONSTRAINT>(m, d, s);
+  // join even after a failed launch, so a capture is never left with unjoined streams
+  if (cudaEventRecord(f.ev[1], f.aux[0]) != cudaSuccess) return MJB_ERR_LAUNCH;
+  if (cudaEventRecord(f.ev[2], f.aux[1]) != cudaSuccess) return MJB_ERR_LAUNCH;
+  if (cudaStreamWaitEvent(s, f.ev[1], 0) != cudaSuccess) return MJB_ERR_LAUNCH;
+  if (cudaStreamWaitEvent(s, f.ev[2], 0) != cudaSuccess) return MJB_ERR_LAUNCH;
+  if (rc0 || rc1 || rc2) return rc0 ? rc0 : (rc1 ? rc1 : rc2);
+  if ((rc = launch_stage<S_FWD_ACCELERATION>(m, d, s))) return rc;
+  if (d->njmax == 0) return launch_stage<S_QACC_SMOOTH_COPY>(m, d, s);
+  return MJB_OK;
+}
+
 int run_forward_plain(const MjbModel* m, const MjbData* d, cudaStream_t s) {
   int rc;
   if ((rc = run_forward_plain_nosolve(m, d, s))) return rc;
@@ -431,7 +486,7 @@ int run_chosen_phase(const MjbModel* m, const MjbData* d, int phase, cudaStream_
   static size_t conf_solve[kSmemDevices], conf_int[kSmemDevices];
   if (phase == 0) {
     reset_counters(d, false, false, false, true, s);
-    int rc = run_forward_plain_nosolve(m, d, s);
+    int rc = run_forward_fork(m, d, s);
     if (rc) return rc;
   } else if (phase == 1) {
     if (d->njmax > 0) {
