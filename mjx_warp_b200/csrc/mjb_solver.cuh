@@ -488,6 +488,10 @@ struct Small {
   int ld, nq;                   // staged row stride and float4 count per row (4 * nq >= nv)
   bool staged;                  // J rows copied to shared memory (else read from efc_J)
   bool own;
+  // With staged rows (n <= 32) lane k owns row k and keeps its scalars in registers; the flat
+  // efc arrays are then only written (they stay the observable outputs).
+  float rJaref = 0.f, rjv = 0.f, rD = 0.f, rq0 = 0.f, rq1 = 0.f, rq2 = 0.f;
+  int ract = 0;
   bool reuse = false;           // keep the factor of H while the active set is unchanged
   bool factored = false;        // Ls holds the factor of H for the active set factored_mask
   unsigned factored_mask = 0u;
@@ -582,15 +586,29 @@ __device__ void small_update_constraint(Small& s) {
   const MjbData& d = s.d;
   s.prev_cost = s.cost;
   float c = 0.f;
-  for (int k = s.lane; k < s.n; k += 32) {
-    const int r = s.adr + k;
-    const float Jaref = d.efc_Jaref[r], D = d.efc_D[r];
-    const int active = Jaref < 0.f;
-    d.efc_active[r] = active;
-    const float f = active ? -1.f * D * Jaref : 0.f;
-    d.efc_force[r] = f;
-    s.F[k] = f;
-    if (active) c += 0.5f * D * Jaref * Jaref;
+  if (s.staged) {
+    if (s.lane < s.n) {
+      const int r = s.adr + s.lane;
+      const float Jaref = s.rJaref, D = s.rD;
+      const int active = Jaref < 0.f;
+      s.ract = active;
+      d.efc_active[r] = active;
+      const float f = active ? -1.f * D * Jaref : 0.f;
+      d.efc_force[r] = f;
+      s.F[s.lane] = f;
+      if (active) c += 0.5f * D * Jaref * Jaref;
+    }
+  } else {
+    for (int k = s.lane; k < s.n; k += 32) {
+      const int r = s.adr + k;
+      const float Jaref = d.efc_Jaref[r], D = d.efc_D[r];
+      const int active = Jaref < 0.f;
+      d.efc_active[r] = active;
+      const float f = active ? -1.f * D * Jaref : 0.f;
+      d.efc_force[r] = f;
+      s.F[k] = f;
+      if (active) c += 0.5f * D * Jaref * Jaref;
+    }
   }
   c = warp_sum(c);
   __syncwarp();
@@ -626,14 +644,12 @@ __device__ void small_update_gradient(Small& s) {
   // the previous call is kept (bit-identical) while the set of active rows is unchanged; rows
   // past the first 32 are not tracked, so such worlds refactor every time.  Without s.reuse every
   // call refactors, as the reference does.
-  const unsigned mask = __ballot_sync(WARP_FULL, lane < s.n && d.efc_active[s.adr + lane]);
-  const bool refactor = !s.reuse || !s.factored || s.n > 32 || mask != s.factored_mask;
   const bool staged = s.staged;  // unstaged rows keep F in efc_force, which must survive
+  const unsigned mask = __ballot_sync(
+      WARP_FULL, lane < s.n && (staged ? s.ract != 0 : d.efc_active[s.adr + lane] != 0));
+  const bool refactor = !s.reuse || !s.factored || s.n > 32 || mask != s.factored_mask;
   if (refactor && staged) {  // coefficient of each row in J^T D J: D when active, else 0
-    for (int k = lane; k < s.n; k += 32) {
-      const int r = s.adr + k;
-      s.F[k] = d.efc_active[r] ? d.efc_D[r] : 0.f;
-    }
+    if (lane < s.n) s.F[lane] = s.ract ? s.rD : 0.f;
     __syncwarp();
   }
   s.Mgrad = newton_direction(s.Ms, s.ld, s.J, s.ldj, staged, staged ? s.F : nullptr,
@@ -648,6 +664,18 @@ __device__ void small_linesearch(Small& s) {
   const MjbModel& m = s.m;
   const MjbData& d = s.d;
   const int nv = s.nv, lane = s.lane;
+  // f(Jaref, jv, quad0, quad1, quad2) for each of this lane's rows (registers when staged)
+  auto rows = [&](auto&& f) {
+    if (s.staged) {
+      if (lane < s.n) f(s.rJaref, s.rjv, s.rq0, s.rq1, s.rq2);
+    } else {
+      for (int k = lane; k < s.n; k += 32) {
+        const int r = s.adr + k;
+        const float* q = d.efc_quad + 3 * r;
+        f(d.efc_Jaref[r], d.efc_jv[r], q[0], q[1], q[2]);
+      }
+    }
+  };
   s.mv = s.mulM(s.search);
   {
     float q0 = s.own ? s.gauss / float(nv) : 0.f;
@@ -658,14 +686,30 @@ __device__ void small_linesearch(Small& s) {
     s.qg[2] = warp_sum(q2);
   }
   s.publish(s.search);
-  for (int k = lane; k < s.n; k += 32) {
-    const int r = s.adr + k;
-    const float jv = s.rowdot(k);
-    const float Jaref = d.efc_Jaref[r], D = d.efc_D[r];
-    d.efc_jv[r] = jv;
-    d.efc_quad[3 * r] = 0.5f * Jaref * Jaref * D;
-    d.efc_quad[3 * r + 1] = jv * Jaref * D;
-    d.efc_quad[3 * r + 2] = 0.5f * jv * jv * D;
+  if (s.staged) {
+    if (lane < s.n) {
+      const int r = s.adr + lane;
+      const float jv = s.rowdot(lane);
+      const float Jaref = s.rJaref, D = s.rD;
+      s.rjv = jv;
+      s.rq0 = 0.5f * Jaref * Jaref * D;
+      s.rq1 = jv * Jaref * D;
+      s.rq2 = 0.5f * jv * jv * D;
+      d.efc_jv[r] = jv;
+      d.efc_quad[3 * r] = s.rq0;
+      d.efc_quad[3 * r + 1] = s.rq1;
+      d.efc_quad[3 * r + 2] = s.rq2;
+    }
+  } else {
+    for (int k = lane; k < s.n; k += 32) {
+      const int r = s.adr + k;
+      const float jv = s.rowdot(k);
+      const float Jaref = d.efc_Jaref[r], D = d.efc_D[r];
+      d.efc_jv[r] = jv;
+      d.efc_quad[3 * r] = 0.5f * Jaref * Jaref * D;
+      d.efc_quad[3 * r + 1] = jv * Jaref * D;
+      d.efc_quad[3 * r + 2] = 0.5f * jv * jv * D;
+    }
   }
   __syncwarp();
   if (m.ls_parallel) {
@@ -674,14 +718,13 @@ __device__ void small_linesearch(Small& s) {
     for (int c = 0; c < m.nlsp; c++) {
       const float a = m.alpha_candidate[c];
       float t0 = 0.f, t1 = 0.f, t2 = 0.f;
-      for (int k = lane; k < s.n; k += 32) {
-        const int r = s.adr + k;
-        if (d.efc_Jaref[r] + a * d.efc_jv[r] < 0.f) {
-          t0 += d.efc_quad[3 * r];
-          t1 += d.efc_quad[3 * r + 1];
-          t2 += d.efc_quad[3 * r + 2];
+      rows([&](float jaref, float jv, float q0, float q1, float q2) {
+        if (jaref + a * jv < 0.f) {
+          t0 += q0;
+          t1 += q1;
+          t2 += q2;
         }
-      }
+      });
       t0 = warp_sum(t0) + s.qg[0];
       t1 = warp_sum(t1) + s.qg[1];
       t2 = warp_sum(t2) + s.qg[2];
@@ -698,23 +741,20 @@ __device__ void small_linesearch(Small& s) {
     float p0[3];
     {
       float a0 = 0.f, a1 = 0.f, a2 = 0.f;
-      for (int k = lane; k < s.n; k += 32) {
-        const int r = s.adr + k;
-        if (d.efc_Jaref[r] >= 0.f) continue;
-        a0 += d.efc_quad[3 * r];
-        a1 += d.efc_quad[3 * r + 1];
-        a2 += 2.f * d.efc_quad[3 * r + 2];
-      }
+      rows([&](float jaref, float, float q0, float q1, float q2) {
+        if (jaref >= 0.f) return;
+        a0 += q0;
+        a1 += q1;
+        a2 += 2.f * q2;
+      });
       p0[0] = s.qg[0] + warp_sum(a0);
       p0[1] = s.qg[1] + warp_sum(a1);
       p0[2] = 2.f * s.qg[2] + warp_sum(a2);
     }
     auto totals = [&](int na, const float* al, float (*out)[3]) {
       float acc[3][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
-      for (int k = lane; k < s.n; k += 32) {
-        const int r = s.adr + k;
-        const float jaref = d.efc_Jaref[r], jv = d.efc_jv[r];
-        const float* q = d.efc_quad + 3 * r;
+      rows([&](float jaref, float jv, float q0, float q1, float q2) {
+        const float q[3] = {q0, q1, q2};
         for (int t = 0; t < na; t++) {
           if (jaref + al[t] * jv < 0.f) {
             float p[3];
@@ -724,7 +764,7 @@ __device__ void small_linesearch(Small& s) {
             acc[t][2] += p[2];
           }
         }
-      }
+      });
       for (int t = 0; t < na; t++) {
         float g[3];
         eval_pt3(s.qg, al[t], g);
@@ -782,7 +822,14 @@ __device__ void small_linesearch(Small& s) {
     s.qacc += s.alpha * s.search;
     s.Ma += s.alpha * s.mv;
   }
-  for (int k = lane; k < s.n; k += 32) d.efc_Jaref[s.adr + k] += s.alpha * d.efc_jv[s.adr + k];
+  if (s.staged) {
+    if (lane < s.n) {
+      s.rJaref += s.alpha * s.rjv;
+      d.efc_Jaref[s.adr + lane] = s.rJaref;
+    }
+  } else {
+    for (int k = lane; k < s.n; k += 32) d.efc_Jaref[s.adr + k] += s.alpha * d.efc_jv[s.adr + k];
+  }
   __syncwarp();
 }
 
@@ -828,7 +875,15 @@ __device__ void solve_small(const MjbModel& m, const MjbData& d, int w, int lane
   // _create_context (solver.py:26-72)
   s.cost = __int_as_float(0x7f800000);
   s.publish(s.qacc);
-  for (int k = lane; k < n; k += 32) d.efc_Jaref[adr + k] = s.rowdot(k) - d.efc_aref[adr + k];
+  if (s.staged) {
+    if (lane < n) {
+      s.rD = d.efc_D[adr + lane];
+      s.rJaref = s.rowdot(lane) - d.efc_aref[adr + lane];
+      d.efc_Jaref[adr + lane] = s.rJaref;
+    }
+  } else {
+    for (int k = lane; k < n; k += 32) d.efc_Jaref[adr + k] = s.rowdot(k) - d.efc_aref[adr + k];
+  }
   __syncwarp();
   s.Ma = s.mulM(s.qacc);
   small_update_constraint(s);
