@@ -273,13 +273,14 @@ __global__ void k_mul_m(const __grid_constant__ MjbModel m, const __grid_constan
   const int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   if (w >= d.nworld) return;
   if (skip && skip[w]) return;
-  mul_m_world(d.qM + W(w, m.nv * m.nv), m.nv, res + W(w, m.nv), vec + W(w, m.nv), lane);
+  if (m.is_sparse) mul_m_sparse(m, d.qM + W(w, m.nM), res + W(w, m.nv), vec + W(w, m.nv), lane);
+  else mul_m_world(d.qM + W(w, m.nv * m.nv), m.nv, res + W(w, m.nv), vec + W(w, m.nv), lane);
 }
 __global__ void k_solve_m(const __grid_constant__ MjbModel m, const __grid_constant__ MjbData d, float* x, const float* y) {
   const int lane = threadIdx.x & 31;
   const int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   if (w >= d.nworld) return;
-  solve_blocks(m, d.qLD + W(w, m.nv * m.nv), x + W(w, m.nv), y + W(w, m.nv), lane);
+  solve_m_world(m, d, w, x + W(w, m.nv), y + W(w, m.nv), lane);
 }
 __global__ void k_xfrc(const __grid_constant__ MjbModel m, const __grid_constant__ MjbData d, float* qfrc) {
   const int lane = threadIdx.x & 31;
@@ -301,10 +302,12 @@ inline int finish() {
   return e == cudaSuccess ? MJB_OK : MJB_ERR_LAUNCH;
 }
 
+// implicitfast needs the dense mass matrix (the reference asserts it, forward.py:268)
+inline bool implicit_unsupported(const MjbModel* m) { return m->is_sparse && m->integrator != 0; }
+
 inline int check(const MjbModel* m, const MjbData* d) {
   if (!m || !d) return MJB_ERR_ARG;
   if (d->nworld <= 0) return d->nworld == 0 ? MJB_OK : MJB_ERR_ARG;
-  if (m->is_sparse) return MJB_ERR_UNSUPPORTED;
   if (m->cone != 0) return MJB_ERR_UNSUPPORTED;
   return MJB_OK;
 }
@@ -543,7 +546,7 @@ const char* mjb_error_string(int status) {
   switch (status) {
     case MJB_OK: return "ok";
     case MJB_ERR_ARG: return "invalid argument";
-    case MJB_ERR_UNSUPPORTED: return "unsupported model feature (sparse mass matrix or elliptic cone)";
+    case MJB_ERR_UNSUPPORTED: return "unsupported model feature (elliptic cone, or implicitfast with the sparse mass matrix)";
     case MJB_ERR_LAUNCH: return cudaGetErrorString(cudaGetLastError());
     case MJB_ERR_SCRATCH: return "model too large for on-chip scratch";
     default: return "unknown status";
@@ -564,6 +567,7 @@ int mjb_forward(const MjbModel* m, const MjbData* d, const MjbRunCfg* cfg, mjbSt
 int mjb_step(const MjbModel* m, const MjbData* d, const MjbRunCfg* cfg, mjbStream stream) {
   int rc = check(m, d);
   if (rc || d->nworld == 0) return rc;
+  if (implicit_unsupported(m)) return MJB_ERR_UNSUPPORTED;
   cudaStream_t s = (cudaStream_t)stream;
   const int form = cfg ? cfg->fused : MJB_FORM_CHOSEN;
   if (form == MJB_FORM_PLAIN) {
@@ -604,7 +608,12 @@ MJB_STAGE_ENTRY(mjb_fwd_velocity, S_FWD_VELOCITY)
 MJB_STAGE_ENTRY(mjb_fwd_actuation, S_FWD_ACTUATION)
 MJB_STAGE_ENTRY(mjb_fwd_acceleration, S_FWD_ACCELERATION)
 MJB_STAGE_ENTRY(mjb_euler, S_EULER)
-MJB_STAGE_ENTRY(mjb_implicit, S_IMPLICIT)
+int mjb_implicit(const MjbModel* m, const MjbData* d, mjbStream stream) {
+  int rc = check(m, d);
+  if (rc || d->nworld == 0) return rc;
+  if (m->is_sparse) return MJB_ERR_UNSUPPORTED;
+  return launch_stage<S_IMPLICIT>(m, d, (cudaStream_t)stream);
+}
 MJB_STAGE_ENTRY(mjb_nxn_broadphase, S_NXN)
 
 int mjb_fwd_position(const MjbModel* m, const MjbData* d, mjbStream stream) {
@@ -734,6 +743,7 @@ extern "C" size_t mjb_implicit_noalloc_max_bytes(void) { return kNoallocScratchB
 extern "C" int mjb_implicit_noalloc(const MjbModel* m, const MjbData* d, mjbStream stream) {
   int rc = check(m, d);
   if (rc || d->nworld == 0) return rc;
+  if (m->is_sparse) return MJB_ERR_UNSUPPORTED;
   const size_t nv = size_t(m->nv);
   const size_t need = size_t(d->nworld) * (2 * nv * nv + nv) * sizeof(float);
   if (need > kNoallocScratchBytes) return MJB_ERR_SCRATCH;

@@ -48,6 +48,12 @@ __device__ __forceinline__ void mul_m_world(const float* qM, int nv, float* res,
   __syncwarp();
 }
 
+// res = M vec for the world's mass matrix, dense or sparse (res must not alias vec)
+__device__ __forceinline__ void mul_m_ctx(SolverCtx& s, float* res, const float* vec) {
+  if (s.m.is_sparse) mul_m_sparse(s.m, s.qM, res, vec, s.lane);
+  else mul_m_world(s.qM, s.nv, res, vec, s.lane);
+}
+
 // solver.py:75-173
 __device__ void update_constraint(SolverCtx& s) {
   const MjbData& d = s.d;
@@ -99,7 +105,7 @@ __device__ void update_gradient(SolverCtx& s) {
   s.grad_dot = warp_sum(gd);
   __syncwarp();
   if (m.solver == 1) {  // CG: Mgrad = M^-1 grad
-    solve_blocks(m, s.qLD, s.Mgrad, s.grad, lane);
+    solve_m_world(m, d, s.w, s.Mgrad, s.grad, lane);
     return;
   }
   // Newton: H = tril(qM) + sum_active D J^T J, then dense Cholesky solve.  With s.reuse the
@@ -111,11 +117,15 @@ __device__ void update_gradient(SolverCtx& s) {
       // dofs of two kinematic chains): the columns are compacted in order into the warp's
       // scratch and the lower-triangle pairs updated, row by row, with the per-entry arithmetic
       // of the dense form (h += J_i * J_j * D in row order; zero terms are skipped).
-      for (int e = lane; e < nv * nv; e += 32) {
-        const int i = e / nv, j = e - i * nv;
-        if (j <= i) H[e] = s.qM[e];
+      if (m.is_sparse) {
+        sparse_to_lower(m, s.qM, H, lane);
+      } else {
+        for (int e = lane; e < nv * nv; e += 32) {
+          const int i = e / nv, j = e - i * nv;
+          if (j <= i) H[e] = s.qM[e];
+        }
+        __syncwarp();
       }
-      __syncwarp();
       int* nzi = reinterpret_cast<int*>(s.nz);
       float* nzv = s.nz + round4i(nv);
       for (int k = 0; k < s.n; k++) {
@@ -148,10 +158,11 @@ __device__ void update_gradient(SolverCtx& s) {
         __syncwarp();
       }
     } else {
+      if (m.is_sparse) sparse_to_lower(m, s.qM, H, lane);
       for (int e = lane; e < nv * nv; e += 32) {
         const int i = e / nv, j = e - i * nv;
         if (j > i) continue;
-        float h = s.qM[e];
+        float h = m.is_sparse ? H[e] : s.qM[e];
         for (int k = 0; k < s.n; k++) {
           const int r = s.adr + k;
           if (!d.efc_active[r]) continue;
@@ -189,7 +200,7 @@ __device__ void linesearch(SolverCtx& s) {
   const MjbModel& m = s.m;
   const MjbData& d = s.d;
   const int nv = s.nv, lane = s.lane;
-  mul_m_world(s.qM, nv, s.mv, s.search, lane);
+  mul_m_ctx(s, s.mv, s.search);
   float q1 = 0.f, q2 = 0.f, q0 = 0.f;
   for (int i = lane; i < nv; i += 32) {
     q0 += s.gauss / float(nv);
@@ -349,8 +360,8 @@ __device__ __noinline__ void solve_generic(const MjbModel& m, const MjbData& d, 
   s.search = d.efc_search + W(w, nv);
   s.mv = d.efc_mv + W(w, nv);
   s.qfrc_constraint = d.qfrc_constraint + W(w, nv);
-  s.qM = d.qM + W(w, nv * nv);
-  s.qLD = d.qLD + W(w, nv * nv);
+  s.qM = d.qM + (m.is_sparse ? W(w, m.nM) : W(w, nv * nv));
+  s.qLD = d.qLD + (m.is_sparse ? W(w, m.nM) : W(w, nv * nv));
   s.qfrc_smooth = d.qfrc_smooth + W(w, nv);
   s.qacc_smooth = d.qacc_smooth + W(w, nv);
   s.hs = hs;
@@ -370,7 +381,7 @@ __device__ __noinline__ void solve_generic(const MjbModel& m, const MjbData& d, 
     for (int i = 0; i < nv; i++) v += J[i] * s.qacc[i];
     d.efc_Jaref[r] = v - d.efc_aref[r];
   }
-  mul_m_world(s.qM, nv, s.Ma, s.qacc, lane);
+  mul_m_ctx(s, s.Ma, s.qacc);
   update_constraint(s);
   update_gradient(s);
   float sd = 0.f;
@@ -946,11 +957,12 @@ __device__ void solve_small(const MjbModel& m, const MjbData& d, int w, int lane
 // Dispatch: the register / shared-memory solver when nv <= 32 and the caller provides its scratch
 // (solver_smem_floats(nv) floats), else the generic solver with an nv x nv Hessian tile `hs`.
 // reuse: keep the Newton Hessian's factor across iterations with an unchanged active set.
-// For nv > 32, sm (when given) is the generic solver's scratch of generic_nz_floats(nv) floats.
+// For nv > 32 or a sparse mass matrix, sm (when given) is the generic solver's scratch of at least
+// generic_nz_floats(nv) floats.
 __device__ __forceinline__ void solve(const MjbModel& m, const MjbData& d, int w, int lane,
                                       float* sm, float* hs, bool reuse = false) {
-  if (m.nv <= 32 && sm) solve_small(m, d, w, lane, sm, reuse);
-  else solve_generic(m, d, w, lane, hs, m.nv > 32 ? sm : nullptr, reuse);
+  if (m.nv <= 32 && sm && !m.is_sparse) solve_small(m, d, w, lane, sm, reuse);
+  else solve_generic(m, d, w, lane, hs, (m.nv > 32 || m.is_sparse) ? sm : nullptr, reuse);
 }
 
 }  // namespace mjb

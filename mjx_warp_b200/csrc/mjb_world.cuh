@@ -209,6 +209,95 @@ __device__ void com_pos(const MjbModel& m, const MjbData& d, int w, int lane) {
 
 // ------------------------------------------------------------------------------------------
 // smooth.py:248-314 — composite rigid body inertia and dense qM
+// ------------------------------------------------------------------------------------------
+// Sparse mass matrix (the reference's layout when opt.is_sparse; MuJoCo's qM / qLD): row i holds
+// M(i,i), M(i,parent(i)), M(i,parent(parent(i))), ... at dof_Madr[i], dof_Madr[i] + 1, ... (the
+// dof's ancestor chain, smooth.py:264-279); qLD holds the L'DL factor in the same slots (D on the
+// diagonal slot, the unit factor's entries below it) and qLDiagInv = 1 / D.  Every kinematic
+// tree's dofs are contiguous (block_adr / block_size) and couple only within the tree, so one
+// lane owns one tree and runs the serial algorithms on it; results do not depend on the lane
+// count.
+
+__device__ __forceinline__ int madr_row_len(const MjbModel& m, int i) {
+  return (i + 1 < m.nv ? m.dof_Madr[i + 1] : m.nM) - m.dof_Madr[i];
+}
+
+// smooth.py:317-351 (mj_factorI): in-place L'DL, each tree's dofs eliminated from its last to its
+// first, each elimination updating its ancestors' rows; Dinv (may be null) = 1 / D
+__device__ void factor_sparse(const MjbModel& m, float* L, float* Dinv, int lane) {
+  for (int blk = lane; blk < m.nblock; blk += 32) {
+    const int a = m.block_adr[blk], n = m.block_size[blk];
+    for (int k = a + n - 1; k >= a; k--) {
+      const int Mkk = m.dof_Madr[k];
+      int Mki = Mkk + 1;
+      for (int i = m.dof_parentid[k]; i >= 0; i = m.dof_parentid[i], Mki++) {
+        const float tmp = L[Mki] / L[Mkk];
+        const int Mi = m.dof_Madr[i], cnt = madr_row_len(m, i);
+        for (int j = 0; j < cnt; j++) L[Mi + j] -= L[Mki + j] * tmp;
+        L[Mki] = tmp;
+      }
+    }
+    if (Dinv)
+      for (int k = a; k < a + n; k++) Dinv[k] = 1.f / L[m.dof_Madr[k]];
+  }
+  __syncwarp();
+}
+
+// x = M^-1 y from the L'DL factor (smooth.py:609-652, mj_solveLD): x <- L'^-1 x from the leaves
+// up, x <- D^-1 x, x <- L^-1 x from the roots down.  Dinv may be null (1 / D is then formed from
+// L).  x may alias y.
+__device__ void solve_sparse(const MjbModel& m, const float* L, const float* Dinv, float* x,
+                             const float* y, int lane) {
+  for (int blk = lane; blk < m.nblock; blk += 32) {
+    const int a = m.block_adr[blk], n = m.block_size[blk];
+    for (int k = a; k < a + n; k++) x[k] = y[k];
+    for (int k = a + n - 1; k >= a; k--) {
+      int Mki = m.dof_Madr[k] + 1;
+      for (int i = m.dof_parentid[k]; i >= 0; i = m.dof_parentid[i], Mki++) x[i] -= L[Mki] * x[k];
+    }
+    for (int k = a; k < a + n; k++) x[k] *= Dinv ? Dinv[k] : 1.f / L[m.dof_Madr[k]];
+    for (int k = a; k < a + n; k++) {
+      int Mki = m.dof_Madr[k] + 1;
+      for (int i = m.dof_parentid[k]; i >= 0; i = m.dof_parentid[i], Mki++) x[k] -= L[Mki] * x[i];
+    }
+  }
+  __syncwarp();
+}
+
+// res = M vec for the sparse M (support.py:96-137: the diagonal, then each stored off-diagonal
+// entry applied to both of its rows); res must not alias vec
+__device__ void mul_m_sparse(const MjbModel& m, const float* M, float* res, const float* vec,
+                             int lane) {
+  for (int blk = lane; blk < m.nblock; blk += 32) {
+    const int a = m.block_adr[blk], n = m.block_size[blk];
+    for (int i = a; i < a + n; i++) res[i] = M[m.dof_Madr[i]] * vec[i];
+    for (int i = a; i < a + n; i++) {
+      int Mij = m.dof_Madr[i] + 1;
+      for (int j = m.dof_parentid[i]; j >= 0; j = m.dof_parentid[j], Mij++) {
+        res[i] += M[Mij] * vec[j];
+        res[j] += M[Mij] * vec[i];
+      }
+    }
+  }
+  __syncwarp();
+}
+
+// Scatters the sparse M into the lower triangle of a dense nv x nv matrix H (upper left alone)
+__device__ void sparse_to_lower(const MjbModel& m, const float* M, float* H, int lane) {
+  const int nv = m.nv;
+  for (int e = lane; e < nv * nv; e += 32) {
+    const int i = e / nv, j = e - i * nv;
+    if (j <= i) H[e] = 0.f;
+  }
+  __syncwarp();
+  for (int i = lane; i < nv; i += 32) {
+    int a = m.dof_Madr[i];
+    H[i * nv + i] = M[a];
+    for (int j = m.dof_parentid[i]; j >= 0; j = m.dof_parentid[j]) H[i * nv + j] = M[++a];
+  }
+  __syncwarp();
+}
+
 __device__ void crb(const MjbModel& m, const MjbData& d, int w, int lane) {
   const int nb = m.nbody, nv = m.nv;
   const float* cinert = d.cinert + W(w, 10 * nb);
@@ -234,9 +323,21 @@ __device__ void crb(const MjbModel& m, const MjbData& d, int w, int lane) {
     }
     __syncwarp();
   }
+  const float* cdof = d.cdof + W(w, 6 * nv);
+  if (m.is_sparse) {  // qM_sparse (smooth.py:263-279)
+    float* qMs = d.qM + W(w, m.nM);
+    for (int i = lane; i < nv; i += 32) {
+      const s6 ci = ld6(cdof + 6 * i);
+      const s6 buf = inert_vec(crb + 10 * m.dof_bodyid[i], ci);
+      int a = m.dof_Madr[i];
+      qMs[a] = m.dof_armature[i] + dot6(ci, buf);
+      for (int j = m.dof_parentid[i]; j >= 0; j = m.dof_parentid[j]) qMs[++a] = dot6(ld6(cdof + 6 * j), buf);
+    }
+    __syncwarp();
+    return;
+  }
   // qM_dense (smooth.py:281-302)
   float* qM = d.qM + W(w, nv * nv);
-  const float* cdof = d.cdof + W(w, 6 * nv);
   for (int e = lane; e < nv * nv; e += 32) qM[e] = 0.f;
   __syncwarp();
   for (int i = lane; i < nv; i += 32) {
@@ -658,7 +759,23 @@ __device__ void solve_blocks(const MjbModel& m, const float* L, float* x, const 
 // smooth.py:392-395
 __device__ void factor_m(const MjbModel& m, const MjbData& d, int w, int lane, float* tile = nullptr) {
   const int nv = m.nv;
+  if (m.is_sparse) {  // smooth.py:317-351
+    const float* M = d.qM + W(w, m.nM);
+    float* L = d.qLD + W(w, m.nM);
+    for (int e = lane; e < m.nM; e += 32) L[e] = M[e];
+    __syncwarp();
+    factor_sparse(m, L, d.qLDiagInv + W(w, nv), lane);
+    return;
+  }
   factor_blocks(m, d.qM + W(w, nv * nv), d.qLD + W(w, nv * nv), lane, nullptr, 0.f, tile);
+}
+
+// x = M^-1 y with the world's mass-matrix factor (qLD), dense or sparse
+__device__ __forceinline__ void solve_m_world(const MjbModel& m, const MjbData& d, int w, float* x,
+                                              const float* y, int lane, float* tile = nullptr,
+                                              bool tile_has_factor = false) {
+  if (m.is_sparse) solve_sparse(m, d.qLD + W(w, m.nM), d.qLDiagInv + W(w, m.nv), x, y, lane);
+  else solve_blocks(m, d.qLD + W(w, m.nv * m.nv), x, y, lane, tile, tile_has_factor);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -938,7 +1055,7 @@ __device__ void fwd_acceleration(const MjbModel& m, const MjbData& d, int w, int
   for (int i = lane; i < nv; i += 32) sm[i] = pas[i] - bias[i] + act[i] + app[i];
   __syncwarp();
   xfrc_accumulate(m, d, w, sm, lane);
-  solve_blocks(m, d.qLD + W(w, nv * nv), d.qacc_smooth + W(w, nv), sm, lane, tile, tile_has_qLD);
+  solve_m_world(m, d, w, d.qacc_smooth + W(w, nv), sm, lane, tile, tile_has_qLD);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -971,10 +1088,33 @@ __device__ void euler(const MjbModel& m, const MjbData& d, int w, int lane, floa
     advance(m, d, w, d.qacc + W(w, nv), lane);
     return;
   }
-  float* L = d.qLD_integration + W(w, nv * nv);
   float* x = d.qacc_integration + W(w, nv);
   const float* sm = d.qfrc_smooth + W(w, nv);
   const float* qc = d.qfrc_constraint + W(w, nv);
+  if (m.is_sparse) {  // eulerdamp_sparse (forward.py:171-193)
+    const float* M = d.qM + W(w, m.nM);
+    float* Mi = d.qM_integration ? d.qM_integration + W(w, m.nM) : nullptr;
+    float* Ls = d.qLD_integration + W(w, m.nM);
+    float* f = d.qfrc_integration ? d.qfrc_integration + W(w, nv) : x;
+    for (int e = lane; e < m.nM; e += 32) {
+      if (Mi) Mi[e] = M[e];
+      Ls[e] = M[e];
+    }
+    __syncwarp();
+    for (int i = lane; i < nv; i += 32) {
+      const int a = m.dof_Madr[i];
+      const float v = M[a] + m.timestep * m.dof_damping[i];
+      if (Mi) Mi[a] = v;
+      Ls[a] = v;
+      f[i] = sm[i] + qc[i];
+    }
+    __syncwarp();
+    factor_sparse(m, Ls, nullptr, lane);
+    solve_sparse(m, Ls, nullptr, x, f, lane);
+    advance(m, d, w, x, lane);
+    return;
+  }
+  float* L = d.qLD_integration + W(w, nv * nv);
   factor_blocks(m, d.qM + W(w, nv * nv), L, lane, m.dof_damping, m.timestep, tile);
   for (int i = lane; i < nv; i += 32) x[i] = sm[i] + qc[i];
   __syncwarp();

@@ -248,6 +248,8 @@ def _data_arrays(mjm, nworld, nconmax, njmax, dev):
   f = lambda *s: torch.zeros(s, dtype=torch.float32, device=dev)  # noqa: E731
   i = lambda *s: torch.zeros(s, dtype=torch.int32, device=dev)  # noqa: E731
   W = nworld
+  # the reference's layout: (nworld, 1, nM) for the sparse mass matrix, (nworld, nv, nv) dense
+  mshape = (W, 1, int(mjm.nM)) if is_sparse(mjm) else (W, nv, nv)
   top = {
     "qpos": f(W, nq), "qvel": f(W, nv), "qacc_warmstart": f(W, nv), "qfrc_applied": f(W, nv),
     "mocap_pos": f(W, nm, 3), "mocap_quat": f(W, nm, 4), "qacc": f(W, nv),
@@ -257,13 +259,13 @@ def _data_arrays(mjm, nworld, nconmax, njmax, dev):
     "site_xpos": f(W, ns, 3), "site_xmat": f(W, ns, 3, 3), "cinert": f(W, nb, 10),
     "cdof": f(W, nv, 6), "ctrl": f(W, nu), "actuator_velocity": f(W, nu),
     "actuator_force": f(W, nu), "actuator_length": f(W, nu), "actuator_moment": f(W, nu, nv),
-    "crb": f(W, nb, 10), "qM": f(W, nv, nv), "qLD": f(W, nv, nv), "act_dot": f(W, na),
+    "crb": f(W, nb, 10), "qM": f(*mshape), "qLD": f(*mshape), "act_dot": f(W, na),
     "act": f(W, na), "qLDiagInv": f(W, nv), "cvel": f(W, nb, 6), "cdof_dot": f(W, nv, 6),
     "qfrc_bias": f(W, nv), "qfrc_passive": f(W, nv), "qfrc_spring": f(W, nv),
     "qfrc_damper": f(W, nv), "qfrc_actuator": f(W, nv), "qfrc_smooth": f(W, nv),
     "qfrc_constraint": f(W, nv), "qacc_smooth": f(W, nv), "rne_cacc": f(W, nb, 6),
     "rne_cfrc": f(W, nb, 6), "xfrc_applied": f(W, nb, 6), "qfrc_integration": f(W, nv),
-    "qacc_integration": f(W, nv), "qM_integration": f(W, nv, nv), "qLD_integration": f(W, nv, nv),
+    "qacc_integration": f(W, nv), "qM_integration": f(*mshape), "qLD_integration": f(*mshape),
     "qLDiagInv_integration": f(W, nv), "act_vel_integration": f(W, nu),
     "sap_geom_sort": f(W, ng, 4), "sap_projection_lower": f(2 * W, ng),
     "sap_projection_upper": f(W, ng), "sap_sort_index": i(2 * W, ng), "sap_range": i(W, ng),
@@ -333,6 +335,47 @@ def make_data(mjm, nworld: int = 1, nconmax: int = -1, njmax: int = -1, device=N
   return d
 
 
+def sparse_from_dense(mjm, M) -> np.ndarray:
+  """The sparse layout (nM,) of a dense nv x nv mass matrix: row i's diagonal, then its entries
+  against the dof's ancestors, at dof_Madr[i] (smooth.py:264-279)."""
+  out = np.zeros(int(mjm.nM))
+  parent = np.asarray(mjm.dof_parentid)
+  for i in range(mjm.nv):
+    a, j = int(mjm.dof_Madr[i]), i
+    while j >= 0:
+      out[a] = M[i, j]
+      a, j = a + 1, parent[j]
+  return out
+
+
+def dense_from_sparse(mjm, Ms) -> np.ndarray:
+  """The dense symmetric nv x nv matrix of a sparse-layout mass matrix (mj_fullM)."""
+  M = np.zeros((mjm.nv, mjm.nv))
+  parent = np.asarray(mjm.dof_parentid)
+  for i in range(mjm.nv):
+    a, j = int(mjm.dof_Madr[i]), i
+    while j >= 0:
+      M[i, j] = M[j, i] = Ms[a]
+      a, j = a + 1, parent[j]
+  return M
+
+
+def factor_sparse_host(mjm, Ms) -> np.ndarray:
+  """L'DL factor of a sparse-layout mass matrix in the same layout (mj_factorI), on the host."""
+  L = np.array(Ms, dtype=float)
+  parent = np.asarray(mjm.dof_parentid)
+  madr = np.asarray(mjm.dof_Madr)
+  rowlen = np.diff(np.append(madr, int(mjm.nM)))
+  for k in range(mjm.nv - 1, -1, -1):
+    mkk, mki, i = madr[k], madr[k] + 1, parent[k]
+    while i >= 0:
+      tmp = L[mki] / L[mkk] if L[mkk] != 0 else 0.0
+      L[madr[i]:madr[i] + rowlen[i]] -= L[mki:mki + rowlen[i]] * tmp
+      L[mki] = tmp
+      i, mki = parent[i], mki + 1
+  return L
+
+
 def _dense_qM(mjm, mjd):
   qM = np.asarray(mjd.qM, dtype=float)
   if qM.ndim == 2:
@@ -387,12 +430,17 @@ def put_data(mjm, mjd, nworld: int = 1, nconmax: int = -1, njmax: int = -1, devi
             "cdof", "crb", "cvel", "cdof_dot", "xfrc_applied"):
     tile(n, getattr(mjd, n))
   qM = _dense_qM(mjm, mjd)
-  tile("qM", qM)
-  try:
-    qLD = np.linalg.cholesky(qM) if np.any(qM) else np.zeros_like(qM)
-  except np.linalg.LinAlgError:
-    qLD = np.zeros_like(qM)
-  tile("qLD", qLD)
+  if is_sparse(mjm):
+    Ms = sparse_from_dense(mjm, qM)
+    tile("qM", Ms)
+    tile("qLD", factor_sparse_host(mjm, Ms))
+  else:
+    tile("qM", qM)
+    try:
+      qLD = np.linalg.cholesky(qM) if np.any(qM) else np.zeros_like(qM)
+    except np.linalg.LinAlgError:
+      qLD = np.zeros_like(qM)
+    tile("qLD", qLD)
   tile("actuator_moment", _dense_moment(mjm, mjd))
 
   # contacts and constraint rows: world i's block at [i * n, (i + 1) * n) (io.py:607-698)
@@ -448,8 +496,12 @@ def get_data_into(result, mjm, d: Data) -> None:
     setattr(result, n, getattr(d, n).numpy()[0].astype(np.float64).copy())
   for n in ("xmat", "ximat", "geom_xmat", "site_xmat"):
     setattr(result, n, getattr(d, n).numpy()[0].reshape(-1, 9).astype(np.float64))
-  result.qM = d.qM.numpy()[0].astype(np.float64)
-  result.qLD = d.qLD.numpy()[0].astype(np.float64)
+  if is_sparse(mjm):  # io.py:803-805
+    result.qM = d.qM.numpy()[0, 0].astype(np.float64)
+    result.qLD = d.qLD.numpy()[0, 0].astype(np.float64)
+  else:
+    result.qM = d.qM.numpy()[0].astype(np.float64)
+    result.qLD = d.qLD.numpy()[0].astype(np.float64)
   result.actuator_moment = d.actuator_moment.numpy()[0].astype(np.float64)
   result.ncon = ncon
   result.nefc = nefc
