@@ -26,6 +26,11 @@
 #ifndef MJB_MINB
 #define MJB_MINB 5
 #endif
+// lanes per world in the chosen form's tree-recursion stage kernels (8, 16 or 32; 16 measured
+// fastest for the humanoid: phase 0 290 us vs 306 at 8 and 323 at 32)
+#ifndef MJB_TREE_LANES
+#define MJB_TREE_LANES 16
+#endif
 
 namespace mjb {
 
@@ -87,6 +92,26 @@ __global__ void __launch_bounds__(128, STAGE == S_SOLVE ? MJB_MINB : 8)
     case S_IMPLICIT: implicit(m, d, w, lane, sm); break;
     case S_QACC_SMOOTH_COPY: copy_qacc_smooth(m, d, w, lane); break;
     case S_CHECK: check_finite(m, d, w, lane); break;
+  }
+}
+
+// The chosen form's tree-recursion stages (kinematics, com_pos, crb, transmission, fwd_velocity,
+// fwd_actuation) with L lanes per world, 32 / L worlds per warp: a BFS level of a few bodies
+// keeps the world's lanes busy instead of leaving most of a warp idle, so the warp instructions
+// per world drop by up to 32 / L.  The stages' arithmetic does not depend on L.
+template <int STAGE, int L>
+__global__ void __launch_bounds__(128, 8)
+    k_stage_lanes(const __grid_constant__ MjbModel m, const __grid_constant__ MjbData d) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int w = int(t / L), lane = int(t % L);
+  if (w >= d.nworld) return;
+  switch (STAGE) {
+    case S_KINEMATICS: kinematics<L>(m, d, w, lane); break;
+    case S_COM_POS: com_pos<L>(m, d, w, lane); break;
+    case S_CRB: crb<L>(m, d, w, lane); break;
+    case S_TRANSMISSION: transmission<L>(m, d, w, lane); break;
+    case S_FWD_VELOCITY: fwd_velocity<L>(m, d, w, lane); break;
+    case S_FWD_ACTUATION: fwd_actuation<L>(m, d, w, lane); break;
   }
 }
 
@@ -386,6 +411,15 @@ int launch_broadphase(const MjbModel* m, const MjbData* d, cudaStream_t s) {
   return m->ngeom > 100 ? launch_stage<S_SAP>(m, d, s) : launch_stage<S_NXN>(m, d, s);
 }
 
+// a tree-recursion stage with MJB_TREE_LANES lanes per world
+template <int STAGE>
+int launch_lanes(const MjbModel* m, const MjbData* d, cudaStream_t s) {
+  constexpr int L = MJB_TREE_LANES;
+  const long long threads = (long long)d->nworld * L;
+  k_stage_lanes<STAGE, L><<<int((threads + 127) / 128), 128, 0, s>>>(*m, *d);
+  return finish();
+}
+
 void reset_counters(const MjbData* d, bool pairs, bool contacts, bool efc, bool status,
                     cudaStream_t s) {
   const int n = status ? d->nworld : 1;
@@ -448,16 +482,16 @@ int run_forward_fork(const MjbModel* m, const MjbData* d, cudaStream_t s) {
     f.ready = true;
   }
   int rc;
-  if ((rc = launch_stage<S_KINEMATICS>(m, d, s))) return rc;
-  if ((rc = launch_stage<S_COM_POS>(m, d, s))) return rc;
+  if ((rc = launch_lanes<S_KINEMATICS>(m, d, s))) return rc;
+  if ((rc = launch_lanes<S_COM_POS>(m, d, s))) return rc;
   if (cudaEventRecord(f.ev[0], s) != cudaSuccess) return MJB_ERR_LAUNCH;
   for (auto& a : f.aux)
     if (cudaStreamWaitEvent(a, f.ev[0], 0) != cudaSuccess) return MJB_ERR_LAUNCH;
-  int rc0 = launch_stage<S_CRB>(m, d, f.aux[0]);
+  int rc0 = launch_lanes<S_CRB>(m, d, f.aux[0]);
   if (!rc0) rc0 = launch_stage<S_FACTOR_M>(m, d, f.aux[0]);
-  int rc1 = launch_stage<S_TRANSMISSION>(m, d, f.aux[1]);
-  if (!rc1) rc1 = launch_stage<S_FWD_VELOCITY>(m, d, f.aux[1]);
-  if (!rc1) rc1 = launch_stage<S_FWD_ACTUATION>(m, d, f.aux[1]);
+  int rc1 = launch_lanes<S_TRANSMISSION>(m, d, f.aux[1]);
+  if (!rc1) rc1 = launch_lanes<S_FWD_VELOCITY>(m, d, f.aux[1]);
+  if (!rc1) rc1 = launch_lanes<S_FWD_ACTUATION>(m, d, f.aux[1]);
   reset_counters(d, true, true, true, false, s);
   int rc2 = launch_broadphase(m, d, s);
   if (!rc2) rc2 = launch_stage<S_NARROW>(m, d, s);

@@ -33,8 +33,19 @@ namespace mjb {
 
 __device__ __forceinline__ size_t W(int w, int n) { return size_t(w) * size_t(n); }
 
+// Stages written for L lanes per world (L = 32: one world per warp; L = 8 or 16: 32 / L worlds per
+// warp, the world's lanes an aligned group): `lane` is the lane within the world's group, loops
+// stride by L and lsync<L> synchronises the group.
+template <int L>
+__device__ __forceinline__ void lsync() {
+  static_assert(L == 8 || L == 16 || L == 32, "lanes per world");
+  if constexpr (L == 32) __syncwarp();
+  else __syncwarp(((1u << L) - 1u) << ((threadIdx.x & 31) & ~(L - 1)));
+}
+
 // ------------------------------------------------------------------------------------------
 // smooth.py:32-145 — forward kinematics
+template <int L = 32>
 __device__ void kinematics(const MjbModel& m, const MjbData& d, int w, int lane) {
   const int nb = m.nbody;
   const float* qpos = d.qpos + W(w, m.nq);
@@ -53,10 +64,10 @@ __device__ void kinematics(const MjbModel& m, const MjbData& d, int w, int lane)
     st9(xmat, eye);
     st9(ximat, eye);
   }
-  __syncwarp();
+  lsync<L>();
   for (int lvl = 1; lvl < m.nlevel; lvl++) {
     const int beg = m.body_treeadr[lvl], end = m.body_treeadr[lvl + 1];
-    for (int n = beg + lane; n < end; n += 32) {  // _level (smooth.py:46-109)
+    for (int n = beg + lane; n < end; n += L) {  // _level (smooth.py:46-109)
       const int b = m.body_tree[n];
       const int jntadr = m.body_jntadr[b], jntnum = m.body_jntnum[b];
       f3 pos;
@@ -97,12 +108,12 @@ __device__ void kinematics(const MjbModel& m, const MjbData& d, int w, int lane)
       st3(xipos + 3 * b, pos + rot_vec_quat(ld3(m.body_ipos + 3 * b), quat));
       st9(ximat + 9 * b, quat_to_mat(mul_quat(quat, ld4(m.body_iquat + 4 * b))));
     }
-    __syncwarp();
+    lsync<L>();
   }
   // geom_local_to_global / site_local_to_global (smooth.py:111-131)
   float* gxpos = d.geom_xpos + W(w, 3 * m.ngeom);
   float* gxmat = d.geom_xmat + W(w, 9 * m.ngeom);
-  for (int g = lane; g < m.ngeom; g += 32) {
+  for (int g = lane; g < m.ngeom; g += L) {
     const int b = m.geom_bodyid[g];
     const q4 q = ld4(xquat + 4 * b);
     st3(gxpos + 3 * g, ld3(xpos + 3 * b) + rot_vec_quat(ld3(m.geom_pos + 3 * g), q));
@@ -111,18 +122,19 @@ __device__ void kinematics(const MjbModel& m, const MjbData& d, int w, int lane)
   if (d.site_xpos) {
     float* sxpos = d.site_xpos + W(w, 3 * m.nsite);
     float* sxmat = d.site_xmat + W(w, 9 * m.nsite);
-    for (int s = lane; s < m.nsite; s += 32) {
+    for (int s = lane; s < m.nsite; s += L) {
       const int b = m.site_bodyid[s];
       const q4 q = ld4(xquat + 4 * b);
       st3(sxpos + 3 * s, ld3(xpos + 3 * b) + rot_vec_quat(ld3(m.site_pos + 3 * s), q));
       st9(sxmat + 9 * s, quat_to_mat(mul_quat(q, ld4(m.site_quat + 4 * s))));
     }
   }
-  __syncwarp();
+  lsync<L>();
 }
 
 // ------------------------------------------------------------------------------------------
 // smooth.py:148-245 — subtree CoM, cinert, cdof
+template <int L = 32>
 __device__ void com_pos(const MjbModel& m, const MjbData& d, int w, int lane) {
   const int nb = m.nbody;
   const float* xipos = d.xipos + W(w, 3 * nb);
@@ -131,13 +143,13 @@ __device__ void com_pos(const MjbModel& m, const MjbData& d, int w, int lane) {
   const float* xanchor = d.xanchor + W(w, 3 * m.njnt);
   const float* xaxis = d.xaxis + W(w, 3 * m.njnt);
   float* sc = d.subtree_com + W(w, 3 * nb);
-  for (int b = lane; b < nb; b += 32) st3(sc + 3 * b, ld3(xipos + 3 * b) * m.body_mass[b]);
-  __syncwarp();
+  for (int b = lane; b < nb; b += L) st3(sc + 3 * b, ld3(xipos + 3 * b) * m.body_mass[b]);
+  lsync<L>();
   // bottom-up gather over children; the world also adds itself (smooth.py:238-241 runs the
   // accumulation on level 0, where body 0 is its own parent)
   for (int lvl = m.nlevel - 1; lvl >= 0; lvl--) {
     const int beg = m.body_treeadr[lvl], end = m.body_treeadr[lvl + 1];
-    for (int n = beg + lane; n < end; n += 32) {
+    for (int n = beg + lane; n < end; n += L) {
       const int b = m.body_tree[n];
       f3 acc = ld3(sc + 3 * b);
       const int ca = m.body_childadr[b], cn = m.body_childnum[b];
@@ -145,17 +157,17 @@ __device__ void com_pos(const MjbModel& m, const MjbData& d, int w, int lane) {
       if (b == 0) acc = acc + acc;
       st3(sc + 3 * b, acc);
     }
-    __syncwarp();
+    lsync<L>();
   }
-  for (int b = lane; b < nb; b += 32) {
+  for (int b = lane; b < nb; b += L) {
     const float sm = m.subtree_mass[b];
     f3 v = ld3(sc + 3 * b);
     st3(sc + 3 * b, mk3(v.x / sm, v.y / sm, v.z / sm));
   }
-  __syncwarp();
+  lsync<L>();
   // cinert (smooth.py:169-201)
   float* cinert = d.cinert + W(w, 10 * nb);
-  for (int b = lane; b < nb; b += 32) {
+  for (int b = lane; b < nb; b += L) {
     const m33 mat = ld9(ximat + 9 * b);
     const f3 inert = ld3(m.body_inertia + 3 * b);
     const float mass = m.body_mass[b];
@@ -182,7 +194,7 @@ __device__ void com_pos(const MjbModel& m, const MjbData& d, int w, int lane) {
   }
   // cdof (smooth.py:203-232)
   float* cdof = d.cdof + W(w, 6 * m.nv);
-  for (int j = lane; j < m.njnt; j += 32) {
+  for (int j = lane; j < m.njnt; j += L) {
     const int b = m.jnt_bodyid[j], dof = m.jnt_dofadr[j], t = m.jnt_type[j];
     const f3 off = ld3(sc + 3 * m.body_rootid[b]) - ld3(xanchor + 3 * j);
     const m33 xm = ld9(xmat + 9 * b);
@@ -204,11 +216,9 @@ __device__ void com_pos(const MjbModel& m, const MjbData& d, int w, int lane) {
       put(dof, ax, cross(ax, off));
     }
   }
-  __syncwarp();
+  lsync<L>();
 }
 
-// ------------------------------------------------------------------------------------------
-// smooth.py:248-314 — composite rigid body inertia and dense qM
 // ------------------------------------------------------------------------------------------
 // Sparse mass matrix (the reference's layout when opt.is_sparse; MuJoCo's qM / qLD): row i holds
 // M(i,i), M(i,parent(i)), M(i,parent(parent(i))), ... at dof_Madr[i], dof_Madr[i] + 1, ... (the
@@ -298,6 +308,9 @@ __device__ void sparse_to_lower(const MjbModel& m, const float* M, float* H, int
   __syncwarp();
 }
 
+// ------------------------------------------------------------------------------------------
+// smooth.py:248-314 — composite rigid body inertia and dense qM
+template <int L = 32>
 __device__ void crb(const MjbModel& m, const MjbData& d, int w, int lane) {
   const int nb = m.nbody, nv = m.nv;
   const float* cinert = d.cinert + W(w, 10 * nb);
@@ -305,7 +318,7 @@ __device__ void crb(const MjbModel& m, const MjbData& d, int w, int lane) {
   // bottom-up gather; children of the world do not add into it (smooth.py:259-260)
   for (int lvl = m.nlevel - 1; lvl >= 0; lvl--) {
     const int beg = m.body_treeadr[lvl], end = m.body_treeadr[lvl + 1];
-    for (int n = beg + lane; n < end; n += 32) {
+    for (int n = beg + lane; n < end; n += L) {
       const int b = m.body_tree[n];
       float acc[10];
 #pragma unroll
@@ -321,26 +334,26 @@ __device__ void crb(const MjbModel& m, const MjbData& d, int w, int lane) {
 #pragma unroll
       for (int k = 0; k < 10; k++) crb[10 * b + k] = acc[k];
     }
-    __syncwarp();
+    lsync<L>();
   }
   const float* cdof = d.cdof + W(w, 6 * nv);
   if (m.is_sparse) {  // qM_sparse (smooth.py:263-279)
     float* qMs = d.qM + W(w, m.nM);
-    for (int i = lane; i < nv; i += 32) {
+    for (int i = lane; i < nv; i += L) {
       const s6 ci = ld6(cdof + 6 * i);
       const s6 buf = inert_vec(crb + 10 * m.dof_bodyid[i], ci);
       int a = m.dof_Madr[i];
       qMs[a] = m.dof_armature[i] + dot6(ci, buf);
       for (int j = m.dof_parentid[i]; j >= 0; j = m.dof_parentid[j]) qMs[++a] = dot6(ld6(cdof + 6 * j), buf);
     }
-    __syncwarp();
+    lsync<L>();
     return;
   }
   // qM_dense (smooth.py:281-302)
   float* qM = d.qM + W(w, nv * nv);
-  for (int e = lane; e < nv * nv; e += 32) qM[e] = 0.f;
-  __syncwarp();
-  for (int i = lane; i < nv; i += 32) {
+  for (int e = lane; e < nv * nv; e += L) qM[e] = 0.f;
+  lsync<L>();
+  for (int i = lane; i < nv; i += L) {
     const s6 ci = ld6(cdof + 6 * i);
     const s6 buf = inert_vec(crb + 10 * m.dof_bodyid[i], ci);
     qM[i * nv + i] = m.dof_armature[i] + dot6(ci, buf);
@@ -350,7 +363,7 @@ __device__ void crb(const MjbModel& m, const MjbData& d, int w, int lane) {
       qM[j * nv + i] = v;
     }
   }
-  __syncwarp();
+  lsync<L>();
 }
 
 // In-place Cholesky A = L L^T (left-looking, column by column) of the n x n SPD matrix at A with
@@ -780,14 +793,15 @@ __device__ __forceinline__ void solve_m_world(const MjbModel& m, const MjbData& 
 
 // ------------------------------------------------------------------------------------------
 // smooth.py:469-536 — transmission (JOINT, JOINTINPARENT)
+template <int L = 32>
 __device__ void transmission(const MjbModel& m, const MjbData& d, int w, int lane) {
   const int nv = m.nv;
   const float* qpos = d.qpos + W(w, m.nq);
   float* length = d.actuator_length + W(w, m.nu);
   float* moment = d.actuator_moment + W(w, m.nu * nv);
-  for (int e = lane; e < m.nu * nv; e += 32) moment[e] = 0.f;  // coalesced; then the nonzeros
-  __syncwarp();
-  for (int a = lane; a < m.nu; a += 32) {
+  for (int e = lane; e < m.nu * nv; e += L) moment[e] = 0.f;  // coalesced; then the nonzeros
+  lsync<L>();
+  for (int a = lane; a < m.nu; a += L) {
     const int j = m.actuator_trnid[2 * a], t = m.jnt_type[j];
     const int qa = m.jnt_qposadr[j], va = m.jnt_dofadr[j], trn = m.actuator_trntype[a];
     const float* gear = m.actuator_gear + 6 * a;
@@ -815,11 +829,12 @@ __device__ void transmission(const MjbModel& m, const MjbData& d, int w, int lan
       mom[va] = gear[0];
     }
   }
-  __syncwarp();
+  lsync<L>();
 }
 
 // ------------------------------------------------------------------------------------------
 // smooth.py:539-606 — cvel, cdof_dot
+template <int L = 32>
 __device__ void com_vel(const MjbModel& m, const MjbData& d, int w, int lane) {
   const int nb = m.nbody, nv = m.nv;
   float* cvel = d.cvel + W(w, 6 * nb);
@@ -827,10 +842,10 @@ __device__ void com_vel(const MjbModel& m, const MjbData& d, int w, int lane) {
   const float* cdof = d.cdof + W(w, 6 * nv);
   const float* qvel = d.qvel + W(w, nv);
   if (lane < 6) cvel[lane] = 0.f;
-  __syncwarp();
+  lsync<L>();
   for (int lvl = 1; lvl < m.nlevel; lvl++) {
     const int beg = m.body_treeadr[lvl], end = m.body_treeadr[lvl + 1];
-    for (int n = beg + lane; n < end; n += 32) {
+    for (int n = beg + lane; n < end; n += L) {
       const int b = m.body_tree[n];
       s6 v = ld6(cvel + 6 * m.body_parentid[b]);
       int dof = m.body_dofadr[b];
@@ -859,26 +874,27 @@ __device__ void com_vel(const MjbModel& m, const MjbData& d, int w, int lane) {
       }
       st6(cvel + 6 * b, v);
     }
-    __syncwarp();
+    lsync<L>();
   }
 }
 
 // passive.py:27-108
+template <int L = 32>
 __device__ void passive(const MjbModel& m, const MjbData& d, int w, int lane) {
   const int nv = m.nv;
   float* qfrc_passive = d.qfrc_passive + W(w, nv);
   if (m.disableflags & DSBL_PASSIVE) {
-    for (int i = lane; i < nv; i += 32) qfrc_passive[i] = 0.f;
-    __syncwarp();
+    for (int i = lane; i < nv; i += L) qfrc_passive[i] = 0.f;
+    lsync<L>();
     return;
   }
   const float* qpos = d.qpos + W(w, m.nq);
   const float* qvel = d.qvel + W(w, nv);
   float* spring = d.qfrc_spring + W(w, nv);
   float* damper = d.qfrc_damper + W(w, nv);
-  for (int i = lane; i < nv; i += 32) spring[i] = 0.f;
-  __syncwarp();
-  for (int j = lane; j < m.njnt; j += 32) {
+  for (int i = lane; i < nv; i += L) spring[i] = 0.f;
+  lsync<L>();
+  for (int j = lane; j < m.njnt; j += L) {
     const float k = m.jnt_stiffness[j];
     if (k == 0.f) continue;
     const int dof = m.jnt_dofadr[j], t = m.jnt_type[j], a = m.jnt_qposadr[j];
@@ -893,16 +909,17 @@ __device__ void passive(const MjbModel& m, const MjbData& d, int w, int lane) {
       spring[dof] = -k * (qpos[a] - m.qpos_spring[a]);
     }
   }
-  __syncwarp();
-  for (int i = lane; i < nv; i += 32) {
+  lsync<L>();
+  for (int i = lane; i < nv; i += L) {
     const float dm = -m.dof_damping[i] * qvel[i];
     damper[i] = dm;
     qfrc_passive[i] = dm + spring[i];
   }
-  __syncwarp();
+  lsync<L>();
 }
 
 // smooth.py:398-466 — recursive Newton-Euler bias forces
+template <int L = 32>
 __device__ void rne(const MjbModel& m, const MjbData& d, int w, int lane) {
   const int nb = m.nbody, nv = m.nv;
   float* cacc = d.rne_cacc + W(w, 6 * nb);
@@ -915,10 +932,10 @@ __device__ void rne(const MjbModel& m, const MjbData& d, int w, int lane) {
     const bool grav = !(m.disableflags & DSBL_GRAVITY);
     cacc[lane] = (lane >= 3 && grav) ? -m.gravity[lane - 3] : 0.f;
   }
-  __syncwarp();
+  lsync<L>();
   for (int lvl = 1; lvl < m.nlevel; lvl++) {
     const int beg = m.body_treeadr[lvl], end = m.body_treeadr[lvl + 1];
-    for (int n = beg + lane; n < end; n += 32) {
+    for (int n = beg + lane; n < end; n += L) {
       const int b = m.body_tree[n];
       s6 a = ld6(cacc + 6 * m.body_parentid[b]);
       const int da = m.body_dofadr[b];
@@ -928,9 +945,9 @@ __device__ void rne(const MjbModel& m, const MjbData& d, int w, int lane) {
       }
       st6(cacc + 6 * b, a);
     }
-    __syncwarp();
+    lsync<L>();
   }
-  for (int b = lane; b < nb; b += 32) {
+  for (int b = lane; b < nb; b += L) {
     const s6 v = ld6(cvel + 6 * b);
     const s6 f = inert_vec(cinert + 10 * b, ld6(cacc + 6 * b));
     const s6 g = motion_cross_force(v, inert_vec(cinert + 10 * b, v));
@@ -938,11 +955,11 @@ __device__ void rne(const MjbModel& m, const MjbData& d, int w, int lane) {
     for (int k = 0; k < 6; k++) r.v[k] = f.v[k] + g.v[k];
     st6(cfrc + 6 * b, r);
   }
-  __syncwarp();
+  lsync<L>();
   // bottom-up gather; level 0 adds the world into itself as smooth.py:461-464 does
   for (int lvl = m.nlevel - 1; lvl >= 0; lvl--) {
     const int beg = m.body_treeadr[lvl], end = m.body_treeadr[lvl + 1];
-    for (int n = beg + lane; n < end; n += 32) {
+    for (int n = beg + lane; n < end; n += L) {
       const int b = m.body_tree[n];
       s6 acc = ld6(cfrc + 6 * b);
       const int ca = m.body_childadr[b], cn = m.body_childnum[b];
@@ -954,47 +971,49 @@ __device__ void rne(const MjbModel& m, const MjbData& d, int w, int lane) {
         for (int k = 0; k < 6; k++) acc.v[k] += acc.v[k];
       st6(cfrc + 6 * b, acc);
     }
-    __syncwarp();
+    lsync<L>();
   }
   const float* cdof = d.cdof + W(w, 6 * nv);
   float* bias = d.qfrc_bias + W(w, nv);
-  for (int i = lane; i < nv; i += 32) bias[i] = dot6(ld6(cdof + 6 * i), ld6(cfrc + 6 * m.dof_bodyid[i]));
-  __syncwarp();
+  for (int i = lane; i < nv; i += L) bias[i] = dot6(ld6(cdof + 6 * i), ld6(cfrc + 6 * m.dof_bodyid[i]));
+  lsync<L>();
 }
 
 // forward.py:423-500 (dense path)
+template <int L = 32>
 __device__ void fwd_velocity(const MjbModel& m, const MjbData& d, int w, int lane) {
   const int nv = m.nv;
   const float* moment = d.actuator_moment + W(w, m.nu * nv);
   const float* qvel = d.qvel + W(w, nv);
   float* vel = d.actuator_velocity + W(w, m.nu);
-  for (int a = lane; a < m.nu; a += 32) {
+  for (int a = lane; a < m.nu; a += L) {
     float s = 0.f;
     for (int i = 0; i < nv; i++) s += moment[a * nv + i] * qvel[i];
     vel[a] = s;
   }
-  __syncwarp();
-  com_vel(m, d, w, lane);
-  passive(m, d, w, lane);
-  rne(m, d, w, lane);
+  lsync<L>();
+  com_vel<L>(m, d, w, lane);
+  passive<L>(m, d, w, lane);
+  rne<L>(m, d, w, lane);
 }
 
 // forward.py:503-641
+template <int L = 32>
 __device__ void fwd_actuation(const MjbModel& m, const MjbData& d, int w, int lane) {
   const int nv = m.nv, nu = m.nu;
   float* qfrc = d.qfrc_actuator + W(w, nv);
   if (!nu || (m.disableflags & DSBL_ACTUATION)) {
     if (d.act_dot)
-      for (int i = lane; i < m.na; i += 32) d.act_dot[W(w, m.na) + i] = 0.f;
-    for (int i = lane; i < nv; i += 32) qfrc[i] = 0.f;
-    __syncwarp();
+      for (int i = lane; i < m.na; i += L) d.act_dot[W(w, m.na) + i] = 0.f;
+    for (int i = lane; i < nv; i += L) qfrc[i] = 0.f;
+    lsync<L>();
     return;
   }
   const float* len = d.actuator_length + W(w, nu);
   const float* vel = d.actuator_velocity + W(w, nu);
   const float* ctrl = d.ctrl + W(w, nu);
   float* force = d.actuator_force + W(w, nu);
-  for (int a = lane; a < nu; a += 32) {
+  for (int a = lane; a < nu; a += L) {
     const float* gp = m.actuator_gainprm + 10 * a;
     const float* bp = m.actuator_biasprm + 10 * a;
     float gain = gp[0];
@@ -1008,16 +1027,16 @@ __device__ void fwd_actuation(const MjbModel& m, const MjbData& d, int w, int la
       c = fminf(fmaxf(c, m.actuator_ctrlrange[2 * a]), m.actuator_ctrlrange[2 * a + 1]);
     force[a] = gain * c + bias;  // forcerange is not applied (forward.py:539-541)
   }
-  __syncwarp();
+  lsync<L>();
   const float* moment = d.actuator_moment + W(w, nu * nv);
-  for (int i = lane; i < nv; i += 32) {
+  for (int i = lane; i < nv; i += L) {
     float s = 0.f;
     for (int a = 0; a < nu; a++) s += moment[a * nv + i] * force[a];
     const int j = m.dof_jntid[i];
     if (m.jnt_actfrclimited[j]) s = fminf(fmaxf(s, m.jnt_actfrcrange[2 * j]), m.jnt_actfrcrange[2 * j + 1]);
     qfrc[i] = s;
   }
-  __syncwarp();
+  lsync<L>();
 }
 
 // support.py:140-172 — qfrc += J^T xfrc_applied (Jacobian at each body's xipos)
