@@ -508,7 +508,8 @@ __host__ __device__ __forceinline__ int tile_floats(int nv) {
 }
 
 // In-place Cholesky of an n x n (n <= 32) SPD tile with row stride ld (lower triangle): the
-// arithmetic of chol_lower (same partial sums, pivot and reciprocal) with float4 row reads.
+// partial sums of chol_lower with float4 row reads; the pivot and its reciprocal come from one
+// rsqrtf (within 2 ulp of the correctly rounded sqrt and reciprocal).
 __device__ MJB_TILE_FN void chol_tile(float* A, int ld, int n, int lane) {
   for (int k = 0; k < n; k++) {
     const float* Ai = A + min(k + lane, n - 1) * ld;  // lanes past the last row reuse it
@@ -526,8 +527,10 @@ __device__ MJB_TILE_FN void chol_tile(float* A, int ld, int n, int lane) {
     }
     for (; m < k; m++) s0 += Ai[m] * Ak[m];
     const float s = Ai[k] - ((s0 + s1) + (s2 + s3));
-    const float lkk = sqrtf(__shfl_sync(WARP_FULL, s, 0));
-    const float inv = __frcp_rn(lkk);
+    // pivot from one reciprocal square root: 1 / L_kk = rsqrt(s_k), L_kk = s_k * rsqrt(s_k)
+    const float sk = __shfl_sync(WARP_FULL, s, 0);
+    const float inv = rsqrtf(sk);
+    const float lkk = sk * inv;
     __syncwarp();
     if (lane == 0) A[k * ld + k] = lkk;
     else if (k + lane < n) A[(k + lane) * ld + k] = s * inv;
