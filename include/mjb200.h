@@ -198,6 +198,24 @@ int mjb_xfrc_accumulate(const MjbModel* m, const MjbData* d, float* qfrc, mjbStr
 /* Copies world_status (nworld words) to host memory; synchronises the stream. */
 int mjb_world_status(const MjbData* d, uint32_t* host_out, mjbStream stream);
 
+/* Launch parameters of the chosen form that the autotuner picks (no counterpart in the reference):
+ * lanes per world of the tree-recursion stages and warps per CTA of the persistent solver. */
+typedef struct MjbTune {
+  int32_t tree_lanes;    /* 8, 16 or 32 */
+  int32_t solver_warps;  /* 1, 2 or 4 */
+  float ms_per_forward;  /* measured chosen-form forward (fwd_position .. solve) at this setting */
+} MjbTune;
+
+/* Autotuner (no counterpart in the reference): times the chosen form's forward for every
+ * tree-lane count and solver CTA width on d's current worlds and keeps the fastest, per device,
+ * for models of this nv and Data of this rows-per-world capacity (njmax / nworld); later chosen-
+ * form calls with the same key use it (others keep 16 lanes and 4 warps).  warmstart_scratch:
+ * nworld * nv floats of caller memory; qacc_warmstart is saved there and restored before every
+ * trial and at the end, so d is left as after one chosen-form forward.  Synchronises the stream;
+ * out may be null. */
+int mjb_autotune(const MjbModel* m, const MjbData* d, float* warmstart_scratch, MjbTune* out,
+                 mjbStream stream);
+
 /* Finite-difference transition Jacobians, no counterpart in the reference (whose API has no
  * derivatives); the scheme is MuJoCo's mjd_transitionFD, batched over worlds.  State
  * x = (qpos in the tangent space, qvel, act), nx = 2 nv + na; input u = ctrl.  `pert` is a Data

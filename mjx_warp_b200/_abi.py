@@ -113,6 +113,11 @@ class MjbData(ctypes.Structure):
               + [(n, ctypes.c_void_p) for n, _ in DATA_PTRS])
 
 
+class MjbTune(ctypes.Structure):
+  _fields_ = [("tree_lanes", ctypes.c_int32), ("solver_warps", ctypes.c_int32),
+              ("ms_per_forward", ctypes.c_float)]
+
+
 class MjbRunCfg(ctypes.Structure):
   _fields_ = [("fused", ctypes.c_int32), ("worlds_per_block", ctypes.c_int32)]
 
@@ -160,6 +165,8 @@ def lib() -> ctypes.CDLL:
   L.mjb_fd_perturb.argtypes = [pm, pd, pd, cf, ci, vp]
   L.mjb_fd_jacobian.restype = ctypes.c_int
   L.mjb_fd_jacobian.argtypes = [pm, pd, ci, cf, ci, vp, vp, vp]
+  L.mjb_autotune.restype = ctypes.c_int
+  L.mjb_autotune.argtypes = [pm, pd, vp, ctypes.POINTER(MjbTune), vp]
   L.mjb_transition_vjp.restype = ctypes.c_int
   L.mjb_transition_vjp.argtypes = [pm, ci, vp, vp, vp, vp, vp, vp]
   if L.mjb_abi_version() != 2:

@@ -251,3 +251,19 @@ def benchmark(fn: Callable[[Model, Data], None], m: Model, d: Data, nstep: int =
   torch.cuda.synchronize()
   t3 = _time.perf_counter()
   return t1 - t0, t3 - t2, d.nworld * nstep
+
+
+def autotune(m: Model, d: Data) -> dict:
+  """Picks the chosen form's launch parameters for this model and Data (an extension; the
+  reference has no autotuner): times the chosen forward for every tree-stage lane count (8, 16,
+  32 lanes per world) and persistent-solver CTA width (1, 2, 4 warps) on d's current worlds and
+  keeps the fastest for later calls with the same nv and rows-per-world capacity on this device.
+  d's qacc_warmstart is saved and restored around the trials; d is left as after one forward.
+  Synchronises; call it before capturing a CUDA graph."""
+  scratch = torch.empty_like(d.qacc_warmstart)
+  out = _abi.MjbTune()
+  rc = _abi.lib().mjb_autotune(ctypes.byref(_abi.model_view(m)), ctypes.byref(_abi.data_view(d)),
+                               _abi._ptr(scratch), ctypes.byref(out), _abi.stream())
+  _abi.check(rc, "autotune")
+  return {"tree_lanes": out.tree_lanes, "solver_warps": out.solver_warps,
+          "ms_per_forward": out.ms_per_forward}

@@ -367,23 +367,32 @@ void allow_smem(K kernel, size_t bytes, size_t (&configured)[kSmemDevices]) {
 }
 
 // CTAs of `kernel` resident on the whole GPU at once for blocks of `threads` threads and `smem`
-// bytes, queried once per device and shared-memory size (the block size is fixed per kernel)
+// bytes, queried once per (device, kernel, block size, shared-memory size)
 template <typename K>
 int resident_ctas(K kernel, int threads, size_t smem) {
-  static int cached[kSmemDevices];
-  static size_t cached_smem[kSmemDevices];
+  struct Entry {
+    int dev;
+    const void* fn;
+    int threads;
+    size_t smem;
+    int ctas;
+  };
+  static Entry cache[64];
+  static int used = 0;
+  static std::mutex mu;
   int dev = 0;
   cudaGetDevice(&dev);
-  const bool slot = dev >= 0 && dev < kSmemDevices;
-  if (slot && cached[dev] > 0 && cached_smem[dev] == smem) return cached[dev];
+  const void* fn = reinterpret_cast<const void*>(kernel);
+  std::lock_guard<std::mutex> lock(mu);
+  for (int i = 0; i < used; i++)
+    if (cache[i].dev == dev && cache[i].fn == fn && cache[i].threads == threads &&
+        cache[i].smem == smem)
+      return cache[i].ctas;
   int sms = 0, per_sm = 0;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem);
   const int n = std::max(1, sms * std::max(1, per_sm));
-  if (slot) {
-    cached[dev] = n;
-    cached_smem[dev] = smem;
-  }
+  if (used < 64) cache[used++] = Entry{dev, fn, threads, smem, n};
   return n;
 }
 
@@ -411,13 +420,59 @@ int launch_broadphase(const MjbModel* m, const MjbData* d, cudaStream_t s) {
   return m->ngeom > 100 ? launch_stage<S_SAP>(m, d, s) : launch_stage<S_NXN>(m, d, s);
 }
 
-// a tree-recursion stage with MJB_TREE_LANES lanes per world
-template <int STAGE>
-int launch_lanes(const MjbModel* m, const MjbData* d, cudaStream_t s) {
-  constexpr int L = MJB_TREE_LANES;
+// a tree-recursion stage with `lanes` (8, 16 or 32) lanes per world
+template <int STAGE, int L>
+int launch_lanes_l(const MjbModel* m, const MjbData* d, cudaStream_t s) {
   const long long threads = (long long)d->nworld * L;
   k_stage_lanes<STAGE, L><<<int((threads + 127) / 128), 128, 0, s>>>(*m, *d);
   return finish();
+}
+template <int STAGE>
+int launch_lanes(const MjbModel* m, const MjbData* d, cudaStream_t s, int lanes) {
+  if (lanes == 8) return launch_lanes_l<STAGE, 8>(m, d, s);
+  if (lanes == 32) return launch_lanes_l<STAGE, 32>(m, d, s);
+  return launch_lanes_l<STAGE, 16>(m, d, s);
+}
+
+// The chosen form's launch parameters: lanes per world of the tree-recursion stages and warps per
+// CTA of the persistent solver.  mjb_autotune measures them per device for a model's nv and a
+// Data's rows-per-world capacity (njmax / nworld, the caller's sizing of its contact density);
+// without a tuned entry the defaults below apply.
+struct ChosenCfg {
+  int lanes = MJB_TREE_LANES;
+  int warps = kDefaultWarps;
+};
+struct TuneEntry {
+  int dev, nv, cap;
+  ChosenCfg cfg;
+};
+std::mutex g_tune_mutex;
+TuneEntry g_tune[64];
+int g_ntune = 0;
+
+inline int rows_capacity(const MjbData* d) { return d->nworld > 0 ? d->njmax / d->nworld : 0; }
+
+ChosenCfg chosen_cfg(const MjbModel* m, const MjbData* d) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  const int cap = rows_capacity(d);
+  std::lock_guard<std::mutex> lock(g_tune_mutex);
+  for (int i = 0; i < g_ntune; i++)
+    if (g_tune[i].dev == dev && g_tune[i].nv == m->nv && g_tune[i].cap == cap) return g_tune[i].cfg;
+  return ChosenCfg{};
+}
+
+void store_cfg(const MjbModel* m, const MjbData* d, ChosenCfg cfg) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  const int cap = rows_capacity(d);
+  std::lock_guard<std::mutex> lock(g_tune_mutex);
+  for (int i = 0; i < g_ntune; i++)
+    if (g_tune[i].dev == dev && g_tune[i].nv == m->nv && g_tune[i].cap == cap) {
+      g_tune[i].cfg = cfg;
+      return;
+    }
+  if (g_ntune < 64) g_tune[g_ntune++] = TuneEntry{dev, m->nv, cap, cfg};
 }
 
 void reset_counters(const MjbData* d, bool pairs, bool contacts, bool efc, bool status,
@@ -468,7 +523,7 @@ struct StageFork {
 std::mutex g_fork_mutex;
 StageFork g_fork[kSmemDevices];
 
-int run_forward_fork(const MjbModel* m, const MjbData* d, cudaStream_t s) {
+int run_forward_fork(const MjbModel* m, const MjbData* d, cudaStream_t s, int lanes) {
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kSmemDevices)
     return run_forward_plain_nosolve(m, d, s);
@@ -482,16 +537,16 @@ int run_forward_fork(const MjbModel* m, const MjbData* d, cudaStream_t s) {
     f.ready = true;
   }
   int rc;
-  if ((rc = launch_lanes<S_KINEMATICS>(m, d, s))) return rc;
-  if ((rc = launch_lanes<S_COM_POS>(m, d, s))) return rc;
+  if ((rc = launch_lanes<S_KINEMATICS>(m, d, s, lanes))) return rc;
+  if ((rc = launch_lanes<S_COM_POS>(m, d, s, lanes))) return rc;
   if (cudaEventRecord(f.ev[0], s) != cudaSuccess) return MJB_ERR_LAUNCH;
   for (auto& a : f.aux)
     if (cudaStreamWaitEvent(a, f.ev[0], 0) != cudaSuccess) return MJB_ERR_LAUNCH;
-  int rc0 = launch_lanes<S_CRB>(m, d, f.aux[0]);
+  int rc0 = launch_lanes<S_CRB>(m, d, f.aux[0], lanes);
   if (!rc0) rc0 = launch_stage<S_FACTOR_M>(m, d, f.aux[0]);
-  int rc1 = launch_lanes<S_TRANSMISSION>(m, d, f.aux[1]);
-  if (!rc1) rc1 = launch_lanes<S_FWD_VELOCITY>(m, d, f.aux[1]);
-  if (!rc1) rc1 = launch_lanes<S_FWD_ACTUATION>(m, d, f.aux[1]);
+  int rc1 = launch_lanes<S_TRANSMISSION>(m, d, f.aux[1], lanes);
+  if (!rc1) rc1 = launch_lanes<S_FWD_VELOCITY>(m, d, f.aux[1], lanes);
+  if (!rc1) rc1 = launch_lanes<S_FWD_ACTUATION>(m, d, f.aux[1], lanes);
   reset_counters(d, true, true, true, false, s);
   int rc2 = launch_broadphase(m, d, s);
   if (!rc2) rc2 = launch_stage<S_NARROW>(m, d, s);
@@ -515,7 +570,9 @@ int run_forward_plain(const MjbModel* m, const MjbData* d, cudaStream_t s) {
 
 // the chosen form's phases: 0 = status reset + the stage kernels up to fwd_acceleration,
 // 1 = k_solve, 2 = k_integrate
-int run_chosen_phase(const MjbModel* m, const MjbData* d, int phase, cudaStream_t s) {
+int run_chosen_phase(const MjbModel* m, const MjbData* d, int phase, cudaStream_t s,
+                     const ChosenCfg* tuned = nullptr) {
+  const ChosenCfg cfg = tuned ? *tuned : chosen_cfg(m, d);
   const int warps = kDefaultWarps;
   const int grid = grid_for(d->nworld, warps);
   const int tpw = tile_floats(m->nv);
@@ -523,19 +580,21 @@ int run_chosen_phase(const MjbModel* m, const MjbData* d, int phase, cudaStream_
   static size_t conf_solve[kSmemDevices], conf_int[kSmemDevices];
   if (phase == 0) {
     reset_counters(d, false, false, false, true, s);
-    int rc = run_forward_fork(m, d, s);
+    int rc = run_forward_fork(m, d, s, cfg.lanes);
     if (rc) return rc;
   } else if (phase == 1) {
     if (d->njmax > 0) {
       const int spw = m->nv <= 32 ? int(solver_smem_floats(m->nv)) : generic_nz_floats(m->nv);
-      const size_t bytes = size_t(spw) * warps * sizeof(float);
       if (d->world_order && d->work_queue && d->world_nefc) {
+        const int qw = cfg.warps;
+        const size_t qbytes = size_t(spw) * qw * sizeof(float);
         static size_t conf_queue[kSmemDevices];
-        allow_smem(k_solve_queue, bytes, conf_queue);
-        const int ctas = resident_ctas(k_solve_queue, 32 * warps, bytes);
+        allow_smem(k_solve_queue, size_t(spw) * kDefaultWarps * sizeof(float), conf_queue);
+        const int ctas = resident_ctas(k_solve_queue, 32 * qw, qbytes);
         k_order_worlds<<<1, 1024, 0, s>>>(d->world_nefc, d->world_order, d->work_queue, d->nworld);
-        k_solve_queue<<<std::min(ctas, grid), 32 * warps, bytes, s>>>(*m, *d, spw);
+        k_solve_queue<<<std::min(ctas, grid_for(d->nworld, qw)), 32 * qw, qbytes, s>>>(*m, *d, spw);
       } else {
+        const size_t bytes = size_t(spw) * warps * sizeof(float);
         allow_smem(k_solve, bytes, conf_solve);
         k_solve<<<grid, 32 * warps, bytes, s>>>(*m, *d, spw);
       }
@@ -788,6 +847,73 @@ extern "C" int mjb_implicit_noalloc(const MjbModel* m, const MjbData* d, mjbStre
   dd.qLD_integration = scratch + size_t(d->nworld) * nv * nv;
   dd.qfrc_integration = scratch + 2 * size_t(d->nworld) * nv * nv;
   return launch_stage<S_IMPLICIT>(m, &dd, (cudaStream_t)stream);
+}
+
+// ------------------------------------------------------------------------------------------
+// Autotuner of the chosen form's launch parameters.
+
+extern "C" int mjb_autotune(const MjbModel* m, const MjbData* d, float* warmstart_scratch,
+                            MjbTune* out, mjbStream stream) {
+  int rc = check(m, d);
+  if (rc || d->nworld == 0) return rc;
+  if (!warmstart_scratch || !d->qacc_warmstart) return MJB_ERR_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  const size_t wsb = size_t(d->nworld) * size_t(m->nv) * sizeof(float);
+  auto restore = [&]() {
+    return cudaMemcpyAsync(d->qacc_warmstart, warmstart_scratch, wsb, cudaMemcpyDeviceToDevice, s);
+  };
+  if (cudaMemcpyAsync(warmstart_scratch, d->qacc_warmstart, wsb, cudaMemcpyDeviceToDevice, s) !=
+      cudaSuccess)
+    return MJB_ERR_LAUNCH;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+    if (e0) cudaEventDestroy(e0);
+    return MJB_ERR_LAUNCH;
+  }
+  const int lanes[3] = {8, 16, 32}, widths[3] = {1, 2, 4};
+  float best = 0.f;
+  ChosenCfg best_cfg;
+  bool have = false;
+  for (int li = 0; li < 3 && !rc; li++) {
+    for (int wi = 0; wi < 3 && !rc; wi++) {
+      ChosenCfg c;
+      c.lanes = lanes[li];
+      c.warps = widths[wi];
+      auto forward = [&]() -> int {
+        if (restore() != cudaSuccess) return MJB_ERR_LAUNCH;
+        int r = run_chosen_phase(m, d, 0, s, &c);
+        return r ? r : run_chosen_phase(m, d, 1, s, &c);
+      };
+      if ((rc = forward())) break;  // warm-up
+      constexpr int kReps = 3;
+      if (cudaEventRecord(e0, s) != cudaSuccess) { rc = MJB_ERR_LAUNCH; break; }
+      for (int r = 0; r < kReps && !rc; r++) rc = forward();
+      if (rc) break;
+      float ms = 0.f;
+      if (cudaEventRecord(e1, s) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+          cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) {
+        rc = MJB_ERR_LAUNCH;
+        break;
+      }
+      ms /= kReps;
+      if (!have || ms < best) {
+        best = ms;
+        best_cfg = c;
+        have = true;
+      }
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (!rc && restore() != cudaSuccess) rc = MJB_ERR_LAUNCH;
+  if (rc) return rc;
+  store_cfg(m, d, best_cfg);
+  if (out) {
+    out->tree_lanes = best_cfg.lanes;
+    out->solver_warps = best_cfg.warps;
+    out->ms_per_forward = best;
+  }
+  return MJB_OK;
 }
 
 // ------------------------------------------------------------------------------------------

@@ -187,3 +187,26 @@ def test_get_data_into_roundtrip():
   assert out.efc_J.shape == (out.nefc, mjm.nv)
   d2 = mjw.put_data(mjm, out)
   np.testing.assert_allclose(d2.qacc.numpy(), d.qacc.numpy(), rtol=1e-6)
+
+
+def test_autotune_picks_a_setting_and_keeps_results():
+  """mjb_autotune (an extension) returns one of its candidate settings, restores the warmstart,
+  and the chosen form's steps are bit-identical with and without the tuned setting (lanes per
+  world and solver CTA width change the schedule, not the arithmetic)."""
+  mjm = humanoid()
+  nworld = 512
+  qpos, qvel, ctrl = humanoid_state(mjm, nworld, seed=9)
+  m = mjw.put_model(mjm)
+  d1 = device_data(mjm, qpos, qvel, ctrl)
+  d2 = device_data(mjm, qpos, qvel, ctrl)
+  for _ in range(3):
+    mjw.step(m, d1)
+  ws, q = d2.qacc_warmstart.clone(), d2.qpos.clone()
+  cfg = mjw.autotune(m, d2)
+  assert cfg["tree_lanes"] in (8, 16, 32) and cfg["solver_warps"] in (1, 2, 4)
+  assert cfg["ms_per_forward"] > 0
+  assert torch.equal(d2.qacc_warmstart, ws) and torch.equal(d2.qpos, q)
+  for _ in range(3):
+    mjw.step(m, d2)
+  torch.cuda.synchronize()
+  assert torch.equal(d1.qpos, d2.qpos) and torch.equal(d1.qvel, d2.qvel)
