@@ -164,13 +164,22 @@ __global__ void __launch_bounds__(128, MJB_MINB) k_solve(const __grid_constant__
 // solves start first and the last ones to finish are short (longest-processing-time-first).
 // Each world's result does not depend on which warp solves it or when.
 constexpr int kOrderBuckets = 256;
+// Worlds with the same bucket in a warp are counted and placed with one shared-memory atomic per
+// bucket (the lanes of a bucket found by __match_any_sync), so the few buckets a model's row
+// counts fall into do not serialise thousands of atomics.
 __global__ void __launch_bounds__(1024) k_order_worlds(const int* nefc, int* order, int* queue,
                                                       int nworld) {
   __shared__ int cnt[kOrderBuckets];
+  const int lane = threadIdx.x & 31;
+  const unsigned below = (1u << lane) - 1u;
+  const int span = (nworld + blockDim.x - 1) / blockDim.x * blockDim.x;  // warp-uniform trip count
   for (int b = threadIdx.x; b < kOrderBuckets; b += blockDim.x) cnt[b] = 0;
   __syncthreads();
-  for (int w = threadIdx.x; w < nworld; w += blockDim.x)
-    atomicAdd(&cnt[min(max(nefc[w], 0), kOrderBuckets - 1)], 1);
+  for (int w = threadIdx.x; w < span; w += blockDim.x) {
+    const int b = w < nworld ? min(max(nefc[w], 0), kOrderBuckets - 1) : -1;
+    const unsigned peers = __match_any_sync(WARP_FULL, b);
+    if (b >= 0 && (peers & below) == 0) atomicAdd(&cnt[b], __popc(peers));
+  }
   __syncthreads();
   if (threadIdx.x == 0) {
     int run = 0;
@@ -182,8 +191,15 @@ __global__ void __launch_bounds__(1024) k_order_worlds(const int* nefc, int* ord
     *queue = 0;
   }
   __syncthreads();
-  for (int w = threadIdx.x; w < nworld; w += blockDim.x)
-    order[atomicAdd(&cnt[min(max(nefc[w], 0), kOrderBuckets - 1)], 1)] = w;
+  for (int w = threadIdx.x; w < span; w += blockDim.x) {
+    const int b = w < nworld ? min(max(nefc[w], 0), kOrderBuckets - 1) : -1;
+    const unsigned peers = __match_any_sync(WARP_FULL, b);
+    const int leader = __ffs(peers) - 1;
+    int base = 0;
+    if (b >= 0 && lane == leader) base = atomicAdd(&cnt[b], __popc(peers));
+    base = __shfl_sync(WARP_FULL, base, leader);
+    if (b >= 0) order[base + __popc(peers & below)] = w;
+  }
 }
 
 __global__ void __launch_bounds__(128, MJB_MINB) k_solve_queue(const __grid_constant__ MjbModel m, const __grid_constant__ MjbData d, int smem_per_warp) {
