@@ -89,8 +89,9 @@ def test_humanoid_steps_converged_vs_fp64():
 
 
 def test_sphere_chain_long_rollout():
-  """Config 1 (sphere + 5-link chain, Euler with eulerdamp): 1000 steps stay finite and track
-  the FP64 oracle closely for the first 50 steps."""
+  """Config 1 (sphere + 5-link chain, Euler with eulerdamp): 1000 steps stay finite and their qpos
+  stays within 1e-4 (relative, every world) of the FP64 oracle's — the drift measured on a B200
+  is ~4e-6 median, 1.6e-5 max at step 1000."""
   mjm = load("sphere_chain.xml")
   rng = np.random.default_rng(0)
   nworld = 32
@@ -108,6 +109,9 @@ def test_sphere_chain_long_rollout():
   assert rel_err(dev(d.qpos), o.get("qpos")).max() < 1e-4
   for _ in range(950):
     mjw.step(m, d)
+  o.run("step", nstep=950)
+  torch.cuda.synchronize()
+  assert rel_err(dev(d.qpos), o.get("qpos")).max() < 1e-4
   assert np.all(np.isfinite(d.qpos.cpu().numpy()))
   assert np.all(mjw.world_status(d) == 0)
   assert float(d.qpos[:, 2].min()) > 0.05  # the ball rests on the floor
