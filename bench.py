@@ -190,7 +190,8 @@ def _qacc_error(mjm, m, d, mjw, torch, restore, forms, sample=256):
   return out
 
 
-def _grad_rate(mjw, torch, nworld=1024, horizon=32, checkpoint=8, reps=2, centered=True):
+def _grad_rate(mjw, torch, nworld=1024, horizon=32, checkpoint=8, reps=2, centered=True,
+               analytic_ctrl=None):
   """grad-steps/s of a differentiated rollout (see the module docstring).  The Newton solve runs
   to convergence (10 iterations, 10 line-search iterations): the 3-iteration iterate of the
   steps/s workload is discontinuous in its inputs, and differences across those jumps make the
@@ -201,7 +202,8 @@ def _grad_rate(mjw, torch, nworld=1024, horizon=32, checkpoint=8, reps=2, center
   qpos, qvel, ctrl0 = _state(mjm, 0, nworld, seed=1)
   m = mjw.put_model(mjm)
   roll = mjw.derivative.Rollout(mjm, m, nworld, checkpoint=checkpoint, eps=1e-3,
-                                centered=centered, nconmax=48, njmax=80)
+                                centered=centered, nconmax=48, njmax=80,
+                                analytic_ctrl=analytic_ctrl)
   rng = np.random.default_rng(2)
   ctrl = np.repeat(ctrl0[None], horizon, axis=0) + rng.normal(0.0, 0.05, (horizon, nworld, mjm.nu))
   q0 = torch.tensor(qpos, dtype=torch.float32, device="cuda")
@@ -234,8 +236,11 @@ def _grad_rate(mjw, torch, nworld=1024, horizon=32, checkpoint=8, reps=2, center
   return {"value": nworld * horizon / t, "unit": "grad-steps/s",
           "config": {"nworld": nworld, "horizon": horizon, "checkpoint": checkpoint,
                      "wrt": "ctrl (32x21), qpos0, qvel0",
-                     "method": f"GPU finite-difference transition Jacobians ({'centered' if centered else 'forward'}, eps 1e-3, "
-                               f"{roll.fd.K} world-steps per world-step) + reverse recursion"},
+                     "method": (f"GPU finite-difference transition Jacobians ({'centered' if centered else 'forward'}, eps 1e-3, "
+                                f"{roll.fd.K} world-steps per world-step"
+                                + (", state columns only; control gradient by implicit differentiation at the "
+                                   "Newton solution" if roll.analytic_ctrl else "")
+                                + ") + reverse recursion")},
           "solver": "Newton 10 it / ls 10 (converged)",
           "forward_ms": fwd * 1e3, "backward_ms": bwd * 1e3,
           "rollout_steps_per_s": nworld * horizon / fwd, "cost_vs_forward": t / fwd,
@@ -395,6 +400,9 @@ def run_ours(args):
     fwd = _grad_rate(mjw, torch, centered=False)
     grad["forward_differences"] = {k: fwd[k] for k in ("value", "unit", "cost_vs_forward",
                                                        "worlds_with_finite_grads")}
+    allfd = _grad_rate(mjw, torch, analytic_ctrl=False)
+    grad["all_columns_by_differences"] = {k: allfd[k] for k in ("value", "unit", "cost_vs_forward",
+                                                               "worlds_with_finite_grads")}
 
   launches_per_step = LAUNCHES[args.form]
   total_worlds = nworld * world_size

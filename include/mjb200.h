@@ -220,15 +220,30 @@ int mjb_autotune(const MjbModel* m, const MjbData* d, float* warmstart_scratch, 
  * derivatives); the scheme is MuJoCo's mjd_transitionFD, batched over worlds.  State
  * x = (qpos in the tangent space, qvel, act), nx = 2 nv + na; input u = ctrl.  `pert` is a Data
  * of nworld * K worlds, K = 1 + ncol (forward differences) or 1 + 2 ncol (centered),
- * ncol = nx + nu.  mjb_fd_perturb copies every base world's state into its K slots and perturbs
+ * ncol = nx + nu, or nx with MJB_FD_STATE_ONLY.  mjb_fd_perturb copies every base world's state into its K slots and perturbs
  * one column per slot by eps (tangent-space rotations for quaternions); the caller then steps
  * `pert` (mjb_step); mjb_fd_jacobian differences the next states into A (nworld x nx x nx) and
  * B (nworld x nx x nu), row-major per world: A[w][i][j] = d x'_i / d x_j.  eps > 0; in FP32 a
  * value near 1e-3 balances truncation and rounding. */
 int mjb_fd_perturb(const MjbModel* m, const MjbData* base, const MjbData* pert, float eps,
-                   int centered, mjbStream stream);
-int mjb_fd_jacobian(const MjbModel* m, const MjbData* pert, int nworld, float eps, int centered,
+                   int flags, mjbStream stream);
+int mjb_fd_jacobian(const MjbModel* m, const MjbData* pert, int nworld, float eps, int flags,
                     float* A, float* B, mjbStream stream);
+/* `flags`: MJB_FD_CENTERED for centered differences; MJB_FD_STATE_ONLY to perturb the state
+ * columns only (ncol = nx; B is not written and may be null).  Both calls take the same flags. */
+#define MJB_FD_CENTERED 1
+#define MJB_FD_STATE_ONLY 2
+
+/* d loss / d ctrl of one step by implicit differentiation at the constraint solver's final
+ * active set (no counterpart in the reference): grad_ctrl (nworld x nu) = (d x' / d ctrl)^T lam,
+ * lam (nworld x nx) the adjoint of the step's next state (qpos tangent, qvel).  d must hold that
+ * step's results (call it right after mjb_step): its qM, constraint rows and active flags,
+ * qLD_integration, actuator arrays and the new qvel.  Exact at a converged Newton solution; with
+ * the dense mass matrix, nv <= 32, na = 0 and, for implicitfast, no velocity-dependent actuator
+ * gains or biases (else MJB_ERR_UNSUPPORTED). */
+int mjb_ctrl_vjp(const MjbModel* m, const MjbData* d, const float* lam, float* grad_ctrl,
+                 mjbStream stream);
+
 /* Reverse step of a rollout adjoint, per world: lam_out = A^T lam, grad_ctrl = B^T lam
  * (B / grad_ctrl may be null); lam and lam_out are nworld x nx and must not alias. */
 int mjb_transition_vjp(const MjbModel* m, int nworld, const float* A, const float* B,

@@ -165,6 +165,8 @@ def lib() -> ctypes.CDLL:
   L.mjb_fd_perturb.argtypes = [pm, pd, pd, cf, ci, vp]
   L.mjb_fd_jacobian.restype = ctypes.c_int
   L.mjb_fd_jacobian.argtypes = [pm, pd, ci, cf, ci, vp, vp, vp]
+  L.mjb_ctrl_vjp.restype = ctypes.c_int
+  L.mjb_ctrl_vjp.argtypes = [pm, pd, vp, vp, vp]
   L.mjb_autotune.restype = ctypes.c_int
   L.mjb_autotune.argtypes = [pm, pd, vp, ctypes.POINTER(MjbTune), vp]
   L.mjb_transition_vjp.restype = ctypes.c_int

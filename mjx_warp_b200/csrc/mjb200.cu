@@ -230,24 +230,34 @@ __global__ void __launch_bounds__(128, 8) k_integrate(const __grid_constant__ Mj
 
 // finite-difference transition Jacobians (mjb_deriv.cuh): one warp per perturbed slot
 __global__ void k_fd_perturb(const __grid_constant__ MjbModel m, const __grid_constant__ MjbData b,
-                             const __grid_constant__ MjbData p, float eps, int centered) {
+                             const __grid_constant__ MjbData p, float eps, int flags) {
   const int lane = threadIdx.x & 31;
   const int pw = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   if (pw >= p.nworld) return;
-  const int K = fd_slots(m, centered), w = pw / K, k = pw - w * K;
+  const int centered = flags & kFdCentered;
+  const int K = fd_slots(m, flags), w = pw / K, k = pw - w * K;
   const int col = k == 0 ? -1 : (centered ? (k - 1) >> 1 : k - 1);
   const float delta = (centered && ((k - 1) & 1)) ? -eps : eps;
   fd_perturb_world(m, b, p, w, pw, col, delta, lane);
 }
 // one warp per (base world, column)
 __global__ void k_fd_jacobian(const __grid_constant__ MjbModel m, const __grid_constant__ MjbData p,
-                              int nworld, float eps, int centered, float* A, float* B) {
+                              int nworld, float eps, int flags, float* A, float* B) {
   const int lane = threadIdx.x & 31;
   const long long t = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  const int ncol = fd_ncol(m);
+  const int ncol = fd_ncol(m, flags);
   if (t >= (long long)nworld * ncol) return;
   const int w = int(t / ncol), col = int(t - (long long)w * ncol);
-  fd_column(m, p, w, col, centered, eps, A, B, lane);
+  fd_column(m, p, w, col, flags, eps, A, B, lane);
+}
+// one warp per world; tile_per_warp floats of dynamic shared memory per warp
+__global__ void __launch_bounds__(128, 4) k_ctrl_vjp(const __grid_constant__ MjbModel m, const __grid_constant__ MjbData d,
+                                                     const float* lam, float* grad_ctrl, int tile_per_warp) {
+  extern __shared__ __align__(16) float smem[];
+  const int lane = threadIdx.x & 31;
+  const int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (w >= d.nworld) return;
+  ctrl_vjp_world(m, d, w, lane, lam, grad_ctrl, smem + size_t(threadIdx.x >> 5) * tile_per_warp);
 }
 // one warp per world
 __global__ void k_transition_vjp(const __grid_constant__ MjbModel m, int nworld, const float* A,
@@ -936,28 +946,44 @@ extern "C" int mjb_autotune(const MjbModel* m, const MjbData* d, float* warmstar
 // Finite-difference transition Jacobians (mjb_deriv.cuh).
 
 extern "C" int mjb_fd_perturb(const MjbModel* m, const MjbData* base, const MjbData* pert,
-                              float eps, int centered, mjbStream stream) {
+                              float eps, int flags, mjbStream stream) {
   int rc = check(m, base);
   if (rc || base->nworld == 0) return rc;
-  if (!pert || !(eps > 0.f)) return MJB_ERR_ARG;
-  if ((long long)pert->nworld != (long long)base->nworld * fd_slots(*m, centered)) return MJB_ERR_ARG;
+  if (!pert || !(eps > 0.f) || (flags & ~3)) return MJB_ERR_ARG;
+  if ((long long)pert->nworld != (long long)base->nworld * fd_slots(*m, flags)) return MJB_ERR_ARG;
   if (!pert->qpos || !pert->qvel || !base->qpos || !base->qvel) return MJB_ERR_ARG;
   if ((m->na && (!pert->act || !base->act)) || (m->nu && (!pert->ctrl || !base->ctrl)))
     return MJB_ERR_ARG;
   k_fd_perturb<<<grid_for(pert->nworld, 4), 128, 0, (cudaStream_t)stream>>>(*m, *base, *pert, eps,
-                                                                            centered);
+                                                                            flags);
   return finish();
 }
 
 extern "C" int mjb_fd_jacobian(const MjbModel* m, const MjbData* pert, int nworld, float eps,
-                               int centered, float* A, float* B, mjbStream stream) {
+                               int flags, float* A, float* B, mjbStream stream) {
   int rc = check(m, pert);
   if (rc || nworld == 0) return rc;
-  if (nworld < 0 || !A || (m->nu && !B) || !(eps > 0.f)) return MJB_ERR_ARG;
-  if ((long long)pert->nworld != (long long)nworld * fd_slots(*m, centered)) return MJB_ERR_ARG;
-  const long long warps = (long long)nworld * fd_ncol(*m);
+  const bool need_b = m->nu && !(flags & kFdStateOnly);
+  if (nworld < 0 || !A || (need_b && !B) || !(eps > 0.f) || (flags & ~3)) return MJB_ERR_ARG;
+  if ((long long)pert->nworld != (long long)nworld * fd_slots(*m, flags)) return MJB_ERR_ARG;
+  const long long warps = (long long)nworld * fd_ncol(*m, flags);
   k_fd_jacobian<<<int((warps + 3) / 4), 128, 0, (cudaStream_t)stream>>>(*m, *pert, nworld, eps,
-                                                                       centered, A, B);
+                                                                       flags, A, B);
+  return finish();
+}
+
+extern "C" int mjb_ctrl_vjp(const MjbModel* m, const MjbData* d, const float* lam, float* grad_ctrl,
+                            mjbStream stream) {
+  int rc = check(m, d);
+  if (rc || d->nworld == 0) return rc;
+  if (!lam || !grad_ctrl) return MJB_ERR_ARG;
+  const bool act_on = !(m->disableflags & DSBL_ACTUATION) && m->actuator_affine_bias_gain;
+  if (m->nv > 32 || m->is_sparse || m->na > 0 || (m->integrator != 0 && act_on))
+    return MJB_ERR_UNSUPPORTED;
+  if (!d->qLD_integration || !d->actuator_moment) return MJB_ERR_ARG;
+  const int tpw = tile_floats(m->nv) + 64;
+  k_ctrl_vjp<<<grid_for(d->nworld, 4), 128, size_t(tpw) * 4 * sizeof(float), (cudaStream_t)stream>>>(
+      *m, *d, lam, grad_ctrl, tpw);
   return finish();
 }
 

@@ -15,13 +15,18 @@
 // copied unperturbed.
 #pragma once
 
-#include "mjb_collide.cuh"
+#include "mjb_solver.cuh"
 
 namespace mjb {
 
-__host__ __device__ __forceinline__ int fd_ncol(const MjbModel& m) { return 2 * m.nv + m.na + m.nu; }
-__host__ __device__ __forceinline__ int fd_slots(const MjbModel& m, int centered) {
-  return 1 + fd_ncol(m) * (centered ? 2 : 1);
+// flags of the finite-difference entry points: bit 0 centered differences, bit 1 state columns
+// only (the nu control columns are left out, e.g. when their derivative is taken analytically)
+constexpr int kFdCentered = 1, kFdStateOnly = 2;
+__host__ __device__ __forceinline__ int fd_ncol(const MjbModel& m, int flags = 0) {
+  return 2 * m.nv + m.na + ((flags & kFdStateOnly) ? 0 : m.nu);
+}
+__host__ __device__ __forceinline__ int fd_slots(const MjbModel& m, int flags) {
+  return 1 + fd_ncol(m, flags) * ((flags & kFdCentered) ? 2 : 1);
 }
 
 // Writes base world w's state into perturbed slot pw and perturbs column col by delta (col < 0:
@@ -66,9 +71,10 @@ __device__ void fd_perturb_world(const MjbModel& m, const MjbData& b, const MjbD
 }
 
 // One column of A or B for base world w from the stepped perturbed batch.
-__device__ void fd_column(const MjbModel& m, const MjbData& p, int w, int col, int centered,
+__device__ void fd_column(const MjbModel& m, const MjbData& p, int w, int col, int flags,
                           float eps, float* A, float* B, int lane) {
-  const int nv = m.nv, na = m.na, nx = 2 * nv + na, K = fd_slots(m, centered);
+  const int centered = flags & kFdCentered;
+  const int nv = m.nv, na = m.na, nx = 2 * nv + na, K = fd_slots(m, flags);
   const int P = w * K + 1 + (centered ? 2 * col : col);
   const int R = centered ? P + 1 : w * K;
   const float scale = 1.f / (centered ? 2.f * eps : eps);
@@ -119,6 +125,130 @@ __device__ void transition_vjp_world(const MjbModel& m, const float* A, const fl
       grad_ctrl[W(w, nu) + j] = s;
     }
   }
+}
+
+// d loss / d ctrl of one step by implicit differentiation at the solver's final active set A
+// (no counterpart in the reference).  With qacc = H^-1 (qfrc_smooth + J_A' D_A aref_A) at the
+// Newton solution (H = M + J_A' D_A J_A), qfrc_constraint = -J_A' D_A (J_A qacc - aref_A), and the
+// integrator's qacc_int = Mt^-1 (qfrc_smooth + qfrc_constraint) (Mt = M - dt qDeriv, qLD_integration
+// its factor; Euler without eulerdamp advances with qacc itself), d qacc_int / d qfrc_smooth is
+// Mt^-1 M H^-1.  Then v' = v + dt qacc_int and q' = q (+) dt v', whose tangent responds to dv' by
+// dt J_r(dt v') on a quaternion's three dofs (J_r the right Jacobian of the rotation exponential)
+// and by dt elsewhere; qfrc_smooth depends on ctrl through moment' (gain * [ctrl inside its range])
+// masked where the joint's actuator force is clamped.  Hence
+//   d loss / d ctrl = dt G' moment mask H^-1 M Mt^-1 (lam_v + dt R' lam_q).
+// d holds the step's intermediates (qM, the final efc rows and active flags, qLD_integration,
+// actuator arrays) and the post-step qvel; lam = (lam_q (nv), lam_v (nv)) of the next state.
+// One warp per world, nv <= 32 (tile: tile_floats(nv) + 64 floats of warp scratch), dense qM,
+// na = 0.
+__device__ void ctrl_vjp_world(const MjbModel& m, const MjbData& d, int w, int lane,
+                               const float* lam, float* grad_ctrl, float* tile) {
+  const int nv = m.nv, nu = m.nu;
+  const float dt = m.timestep;
+  const bool own = lane < nv;
+  const float* lq = lam + W(w, 2 * nv + m.na);
+  const float* lv = lq + nv;
+  const float* qvel = d.qvel + W(w, nv);
+  // y = lam_v + dt R' lam_q
+  float y = 0.f;
+  if (own) {
+    float rl = lq[lane];
+    const int j = m.dof_jntid[lane], t = m.jnt_type[j], r = lane - m.jnt_dofadr[j];
+    if ((t == JNT_FREE && r >= 3) || t == JNT_BALL) {
+      const int b = lane - (t == JNT_FREE ? r - 3 : r);  // first rotational dof of the joint
+      const int k = lane - b;
+      const f3 phi = ld3(qvel + b) * dt;
+      const float th2 = dot(phi, phi), th = sqrtf(th2);
+      float c1, c2;  // (1 - cos th) / th^2, (th - sin th) / th^3
+      if (th < 1e-3f) {
+        c1 = 0.5f - th2 / 24.f;
+        c2 = 1.f / 6.f - th2 / 120.f;
+      } else {
+        c1 = (1.f - cosf(th)) / th2;
+        c2 = (th - sinf(th)) / (th2 * th);
+      }
+      // J_r = I - c1 [phi]x + c2 [phi]x^2; row k of J_r^T = column k of J_r
+      const float p[3] = {phi.x, phi.y, phi.z};
+      float col[3];
+      for (int i = 0; i < 3; i++) {
+        // [phi]x (i, k) = -eps_ikl phi_l ; [phi]x^2 = phi phi^T - |phi|^2 I
+        const float cx = (i == k) ? 0.f : ((i + 1) % 3 == k ? -p[(k + 1) % 3] : p[(i + 1) % 3]);
+        const float cx2 = p[i] * p[k] - (i == k ? th2 : 0.f);
+        col[i] = (i == k ? 1.f : 0.f) - c1 * cx + c2 * cx2;
+      }
+      rl = col[0] * lq[b] + col[1] * lq[b + 1] + col[2] * lq[b + 2];
+    }
+    y = lv[lane] + dt * rl;
+  }
+  // w = M Mt^-1 y (implicitfast, eulerdamp), else y
+  const bool passive_on = !(m.disableflags & DSBL_PASSIVE);
+  const bool mt = m.integrator == 0 ? !(m.disableflags & DSBL_EULERDAMP) : passive_on;
+  float* zv = tile + tile_floats(nv);  // two 32-float vectors after the tile
+  float* wv = zv + 32;
+  if (own) zv[lane] = y;
+  __syncwarp();
+  if (mt) {
+    solve_blocks(m, d.qLD_integration + W(w, nv * nv), zv, zv, lane, tile, false);
+    mul_m_world(d.qM + W(w, nv * nv), nv, wv, zv, lane);
+  } else if (own) {
+    wv[lane] = zv[lane];
+  }
+  __syncwarp();
+  // s = H^-1 w, H assembled at the final active set in the tile
+  const int ld = tile_ld(nv);
+  const float* qM = d.qM + W(w, nv * nv);
+  const int adr = d.world_efcadr[w], n = d.world_nefc[w];
+  for (int r = 0; r < nv; r++)
+    if (lane < 4 * ((nv + 3) >> 2)) tile[r * ld + lane] = lane < nv ? qM[r * nv + lane] : 0.f;
+  __syncwarp();
+  if (own) {
+    float h[32];
+    for (int c = 0; c < nv; c++) h[c] = tile[lane * ld + c];
+    for (int k = 0; k < n; k++) {
+      const int r = adr + k;
+      if (!d.efc_active[r]) continue;
+      const float D = d.efc_D[r];
+      if (D == 0.f) continue;
+      const float* J = d.efc_J + size_t(r) * nv;
+      const float a = D * J[lane];
+      for (int c = 0; c < nv; c++) h[c] += a * J[c];
+    }
+    for (int c = 0; c < nv; c++) tile[lane * ld + c] = h[c];
+  }
+  __syncwarp();
+  chol_tile(tile, ld, nv, lane);
+  const float sv = cho_solve_tile(tile, ld, nv, own ? wv[lane] : 0.f, lane);
+  __syncwarp();
+  if (own) zv[lane] = sv;
+  // mask of the dofs whose actuator force is not clamped
+  const float* moment = d.actuator_moment + W(w, nu * nv);
+  const float* force = d.actuator_force + W(w, nu);
+  if (own) {
+    float f = 0.f;
+    for (int a = 0; a < nu; a++) f += moment[a * nv + lane] * force[a];
+    const int j = m.dof_jntid[lane];
+    const bool clamped = m.jnt_actfrclimited[j] &&
+                         !(f > m.jnt_actfrcrange[2 * j] && f < m.jnt_actfrcrange[2 * j + 1]);
+    if (clamped) zv[lane] = 0.f;
+  }
+  __syncwarp();
+  const float* len = d.actuator_length + W(w, nu);
+  const float* vel = d.actuator_velocity + W(w, nu);
+  const float* ctrl = d.ctrl + W(w, nu);
+  for (int a = lane; a < nu; a += 32) {
+    const float* gp = m.actuator_gainprm + 10 * a;
+    const float gain = gp[0] + gp[1] * len[a] + gp[2] * vel[a];
+    const float c = ctrl[a];
+    const bool clamp = m.actuator_ctrllimited[a] && !(m.disableflags & DSBL_CLAMPCTRL) &&
+                       !(c > m.actuator_ctrlrange[2 * a] && c < m.actuator_ctrlrange[2 * a + 1]);
+    float g = 0.f;
+    if (!clamp) {
+      for (int i = 0; i < nv; i++) g += moment[a * nv + i] * zv[i];
+      g *= dt * gain;
+    }
+    grad_ctrl[W(w, nu) + a] = g;
+  }
+  __syncwarp();
 }
 
 }  // namespace mjb

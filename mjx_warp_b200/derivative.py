@@ -16,7 +16,13 @@ from its checkpoint and applies lam <- A^T lam, dL/du_t = B^T lam (``mjb_transit
 the last step to the first.  qacc_warmstart is part of each step's saved state but is not
 differentiated (it is held fixed in every perturbed slot, as mjd_transitionFD does).
 
-These are finite-difference derivatives, not an analytic adjoint: their cost is ncol (or
+The control part can instead be taken analytically (``ctrl_vjp``, ``mjb_ctrl_vjp``): at the
+Newton solution the step's velocity responds to qfrc_smooth through Mt^-1 M H^-1 (Mt the
+integrator's matrix, H the solver's Hessian at its final active set), so (d x' / d ctrl)^T lam
+needs one assembly and factorisation of H, two solves and a product per world; ``Rollout`` does
+this by default where it applies and differences only the state columns.
+
+The state columns are finite-difference derivatives, not an analytic adjoint: their cost is ncol (or
 2 ncol) extra world-steps per world-step, and across a contact or active-set switch they
 describe the secant of the switch.  They need a step that is (piecewise) smooth in its inputs:
 a Newton solve stopped after 1-3 iterations returns an iterate that jumps when the active set
@@ -56,9 +62,13 @@ class TransitionFD:
   """
 
   def __init__(self, mjm, m: Model, nworld: int, eps: float = 1e-3, centered: bool = True,
-               nconmax: int = 64, njmax: int = 128, fused=True):
+               nconmax: int = 64, njmax: int = 128, fused=True, state_only: bool = False):
     self.m, self.nworld, self.eps, self.centered, self.fused = m, nworld, float(eps), centered, fused
+    self.state_only = state_only
     self.nx, self.ncol = _sizes(m)
+    if state_only:  # the control columns are left to ctrl_vjp
+      self.ncol = self.nx
+    self.flags = (1 if centered else 0) | (2 if state_only else 0)
     self.K = 1 + self.ncol * (2 if centered else 1)
     n = nworld * self.K
     self.pert = make_data(mjm, n, nconmax=nconmax * n, njmax=njmax * n)
@@ -73,12 +83,12 @@ class TransitionFD:
     L = _abi.lib()
     mv = _abi.model_view(self.m)
     rc = L.mjb_fd_perturb(ctypes.byref(mv), ctypes.byref(_abi.data_view(d)),
-                          ctypes.byref(_abi.data_view(self.pert)), self.eps, int(self.centered),
+                          ctypes.byref(_abi.data_view(self.pert)), self.eps, self.flags,
                           _abi.stream())
     _abi.check(rc, "fd_perturb")
     step(self.m, self.pert, fused=self.fused)
     rc = L.mjb_fd_jacobian(ctypes.byref(mv), ctypes.byref(_abi.data_view(self.pert)), self.nworld,
-                           self.eps, int(self.centered), _abi._ptr(self.A), _abi._ptr(self.B),
+                           self.eps, self.flags, _abi._ptr(self.A), _abi._ptr(self.B),
                            _abi.stream())
     _abi.check(rc, "fd_jacobian")
     return self.A, self.B
@@ -96,6 +106,25 @@ def transition_vjp(m: Model, A: torch.Tensor, B: Optional[torch.Tensor], lam: to
                                      _abi._ptr(gu) if gu is not None else None, _abi.stream())
   _abi.check(rc, "transition_vjp")
   return out, gu
+
+
+def ctrl_vjp_supported(m: Model) -> bool:
+  """Whether ctrl_vjp applies to m: dense mass matrix, nv <= 32, no activations, and for
+  implicitfast no velocity-dependent actuator gains or biases."""
+  act_on = not (int(m.opt.disableflags) & (1 << 10)) and bool(m.actuator_affine_bias_gain)
+  return (m.nv <= 32 and not m.opt.is_sparse and m.na == 0
+          and not (int(m.opt.integrator) != 0 and act_on))
+
+
+def ctrl_vjp(m: Model, d: Data, lam: torch.Tensor) -> torch.Tensor:
+  """(d x' / d ctrl)^T lam per world, by implicit differentiation at the solver's final active set
+  (mjb_ctrl_vjp): d must hold the step's results (call right after step); lam is the adjoint of
+  the next state, (nworld, 2 nv) in (qpos tangent, qvel) order."""
+  gu = torch.empty((d.nworld, m.nu), dtype=torch.float32, device=lam.device)
+  rc = _abi.lib().mjb_ctrl_vjp(ctypes.byref(_abi.model_view(m)), ctypes.byref(_abi.data_view(d)),
+                               _abi._ptr(lam.contiguous()), _abi._ptr(gu), _abi.stream())
+  _abi.check(rc, "ctrl_vjp")
+  return gu
 
 
 def _quat_joints(m: Model):
@@ -229,9 +258,15 @@ class _Rollout(torch.autograd.Function):
       for t in reversed(range(t0, t1)):
         _restore(d, states[t - t0])
         d.ctrl.copy_(ctrl[t])
-        A, B = r.fd(d)
-        lam, gu = transition_vjp(m, A, B, lam)
-        grad_ctrl[t] = gu
+        if r.analytic_ctrl:  # state columns by differences, controls by ctrl_vjp
+          A, _ = r.fd(d)
+          step(m, d, fused=r.fused)
+          grad_ctrl[t] = ctrl_vjp(m, d, lam)
+          lam, _ = transition_vjp(m, A, None, lam)
+        else:
+          A, B = r.fd(d)
+          lam, gu = transition_vjp(m, A, B, lam)
+          grad_ctrl[t] = gu
     grad_qpos0 = tangent_grad_to_qpos(m, ctx.qpos0, lam[:, :nv])
     grad_qvel0 = lam[:, nv:2 * nv].clone()
     return grad_qpos0, grad_qvel0, grad_ctrl, None
@@ -243,15 +278,19 @@ class Rollout:
   Calling it returns (qpos_T, qvel_T); gradients flow to qpos0 (per qpos coordinate), qvel0 and
   ctrl through finite-difference transition Jacobians (TransitionFD), with the forward states
   checkpointed every `checkpoint` steps and recomputed segment by segment in the backward pass.
-  Each rollout starts from zero act and qacc_warmstart.
+  Each rollout starts from zero act and qacc_warmstart.  analytic_ctrl (default: whenever
+  ctrl_vjp_supported) takes the control gradient from ctrl_vjp and differences only the state
+  columns (2 nv of 2 nv + nu).
   """
 
   def __init__(self, mjm, m: Model, nworld: int, checkpoint: int = 8, eps: float = 1e-3,
-               centered: bool = True, nconmax: int = 64, njmax: int = 128, fused=True):
+               centered: bool = True, nconmax: int = 64, njmax: int = 128, fused=True,
+               analytic_ctrl: Optional[bool] = None):
     self.m, self.checkpoint, self.fused = m, int(checkpoint), fused
+    self.analytic_ctrl = ctrl_vjp_supported(m) if analytic_ctrl is None else bool(analytic_ctrl)
     self.d = make_data(mjm, nworld, nconmax=nconmax * nworld, njmax=njmax * nworld)
     self.fd = TransitionFD(mjm, m, nworld, eps=eps, centered=centered, nconmax=nconmax,
-                           njmax=njmax, fused=fused)
+                           njmax=njmax, fused=fused, state_only=self.analytic_ctrl)
 
   def __call__(self, qpos0: torch.Tensor, qvel0: torch.Tensor, ctrl: torch.Tensor):
     return _Rollout.apply(qpos0, qvel0, ctrl, self)

@@ -149,9 +149,11 @@ def test_forward_and_centered_differences_agree():
   assert torch.linalg.norm(Bf - Bc) / torch.linalg.norm(Bc) < 2e-2
 
 
-def test_rollout_gradient_vs_fp64_central_fd():
+@pytest.mark.parametrize("analytic_ctrl", [True, False])
+def test_rollout_gradient_vs_fp64_central_fd(analytic_ctrl):
   """d/d(ctrl, qvel0, qpos0) of ||root_pos_T - target||^2 + 1e-3 ||ctrl||^2 over an 8-step
-  rollout (checkpoints every 4 steps) vs central FP64 differences of the oracle's loss."""
+  rollout (checkpoints every 4 steps) vs central FP64 differences of the oracle's loss, with the
+  control gradient from ctrl_vjp or from differences."""
   mjm = humanoid()
   nworld, T = 2, 8
   qpos, qvel, _ = _lifted_humanoid(mjm, nworld, seed=4)
@@ -159,7 +161,7 @@ def test_rollout_gradient_vs_fp64_central_fd():
   ctrl = rng.uniform(-0.4, 0.4, (T, nworld, mjm.nu))
   target = np.array([0.1, -0.1, 2.0])
   m = mjw.put_model(mjm)
-  roll = mjw.derivative.Rollout(mjm, m, nworld, checkpoint=4)
+  roll = mjw.derivative.Rollout(mjm, m, nworld, checkpoint=4, analytic_ctrl=analytic_ctrl)
   q0 = torch.tensor(qpos, dtype=torch.float32, device="cuda", requires_grad=True)
   v0 = torch.tensor(qvel, dtype=torch.float32, device="cuda", requires_grad=True)
   u = torch.tensor(ctrl, dtype=torch.float32, device="cuda", requires_grad=True)
@@ -195,3 +197,34 @@ def test_rollout_gradient_vs_fp64_central_fd():
   scale = max(abs(c[1]) for c in checks)
   for g, f in checks:
     assert abs(g - f) <= 1e-2 * abs(f) + 2e-3 * scale, checks
+
+
+@pytest.mark.parametrize("case", ["lifted", "standing"])
+def test_ctrl_vjp_matches_differences(case):
+  """ctrl_vjp after a step equals B^T lam from centered differences of the same step, in the air
+  and standing on the floor (contacts, the solve run to convergence)."""
+  mjm = humanoid(iterations=30, ls_iterations=30)
+  mjm.opt.tolerance = 1e-10
+  nworld = 16
+  if case == "lifted":
+    qpos, qvel, ctrl = _lifted_humanoid(mjm, nworld, seed=6)
+  else:
+    qpos, qvel, ctrl = humanoid_state(mjm, nworld, seed=6)
+  m = mjw.put_model(mjm)
+  d = device_data(mjm, qpos, qvel, ctrl)
+  if case == "standing":  # settle into contact with a warmstart
+    for _ in range(10):
+      mjw.step(m, d)
+  fd = mjw.derivative.TransitionFD(mjm, m, nworld, eps=1e-3, centered=True)
+  _, B = fd(d)
+  B = B.clone()
+  lam = torch.as_tensor(np.random.default_rng(7).normal(size=(nworld, 2 * mjm.nv)),
+                        dtype=torch.float32, device="cuda")
+  ref = torch.einsum("wij,wi->wj", B, lam)
+  mjw.step(m, d)
+  if case == "standing":
+    assert int(d.nefc.cpu()[0]) > 0
+  got = mjw.derivative.ctrl_vjp(m, d, lam)
+  torch.cuda.synchronize()
+  err = torch.linalg.norm(got - ref, dim=1) / torch.linalg.norm(ref, dim=1)
+  assert float(torch.median(err)) < 1e-3 and float(err.max()) < (5e-3 if case == "lifted" else 5e-2), err
