@@ -191,7 +191,7 @@ def _qacc_error(mjm, m, d, mjw, torch, restore, forms, sample=256):
 
 
 def _grad_rate(mjw, torch, nworld=1024, horizon=32, checkpoint=8, reps=2, centered=True,
-               analytic_ctrl=None):
+               analytic=None):
   """grad-steps/s of a differentiated rollout (see the module docstring).  The Newton solve runs
   to convergence (10 iterations, 10 line-search iterations): the 3-iteration iterate of the
   steps/s workload is discontinuous in its inputs, and differences across those jumps make the
@@ -203,7 +203,7 @@ def _grad_rate(mjw, torch, nworld=1024, horizon=32, checkpoint=8, reps=2, center
   m = mjw.put_model(mjm)
   roll = mjw.derivative.Rollout(mjm, m, nworld, checkpoint=checkpoint, eps=1e-3,
                                 centered=centered, nconmax=48, njmax=80,
-                                analytic_ctrl=analytic_ctrl)
+                                analytic=analytic)
   rng = np.random.default_rng(2)
   ctrl = np.repeat(ctrl0[None], horizon, axis=0) + rng.normal(0.0, 0.05, (horizon, nworld, mjm.nu))
   q0 = torch.tensor(qpos, dtype=torch.float32, device="cuda")
@@ -238,8 +238,11 @@ def _grad_rate(mjw, torch, nworld=1024, horizon=32, checkpoint=8, reps=2, center
                      "wrt": "ctrl (32x21), qpos0, qvel0",
                      "method": (f"GPU finite-difference transition Jacobians ({'centered' if centered else 'forward'}, eps 1e-3, "
                                 f"{roll.fd.K} world-steps per world-step"
-                                + (", state columns only; control gradient by implicit differentiation at the "
-                                   "Newton solution" if roll.analytic_ctrl else "")
+                                + {"qvel_ctrl": ", qpos columns only; velocity and control gradients by implicit "
+                                                "differentiation at the Newton solution",
+                                   "ctrl": ", state columns only; control gradient by implicit differentiation "
+                                           "at the Newton solution",
+                                   "none": ""}[roll.analytic]
                                 + ") + reverse recursion")},
           "solver": "Newton 10 it / ls 10 (converged)",
           "forward_ms": fwd * 1e3, "backward_ms": bwd * 1e3,
@@ -400,9 +403,9 @@ def run_ours(args):
     fwd = _grad_rate(mjw, torch, centered=False)
     grad["forward_differences"] = {k: fwd[k] for k in ("value", "unit", "cost_vs_forward",
                                                        "worlds_with_finite_grads")}
-    allfd = _grad_rate(mjw, torch, analytic_ctrl=False)
-    grad["all_columns_by_differences"] = {k: allfd[k] for k in ("value", "unit", "cost_vs_forward",
-                                                               "worlds_with_finite_grads")}
+    for mode, key in (("ctrl", "state_columns_by_differences"), ("none", "all_columns_by_differences")):
+      other = _grad_rate(mjw, torch, analytic=mode)
+      grad[key] = {k: other[k] for k in ("value", "unit", "cost_vs_forward", "worlds_with_finite_grads")}
 
   launches_per_step = LAUNCHES[args.form]
   total_worlds = nworld * world_size

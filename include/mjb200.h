@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define MJB_ABI_VERSION 2
+#define MJB_ABI_VERSION 3
 
 typedef struct CUstream_st* mjbStream; /* == cudaStream_t */
 
@@ -132,6 +132,9 @@ typedef struct MjbData {
      world_order (nworld) receives the worlds sorted by constraint rows, largest first, and
      work_queue (1) is the persistent solver's next-world counter */
   int32_t *world_order, *work_queue;
+  /* per constraint row (njmax, may be null): the velocity coefficient b of the reference
+     acceleration aref = -k imp pos - b J qvel, kept for the step's velocity adjoint */
+  float* efc_b;
 } MjbData;
 
 /* Launch configuration for the step entry points. */
@@ -220,19 +223,23 @@ int mjb_autotune(const MjbModel* m, const MjbData* d, float* warmstart_scratch, 
  * derivatives); the scheme is MuJoCo's mjd_transitionFD, batched over worlds.  State
  * x = (qpos in the tangent space, qvel, act), nx = 2 nv + na; input u = ctrl.  `pert` is a Data
  * of nworld * K worlds, K = 1 + ncol (forward differences) or 1 + 2 ncol (centered),
- * ncol = nx + nu, or nx with MJB_FD_STATE_ONLY.  mjb_fd_perturb copies every base world's state into its K slots and perturbs
- * one column per slot by eps (tangent-space rotations for quaternions); the caller then steps
- * `pert` (mjb_step); mjb_fd_jacobian differences the next states into A (nworld x nx x nx) and
- * B (nworld x nx x nu), row-major per world: A[w][i][j] = d x'_i / d x_j.  eps > 0; in FP32 a
- * value near 1e-3 balances truncation and rounding. */
+ * ncol = nx + nu (nx with MJB_FD_STATE_ONLY, nv with MJB_FD_QPOS_ONLY).  mjb_fd_perturb copies
+ * every base world's state into its K slots and perturbs one column per slot by eps
+ * (tangent-space rotations for quaternions); the caller then steps `pert` (mjb_step);
+ * mjb_fd_jacobian differences the next states into A (nworld x nx x nx) and B (nworld x nx x nu),
+ * row-major per world: A[w][i][j] = d x'_i / d x_j.  eps > 0; in FP32 a value near 1e-3 balances
+ * truncation and rounding. */
 int mjb_fd_perturb(const MjbModel* m, const MjbData* base, const MjbData* pert, float eps,
                    int flags, mjbStream stream);
 int mjb_fd_jacobian(const MjbModel* m, const MjbData* pert, int nworld, float eps, int flags,
                     float* A, float* B, mjbStream stream);
 /* `flags`: MJB_FD_CENTERED for centered differences; MJB_FD_STATE_ONLY to perturb the state
- * columns only (ncol = nx; B is not written and may be null).  Both calls take the same flags. */
+ * columns only (ncol = nx; B is not written and may be null); MJB_FD_QPOS_ONLY to perturb the
+ * nv qpos columns only (ncol = nv; only A's first nv columns are written).  Both calls take the
+ * same flags. */
 #define MJB_FD_CENTERED 1
 #define MJB_FD_STATE_ONLY 2
+#define MJB_FD_QPOS_ONLY 4
 
 /* d loss / d ctrl of one step by implicit differentiation at the constraint solver's final
  * active set (no counterpart in the reference): grad_ctrl (nworld x nu) = (d x' / d ctrl)^T lam,
@@ -243,6 +250,14 @@ int mjb_fd_jacobian(const MjbModel* m, const MjbData* pert, int nworld, float ep
  * gains or biases (else MJB_ERR_UNSUPPORTED). */
 int mjb_ctrl_vjp(const MjbModel* m, const MjbData* d, const float* lam, float* grad_ctrl,
                  mjbStream stream);
+/* As mjb_ctrl_vjp, and also grad_qvel (nworld x nv) = (d x' / d qvel)^T lam through the identity
+ * in qvel' = qvel + dt qacc_int, the damper, the bias forces (the com_vel / rne recursions run
+ * backwards), the actuator velocity terms and the constraint reference's -b J qvel.  qvel_prev is
+ * the qvel the step started from (d's qvel is the step's result); d needs efc_b.  grad_ctrl may
+ * be null.  With the qpos columns from mjb_fd_* under MJB_FD_QPOS_ONLY this gives the whole
+ * transposed transition Jacobian-vector product. */
+int mjb_qvel_ctrl_vjp(const MjbModel* m, const MjbData* d, const float* qvel_prev,
+                      const float* lam, float* grad_qvel, float* grad_ctrl, mjbStream stream);
 
 /* Reverse step of a rollout adjoint, per world: lam_out = A^T lam, grad_ctrl = B^T lam
  * (B / grad_ctrl may be null); lam and lam_out are nworld x nx and must not alias. */

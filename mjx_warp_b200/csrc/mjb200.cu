@@ -250,14 +250,16 @@ __global__ void k_fd_jacobian(const __grid_constant__ MjbModel m, const __grid_c
   const int w = int(t / ncol), col = int(t - (long long)w * ncol);
   fd_column(m, p, w, col, flags, eps, A, B, lane);
 }
-// one warp per world; tile_per_warp floats of dynamic shared memory per warp
-__global__ void __launch_bounds__(128, 4) k_ctrl_vjp(const __grid_constant__ MjbModel m, const __grid_constant__ MjbData d,
-                                                     const float* lam, float* grad_ctrl, int tile_per_warp) {
+// one warp per world; per_warp floats of dynamic shared memory per warp (step_vjp_floats)
+__global__ void __launch_bounds__(128) k_step_vjp(const __grid_constant__ MjbModel m, const __grid_constant__ MjbData d,
+                                                  const float* lam, const float* qvel_prev,
+                                                  float* grad_ctrl, float* grad_qvel, int per_warp) {
   extern __shared__ __align__(16) float smem[];
   const int lane = threadIdx.x & 31;
   const int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   if (w >= d.nworld) return;
-  ctrl_vjp_world(m, d, w, lane, lam, grad_ctrl, smem + size_t(threadIdx.x >> 5) * tile_per_warp);
+  step_vjp_world(m, d, w, lane, lam, qvel_prev, grad_ctrl, grad_qvel,
+                 smem + size_t(threadIdx.x >> 5) * per_warp);
 }
 // one warp per world
 __global__ void k_transition_vjp(const __grid_constant__ MjbModel m, int nworld, const float* A,
@@ -949,7 +951,7 @@ extern "C" int mjb_fd_perturb(const MjbModel* m, const MjbData* base, const MjbD
                               float eps, int flags, mjbStream stream) {
   int rc = check(m, base);
   if (rc || base->nworld == 0) return rc;
-  if (!pert || !(eps > 0.f) || (flags & ~3)) return MJB_ERR_ARG;
+  if (!pert || !(eps > 0.f) || (flags & ~7)) return MJB_ERR_ARG;
   if ((long long)pert->nworld != (long long)base->nworld * fd_slots(*m, flags)) return MJB_ERR_ARG;
   if (!pert->qpos || !pert->qvel || !base->qpos || !base->qvel) return MJB_ERR_ARG;
   if ((m->na && (!pert->act || !base->act)) || (m->nu && (!pert->ctrl || !base->ctrl)))
@@ -963,8 +965,8 @@ extern "C" int mjb_fd_jacobian(const MjbModel* m, const MjbData* pert, int nworl
                                int flags, float* A, float* B, mjbStream stream) {
   int rc = check(m, pert);
   if (rc || nworld == 0) return rc;
-  const bool need_b = m->nu && !(flags & kFdStateOnly);
-  if (nworld < 0 || !A || (need_b && !B) || !(eps > 0.f) || (flags & ~3)) return MJB_ERR_ARG;
+  const bool need_b = m->nu && !(flags & (kFdStateOnly | kFdQposOnly));
+  if (nworld < 0 || !A || (need_b && !B) || !(eps > 0.f) || (flags & ~7)) return MJB_ERR_ARG;
   if ((long long)pert->nworld != (long long)nworld * fd_slots(*m, flags)) return MJB_ERR_ARG;
   const long long warps = (long long)nworld * fd_ncol(*m, flags);
   k_fd_jacobian<<<int((warps + 3) / 4), 128, 0, (cudaStream_t)stream>>>(*m, *pert, nworld, eps,
@@ -972,19 +974,45 @@ extern "C" int mjb_fd_jacobian(const MjbModel* m, const MjbData* pert, int nworl
   return finish();
 }
 
-extern "C" int mjb_ctrl_vjp(const MjbModel* m, const MjbData* d, const float* lam, float* grad_ctrl,
-                            mjbStream stream) {
+static int launch_step_vjp(const MjbModel* m, const MjbData* d, const float* lam,
+                           const float* qvel_prev, float* grad_ctrl, float* grad_qvel,
+                           mjbStream stream) {
   int rc = check(m, d);
   if (rc || d->nworld == 0) return rc;
-  if (!lam || !grad_ctrl) return MJB_ERR_ARG;
+  if (!lam || (!grad_ctrl && !grad_qvel) || (grad_qvel && !qvel_prev)) return MJB_ERR_ARG;
   const bool act_on = !(m->disableflags & DSBL_ACTUATION) && m->actuator_affine_bias_gain;
   if (m->nv > 32 || m->is_sparse || m->na > 0 || (m->integrator != 0 && act_on))
     return MJB_ERR_UNSUPPORTED;
-  if (!d->qLD_integration || !d->actuator_moment) return MJB_ERR_ARG;
-  const int tpw = tile_floats(m->nv) + 64;
-  k_ctrl_vjp<<<grid_for(d->nworld, 4), 128, size_t(tpw) * 4 * sizeof(float), (cudaStream_t)stream>>>(
-      *m, *d, lam, grad_ctrl, tpw);
+  if (!d->qLD_integration || (m->nu && !d->actuator_moment)) return MJB_ERR_ARG;
+  if (grad_qvel && (!d->efc_b || !d->cvel || !d->cdof_dot || !d->cinert || !d->cdof))
+    return MJB_ERR_ARG;
+  const int per_warp = (step_vjp_floats(*m, grad_qvel != nullptr) + 3) & ~3;
+  const size_t warp_bytes = size_t(per_warp) * sizeof(float);
+  int warps = 4;
+  while (warps > 1 && warps * warp_bytes > 48 * 1024) warps >>= 1;
+  const size_t bytes = warps * warp_bytes;
+  if (bytes > 227 * 1024) return MJB_ERR_SCRATCH;
+  if (bytes > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(k_step_vjp, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         int(bytes));
+    if (e != cudaSuccess) return MJB_ERR_LAUNCH;
+  }
+  k_step_vjp<<<grid_for(d->nworld, warps), 32 * warps, bytes, (cudaStream_t)stream>>>(
+      *m, *d, lam, qvel_prev, grad_ctrl, grad_qvel, per_warp);
   return finish();
+}
+
+extern "C" int mjb_ctrl_vjp(const MjbModel* m, const MjbData* d, const float* lam, float* grad_ctrl,
+                            mjbStream stream) {
+  if (!grad_ctrl) return MJB_ERR_ARG;
+  return launch_step_vjp(m, d, lam, nullptr, grad_ctrl, nullptr, stream);
+}
+
+extern "C" int mjb_qvel_ctrl_vjp(const MjbModel* m, const MjbData* d, const float* qvel_prev,
+                                 const float* lam, float* grad_qvel, float* grad_ctrl,
+                                 mjbStream stream) {
+  if (!grad_qvel) return MJB_ERR_ARG;
+  return launch_step_vjp(m, d, lam, qvel_prev, grad_ctrl, grad_qvel, stream);
 }
 
 extern "C" int mjb_transition_vjp(const MjbModel* m, int nworld, const float* A, const float* B,

@@ -20,9 +20,11 @@
 namespace mjb {
 
 // flags of the finite-difference entry points: bit 0 centered differences, bit 1 state columns
-// only (the nu control columns are left out, e.g. when their derivative is taken analytically)
-constexpr int kFdCentered = 1, kFdStateOnly = 2;
+// only (the nu control columns are left out, e.g. when their derivative is taken analytically),
+// bit 2 the nv qpos columns only (velocities and controls by step_vjp_world)
+constexpr int kFdCentered = 1, kFdStateOnly = 2, kFdQposOnly = 4;
 __host__ __device__ __forceinline__ int fd_ncol(const MjbModel& m, int flags = 0) {
+  if (flags & kFdQposOnly) return m.nv;
   return 2 * m.nv + m.na + ((flags & kFdStateOnly) ? 0 : m.nu);
 }
 __host__ __device__ __forceinline__ int fd_slots(const MjbModel& m, int flags) {
@@ -127,22 +129,113 @@ __device__ void transition_vjp_world(const MjbModel& m, const float* A, const fl
   }
 }
 
-// d loss / d ctrl of one step by implicit differentiation at the solver's final active set A
-// (no counterpart in the reference).  With qacc = H^-1 (qfrc_smooth + J_A' D_A aref_A) at the
-// Newton solution (H = M + J_A' D_A J_A), qfrc_constraint = -J_A' D_A (J_A qacc - aref_A), and the
-// integrator's qacc_int = Mt^-1 (qfrc_smooth + qfrc_constraint) (Mt = M - dt qDeriv, qLD_integration
-// its factor; Euler without eulerdamp advances with qacc itself), d qacc_int / d qfrc_smooth is
-// Mt^-1 M H^-1.  Then v' = v + dt qacc_int and q' = q (+) dt v', whose tangent responds to dv' by
-// dt J_r(dt v') on a quaternion's three dofs (J_r the right Jacobian of the rotation exponential)
-// and by dt elsewhere; qfrc_smooth depends on ctrl through moment' (gain * [ctrl inside its range])
-// masked where the joint's actuator force is clamped.  Hence
-//   d loss / d ctrl = dt G' moment mask H^-1 M Mt^-1 (lam_v + dt R' lam_q).
-// d holds the step's intermediates (qM, the final efc rows and active flags, qLD_integration,
-// actuator arrays) and the post-step qvel; lam = (lam_q (nv), lam_v (nv)) of the next state.
-// One warp per world, nv <= 32 (tile: tile_floats(nv) + 64 floats of warp scratch), dense qM,
-// na = 0.
-__device__ void ctrl_vjp_world(const MjbModel& m, const MjbData& d, int w, int lane,
-                               const float* lam, float* grad_ctrl, float* tile) {
+// Shared-memory floats per warp of step_vjp_world: the Hessian tile, three 32-float vectors and,
+// for the velocity adjoint, three spatial vectors per body.
+__host__ __device__ __forceinline__ int step_vjp_floats(const MjbModel& m, bool vel) {
+  return tile_floats(m.nv) + 96 + (vel ? 18 * m.nbody : 0);
+}
+
+// Reverse sweep of the bias forces' velocity dependence (smooth.py:539-606 com_vel and
+// smooth.py:398-466 rne run backwards): rq_i = d (s . qfrc_bias) / d qvel_i, for s (nv, shared).
+// With u_b = sum of s_i cdof_i over the dofs from the root to body b, s . qfrc_bias =
+// sum_b u_b . cfrc_b, cfrc_b = I_b cacc_b + cvel_b x* (I_b cvel_b).  The adjoint of cacc_b is
+// G_b = sum over b's subtree of I_c u_c; cvel_b gets I_b (u_b x cvel_b) - u_b x* (I_b cvel_b)
+// directly, and the adjoint of the velocity entering each dof's cdof_dot = v x cdof gets
+// qvel_i cdof_i x* G_b.  Walking every body's joints backwards (the order com_vel adds them in),
+// rq_i = G_b . cdof_dot_i + cdof_i . (adjoint of the body velocity after dof i's joint).
+__device__ void rne_vel_vjp(const MjbModel& m, const MjbData& d, int w, int lane, const float* s,
+                            const float* qvel, float* rq, float* U, float* G, float* R) {
+  const int nb = m.nbody, nv = m.nv;
+  const float* cdof = d.cdof + W(w, 6 * nv);
+  const float* cdd = d.cdof_dot + W(w, 6 * nv);
+  const float* cvel = d.cvel + W(w, 6 * nb);
+  const float* cinert = d.cinert + W(w, 10 * nb);
+  if (lane < 6) U[lane] = G[lane] = R[lane] = 0.f;
+  __syncwarp();
+  for (int lvl = 1; lvl < m.nlevel; lvl++) {
+    const int beg = m.body_treeadr[lvl], end = m.body_treeadr[lvl + 1];
+    for (int n = beg + lane; n < end; n += 32) {
+      const int b = m.body_tree[n];
+      s6 u = ld6(U + 6 * m.body_parentid[b]);
+      const int da = m.body_dofadr[b];
+      for (int i = 0; i < m.body_dofnum[b]; i++) {
+        const s6 c = ld6(cdof + 6 * (da + i));
+        for (int k = 0; k < 6; k++) u.v[k] += c.v[k] * s[da + i];
+      }
+      st6(U + 6 * b, u);
+      const s6 v = ld6(cvel + 6 * b);
+      st6(G + 6 * b, inert_vec(cinert + 10 * b, u));
+      const s6 a = inert_vec(cinert + 10 * b, motion_cross(u, v));
+      const s6 c = motion_cross_force(u, inert_vec(cinert + 10 * b, v));
+      s6 r;
+      for (int k = 0; k < 6; k++) r.v[k] = a.v[k] - c.v[k];
+      st6(R + 6 * b, r);
+    }
+    __syncwarp();
+  }
+  for (int lvl = m.nlevel - 1; lvl >= 1; lvl--) {
+    const int beg = m.body_treeadr[lvl], end = m.body_treeadr[lvl + 1];
+    for (int n = beg + lane; n < end; n += 32) {
+      const int b = m.body_tree[n];
+      s6 g = ld6(G + 6 * b), r = ld6(R + 6 * b);
+      const int ca = m.body_childadr[b], cn = m.body_childnum[b];
+      for (int c = 0; c < cn; c++) {
+        const int ch = m.body_child[ca + c];
+        const s6 x = ld6(G + 6 * ch), y = ld6(R + 6 * ch);
+        for (int k = 0; k < 6; k++) {
+          g.v[k] += x.v[k];
+          r.v[k] += y.v[k];
+        }
+      }
+      st6(G + 6 * b, g);
+      // joints of b in reverse; r is the adjoint of the body velocity after the joint
+      const int j0 = m.body_jntadr[b];
+      int dof_end = m.body_dofadr[b] + m.body_dofnum[b];
+      for (int j = j0 + m.body_jntnum[b] - 1; j >= j0; j--) {
+        const int t = m.jnt_type[j];
+        const int nd = t == JNT_FREE ? 6 : (t == JNT_BALL ? 3 : 1);
+        const int dof = dof_end - nd;
+        const int rot = t == JNT_FREE ? 3 : 0;  // a free joint's cdof_dot uses v after its translation
+        s6 acc{{0, 0, 0, 0, 0, 0}};
+        for (int i = dof + rot; i < dof_end; i++) {
+          const s6 c = ld6(cdof + 6 * i);
+          rq[i] = dot6(g, ld6(cdd + 6 * i)) + dot6(c, r);
+          const s6 x = motion_cross_force(c, g);
+          for (int k = 0; k < 6; k++) acc.v[k] += qvel[i] * x.v[k];
+        }
+        for (int k = 0; k < 6; k++) r.v[k] += acc.v[k];
+        for (int i = dof; i < dof + rot; i++) rq[i] = dot6(g, ld6(cdd + 6 * i)) + dot6(ld6(cdof + 6 * i), r);
+        dof_end = dof;
+      }
+      st6(R + 6 * b, r);  // now the adjoint of the parent's velocity, summed by the parent
+    }
+    __syncwarp();
+  }
+}
+
+// VJP of one step by implicit differentiation at the solver's final active set A (no counterpart
+// in the reference).  With qacc = H^-1 (qfrc_smooth + J_A' D_A aref_A) at the Newton solution
+// (H = M + J_A' D_A J_A), qfrc_constraint = -J_A' D_A (J_A qacc - aref_A), and the integrator's
+// qacc_int = Mt^-1 (qfrc_smooth + qfrc_constraint) (Mt = M - dt qDeriv, qLD_integration its
+// factor; Euler without eulerdamp advances with qacc itself), d qacc_int / d qfrc_smooth and
+// d qacc_int / d (J_A' D_A aref_A) are Mt^-1 M H^-1.  Then v' = v + dt qacc_int and
+// q' = q (+) dt v', whose tangent responds to dv' by dt J_r(dt v') on a quaternion's three dofs
+// (J_r the right Jacobian of the rotation exponential) and by dt elsewhere.  With
+//   y = lam_v + dt J_r' lam_q,   s = H^-1 M Mt^-1 y:
+// controls enter qfrc_smooth through moment' (gain * [ctrl inside its range]), masked (mask) where
+// the joint's actuator force is clamped:  d loss / d ctrl = dt G' moment mask s;
+// velocities enter through the identity in v', the damper -damping v, the bias forces (rne), the
+// actuator velocity terms (force += (gainprm[2] ctrl + biasprm[2]) moment v) and
+// aref = -k imp pos - b J v:
+//   d loss / d qvel = y + dt (-damping s - d(s . qfrc_bias)/dv + moment' K moment mask s
+//                             - J_A' D_A b_A J_A s).
+// d holds the step's intermediates (qM, the final efc rows, active flags and b, qLD_integration,
+// actuator and com_vel / rne arrays) and the post-step qvel; qvel_prev is the pre-step qvel;
+// lam = (lam_q (nv), lam_v (nv)) of the next state.  grad_qvel may be null (controls only).
+// One warp per world, nv <= 32 (scratch: step_vjp_floats), dense qM, na = 0.
+__device__ void step_vjp_world(const MjbModel& m, const MjbData& d, int w, int lane,
+                               const float* lam, const float* qvel_prev, float* grad_ctrl,
+                               float* grad_qvel, float* tile) {
   const int nv = m.nv, nu = m.nu;
   const float dt = m.timestep;
   const bool own = lane < nv;
@@ -183,8 +276,9 @@ __device__ void ctrl_vjp_world(const MjbModel& m, const MjbData& d, int w, int l
   // w = M Mt^-1 y (implicitfast, eulerdamp), else y
   const bool passive_on = !(m.disableflags & DSBL_PASSIVE);
   const bool mt = m.integrator == 0 ? !(m.disableflags & DSBL_EULERDAMP) : passive_on;
-  float* zv = tile + tile_floats(nv);  // two 32-float vectors after the tile
+  float* zv = tile + tile_floats(nv);  // three 32-float vectors after the tile
   float* wv = zv + 32;
+  float* xv = wv + 32;
   if (own) zv[lane] = y;
   __syncwarp();
   if (mt) {
@@ -220,10 +314,35 @@ __device__ void ctrl_vjp_world(const MjbModel& m, const MjbData& d, int w, int l
   const float sv = cho_solve_tile(tile, ld, nv, own ? wv[lane] : 0.f, lane);
   __syncwarp();
   if (own) zv[lane] = sv;
+  __syncwarp();
+  float gv = 0.f;  // dt^-1 (d loss / d qvel - y), lane = dof
+  if (grad_qvel) {
+    float* body = xv + 32;
+    rne_vel_vjp(m, d, w, lane, zv, qvel_prev + W(w, nv), wv, body, body + 6 * m.nbody,
+                body + 12 * m.nbody);
+    if (own) gv = -wv[lane] - (passive_on ? m.dof_damping[lane] * sv : 0.f);
+    // -J_A' D_A b_A J_A s over the rows, 32 at a time
+    for (int k0 = 0; k0 < n; k0 += 32) {
+      float coef = 0.f;
+      const int r = adr + k0 + lane;
+      if (k0 + lane < n && d.efc_active[r] && d.efc_D[r] != 0.f) {
+        const float* J = d.efc_J + size_t(r) * nv;
+        float js = 0.f;
+        for (int c = 0; c < nv; c++) js += J[c] * zv[c];
+        coef = d.efc_D[r] * d.efc_b[r] * js;
+      }
+      const int cnt = min(32, n - k0);
+      for (int k = 0; k < cnt; k++) {
+        const float ck = __shfl_sync(0xffffffffu, coef, k);
+        if (ck != 0.f && own) gv -= ck * d.efc_J[size_t(adr + k0 + k) * nv + lane];
+      }
+    }
+  }
   // mask of the dofs whose actuator force is not clamped
+  const bool act = nu > 0 && !(m.disableflags & DSBL_ACTUATION);
   const float* moment = d.actuator_moment + W(w, nu * nv);
   const float* force = d.actuator_force + W(w, nu);
-  if (own) {
+  if (own && act) {
     float f = 0.f;
     for (int a = 0; a < nu; a++) f += moment[a * nv + lane] * force[a];
     const int j = m.dof_jntid[lane];
@@ -235,19 +354,35 @@ __device__ void ctrl_vjp_world(const MjbModel& m, const MjbData& d, int w, int l
   const float* len = d.actuator_length + W(w, nu);
   const float* vel = d.actuator_velocity + W(w, nu);
   const float* ctrl = d.ctrl + W(w, nu);
-  for (int a = lane; a < nu; a += 32) {
-    const float* gp = m.actuator_gainprm + 10 * a;
-    const float gain = gp[0] + gp[1] * len[a] + gp[2] * vel[a];
-    const float c = ctrl[a];
-    const bool clamp = m.actuator_ctrllimited[a] && !(m.disableflags & DSBL_CLAMPCTRL) &&
-                       !(c > m.actuator_ctrlrange[2 * a] && c < m.actuator_ctrlrange[2 * a + 1]);
-    float g = 0.f;
-    if (!clamp) {
-      for (int i = 0; i < nv; i++) g += moment[a * nv + i] * zv[i];
-      g *= dt * gain;
+  for (int a0 = 0; a0 < nu; a0 += 32) {
+    const int a = a0 + lane;
+    float kappa_ms = 0.f;  // (gainprm[2] ctrl + biasprm[2]) moment_a . mask s
+    if (a < nu) {
+      float g = 0.f;
+      if (act) {
+        const float* gp = m.actuator_gainprm + 10 * a;
+        const float gain = gp[0] + gp[1] * len[a] + gp[2] * vel[a];
+        float c = ctrl[a];
+        const bool limited = m.actuator_ctrllimited[a] && !(m.disableflags & DSBL_CLAMPCTRL);
+        const bool clamp = limited && !(c > m.actuator_ctrlrange[2 * a] &&
+                                        c < m.actuator_ctrlrange[2 * a + 1]);
+        if (limited) c = fminf(fmaxf(c, m.actuator_ctrlrange[2 * a]), m.actuator_ctrlrange[2 * a + 1]);
+        float ms = 0.f;
+        for (int i = 0; i < nv; i++) ms += moment[a * nv + i] * zv[i];
+        if (!clamp) g = dt * gain * ms;
+        kappa_ms = (gp[2] * c + m.actuator_biasprm[10 * a + 2]) * ms;
+      }
+      if (grad_ctrl) grad_ctrl[W(w, nu) + a] = g;
     }
-    grad_ctrl[W(w, nu) + a] = g;
+    if (grad_qvel) {
+      const int cnt = min(32, nu - a0);
+      for (int k = 0; k < cnt; k++) {
+        const float ck = __shfl_sync(0xffffffffu, kappa_ms, k);
+        if (ck != 0.f && own) gv += ck * moment[(a0 + k) * nv + lane];
+      }
+    }
   }
+  if (grad_qvel && own) grad_qvel[W(w, nv) + lane] = y + dt * gv;
   __syncwarp();
 }
 

@@ -16,13 +16,15 @@ from its checkpoint and applies lam <- A^T lam, dL/du_t = B^T lam (``mjb_transit
 the last step to the first.  qacc_warmstart is part of each step's saved state but is not
 differentiated (it is held fixed in every perturbed slot, as mjd_transitionFD does).
 
-The control part can instead be taken analytically (``ctrl_vjp``, ``mjb_ctrl_vjp``): at the
-Newton solution the step's velocity responds to qfrc_smooth through Mt^-1 M H^-1 (Mt the
-integrator's matrix, H the solver's Hessian at its final active set), so (d x' / d ctrl)^T lam
-needs one assembly and factorisation of H, two solves and a product per world; ``Rollout`` does
-this by default where it applies and differences only the state columns.
+The velocity and control parts can instead be taken analytically (``qvel_ctrl_vjp``,
+``mjb_qvel_ctrl_vjp``; ``ctrl_vjp`` for the controls alone): at the Newton solution the step's
+velocity responds to qfrc_smooth and to the constraint reference through Mt^-1 M H^-1 (Mt the
+integrator's matrix, H the solver's Hessian at its final active set), so both products need one
+assembly and factorisation of H, two solves, a product and a reverse sweep of the bias-force
+recursion per world; ``Rollout`` does this by default where it applies and differences only the
+nv qpos columns.
 
-The state columns are finite-difference derivatives, not an analytic adjoint: their cost is ncol (or
+The qpos columns are finite-difference derivatives, not an analytic adjoint: their cost is ncol (or
 2 ncol) extra world-steps per world-step, and across a contact or active-set switch they
 describe the secant of the switch.  They need a step that is (piecewise) smooth in its inputs:
 a Newton solve stopped after 1-3 iterations returns an iterate that jumps when the active set
@@ -62,13 +64,16 @@ class TransitionFD:
   """
 
   def __init__(self, mjm, m: Model, nworld: int, eps: float = 1e-3, centered: bool = True,
-               nconmax: int = 64, njmax: int = 128, fused=True, state_only: bool = False):
+               nconmax: int = 64, njmax: int = 128, fused=True, state_only: bool = False,
+               qpos_only: bool = False):
     self.m, self.nworld, self.eps, self.centered, self.fused = m, nworld, float(eps), centered, fused
-    self.state_only = state_only
+    self.state_only, self.qpos_only = state_only, qpos_only
     self.nx, self.ncol = _sizes(m)
-    if state_only:  # the control columns are left to ctrl_vjp
+    if qpos_only:  # velocity and control columns are left to qvel_ctrl_vjp (A's other columns stay 0)
+      self.ncol = m.nv
+    elif state_only:  # the control columns are left to ctrl_vjp
       self.ncol = self.nx
-    self.flags = (1 if centered else 0) | (2 if state_only else 0)
+    self.flags = (1 if centered else 0) | (2 if state_only else 0) | (4 if qpos_only else 0)
     self.K = 1 + self.ncol * (2 if centered else 1)
     n = nworld * self.K
     self.pert = make_data(mjm, n, nconmax=nconmax * n, njmax=njmax * n)
@@ -125,6 +130,21 @@ def ctrl_vjp(m: Model, d: Data, lam: torch.Tensor) -> torch.Tensor:
                                _abi._ptr(lam.contiguous()), _abi._ptr(gu), _abi.stream())
   _abi.check(rc, "ctrl_vjp")
   return gu
+
+
+def qvel_ctrl_vjp(m: Model, d: Data, qvel_prev: torch.Tensor, lam: torch.Tensor
+                  ) -> Tuple[torch.Tensor, torch.Tensor]:
+  """((d x' / d qvel)^T lam, (d x' / d ctrl)^T lam) per world at the solver's final active set
+  (mjb_qvel_ctrl_vjp): d holds the step's results, qvel_prev (nworld, nv) the velocities the step
+  started from.  Same applicability as ctrl_vjp."""
+  gv = torch.empty((d.nworld, m.nv), dtype=torch.float32, device=lam.device)
+  gu = torch.empty((d.nworld, m.nu), dtype=torch.float32, device=lam.device)
+  rc = _abi.lib().mjb_qvel_ctrl_vjp(ctypes.byref(_abi.model_view(m)),
+                                    ctypes.byref(_abi.data_view(d)),
+                                    _abi._ptr(qvel_prev.contiguous()), _abi._ptr(lam.contiguous()),
+                                    _abi._ptr(gv), _abi._ptr(gu) if m.nu else None, _abi.stream())
+  _abi.check(rc, "qvel_ctrl_vjp")
+  return gv, gu
 
 
 def _quat_joints(m: Model):
@@ -258,7 +278,14 @@ class _Rollout(torch.autograd.Function):
       for t in reversed(range(t0, t1)):
         _restore(d, states[t - t0])
         d.ctrl.copy_(ctrl[t])
-        if r.analytic_ctrl:  # state columns by differences, controls by ctrl_vjp
+        if r.analytic == "qvel_ctrl":  # qpos columns by differences, the rest analytic
+          A, _ = r.fd(d)
+          qvel_prev = d.qvel.clone()
+          step(m, d, fused=r.fused)
+          gv, grad_ctrl[t] = qvel_ctrl_vjp(m, d, qvel_prev, lam)
+          lam_q, _ = transition_vjp(m, A, None, lam)
+          lam = torch.cat([lam_q[:, :nv], gv], 1)
+        elif r.analytic == "ctrl":  # state columns by differences, controls by ctrl_vjp
           A, _ = r.fd(d)
           step(m, d, fused=r.fused)
           grad_ctrl[t] = ctrl_vjp(m, d, lam)
@@ -278,19 +305,29 @@ class Rollout:
   Calling it returns (qpos_T, qvel_T); gradients flow to qpos0 (per qpos coordinate), qvel0 and
   ctrl through finite-difference transition Jacobians (TransitionFD), with the forward states
   checkpointed every `checkpoint` steps and recomputed segment by segment in the backward pass.
-  Each rollout starts from zero act and qacc_warmstart.  analytic_ctrl (default: whenever
-  ctrl_vjp_supported) takes the control gradient from ctrl_vjp and differences only the state
-  columns (2 nv of 2 nv + nu).
+  Each rollout starts from zero act and qacc_warmstart.  `analytic` picks which columns of the
+  transition Jacobian are not differenced: "qvel_ctrl" (the default where ctrl_vjp_supported)
+  takes the velocity and control parts from qvel_ctrl_vjp and differences the nv qpos columns,
+  "ctrl" differences the 2 nv state columns and takes the controls from ctrl_vjp, "none"
+  differences all 2 nv + na + nu columns.
   """
 
   def __init__(self, mjm, m: Model, nworld: int, checkpoint: int = 8, eps: float = 1e-3,
                centered: bool = True, nconmax: int = 64, njmax: int = 128, fused=True,
-               analytic_ctrl: Optional[bool] = None):
+               analytic: Optional[str] = None):
     self.m, self.checkpoint, self.fused = m, int(checkpoint), fused
-    self.analytic_ctrl = ctrl_vjp_supported(m) if analytic_ctrl is None else bool(analytic_ctrl)
+    if analytic is None:
+      analytic = "qvel_ctrl" if ctrl_vjp_supported(m) else "none"
+    if analytic not in ("qvel_ctrl", "ctrl", "none"):
+      raise ValueError(f"analytic must be 'qvel_ctrl', 'ctrl' or 'none', got {analytic!r}")
+    if analytic != "none" and not ctrl_vjp_supported(m):
+      raise NotImplementedError("analytic step VJP: needs a dense mass matrix, nv <= 32, na == 0 "
+                                "and, for implicitfast, no affine actuator gains or biases")
+    self.analytic = analytic
     self.d = make_data(mjm, nworld, nconmax=nconmax * nworld, njmax=njmax * nworld)
     self.fd = TransitionFD(mjm, m, nworld, eps=eps, centered=centered, nconmax=nconmax,
-                           njmax=njmax, fused=fused, state_only=self.analytic_ctrl)
+                           njmax=njmax, fused=fused, state_only=analytic == "ctrl",
+                           qpos_only=analytic == "qvel_ctrl")
 
   def __call__(self, qpos0: torch.Tensor, qvel0: torch.Tensor, ctrl: torch.Tensor):
     return _Rollout.apply(qpos0, qvel0, ctrl, self)

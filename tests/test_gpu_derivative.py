@@ -149,11 +149,11 @@ def test_forward_and_centered_differences_agree():
   assert torch.linalg.norm(Bf - Bc) / torch.linalg.norm(Bc) < 2e-2
 
 
-@pytest.mark.parametrize("analytic_ctrl", [True, False])
-def test_rollout_gradient_vs_fp64_central_fd(analytic_ctrl):
+@pytest.mark.parametrize("analytic", ["qvel_ctrl", "ctrl", "none"])
+def test_rollout_gradient_vs_fp64_central_fd(analytic):
   """d/d(ctrl, qvel0, qpos0) of ||root_pos_T - target||^2 + 1e-3 ||ctrl||^2 over an 8-step
   rollout (checkpoints every 4 steps) vs central FP64 differences of the oracle's loss, with the
-  control gradient from ctrl_vjp or from differences."""
+  velocity and control columns analytic, only the controls analytic, or all by differences."""
   mjm = humanoid()
   nworld, T = 2, 8
   qpos, qvel, _ = _lifted_humanoid(mjm, nworld, seed=4)
@@ -161,7 +161,7 @@ def test_rollout_gradient_vs_fp64_central_fd(analytic_ctrl):
   ctrl = rng.uniform(-0.4, 0.4, (T, nworld, mjm.nu))
   target = np.array([0.1, -0.1, 2.0])
   m = mjw.put_model(mjm)
-  roll = mjw.derivative.Rollout(mjm, m, nworld, checkpoint=4, analytic_ctrl=analytic_ctrl)
+  roll = mjw.derivative.Rollout(mjm, m, nworld, checkpoint=4, analytic=analytic)
   q0 = torch.tensor(qpos, dtype=torch.float32, device="cuda", requires_grad=True)
   v0 = torch.tensor(qvel, dtype=torch.float32, device="cuda", requires_grad=True)
   u = torch.tensor(ctrl, dtype=torch.float32, device="cuda", requires_grad=True)
@@ -228,3 +228,88 @@ def test_ctrl_vjp_matches_differences(case):
   torch.cuda.synchronize()
   err = torch.linalg.norm(got - ref, dim=1) / torch.linalg.norm(ref, dim=1)
   assert float(torch.median(err)) < 1e-3 and float(err.max()) < (5e-3 if case == "lifted" else 5e-2), err
+
+
+# ball, slide and hinge joints in a chain, a free sphere, dampers and motors; no contacts within
+# the tested steps (nv = 11)
+_JOINTS_XML = """
+<mujoco>
+  <option timestep="0.004" iterations="30" ls_iterations="30"/>
+  <worldbody>
+    <geom type="plane" size="2 2 0.1"/>
+    <body pos="0 0 1.2">
+      <joint name="ball" type="ball" damping="0.1"/>
+      <geom type="capsule" fromto="0 0 0 0.05 0 -0.3" size="0.03"/>
+      <body pos="0.05 0 -0.3">
+        <joint name="slide" type="slide" axis="0 0.3 1" damping="0.2"/>
+        <geom type="sphere" size="0.05"/>
+        <body pos="0 0 -0.1">
+          <joint name="hinge" type="hinge" axis="0 1 0.2" damping="0.05"/>
+          <geom type="capsule" fromto="0 0 0 0.2 0.02 0" size="0.02"/>
+        </body>
+      </body>
+    </body>
+    <body pos="1 0 0.8">
+      <freejoint/>
+      <geom type="sphere" size="0.1"/>
+    </body>
+  </worldbody>
+  <actuator>
+    <motor joint="slide" gear="2"/>
+    <motor joint="hinge" gear="0.5"/>
+  </actuator>
+</mujoco>
+"""
+
+
+def _vjp_case(case, nworld):
+  """(mjm, qpos, qvel, ctrl, settle steps) for the analytic VJP tests, the solve converged."""
+  if case in ("lifted", "standing"):
+    mjm = humanoid(iterations=30, ls_iterations=30)
+    fn = _lifted_humanoid if case == "lifted" else humanoid_state
+    qpos, qvel, ctrl = fn(mjm, nworld, seed=6)
+    settle = 10 if case == "standing" else 0
+  else:
+    mjm = load(_JOINTS_XML if case == "joints" else case)
+    mjm.opt.iterations, mjm.opt.ls_iterations = 30, 30
+    qpos, qvel, ctrl = generic_state(mjm, nworld, seed=6, qscale=0.05, vscale=0.5)
+    qpos = _mid_range(mjm, qpos)
+    settle = 5
+  mjm.opt.tolerance = 1e-10
+  return mjm, qpos, qvel, ctrl, settle
+
+
+@pytest.mark.parametrize("case", ["lifted", "standing", "sphere_chain.xml", "joints"])
+def test_qvel_ctrl_vjp_matches_differences(case):
+  """qvel_ctrl_vjp after a step equals (A_v^T lam, B^T lam) from central FP64 differences of the
+  oracle's step at the same state (A_v the velocity columns of A): the humanoid in the air and
+  standing on the floor (implicitfast, contacts and limits), the sphere + chain (Euler with
+  eulerdamp, damping, a resting contact), a ball / slide / hinge chain with a free body.
+  ctrl_vjp gives the same control gradient."""
+  nworld = 8
+  mjm, qpos, qvel, ctrl, settle = _vjp_case(case, nworld)
+  m = mjw.put_model(mjm)
+  d = device_data(mjm, qpos, qvel, ctrl)
+  for _ in range(settle):
+    mjw.step(m, d)
+  nv = mjm.nv
+  q64, v64 = (t.cpu().numpy().astype(np.float64) for t in (d.qpos, d.qvel))
+  A, B = _oracle_fd(mjm, q64, v64, ctrl.astype(np.float32).astype(np.float64))
+  lam_np = np.random.default_rng(7).normal(size=(nworld, 2 * nv))
+  ref_v = np.einsum("wij,wi->wj", A[:, :, nv:], lam_np)
+  ref_u = np.einsum("wij,wi->wj", B, lam_np)
+  lam = torch.as_tensor(lam_np, dtype=torch.float32, device="cuda")
+  qvel_prev = d.qvel.clone()
+  mjw.step(m, d)
+  gv, gu = mjw.derivative.qvel_ctrl_vjp(m, d, qvel_prev, lam)
+  gu2 = mjw.derivative.ctrl_vjp(m, d, lam)
+  torch.cuda.synchronize()
+  if case == "standing":
+    assert int(d.nefc.cpu()[0]) > 0
+  assert torch.equal(gu, gu2)
+  gv, gu = gv.cpu().numpy(), gu.cpu().numpy()
+  ev = np.linalg.norm(gv - ref_v, axis=1) / np.linalg.norm(ref_v, axis=1)
+  eu = np.linalg.norm(gu - ref_u, axis=1) / np.linalg.norm(ref_u, axis=1)
+  print(case, "qvel", np.median(ev), ev.max(), "ctrl", np.median(eu), eu.max())
+  # measured on a B200: max 1.5e-6 (lifted), 3.5e-5 (standing), 2.5e-5 (sphere chain), 1.1e-6
+  assert ev.max() < 5e-4 and eu.max() < 5e-4, (ev, eu)
