@@ -231,12 +231,14 @@ def _grad_rate(mjw, torch, nworld=1024, horizon=32, checkpoint=8, reps=2, center
     f, b, ok, gmax = once()
     fwd, bwd = fwd + f / reps, bwd + b / reps
   t = fwd + bwd
-  flags = mjw.world_status(roll.fd.pert)
+  flags = mjw.world_status(roll.fd.pert) if roll.fd is not None else np.zeros(1, np.uint32)
   q = np.quantile(gmax.cpu().numpy(), [0.5, 0.99]) if gmax.numel() else [None, None]
   return {"value": nworld * horizon / t, "unit": "grad-steps/s",
           "config": {"nworld": nworld, "horizon": horizon, "checkpoint": checkpoint,
                      "wrt": "ctrl (32x21), qpos0, qvel0",
-                     "method": (f"GPU finite-difference transition Jacobians ({'centered' if centered else 'forward'}, eps 1e-3, "
+                     "method": ("analytic adjoint of the step (implicit differentiation at the Newton "
+                                "solution, mjb_step_vjp), no finite differences" if roll.fd is None else
+                                f"GPU finite-difference transition Jacobians ({'centered' if centered else 'forward'}, eps 1e-3, "
                                 f"{roll.fd.K} world-steps per world-step"
                                 + {"qvel_ctrl": ", qpos columns only; velocity and control gradients by implicit "
                                                 "differentiation at the Newton solution",
@@ -400,12 +402,11 @@ def run_ours(args):
   grad = None
   if rank == 0 and not args.no_grad:
     grad = _grad_rate(mjw, torch)
-    fwd = _grad_rate(mjw, torch, centered=False)
-    grad["forward_differences"] = {k: fwd[k] for k in ("value", "unit", "cost_vs_forward",
-                                                       "worlds_with_finite_grads")}
-    for mode, key in (("ctrl", "state_columns_by_differences"), ("none", "all_columns_by_differences")):
+    for mode, key in (("qvel_ctrl", "qpos_columns_by_differences"),
+                      ("none", "all_columns_by_differences")):
       other = _grad_rate(mjw, torch, analytic=mode)
       grad[key] = {k: other[k] for k in ("value", "unit", "cost_vs_forward", "worlds_with_finite_grads")}
+      grad[key]["method"] = other["config"]["method"]
 
   launches_per_step = LAUNCHES[args.form]
   total_worlds = nworld * world_size

@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define MJB_ABI_VERSION 3
+#define MJB_ABI_VERSION 4
 
 typedef struct CUstream_st* mjbStream; /* == cudaStream_t */
 
@@ -132,9 +132,6 @@ typedef struct MjbData {
      world_order (nworld) receives the worlds sorted by constraint rows, largest first, and
      work_queue (1) is the persistent solver's next-world counter */
   int32_t *world_order, *work_queue;
-  /* per constraint row (njmax, may be null): the velocity coefficient b of the reference
-     acceleration aref = -k imp pos - b J qvel, kept for the step's velocity adjoint */
-  float* efc_b;
 } MjbData;
 
 /* Launch configuration for the step entry points. */
@@ -241,23 +238,23 @@ int mjb_fd_jacobian(const MjbModel* m, const MjbData* pert, int nworld, float ep
 #define MJB_FD_STATE_ONLY 2
 #define MJB_FD_QPOS_ONLY 4
 
-/* d loss / d ctrl of one step by implicit differentiation at the constraint solver's final
- * active set (no counterpart in the reference): grad_ctrl (nworld x nu) = (d x' / d ctrl)^T lam,
- * lam (nworld x nx) the adjoint of the step's next state (qpos tangent, qvel).  d must hold that
- * step's results (call it right after mjb_step): its qM, constraint rows and active flags,
- * qLD_integration, actuator arrays and the new qvel.  Exact at a converged Newton solution; with
- * the dense mass matrix, nv <= 32, na = 0 and, for implicitfast, no velocity-dependent actuator
- * gains or biases (else MJB_ERR_UNSUPPORTED). */
+/* Adjoint of one step by implicit differentiation at the constraint solver's final active set
+ * (no counterpart in the reference): for lam (nworld x nx) the adjoint of the step's next state
+ * (qpos tangent, qvel), writes grad_qpos (nworld x nv, qpos tangent: free / ball rotations about
+ * local axes) = (d x' / d qpos)^T lam, grad_qvel (nworld x nv) and grad_ctrl (nworld x nu); any
+ * of the three may be null.  d must hold that step's results (call it right after mjb_step): its
+ * qM, constraint rows and active flags, contacts, qLD_integration, qacc_integration, kinematics,
+ * com / rne and actuator arrays and the new qvel; qvel_prev is the qvel the step started from
+ * (not needed for grad_ctrl alone).  Exact at a converged Newton solution (the active set and the
+ * contacts held fixed).  Needs the dense mass matrix, nv <= 32 and na = 0, and for implicitfast no
+ * affine actuator gains or biases (else MJB_ERR_UNSUPPORTED); grad_qpos further assumes: ball
+ * joints alone on their body, no stiffness on free / ball joints, actuators on hinge / slide
+ * joints, planes on bodies welded to the world, zero xfrc_applied. */
+int mjb_step_vjp(const MjbModel* m, const MjbData* d, const float* qvel_prev, const float* lam,
+                 float* grad_qpos, float* grad_qvel, float* grad_ctrl, mjbStream stream);
+/* mjb_step_vjp for grad_ctrl alone */
 int mjb_ctrl_vjp(const MjbModel* m, const MjbData* d, const float* lam, float* grad_ctrl,
                  mjbStream stream);
-/* As mjb_ctrl_vjp, and also grad_qvel (nworld x nv) = (d x' / d qvel)^T lam through the identity
- * in qvel' = qvel + dt qacc_int, the damper, the bias forces (the com_vel / rne recursions run
- * backwards), the actuator velocity terms and the constraint reference's -b J qvel.  qvel_prev is
- * the qvel the step started from (d's qvel is the step's result); d needs efc_b.  grad_ctrl may
- * be null.  With the qpos columns from mjb_fd_* under MJB_FD_QPOS_ONLY this gives the whole
- * transposed transition Jacobian-vector product. */
-int mjb_qvel_ctrl_vjp(const MjbModel* m, const MjbData* d, const float* qvel_prev,
-                      const float* lam, float* grad_qvel, float* grad_ctrl, mjbStream stream);
 
 /* Reverse step of a rollout adjoint, per world: lam_out = A^T lam, grad_ctrl = B^T lam
  * (B / grad_ctrl may be null); lam and lam_out are nworld x nx and must not alias. */

@@ -98,7 +98,6 @@ DATA_PTRS = (
   ("world_efcadr", "world_efcadr"), ("world_nefc", "world_nefc"),
   ("world_status", "world_status"),
   ("world_order", "world_order"), ("work_queue", "work_queue"),
-  ("efc_b", "efc.b"),
 )
 
 
@@ -168,13 +167,13 @@ def lib() -> ctypes.CDLL:
   L.mjb_fd_jacobian.argtypes = [pm, pd, ci, cf, ci, vp, vp, vp]
   L.mjb_ctrl_vjp.restype = ctypes.c_int
   L.mjb_ctrl_vjp.argtypes = [pm, pd, vp, vp, vp]
-  L.mjb_qvel_ctrl_vjp.restype = ctypes.c_int
-  L.mjb_qvel_ctrl_vjp.argtypes = [pm, pd, vp, vp, vp, vp, vp]
+  L.mjb_step_vjp.restype = ctypes.c_int
+  L.mjb_step_vjp.argtypes = [pm, pd, vp, vp, vp, vp, vp, vp]
   L.mjb_autotune.restype = ctypes.c_int
   L.mjb_autotune.argtypes = [pm, pd, vp, ctypes.POINTER(MjbTune), vp]
   L.mjb_transition_vjp.restype = ctypes.c_int
   L.mjb_transition_vjp.argtypes = [pm, ci, vp, vp, vp, vp, vp, vp]
-  if L.mjb_abi_version() != 3:
+  if L.mjb_abi_version() != 4:
     raise RuntimeError("libmjb200.so ABI version mismatch")
   _lib = L
   return L

@@ -253,12 +253,13 @@ __global__ void k_fd_jacobian(const __grid_constant__ MjbModel m, const __grid_c
 // one warp per world; per_warp floats of dynamic shared memory per warp (step_vjp_floats)
 __global__ void __launch_bounds__(128) k_step_vjp(const __grid_constant__ MjbModel m, const __grid_constant__ MjbData d,
                                                   const float* lam, const float* qvel_prev,
-                                                  float* grad_ctrl, float* grad_qvel, int per_warp) {
+                                                  float* grad_ctrl, float* grad_qvel,
+                                                  float* grad_qpos, int per_warp) {
   extern __shared__ __align__(16) float smem[];
   const int lane = threadIdx.x & 31;
   const int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   if (w >= d.nworld) return;
-  step_vjp_world(m, d, w, lane, lam, qvel_prev, grad_ctrl, grad_qvel,
+  step_vjp_world(m, d, w, lane, lam, qvel_prev, grad_ctrl, grad_qvel, grad_qpos,
                  smem + size_t(threadIdx.x >> 5) * per_warp);
 }
 // one warp per world
@@ -976,17 +977,20 @@ extern "C" int mjb_fd_jacobian(const MjbModel* m, const MjbData* pert, int nworl
 
 static int launch_step_vjp(const MjbModel* m, const MjbData* d, const float* lam,
                            const float* qvel_prev, float* grad_ctrl, float* grad_qvel,
-                           mjbStream stream) {
+                           float* grad_qpos, mjbStream stream) {
   int rc = check(m, d);
   if (rc || d->nworld == 0) return rc;
-  if (!lam || (!grad_ctrl && !grad_qvel) || (grad_qvel && !qvel_prev)) return MJB_ERR_ARG;
+  const bool sweep = grad_qvel || grad_qpos;
+  if (!lam || (!grad_ctrl && !sweep) || (sweep && !qvel_prev)) return MJB_ERR_ARG;
   const bool act_on = !(m->disableflags & DSBL_ACTUATION) && m->actuator_affine_bias_gain;
   if (m->nv > 32 || m->is_sparse || m->na > 0 || (m->integrator != 0 && act_on))
     return MJB_ERR_UNSUPPORTED;
   if (!d->qLD_integration || (m->nu && !d->actuator_moment)) return MJB_ERR_ARG;
-  if (grad_qvel && (!d->efc_b || !d->cvel || !d->cdof_dot || !d->cinert || !d->cdof))
+  if (sweep && (!d->cvel || !d->cdof_dot || !d->cinert || !d->cdof)) return MJB_ERR_ARG;
+  if (grad_qpos && (!d->rne_cacc || !d->rne_cfrc || !d->xanchor || !d->xaxis || !d->xipos ||
+                    !d->ximat || !d->subtree_com || !d->qacc_integration))
     return MJB_ERR_ARG;
-  const int per_warp = (step_vjp_floats(*m, grad_qvel != nullptr) + 3) & ~3;
+  const int per_warp = (step_vjp_floats(*m, grad_qvel != nullptr, grad_qpos != nullptr) + 3) & ~3;
   const size_t warp_bytes = size_t(per_warp) * sizeof(float);
   int warps = 4;
   while (warps > 1 && warps * warp_bytes > 48 * 1024) warps >>= 1;
@@ -998,21 +1002,20 @@ static int launch_step_vjp(const MjbModel* m, const MjbData* d, const float* lam
     if (e != cudaSuccess) return MJB_ERR_LAUNCH;
   }
   k_step_vjp<<<grid_for(d->nworld, warps), 32 * warps, bytes, (cudaStream_t)stream>>>(
-      *m, *d, lam, qvel_prev, grad_ctrl, grad_qvel, per_warp);
+      *m, *d, lam, qvel_prev, grad_ctrl, grad_qvel, grad_qpos, per_warp);
   return finish();
 }
 
 extern "C" int mjb_ctrl_vjp(const MjbModel* m, const MjbData* d, const float* lam, float* grad_ctrl,
                             mjbStream stream) {
   if (!grad_ctrl) return MJB_ERR_ARG;
-  return launch_step_vjp(m, d, lam, nullptr, grad_ctrl, nullptr, stream);
+  return launch_step_vjp(m, d, lam, nullptr, grad_ctrl, nullptr, nullptr, stream);
 }
 
-extern "C" int mjb_qvel_ctrl_vjp(const MjbModel* m, const MjbData* d, const float* qvel_prev,
-                                 const float* lam, float* grad_qvel, float* grad_ctrl,
-                                 mjbStream stream) {
-  if (!grad_qvel) return MJB_ERR_ARG;
-  return launch_step_vjp(m, d, lam, qvel_prev, grad_ctrl, grad_qvel, stream);
+extern "C" int mjb_step_vjp(const MjbModel* m, const MjbData* d, const float* qvel_prev,
+                            const float* lam, float* grad_qpos, float* grad_qvel, float* grad_ctrl,
+                            mjbStream stream) {
+  return launch_step_vjp(m, d, lam, qvel_prev, grad_ctrl, grad_qvel, grad_qpos, stream);
 }
 
 extern "C" int mjb_transition_vjp(const MjbModel* m, int nworld, const float* A, const float* B,

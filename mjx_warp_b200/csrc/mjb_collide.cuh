@@ -521,7 +521,6 @@ __device__ void update_efc_row(const MjbModel& m, const MjbData& d, int r, float
   }
   d.efc_D[r] = 1.f / fmaxf(invweight * (1.f - imp) / imp, kMinVal);
   d.efc_aref[r] = -k * imp * pos_aref - b * Jqvel;
-  if (d.efc_b) d.efc_b[r] = b;
   d.efc_pos[r] = pos_aref + margin;
   d.efc_margin[r] = margin;
 }

@@ -15,7 +15,7 @@
 // copied unperturbed.
 #pragma once
 
-#include "mjb_solver.cuh"
+#include "mjb_adjoint.cuh"
 
 namespace mjb {
 
@@ -129,10 +129,15 @@ __device__ void transition_vjp_world(const MjbModel& m, const float* A, const fl
   }
 }
 
-// Shared-memory floats per warp of step_vjp_world: the Hessian tile, three 32-float vectors and,
-// for the velocity adjoint, three spatial vectors per body.
-__host__ __device__ __forceinline__ int step_vjp_floats(const MjbModel& m, bool vel) {
-  return tile_floats(m.nv) + 96 + (vel ? 18 * m.nbody : 0);
+// Shared-memory floats per warp of step_vjp_world: the Hessian tile, seven 32-float vectors and,
+// for the velocity or position adjoint, four spatial vectors per body; for the position adjoint
+// also the cdof bars (6 per dof), body force / torque / cinert / subtree_com bars (19 per body)
+// and the joints' anchor / axis / subtree_com bars (9 per joint).
+__host__ __device__ __forceinline__ int step_vjp_floats(const MjbModel& m, bool vel, bool pos) {
+  int n = tile_floats(m.nv) + 7 * 32;
+  if (vel || pos) n += 24 * m.nbody;
+  if (pos) n += 6 * m.nv + 19 * m.nbody + 9 * m.njnt;
+  return n;
 }
 
 // Reverse sweep of the bias forces' velocity dependence (smooth.py:539-606 com_vel and
@@ -217,75 +222,112 @@ __device__ void rne_vel_vjp(const MjbModel& m, const MjbData& d, int w, int lane
 // in the reference).  With qacc = H^-1 (qfrc_smooth + J_A' D_A aref_A) at the Newton solution
 // (H = M + J_A' D_A J_A), qfrc_constraint = -J_A' D_A (J_A qacc - aref_A), and the integrator's
 // qacc_int = Mt^-1 (qfrc_smooth + qfrc_constraint) (Mt = M - dt qDeriv, qLD_integration its
-// factor; Euler without eulerdamp advances with qacc itself), d qacc_int / d qfrc_smooth and
-// d qacc_int / d (J_A' D_A aref_A) are Mt^-1 M H^-1.  Then v' = v + dt qacc_int and
+// factor; Euler without eulerdamp advances with qacc itself), v' = v + dt qacc_int and
 // q' = q (+) dt v', whose tangent responds to dv' by dt J_r(dt v') on a quaternion's three dofs
 // (J_r the right Jacobian of the rotation exponential) and by dt elsewhere.  With
-//   y = lam_v + dt J_r' lam_q,   s = H^-1 M Mt^-1 y:
+//   y = lam_v + dt J_r' lam_q,   z = Mt^-1 y,   s = H^-1 M z   (z = 0, s = H^-1 y without Mt):
 // controls enter qfrc_smooth through moment' (gain * [ctrl inside its range]), masked (mask) where
 // the joint's actuator force is clamped:  d loss / d ctrl = dt G' moment mask s;
 // velocities enter through the identity in v', the damper -damping v, the bias forces (rne), the
 // actuator velocity terms (force += (gainprm[2] ctrl + biasprm[2]) moment v) and
 // aref = -k imp pos - b J v:
 //   d loss / d qvel = y + dt (-damping s - d(s . qfrc_bias)/dv + moment' K moment mask s
-//                             - J_A' D_A b_A J_A s).
-// d holds the step's intermediates (qM, the final efc rows, active flags and b, qLD_integration,
-// actuator and com_vel / rne arrays) and the post-step qvel; qvel_prev is the pre-step qvel;
-// lam = (lam_q (nv), lam_v (nv)) of the next state.  grad_qvel may be null (controls only).
-// One warp per world, nv <= 32 (scratch: step_vjp_floats), dense qM, na = 0.
+//                             - J_A' D_A b_A J_A s);
+// positions enter through q' directly (a quaternion's tangent is carried by R(dt v'), the rotation
+// of the step) and through every position-dependent quantity of the step:
+//   d loss / d qpos = R' lam_q + dt d/dq [z' M (qacc - qacc_int) - s' M qacc + s' qfrc_smooth
+//                                         + sum_A (D t e + D t aref)]
+// with the row terms of row_q_bars (t = J s, e = aref - J qacc, every factor but the
+// differentiated one held fixed).  d holds the step's intermediates (qM, the final efc rows and
+// active flags, contacts, qLD_integration, qacc_integration, kinematics, com / rne arrays,
+// actuator arrays) and the post-step qvel; qvel_prev is the pre-step qvel; lam = (lam_q (nv),
+// lam_v (nv)) of the next state.  Any of grad_qpos / grad_qvel / grad_ctrl may be null.  One warp
+// per world, nv <= 32 (scratch: step_vjp_floats), dense qM, na = 0.
 __device__ void step_vjp_world(const MjbModel& m, const MjbData& d, int w, int lane,
                                const float* lam, const float* qvel_prev, float* grad_ctrl,
-                               float* grad_qvel, float* tile) {
-  const int nv = m.nv, nu = m.nu;
+                               float* grad_qvel, float* grad_qpos, float* tile) {
+  const int nv = m.nv, nu = m.nu, nb = m.nbody;
   const float dt = m.timestep;
   const bool own = lane < nv;
+  const bool velg = grad_qvel != nullptr, posg = grad_qpos != nullptr;
   const float* lq = lam + W(w, 2 * nv + m.na);
   const float* lv = lq + nv;
   const float* qvel = d.qvel + W(w, nv);
-  // y = lam_v + dt R' lam_q
-  float y = 0.f;
+  const float* qv = qvel_prev ? qvel_prev + W(w, nv) : nullptr;
+  float* Y = tile + tile_floats(nv);
+  float* Z = Y + 32;
+  float* S = Z + 32;
+  float* St = S + 32;
+  float* WV = St + 32;
+  float* Q = WV + 32;
+  float* GV = Q + 32;
+  float* SA = GV + 32;
+  float* SB = SA + 6 * nb;
+  float* SC = SB + 6 * nb;
+  float* SD = SC + 6 * nb;
+  float* CB = SD + 6 * nb;
+  float* BF = CB + 6 * nv;
+  float* BT = BF + 3 * nb;
+  float* CIB = BT + 3 * nb;
+  float* SCB = CIB + 10 * nb;
+  float* JA = SCB + 3 * nb;
+  float* JX = JA + 3 * m.njnt;
+  float* JS = JX + 3 * m.njnt;
+  // y = lam_v + dt J_r' lam_q, and for the position part R(dt v') lam_q
+  float y = 0.f, direct = 0.f;
   if (own) {
     float rl = lq[lane];
+    direct = lq[lane];
     const int j = m.dof_jntid[lane], t = m.jnt_type[j], r = lane - m.jnt_dofadr[j];
     if ((t == JNT_FREE && r >= 3) || t == JNT_BALL) {
       const int b = lane - (t == JNT_FREE ? r - 3 : r);  // first rotational dof of the joint
       const int k = lane - b;
       const f3 phi = ld3(qvel + b) * dt;
       const float th2 = dot(phi, phi), th = sqrtf(th2);
-      float c1, c2;  // (1 - cos th) / th^2, (th - sin th) / th^3
+      float c1, c2, sa;  // (1 - cos th) / th^2, (th - sin th) / th^3, sin th / th
       if (th < 1e-3f) {
         c1 = 0.5f - th2 / 24.f;
         c2 = 1.f / 6.f - th2 / 120.f;
+        sa = 1.f - th2 / 6.f;
       } else {
         c1 = (1.f - cosf(th)) / th2;
         c2 = (th - sinf(th)) / (th2 * th);
+        sa = sinf(th) / th;
       }
       // J_r = I - c1 [phi]x + c2 [phi]x^2; row k of J_r^T = column k of J_r
       const float p[3] = {phi.x, phi.y, phi.z};
-      float col[3];
+      float colk[3];
       for (int i = 0; i < 3; i++) {
         // [phi]x (i, k) = -eps_ikl phi_l ; [phi]x^2 = phi phi^T - |phi|^2 I
         const float cx = (i == k) ? 0.f : ((i + 1) % 3 == k ? -p[(k + 1) % 3] : p[(i + 1) % 3]);
         const float cx2 = p[i] * p[k] - (i == k ? th2 : 0.f);
-        col[i] = (i == k ? 1.f : 0.f) - c1 * cx + c2 * cx2;
+        colk[i] = (i == k ? 1.f : 0.f) - c1 * cx + c2 * cx2;
       }
-      rl = col[0] * lq[b] + col[1] * lq[b + 1] + col[2] * lq[b + 2];
+      rl = colk[0] * lq[b] + colk[1] * lq[b + 1] + colk[2] * lq[b + 2];
+      // R(phi) lam = lam + sa phi x lam + c1 phi x (phi x lam), component k
+      const f3 l3 = ld3(lq + b);
+      const f3 a = cross(phi, l3), a2 = cross(phi, a);
+      const f3 rv = l3 + a * sa + a2 * c1;
+      direct = k == 0 ? rv.x : (k == 1 ? rv.y : rv.z);
     }
     y = lv[lane] + dt * rl;
   }
-  // w = M Mt^-1 y (implicitfast, eulerdamp), else y
+  // z = Mt^-1 y and w = M z (implicitfast, eulerdamp), else w = y
   const bool passive_on = !(m.disableflags & DSBL_PASSIVE);
   const bool mt = m.integrator == 0 ? !(m.disableflags & DSBL_EULERDAMP) : passive_on;
-  float* zv = tile + tile_floats(nv);  // three 32-float vectors after the tile
-  float* wv = zv + 32;
-  float* xv = wv + 32;
-  if (own) zv[lane] = y;
+  if (lane < 32) {
+    Y[lane] = own ? y : 0.f;
+    Z[lane] = own ? y : 0.f;
+    Q[lane] = 0.f;
+    GV[lane] = 0.f;
+  }
   __syncwarp();
   if (mt) {
-    solve_blocks(m, d.qLD_integration + W(w, nv * nv), zv, zv, lane, tile, false);
-    mul_m_world(d.qM + W(w, nv * nv), nv, wv, zv, lane);
-  } else if (own) {
-    wv[lane] = zv[lane];
+    solve_blocks(m, d.qLD_integration + W(w, nv * nv), Z, Z, lane, tile, false);
+    mul_m_world(d.qM + W(w, nv * nv), nv, WV, Z, lane);
+  } else {
+    if (own) WV[lane] = y;
+    Z[lane] = 0.f;
   }
   __syncwarp();
   // s = H^-1 w, H assembled at the final active set in the tile
@@ -311,32 +353,17 @@ __device__ void step_vjp_world(const MjbModel& m, const MjbData& d, int w, int l
   }
   __syncwarp();
   chol_tile(tile, ld, nv, lane);
-  const float sv = cho_solve_tile(tile, ld, nv, own ? wv[lane] : 0.f, lane);
+  const float sv = cho_solve_tile(tile, ld, nv, own ? WV[lane] : 0.f, lane);
   __syncwarp();
-  if (own) zv[lane] = sv;
+  S[lane] = own ? sv : 0.f;
+  St[lane] = own ? sv : 0.f;
   __syncwarp();
-  float gv = 0.f;  // dt^-1 (d loss / d qvel - y), lane = dof
-  if (grad_qvel) {
-    float* body = xv + 32;
-    rne_vel_vjp(m, d, w, lane, zv, qvel_prev + W(w, nv), wv, body, body + 6 * m.nbody,
-                body + 12 * m.nbody);
-    if (own) gv = -wv[lane] - (passive_on ? m.dof_damping[lane] * sv : 0.f);
-    // -J_A' D_A b_A J_A s over the rows, 32 at a time
-    for (int k0 = 0; k0 < n; k0 += 32) {
-      float coef = 0.f;
-      const int r = adr + k0 + lane;
-      if (k0 + lane < n && d.efc_active[r] && d.efc_D[r] != 0.f) {
-        const float* J = d.efc_J + size_t(r) * nv;
-        float js = 0.f;
-        for (int c = 0; c < nv; c++) js += J[c] * zv[c];
-        coef = d.efc_D[r] * d.efc_b[r] * js;
-      }
-      const int cnt = min(32, n - k0);
-      for (int k = 0; k < cnt; k++) {
-        const float ck = __shfl_sync(0xffffffffu, coef, k);
-        if (ck != 0.f && own) gv -= ck * d.efc_J[size_t(adr + k0 + k) * nv + lane];
-      }
-    }
+  // velocity: bias forces, damper, rows
+  if (velg) {
+    rne_vel_vjp(m, d, w, lane, S, qv, WV, SA, SB, SC);
+    if (own) GV[lane] = -WV[lane] - (passive_on ? m.dof_damping[lane] * sv : 0.f);
+    __syncwarp();
+    row_q_bars(m, d, w, lane, S, qv, Q, nullptr, nullptr, nullptr, nullptr, GV);
   }
   // mask of the dofs whose actuator force is not clamped
   const bool act = nu > 0 && !(m.disableflags & DSBL_ACTUATION);
@@ -348,19 +375,21 @@ __device__ void step_vjp_world(const MjbModel& m, const MjbData& d, int w, int l
     const int j = m.dof_jntid[lane];
     const bool clamped = m.jnt_actfrclimited[j] &&
                          !(f > m.jnt_actfrcrange[2 * j] && f < m.jnt_actfrcrange[2 * j + 1]);
-    if (clamped) zv[lane] = 0.f;
+    if (clamped) St[lane] = 0.f;
   }
   __syncwarp();
+  // controls, and the actuators' velocity (gv) and length (Q) terms
   const float* len = d.actuator_length + W(w, nu);
   const float* vel = d.actuator_velocity + W(w, nu);
   const float* ctrl = d.ctrl + W(w, nu);
   for (int a0 = 0; a0 < nu; a0 += 32) {
     const int a = a0 + lane;
-    float kappa_ms = 0.f;  // (gainprm[2] ctrl + biasprm[2]) moment_a . mask s
+    float kv = 0.f, kq = 0.f;  // (gainprm[2] ctrl + biasprm[2]), (gainprm[1] ctrl + biasprm[1]) x moment_a . St
     if (a < nu) {
       float g = 0.f;
       if (act) {
         const float* gp = m.actuator_gainprm + 10 * a;
+        const float* bp = m.actuator_biasprm + 10 * a;
         const float gain = gp[0] + gp[1] * len[a] + gp[2] * vel[a];
         float c = ctrl[a];
         const bool limited = m.actuator_ctrllimited[a] && !(m.disableflags & DSBL_CLAMPCTRL);
@@ -368,21 +397,58 @@ __device__ void step_vjp_world(const MjbModel& m, const MjbData& d, int w, int l
                                         c < m.actuator_ctrlrange[2 * a + 1]);
         if (limited) c = fminf(fmaxf(c, m.actuator_ctrlrange[2 * a]), m.actuator_ctrlrange[2 * a + 1]);
         float ms = 0.f;
-        for (int i = 0; i < nv; i++) ms += moment[a * nv + i] * zv[i];
+        for (int i = 0; i < nv; i++) ms += moment[a * nv + i] * St[i];
         if (!clamp) g = dt * gain * ms;
-        kappa_ms = (gp[2] * c + m.actuator_biasprm[10 * a + 2]) * ms;
+        kv = (gp[2] * c + bp[2]) * ms;
+        kq = (gp[1] * c + bp[1]) * ms;
       }
       if (grad_ctrl) grad_ctrl[W(w, nu) + a] = g;
     }
-    if (grad_qvel) {
-      const int cnt = min(32, nu - a0);
-      for (int k = 0; k < cnt; k++) {
-        const float ck = __shfl_sync(0xffffffffu, kappa_ms, k);
-        if (ck != 0.f && own) gv += ck * moment[(a0 + k) * nv + lane];
-      }
+    const int cnt = min(32, nu - a0);
+    for (int k = 0; k < cnt; k++) {
+      const float cv = __shfl_sync(0xffffffffu, kv, k), cq = __shfl_sync(0xffffffffu, kq, k);
+      if (own && cv != 0.f) GV[lane] += cv * moment[(a0 + k) * nv + lane];
+      if (own && cq != 0.f) Q[lane] += cq * moment[(a0 + k) * nv + lane];
     }
   }
-  if (grad_qvel && own) grad_qvel[W(w, nv) + lane] = y + dt * gv;
+  __syncwarp();
+  if (velg && own) grad_qvel[W(w, nv) + lane] = y + dt * GV[lane];
+  if (!posg) {
+    __syncwarp();
+    return;
+  }
+  // position: bars on cdof / cinert / subtree_com / contacts, then the joints
+  for (int e = lane; e < 6 * nv; e += 32) CB[e] = 0.f;
+  for (int e = lane; e < 19 * nb; e += 32) BF[e] = 0.f;  // BF, BT, CIB, SCB are contiguous
+  for (int e = lane; e < 9 * m.njnt; e += 32) JA[e] = 0.f;  // JA, JX, JS
+  __syncwarp();
+  const float* qacc = d.qacc + W(w, nv);
+  if (mt) {
+    const float* aint = d.qacc_integration + W(w, nv);
+    if (lane < 32) WV[lane] = own ? qacc[lane] - aint[lane] : 0.f;
+    __syncwarp();
+    mass_product_bars(m, d, w, lane, Z, WV, CB, CIB, SA, SB, SC, SD);
+  }
+  if (lane < 32) WV[lane] = own ? -S[lane] : 0.f;
+  __syncwarp();
+  mass_product_bars(m, d, w, lane, WV, qacc, CB, CIB, SA, SB, SC, SD);
+  bias_q_bars(m, d, w, lane, WV, qv, CB, CIB, SA, SB, SC);
+  if (passive_on) {  // hinge / slide springs -k (q - q_spring)
+    for (int j = lane; j < m.njnt; j += 32) {
+      const int t = m.jnt_type[j];
+      if ((t == JNT_HINGE || t == JNT_SLIDE) && m.jnt_stiffness[j] != 0.f) {
+        const int dof = m.jnt_dofadr[j];
+        Q[dof] -= m.jnt_stiffness[j] * S[dof];
+      }
+    }
+    __syncwarp();
+  }
+  row_q_bars(m, d, w, lane, S, qv, Q, CB, BF, BT, SCB, nullptr);
+  cdof_joint_bars(m, d, w, lane, CB, JA, JX, JS, BT);
+  cinert_body_bars(m, d, w, lane, CIB, BF, BT, SCB);
+  subtree_com_bars(m, d, w, lane, SCB, JS, BF, BT, SA);
+  kinematic_sweep(m, d, w, lane, JA, JX, BF, BT, Q);
+  if (own) grad_qpos[W(w, nv) + lane] = direct + dt * Q[lane];
   __syncwarp();
 }
 

@@ -132,18 +132,58 @@ def ctrl_vjp(m: Model, d: Data, lam: torch.Tensor) -> torch.Tensor:
   return gu
 
 
+def qpos_vjp_supported(m: Model) -> bool:
+  """Whether step_vjp can give the qpos gradient for m: ctrl_vjp_supported, ball joints alone on
+  their body, no stiffness on free / ball joints, actuators on hinge / slide joints, planes on
+  bodies welded to the world (xfrc_applied is taken to be zero)."""
+  if not ctrl_vjp_supported(m):
+    return False
+  cache = m.__dict__.get("_qpos_vjp_ok")
+  if cache is None:
+    jt = m.jnt_type.cpu().numpy()
+    jb = m.jnt_bodyid.cpu().numpy()
+    nj = m.body_jntnum.cpu().numpy()
+    k = m.jnt_stiffness.cpu().numpy()
+    ok = all(nj[jb[j]] == 1 for j in range(len(jt)) if jt[j] == JNT_BALL)
+    ok &= not any(k[j] != 0 for j in range(len(jt)) if jt[j] in (JNT_FREE, JNT_BALL))
+    if m.nu:
+      tt = m.actuator_trntype.cpu().numpy()
+      tid = m.actuator_trnid.cpu().numpy().reshape(m.nu, -1)[:, 0]
+      ok &= bool(np.all(tt <= 1)) and all(jt[tid[a]] in (2, 3) for a in range(m.nu))
+    gt = m.geom_type.cpu().numpy()
+    gb = m.geom_bodyid.cpu().numpy()
+    wb = m.body_weldid.cpu().numpy()
+    ok &= all(wb[gb[g]] == 0 for g in range(len(gt)) if gt[g] == 0)
+    cache = bool(ok)
+    object.__setattr__(m, "_qpos_vjp_ok", cache)
+  return cache
+
+
+def step_vjp(m: Model, d: Data, qvel_prev: torch.Tensor, lam: torch.Tensor, qpos: bool = True,
+             qvel: bool = True, ctrl: bool = True):
+  """Adjoint of one step at the solver's final active set (mjb_step_vjp): for lam (nworld, 2 nv),
+  the adjoint of the next state in (qpos tangent, qvel) order, returns (grad_qpos, grad_qvel,
+  grad_ctrl) per world, each None unless requested; grad_qpos is in the qpos tangent space.  d
+  holds the step's results (call right after step), qvel_prev (nworld, nv) the velocities the
+  step started from."""
+  if qpos and not qpos_vjp_supported(m):
+    raise NotImplementedError("step_vjp: the qpos adjoint does not cover this model")
+  dev = lam.device
+  gq = torch.empty((d.nworld, m.nv), dtype=torch.float32, device=dev) if qpos else None
+  gv = torch.empty((d.nworld, m.nv), dtype=torch.float32, device=dev) if qvel else None
+  gu = torch.empty((d.nworld, m.nu), dtype=torch.float32, device=dev) if ctrl and m.nu else None
+  P = lambda t: _abi._ptr(t) if t is not None else None
+  rc = _abi.lib().mjb_step_vjp(ctypes.byref(_abi.model_view(m)), ctypes.byref(_abi.data_view(d)),
+                               _abi._ptr(qvel_prev.contiguous()), _abi._ptr(lam.contiguous()),
+                               P(gq), P(gv), P(gu), _abi.stream())
+  _abi.check(rc, "step_vjp")
+  return gq, gv, gu
+
+
 def qvel_ctrl_vjp(m: Model, d: Data, qvel_prev: torch.Tensor, lam: torch.Tensor
                   ) -> Tuple[torch.Tensor, torch.Tensor]:
-  """((d x' / d qvel)^T lam, (d x' / d ctrl)^T lam) per world at the solver's final active set
-  (mjb_qvel_ctrl_vjp): d holds the step's results, qvel_prev (nworld, nv) the velocities the step
-  started from.  Same applicability as ctrl_vjp."""
-  gv = torch.empty((d.nworld, m.nv), dtype=torch.float32, device=lam.device)
-  gu = torch.empty((d.nworld, m.nu), dtype=torch.float32, device=lam.device)
-  rc = _abi.lib().mjb_qvel_ctrl_vjp(ctypes.byref(_abi.model_view(m)),
-                                    ctypes.byref(_abi.data_view(d)),
-                                    _abi._ptr(qvel_prev.contiguous()), _abi._ptr(lam.contiguous()),
-                                    _abi._ptr(gv), _abi._ptr(gu) if m.nu else None, _abi.stream())
-  _abi.check(rc, "qvel_ctrl_vjp")
+  """((d x' / d qvel)^T lam, (d x' / d ctrl)^T lam) per world (step_vjp without the qpos part)."""
+  _, gv, gu = step_vjp(m, d, qvel_prev, lam, qpos=False)
   return gv, gu
 
 
@@ -231,6 +271,10 @@ def _snapshot(d: Data):
   return tuple(getattr(d, k).clone() for k in _STATE)
 
 
+def _snapshot_view(d: Data):
+  return tuple(getattr(d, k) for k in _STATE)
+
+
 def _restore(d: Data, s) -> None:
   for k, v in zip(_STATE, s):
     getattr(d, k).copy_(v)
@@ -269,6 +313,18 @@ class _Rollout(torch.autograd.Function):
     grad_ctrl = torch.zeros_like(ctrl)
     for seg in reversed(range(len(ctx.ckpts))):
       t0, t1 = seg * r.checkpoint, min(T, (seg + 1) * r.checkpoint)
+      if r.analytic == "full":  # one Data per step of the segment: each is stepped once
+        qvel_prev = []
+        for k, t in enumerate(range(t0, t1)):
+          dk = r.seg[k]
+          _restore(dk, ctx.ckpts[seg] if k == 0 else _snapshot_view(r.seg[k - 1]))
+          qvel_prev.append(dk.qvel.clone())
+          dk.ctrl.copy_(ctrl[t])
+          step(m, dk, fused=r.fused)
+        for k in reversed(range(t1 - t0)):
+          gq, gv, grad_ctrl[t0 + k] = step_vjp(m, r.seg[k], qvel_prev[k], lam)
+          lam = torch.cat([gq, gv], 1)
+        continue
       _restore(d, ctx.ckpts[seg])
       states = []
       for t in range(t0, t1):  # recompute the segment's states from its checkpoint
@@ -306,8 +362,9 @@ class Rollout:
   ctrl through finite-difference transition Jacobians (TransitionFD), with the forward states
   checkpointed every `checkpoint` steps and recomputed segment by segment in the backward pass.
   Each rollout starts from zero act and qacc_warmstart.  `analytic` picks which columns of the
-  transition Jacobian are not differenced: "qvel_ctrl" (the default where ctrl_vjp_supported)
-  takes the velocity and control parts from qvel_ctrl_vjp and differences the nv qpos columns,
+  transition Jacobian are not differenced: "full" (the default where qpos_vjp_supported) takes
+  every column from step_vjp, "qvel_ctrl" (the default where only ctrl_vjp_supported) takes the
+  velocity and control parts from step_vjp and differences the nv qpos columns,
   "ctrl" differences the 2 nv state columns and takes the controls from ctrl_vjp, "none"
   differences all 2 nv + na + nu columns.
   """
@@ -317,17 +374,23 @@ class Rollout:
                analytic: Optional[str] = None):
     self.m, self.checkpoint, self.fused = m, int(checkpoint), fused
     if analytic is None:
-      analytic = "qvel_ctrl" if ctrl_vjp_supported(m) else "none"
-    if analytic not in ("qvel_ctrl", "ctrl", "none"):
-      raise ValueError(f"analytic must be 'qvel_ctrl', 'ctrl' or 'none', got {analytic!r}")
+      analytic = ("full" if qpos_vjp_supported(m) else
+                  "qvel_ctrl" if ctrl_vjp_supported(m) else "none")
+    if analytic not in ("full", "qvel_ctrl", "ctrl", "none"):
+      raise ValueError(f"analytic must be 'full', 'qvel_ctrl', 'ctrl' or 'none', got {analytic!r}")
     if analytic != "none" and not ctrl_vjp_supported(m):
       raise NotImplementedError("analytic step VJP: needs a dense mass matrix, nv <= 32, na == 0 "
                                 "and, for implicitfast, no affine actuator gains or biases")
+    if analytic == "full" and not qpos_vjp_supported(m):
+      raise NotImplementedError("analytic qpos adjoint: the model has a feature it does not cover")
     self.analytic = analytic
     self.d = make_data(mjm, nworld, nconmax=nconmax * nworld, njmax=njmax * nworld)
-    self.fd = TransitionFD(mjm, m, nworld, eps=eps, centered=centered, nconmax=nconmax,
-                           njmax=njmax, fused=fused, state_only=analytic == "ctrl",
-                           qpos_only=analytic == "qvel_ctrl")
+    # the backward of the analytic adjoint keeps every step of a segment in its own Data
+    self.seg = [make_data(mjm, nworld, nconmax=nconmax * nworld, njmax=njmax * nworld)
+                for _ in range(self.checkpoint)] if analytic == "full" else []
+    self.fd = None if analytic == "full" else TransitionFD(
+        mjm, m, nworld, eps=eps, centered=centered, nconmax=nconmax, njmax=njmax, fused=fused,
+        state_only=analytic == "ctrl", qpos_only=analytic == "qvel_ctrl")
 
   def __call__(self, qpos0: torch.Tensor, qvel0: torch.Tensor, ctrl: torch.Tensor):
     return _Rollout.apply(qpos0, qvel0, ctrl, self)

@@ -285,7 +285,7 @@ def _data_arrays(mjm, nworld, nconmax, njmax, dev):
   }
   nls = max(int(mjm.opt.ls_iterations), 1)
   efc = {
-    "J": f(njmax, nv), "D": f(njmax), "pos": f(njmax), "aref": f(njmax), "b": f(njmax), "force": f(njmax),
+    "J": f(njmax, nv), "D": f(njmax), "pos": f(njmax), "aref": f(njmax), "force": f(njmax),
     "margin": f(njmax), "worldid": i(njmax), "Jaref": f(njmax), "Ma": f(W, nv), "grad": f(W, nv),
     "grad_dot": f(W), "Mgrad": f(W, nv), "search": f(W, nv), "search_dot": f(W), "gauss": f(W),
     "cost": f(W), "prev_cost": f(W), "solver_niter": i(W), "active": i(njmax), "gtol": f(W),

@@ -149,11 +149,12 @@ def test_forward_and_centered_differences_agree():
   assert torch.linalg.norm(Bf - Bc) / torch.linalg.norm(Bc) < 2e-2
 
 
-@pytest.mark.parametrize("analytic", ["qvel_ctrl", "ctrl", "none"])
+@pytest.mark.parametrize("analytic", ["full", "qvel_ctrl", "ctrl", "none"])
 def test_rollout_gradient_vs_fp64_central_fd(analytic):
   """d/d(ctrl, qvel0, qpos0) of ||root_pos_T - target||^2 + 1e-3 ||ctrl||^2 over an 8-step
   rollout (checkpoints every 4 steps) vs central FP64 differences of the oracle's loss, with the
-  velocity and control columns analytic, only the controls analytic, or all by differences."""
+  step's adjoint fully analytic, only its velocity and control columns analytic, only the
+  controls analytic, or all by differences."""
   mjm = humanoid()
   nworld, T = 2, 8
   qpos, qvel, _ = _lifted_humanoid(mjm, nworld, seed=4)
@@ -280,15 +281,16 @@ def _vjp_case(case, nworld):
 
 
 @pytest.mark.parametrize("case", ["lifted", "standing", "sphere_chain.xml", "joints"])
-def test_qvel_ctrl_vjp_matches_differences(case):
-  """qvel_ctrl_vjp after a step equals (A_v^T lam, B^T lam) from central FP64 differences of the
-  oracle's step at the same state (A_v the velocity columns of A): the humanoid in the air and
-  standing on the floor (implicitfast, contacts and limits), the sphere + chain (Euler with
-  eulerdamp, damping, a resting contact), a ball / slide / hinge chain with a free body.
-  ctrl_vjp gives the same control gradient."""
+def test_step_vjp_matches_differences(case):
+  """step_vjp after a step equals (A_q^T lam, A_v^T lam, B^T lam) from central FP64 differences
+  of the oracle's step at the same state (A_q, A_v the qpos-tangent and velocity columns of A):
+  the humanoid in the air and standing on the floor (implicitfast, contacts and limits), the
+  sphere + chain (Euler with eulerdamp, damping, a resting contact), a ball / slide / hinge chain
+  with a free body.  qvel_ctrl_vjp and ctrl_vjp give the same velocity and control gradients."""
   nworld = 8
   mjm, qpos, qvel, ctrl, settle = _vjp_case(case, nworld)
   m = mjw.put_model(mjm)
+  assert mjw.derivative.qpos_vjp_supported(m)
   d = device_data(mjm, qpos, qvel, ctrl)
   for _ in range(settle):
     mjw.step(m, d)
@@ -296,20 +298,75 @@ def test_qvel_ctrl_vjp_matches_differences(case):
   q64, v64 = (t.cpu().numpy().astype(np.float64) for t in (d.qpos, d.qvel))
   A, B = _oracle_fd(mjm, q64, v64, ctrl.astype(np.float32).astype(np.float64))
   lam_np = np.random.default_rng(7).normal(size=(nworld, 2 * nv))
+  ref_q = np.einsum("wij,wi->wj", A[:, :, :nv], lam_np)
   ref_v = np.einsum("wij,wi->wj", A[:, :, nv:], lam_np)
   ref_u = np.einsum("wij,wi->wj", B, lam_np)
   lam = torch.as_tensor(lam_np, dtype=torch.float32, device="cuda")
   qvel_prev = d.qvel.clone()
   mjw.step(m, d)
-  gv, gu = mjw.derivative.qvel_ctrl_vjp(m, d, qvel_prev, lam)
-  gu2 = mjw.derivative.ctrl_vjp(m, d, lam)
+  gq, gv, gu = mjw.derivative.step_vjp(m, d, qvel_prev, lam)
+  gv2, gu2 = mjw.derivative.qvel_ctrl_vjp(m, d, qvel_prev, lam)
+  gu3 = mjw.derivative.ctrl_vjp(m, d, lam)
   torch.cuda.synchronize()
   if case == "standing":
     assert int(d.nefc.cpu()[0]) > 0
-  assert torch.equal(gu, gu2)
-  gv, gu = gv.cpu().numpy(), gu.cpu().numpy()
-  ev = np.linalg.norm(gv - ref_v, axis=1) / np.linalg.norm(ref_v, axis=1)
-  eu = np.linalg.norm(gu - ref_u, axis=1) / np.linalg.norm(ref_u, axis=1)
-  print(case, "qvel", np.median(ev), ev.max(), "ctrl", np.median(eu), eu.max())
-  # measured on a B200: max 1.5e-6 (lifted), 3.5e-5 (standing), 2.5e-5 (sphere chain), 1.1e-6
+  assert torch.equal(gu, gu2) and torch.equal(gu, gu3) and torch.equal(gv, gv2)
+  gq, gv, gu = gq.cpu().numpy(), gv.cpu().numpy(), gu.cpu().numpy()
+  rel = lambda g, r: np.linalg.norm(g - r, axis=1) / np.linalg.norm(r, axis=1)
+  eq, ev, eu = rel(gq, ref_q), rel(gv, ref_v), rel(gu, ref_u)
+  print(case, "qpos", np.median(eq), eq.max(), "qvel", np.median(ev), ev.max(), "ctrl",
+        np.median(eu), eu.max())
+  # velocity / control measured on a B200: max 1.5e-6 (lifted), 3.5e-5 (standing), 2.5e-5
+  # (sphere chain), 1.1e-6
   assert ev.max() < 5e-4 and eu.max() < 5e-4, (ev, eu)
+  assert eq.max() < 1e-3, eq
+
+
+def test_rollout_gradient_standing_vs_fp64_central_fd():
+  """The analytic rollout gradient with the humanoid standing on the floor (contacts and limits
+  in every step, the solve converged) vs central FP64 differences of the oracle's loss."""
+  mjm = humanoid(iterations=30, ls_iterations=30)
+  mjm.opt.tolerance = 1e-10
+  nworld, T = 2, 8
+  qpos, qvel, _ = humanoid_state(mjm, nworld, seed=4)
+  rng = np.random.default_rng(5)
+  ctrl = rng.uniform(-0.4, 0.4, (T, nworld, mjm.nu))
+  target = np.array([0.1, -0.1, 1.0])
+  m = mjw.put_model(mjm)
+  roll = mjw.derivative.Rollout(mjm, m, nworld, checkpoint=4, analytic="full")
+  q0 = torch.tensor(qpos, dtype=torch.float32, device="cuda", requires_grad=True)
+  v0 = torch.tensor(qvel, dtype=torch.float32, device="cuda", requires_grad=True)
+  u = torch.tensor(ctrl, dtype=torch.float32, device="cuda", requires_grad=True)
+  qT, _ = roll(q0, v0, u)
+  tgt = torch.tensor(target, dtype=torch.float32, device="cuda")
+  loss = ((qT[:, :3] - tgt) ** 2).sum() + 1e-3 * (u ** 2).sum()
+  loss.backward()
+
+  def loss64(qp, qv, cu):
+    o = oracle(mjm, qp, qv, cu[0], 64)
+    for t in range(T):
+      o.set("ctrl", cu[t])
+      o.run("step")
+    return float(((o.get("qpos")[:, :3] - target) ** 2).sum() + 1e-3 * (cu ** 2).sum())
+
+  h = 1e-6
+  checks = []
+  for (t, w, a) in [(0, 0, 3), (3, 1, 10), (7, 0, 20), (5, 1, 0), (1, 0, 15)]:
+    cp, cm = ctrl.copy(), ctrl.copy()
+    cp[t, w, a] += h
+    cm[t, w, a] -= h
+    checks.append((u.grad[t, w, a].item(), (loss64(qpos, qvel, cp) - loss64(qpos, qvel, cm)) / (2 * h)))
+  for (w, i) in [(0, 2), (1, 8), (0, 20)]:
+    vp, vm = qvel.copy(), qvel.copy()
+    vp[w, i] += h
+    vm[w, i] -= h
+    checks.append((v0.grad[w, i].item(), (loss64(qpos, vp, ctrl) - loss64(qpos, vm, ctrl)) / (2 * h)))
+  for (w, i) in [(1, 0), (0, 2), (1, 10), (0, 12)]:  # root x, root z, hinges
+    pp, pm = qpos.copy(), qpos.copy()
+    pp[w, i] += h
+    pm[w, i] -= h
+    checks.append((q0.grad[w, i].item(), (loss64(pp, qvel, ctrl) - loss64(pm, qvel, ctrl)) / (2 * h)))
+  print("standing rollout", checks)
+  scale = max(abs(c[1]) for c in checks)
+  for g, f in checks:
+    assert abs(g - f) <= 1e-2 * abs(f) + 2e-3 * scale, checks
