@@ -246,10 +246,11 @@ int mjb_fd_jacobian(const MjbModel* m, const MjbData* pert, int nworld, float ep
  * qM, constraint rows and active flags, contacts, qLD_integration, qacc_integration, kinematics,
  * com / rne and actuator arrays and the new qvel; qvel_prev is the qvel the step started from
  * (not needed for grad_ctrl alone).  Exact at a converged Newton solution (the active set and the
- * contacts held fixed).  Needs the dense mass matrix, nv <= 32 and na = 0, and for implicitfast no
+ * contacts held fixed).  Needs the dense mass matrix and na = 0, and for implicitfast no
  * affine actuator gains or biases (else MJB_ERR_UNSUPPORTED); grad_qpos further assumes: ball
  * joints alone on their body, no stiffness on free / ball joints, actuators on hinge / slide
- * joints, planes on bodies welded to the world, zero xfrc_applied. */
+ * joints, planes on bodies welded to the world, zero xfrc_applied.  For nv > 32 the Hessian and its
+ * factor are written to d->efc_h. */
 int mjb_step_vjp(const MjbModel* m, const MjbData* d, const float* qvel_prev, const float* lam,
                  float* grad_qpos, float* grad_qvel, float* grad_ctrl, mjbStream stream);
 /* mjb_step_vjp for grad_ctrl alone */

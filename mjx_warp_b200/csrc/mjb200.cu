@@ -983,9 +983,9 @@ static int launch_step_vjp(const MjbModel* m, const MjbData* d, const float* lam
   const bool sweep = grad_qvel || grad_qpos;
   if (!lam || (!grad_ctrl && !sweep) || (sweep && !qvel_prev)) return MJB_ERR_ARG;
   const bool act_on = !(m->disableflags & DSBL_ACTUATION) && m->actuator_affine_bias_gain;
-  if (m->nv > 32 || m->is_sparse || m->na > 0 || (m->integrator != 0 && act_on))
-    return MJB_ERR_UNSUPPORTED;
+  if (m->is_sparse || m->na > 0 || (m->integrator != 0 && act_on)) return MJB_ERR_UNSUPPORTED;
   if (!d->qLD_integration || (m->nu && !d->actuator_moment)) return MJB_ERR_ARG;
+  if (m->nv > 32 && !d->efc_h) return MJB_ERR_ARG;
   if (sweep && (!d->cvel || !d->cdof_dot || !d->cinert || !d->cdof)) return MJB_ERR_ARG;
   if (grad_qpos && (!d->rne_cacc || !d->rne_cfrc || !d->xanchor || !d->xaxis || !d->xipos ||
                     !d->ximat || !d->subtree_com || !d->qacc_integration))

@@ -129,12 +129,14 @@ __device__ void transition_vjp_world(const MjbModel& m, const float* A, const fl
   }
 }
 
-// Shared-memory floats per warp of step_vjp_world: the Hessian tile, seven 32-float vectors and,
+// Shared-memory floats per warp of step_vjp_world: the Hessian tile (nv <= 32) or the sparse-row
+// assembly / blocked-Cholesky scratch (nv > 32), eight vectors of 32 ceil(nv / 32) floats and,
 // for the velocity or position adjoint, four spatial vectors per body; for the position adjoint
 // also the cdof bars (6 per dof), body force / torque / cinert / subtree_com bars (19 per body)
 // and the joints' anchor / axis / subtree_com bars (9 per joint).
+__host__ __device__ __forceinline__ int step_vjp_vec(int nv) { return 32 * ((nv + 31) / 32); }
 __host__ __device__ __forceinline__ int step_vjp_floats(const MjbModel& m, bool vel, bool pos) {
-  int n = tile_floats(m.nv) + 7 * 32;
+  int n = (m.nv <= 32 ? tile_floats(m.nv) : generic_nz_floats(m.nv)) + 8 * step_vjp_vec(m.nv);
   if (vel || pos) n += 24 * m.nbody;
   if (pos) n += 6 * m.nv + 19 * m.nbody + 9 * m.njnt;
   return n;
@@ -242,26 +244,27 @@ __device__ void rne_vel_vjp(const MjbModel& m, const MjbData& d, int w, int lane
 // active flags, contacts, qLD_integration, qacc_integration, kinematics, com / rne arrays,
 // actuator arrays) and the post-step qvel; qvel_prev is the pre-step qvel; lam = (lam_q (nv),
 // lam_v (nv)) of the next state.  Any of grad_qpos / grad_qvel / grad_ctrl may be null.  One warp
-// per world, nv <= 32 (scratch: step_vjp_floats), dense qM, na = 0.
+// per world (scratch: step_vjp_floats; for nv > 32 H and its factor are written to efc_h), dense
+// qM, na = 0.
 __device__ void step_vjp_world(const MjbModel& m, const MjbData& d, int w, int lane,
                                const float* lam, const float* qvel_prev, float* grad_ctrl,
                                float* grad_qvel, float* grad_qpos, float* tile) {
-  const int nv = m.nv, nu = m.nu, nb = m.nbody;
+  const int nv = m.nv, nu = m.nu, nb = m.nbody, VL = step_vjp_vec(nv);
   const float dt = m.timestep;
-  const bool own = lane < nv;
   const bool velg = grad_qvel != nullptr, posg = grad_qpos != nullptr;
   const float* lq = lam + W(w, 2 * nv + m.na);
   const float* lv = lq + nv;
   const float* qvel = d.qvel + W(w, nv);
   const float* qv = qvel_prev ? qvel_prev + W(w, nv) : nullptr;
-  float* Y = tile + tile_floats(nv);
-  float* Z = Y + 32;
-  float* S = Z + 32;
-  float* St = S + 32;
-  float* WV = St + 32;
-  float* Q = WV + 32;
-  float* GV = Q + 32;
-  float* SA = GV + 32;
+  float* Y = tile + (nv <= 32 ? tile_floats(nv) : generic_nz_floats(nv));
+  float* Z = Y + VL;
+  float* S = Z + VL;
+  float* St = S + VL;
+  float* WV = St + VL;
+  float* Q = WV + VL;
+  float* GV = Q + VL;
+  float* DIR = GV + VL;
+  float* SA = DIR + VL;
   float* SB = SA + 6 * nb;
   float* SC = SB + 6 * nb;
   float* SD = SC + 6 * nb;
@@ -274,94 +277,108 @@ __device__ void step_vjp_world(const MjbModel& m, const MjbData& d, int w, int l
   float* JX = JA + 3 * m.njnt;
   float* JS = JX + 3 * m.njnt;
   // y = lam_v + dt J_r' lam_q, and for the position part R(dt v') lam_q
-  float y = 0.f, direct = 0.f;
-  if (own) {
-    float rl = lq[lane];
-    direct = lq[lane];
-    const int j = m.dof_jntid[lane], t = m.jnt_type[j], r = lane - m.jnt_dofadr[j];
-    if ((t == JNT_FREE && r >= 3) || t == JNT_BALL) {
-      const int b = lane - (t == JNT_FREE ? r - 3 : r);  // first rotational dof of the joint
-      const int k = lane - b;
-      const f3 phi = ld3(qvel + b) * dt;
-      const float th2 = dot(phi, phi), th = sqrtf(th2);
-      float c1, c2, sa;  // (1 - cos th) / th^2, (th - sin th) / th^3, sin th / th
-      if (th < 1e-3f) {
-        c1 = 0.5f - th2 / 24.f;
-        c2 = 1.f / 6.f - th2 / 120.f;
-        sa = 1.f - th2 / 6.f;
-      } else {
-        c1 = (1.f - cosf(th)) / th2;
-        c2 = (th - sinf(th)) / (th2 * th);
-        sa = sinf(th) / th;
+  for (int i = lane; i < VL; i += 32) {
+    float y = 0.f, direct = 0.f;
+    if (i < nv) {
+      float rl = lq[i];
+      direct = lq[i];
+      const int j = m.dof_jntid[i], t = m.jnt_type[j], r = i - m.jnt_dofadr[j];
+      if ((t == JNT_FREE && r >= 3) || t == JNT_BALL) {
+        const int b = i - (t == JNT_FREE ? r - 3 : r);  // first rotational dof of the joint
+        const int k = i - b;
+        const f3 phi = ld3(qvel + b) * dt;
+        const float th2 = dot(phi, phi), th = sqrtf(th2);
+        float c1, c2, sa;  // (1 - cos th) / th^2, (th - sin th) / th^3, sin th / th
+        if (th < 1e-3f) {
+          c1 = 0.5f - th2 / 24.f;
+          c2 = 1.f / 6.f - th2 / 120.f;
+          sa = 1.f - th2 / 6.f;
+        } else {
+          c1 = (1.f - cosf(th)) / th2;
+          c2 = (th - sinf(th)) / (th2 * th);
+          sa = sinf(th) / th;
+        }
+        // J_r = I - c1 [phi]x + c2 [phi]x^2; row k of J_r^T = column k of J_r
+        const float p[3] = {phi.x, phi.y, phi.z};
+        float colk[3];
+        for (int e = 0; e < 3; e++) {
+          // [phi]x (e, k) = -eps_ekl phi_l ; [phi]x^2 = phi phi^T - |phi|^2 I
+          const float cx = (e == k) ? 0.f : ((e + 1) % 3 == k ? -p[(k + 1) % 3] : p[(e + 1) % 3]);
+          const float cx2 = p[e] * p[k] - (e == k ? th2 : 0.f);
+          colk[e] = (e == k ? 1.f : 0.f) - c1 * cx + c2 * cx2;
+        }
+        rl = colk[0] * lq[b] + colk[1] * lq[b + 1] + colk[2] * lq[b + 2];
+        // R(phi) lam = lam + sa phi x lam + c1 phi x (phi x lam), component k
+        const f3 l3 = ld3(lq + b);
+        const f3 a = cross(phi, l3), a2 = cross(phi, a);
+        const f3 rv = l3 + a * sa + a2 * c1;
+        direct = k == 0 ? rv.x : (k == 1 ? rv.y : rv.z);
       }
-      // J_r = I - c1 [phi]x + c2 [phi]x^2; row k of J_r^T = column k of J_r
-      const float p[3] = {phi.x, phi.y, phi.z};
-      float colk[3];
-      for (int i = 0; i < 3; i++) {
-        // [phi]x (i, k) = -eps_ikl phi_l ; [phi]x^2 = phi phi^T - |phi|^2 I
-        const float cx = (i == k) ? 0.f : ((i + 1) % 3 == k ? -p[(k + 1) % 3] : p[(i + 1) % 3]);
-        const float cx2 = p[i] * p[k] - (i == k ? th2 : 0.f);
-        colk[i] = (i == k ? 1.f : 0.f) - c1 * cx + c2 * cx2;
-      }
-      rl = colk[0] * lq[b] + colk[1] * lq[b + 1] + colk[2] * lq[b + 2];
-      // R(phi) lam = lam + sa phi x lam + c1 phi x (phi x lam), component k
-      const f3 l3 = ld3(lq + b);
-      const f3 a = cross(phi, l3), a2 = cross(phi, a);
-      const f3 rv = l3 + a * sa + a2 * c1;
-      direct = k == 0 ? rv.x : (k == 1 ? rv.y : rv.z);
+      y = lv[i] + dt * rl;
     }
-    y = lv[lane] + dt * rl;
+    Y[i] = y;
+    Z[i] = y;
+    DIR[i] = direct;
+    Q[i] = 0.f;
+    GV[i] = 0.f;
   }
+  __syncwarp();
   // z = Mt^-1 y and w = M z (implicitfast, eulerdamp), else w = y
   const bool passive_on = !(m.disableflags & DSBL_PASSIVE);
   const bool mt = m.integrator == 0 ? !(m.disableflags & DSBL_EULERDAMP) : passive_on;
-  if (lane < 32) {
-    Y[lane] = own ? y : 0.f;
-    Z[lane] = own ? y : 0.f;
-    Q[lane] = 0.f;
-    GV[lane] = 0.f;
-  }
-  __syncwarp();
   if (mt) {
     solve_blocks(m, d.qLD_integration + W(w, nv * nv), Z, Z, lane, tile, false);
     mul_m_world(d.qM + W(w, nv * nv), nv, WV, Z, lane);
   } else {
-    if (own) WV[lane] = y;
-    Z[lane] = 0.f;
+    for (int i = lane; i < VL; i += 32) {
+      WV[i] = Y[i];
+      Z[i] = 0.f;
+    }
   }
   __syncwarp();
-  // s = H^-1 w, H assembled at the final active set in the tile
-  const int ld = tile_ld(nv);
+  // s = H^-1 w with H assembled at the final active set: in the tile (nv <= 32) or in efc_h
   const float* qM = d.qM + W(w, nv * nv);
   const int adr = d.world_efcadr[w], n = d.world_nefc[w];
-  for (int r = 0; r < nv; r++)
-    if (lane < 4 * ((nv + 3) >> 2)) tile[r * ld + lane] = lane < nv ? qM[r * nv + lane] : 0.f;
-  __syncwarp();
-  if (own) {
-    float h[32];
-    for (int c = 0; c < nv; c++) h[c] = tile[lane * ld + c];
-    for (int k = 0; k < n; k++) {
-      const int r = adr + k;
-      if (!d.efc_active[r]) continue;
-      const float D = d.efc_D[r];
-      if (D == 0.f) continue;
-      const float* J = d.efc_J + size_t(r) * nv;
-      const float a = D * J[lane];
-      for (int c = 0; c < nv; c++) h[c] += a * J[c];
+  if (nv <= 32) {
+    const int ld = tile_ld(nv);
+    const bool own = lane < nv;
+    for (int r = 0; r < nv; r++)
+      if (lane < 4 * ((nv + 3) >> 2)) tile[r * ld + lane] = lane < nv ? qM[r * nv + lane] : 0.f;
+    __syncwarp();
+    if (own) {
+      float h[32];
+      for (int c = 0; c < nv; c++) h[c] = tile[lane * ld + c];
+      for (int k = 0; k < n; k++) {
+        const int r = adr + k;
+        if (!d.efc_active[r]) continue;
+        const float D = d.efc_D[r];
+        if (D == 0.f) continue;
+        const float* J = d.efc_J + size_t(r) * nv;
+        const float a = D * J[lane];
+        for (int c = 0; c < nv; c++) h[c] += a * J[c];
+      }
+      for (int c = 0; c < nv; c++) tile[lane * ld + c] = h[c];
     }
-    for (int c = 0; c < nv; c++) tile[lane * ld + c] = h[c];
+    __syncwarp();
+    chol_tile(tile, ld, nv, lane);
+    const float sv = cho_solve_tile(tile, ld, nv, own ? WV[lane] : 0.f, lane);
+    __syncwarp();
+    S[lane] = own ? sv : 0.f;
+  } else {
+    float* H = d.efc_h + W(w, nv * nv);
+    assemble_hessian(m, d, qM, H, adr, n, tile, lane);
+    chol_any(H, nv, nv, lane, tile);
+    warp_cho_solve(H, nv, nv, S, WV, lane);
+    for (int i = nv + lane; i < VL; i += 32) S[i] = 0.f;
   }
   __syncwarp();
-  chol_tile(tile, ld, nv, lane);
-  const float sv = cho_solve_tile(tile, ld, nv, own ? WV[lane] : 0.f, lane);
-  __syncwarp();
-  S[lane] = own ? sv : 0.f;
-  St[lane] = own ? sv : 0.f;
+  for (int i = lane; i < VL; i += 32) St[i] = S[i];
   __syncwarp();
   // velocity: bias forces, damper, rows
   if (velg) {
     rne_vel_vjp(m, d, w, lane, S, qv, WV, SA, SB, SC);
-    if (own) GV[lane] = -WV[lane] - (passive_on ? m.dof_damping[lane] * sv : 0.f);
+    for (int i = lane; i < nv; i += 32)
+      GV[i] = -WV[i] - (passive_on ? m.dof_damping[i] * S[i] : 0.f);
     __syncwarp();
     row_q_bars(m, d, w, lane, S, qv, Q, nullptr, nullptr, nullptr, nullptr, GV);
   }
@@ -369,16 +386,18 @@ __device__ void step_vjp_world(const MjbModel& m, const MjbData& d, int w, int l
   const bool act = nu > 0 && !(m.disableflags & DSBL_ACTUATION);
   const float* moment = d.actuator_moment + W(w, nu * nv);
   const float* force = d.actuator_force + W(w, nu);
-  if (own && act) {
-    float f = 0.f;
-    for (int a = 0; a < nu; a++) f += moment[a * nv + lane] * force[a];
-    const int j = m.dof_jntid[lane];
-    const bool clamped = m.jnt_actfrclimited[j] &&
-                         !(f > m.jnt_actfrcrange[2 * j] && f < m.jnt_actfrcrange[2 * j + 1]);
-    if (clamped) St[lane] = 0.f;
+  if (act) {
+    for (int i = lane; i < nv; i += 32) {
+      float f = 0.f;
+      for (int a = 0; a < nu; a++) f += moment[a * nv + i] * force[a];
+      const int j = m.dof_jntid[i];
+      const bool clamped = m.jnt_actfrclimited[j] &&
+                           !(f > m.jnt_actfrcrange[2 * j] && f < m.jnt_actfrcrange[2 * j + 1]);
+      if (clamped) St[i] = 0.f;
+    }
   }
   __syncwarp();
-  // controls, and the actuators' velocity (gv) and length (Q) terms
+  // controls, and the actuators' velocity (GV) and length (Q) terms
   const float* len = d.actuator_length + W(w, nu);
   const float* vel = d.actuator_velocity + W(w, nu);
   const float* ctrl = d.ctrl + W(w, nu);
@@ -407,12 +426,17 @@ __device__ void step_vjp_world(const MjbModel& m, const MjbData& d, int w, int l
     const int cnt = min(32, nu - a0);
     for (int k = 0; k < cnt; k++) {
       const float cv = __shfl_sync(0xffffffffu, kv, k), cq = __shfl_sync(0xffffffffu, kq, k);
-      if (own && cv != 0.f) GV[lane] += cv * moment[(a0 + k) * nv + lane];
-      if (own && cq != 0.f) Q[lane] += cq * moment[(a0 + k) * nv + lane];
+      if (cv == 0.f && cq == 0.f) continue;
+      const float* mo = moment + (a0 + k) * nv;
+      for (int i = lane; i < nv; i += 32) {
+        GV[i] += cv * mo[i];
+        Q[i] += cq * mo[i];
+      }
     }
   }
   __syncwarp();
-  if (velg && own) grad_qvel[W(w, nv) + lane] = y + dt * GV[lane];
+  if (velg)
+    for (int i = lane; i < nv; i += 32) grad_qvel[W(w, nv) + i] = Y[i] + dt * GV[i];
   if (!posg) {
     __syncwarp();
     return;
@@ -425,11 +449,11 @@ __device__ void step_vjp_world(const MjbModel& m, const MjbData& d, int w, int l
   const float* qacc = d.qacc + W(w, nv);
   if (mt) {
     const float* aint = d.qacc_integration + W(w, nv);
-    if (lane < 32) WV[lane] = own ? qacc[lane] - aint[lane] : 0.f;
+    for (int i = lane; i < VL; i += 32) WV[i] = i < nv ? qacc[i] - aint[i] : 0.f;
     __syncwarp();
     mass_product_bars(m, d, w, lane, Z, WV, CB, CIB, SA, SB, SC, SD);
   }
-  if (lane < 32) WV[lane] = own ? -S[lane] : 0.f;
+  for (int i = lane; i < VL; i += 32) WV[i] = -S[i];
   __syncwarp();
   mass_product_bars(m, d, w, lane, WV, qacc, CB, CIB, SA, SB, SC, SD);
   bias_q_bars(m, d, w, lane, WV, qv, CB, CIB, SA, SB, SC);
@@ -448,7 +472,7 @@ __device__ void step_vjp_world(const MjbModel& m, const MjbData& d, int w, int l
   cinert_body_bars(m, d, w, lane, CIB, BF, BT, SCB);
   subtree_com_bars(m, d, w, lane, SCB, JS, BF, BT, SA);
   kinematic_sweep(m, d, w, lane, JA, JX, BF, BT, Q);
-  if (own) grad_qpos[W(w, nv) + lane] = direct + dt * Q[lane];
+  for (int i = lane; i < nv; i += 32) grad_qpos[W(w, nv) + i] = DIR[i] + dt * Q[i];
   __syncwarp();
 }
 

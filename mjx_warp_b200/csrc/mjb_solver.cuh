@@ -92,6 +92,77 @@ __device__ void update_constraint(SolverCtx& s) {
 }
 
 // solver.py:176-312
+// H = tril(qM) + sum over the world's active rows of D J'J: the lower triangle of the dense
+// nv x nv matrix at H (update_gradient's Newton Hessian, solver.py:249-276).  nz: null or
+// generic_nz_floats(nv) floats of warp scratch for the sparse-row assembly.
+__device__ void assemble_hessian(const MjbModel& m, const MjbData& d, const float* qM, float* H,
+                                 int adr, int n, float* nz, int lane) {
+  const int nv = m.nv;
+  if (nz) {
+    // Each row's outer product touches only the row's nonzero columns (a contact row has the
+    // dofs of two kinematic chains): the columns are compacted in order into the warp's
+    // scratch and the lower-triangle pairs updated, row by row, with the per-entry arithmetic
+    // of the dense form (h += J_i * J_j * D in row order; zero terms are skipped).
+    if (m.is_sparse) {
+      sparse_to_lower(m, qM, H, lane);
+    } else {
+      for (int e = lane; e < nv * nv; e += 32) {
+        const int i = e / nv, j = e - i * nv;
+        if (j <= i) H[e] = qM[e];
+      }
+      __syncwarp();
+    }
+    int* nzi = reinterpret_cast<int*>(nz);
+    float* nzv = nz + round4i(nv);
+    for (int k = 0; k < n; k++) {
+      const int r = adr + k;
+      if (!d.efc_active[r]) continue;
+      const float D = d.efc_D[r];
+      if (D == 0.f) continue;
+      const float* J = d.efc_J + size_t(r) * nv;
+      int cnt = 0;
+      for (int base = 0; base < nv; base += 32) {
+        const int c = base + lane;
+        const float v = c < nv ? J[c] : 0.f;
+        const unsigned mk = __ballot_sync(WARP_FULL, v != 0.f);
+        if (v != 0.f) {
+          const int p = cnt + __popc(mk & ((1u << lane) - 1u));
+          nzi[p] = c;
+          nzv[p] = v;
+        }
+        cnt += __popc(mk);
+      }
+      __syncwarp();
+      const int npair = cnt * (cnt + 1) / 2;
+      for (int t = lane; t < npair; t += 32) {  // pair t = (a, b), b <= a, in triangle order
+        int a = int((sqrtf(8.f * float(t) + 1.f) - 1.f) * 0.5f);
+        while (a * (a + 1) / 2 > t) a--;
+        while ((a + 1) * (a + 2) / 2 <= t) a++;
+        const int b = t - a * (a + 1) / 2;
+        H[nzi[a] * nv + nzi[b]] += nzv[a] * nzv[b] * D;
+      }
+      __syncwarp();
+    }
+  } else {
+    if (m.is_sparse) sparse_to_lower(m, qM, H, lane);
+    for (int e = lane; e < nv * nv; e += 32) {
+      const int i = e / nv, j = e - i * nv;
+      if (j > i) continue;
+      float h = m.is_sparse ? H[e] : qM[e];
+      for (int k = 0; k < n; k++) {
+        const int r = adr + k;
+        if (!d.efc_active[r]) continue;
+        const float D = d.efc_D[r];
+        if (D == 0.f) continue;
+        const float* J = d.efc_J + size_t(r) * nv;
+        h += J[i] * J[j] * D;
+      }
+      H[e] = h;
+    }
+    __syncwarp();
+  }
+}
+
 __device__ void update_gradient(SolverCtx& s) {
   const MjbModel& m = s.m;
   const MjbData& d = s.d;
@@ -112,69 +183,7 @@ __device__ void update_gradient(SolverCtx& s) {
   // factor of the previous call is kept while no active flag changed (the same H, the same bits).
   float* H = s.hs;
   if (!(s.reuse && s.factored && !s.changed)) {
-    if (s.nz) {
-      // Each row's outer product touches only the row's nonzero columns (a contact row has the
-      // dofs of two kinematic chains): the columns are compacted in order into the warp's
-      // scratch and the lower-triangle pairs updated, row by row, with the per-entry arithmetic
-      // of the dense form (h += J_i * J_j * D in row order; zero terms are skipped).
-      if (m.is_sparse) {
-        sparse_to_lower(m, s.qM, H, lane);
-      } else {
-        for (int e = lane; e < nv * nv; e += 32) {
-          const int i = e / nv, j = e - i * nv;
-          if (j <= i) H[e] = s.qM[e];
-        }
-        __syncwarp();
-      }
-      int* nzi = reinterpret_cast<int*>(s.nz);
-      float* nzv = s.nz + round4i(nv);
-      for (int k = 0; k < s.n; k++) {
-        const int r = s.adr + k;
-        if (!d.efc_active[r]) continue;
-        const float D = d.efc_D[r];
-        if (D == 0.f) continue;
-        const float* J = d.efc_J + size_t(r) * nv;
-        int cnt = 0;
-        for (int base = 0; base < nv; base += 32) {
-          const int c = base + lane;
-          const float v = c < nv ? J[c] : 0.f;
-          const unsigned mk = __ballot_sync(WARP_FULL, v != 0.f);
-          if (v != 0.f) {
-            const int p = cnt + __popc(mk & ((1u << lane) - 1u));
-            nzi[p] = c;
-            nzv[p] = v;
-          }
-          cnt += __popc(mk);
-        }
-        __syncwarp();
-        const int npair = cnt * (cnt + 1) / 2;
-        for (int t = lane; t < npair; t += 32) {  // pair t = (a, b), b <= a, in triangle order
-          int a = int((sqrtf(8.f * float(t) + 1.f) - 1.f) * 0.5f);
-          while (a * (a + 1) / 2 > t) a--;
-          while ((a + 1) * (a + 2) / 2 <= t) a++;
-          const int b = t - a * (a + 1) / 2;
-          H[nzi[a] * nv + nzi[b]] += nzv[a] * nzv[b] * D;
-        }
-        __syncwarp();
-      }
-    } else {
-      if (m.is_sparse) sparse_to_lower(m, s.qM, H, lane);
-      for (int e = lane; e < nv * nv; e += 32) {
-        const int i = e / nv, j = e - i * nv;
-        if (j > i) continue;
-        float h = m.is_sparse ? H[e] : s.qM[e];
-        for (int k = 0; k < s.n; k++) {
-          const int r = s.adr + k;
-          if (!d.efc_active[r]) continue;
-          const float D = d.efc_D[r];
-          if (D == 0.f) continue;
-          const float* J = d.efc_J + size_t(r) * nv;
-          h += J[i] * J[j] * D;
-        }
-        H[e] = h;
-      }
-      __syncwarp();
-    }
+    assemble_hessian(m, d, s.qM, H, s.adr, s.n, s.nz, lane);
     if (d.efc_h) {  // keep the assembled Hessian observable (lower triangle), as the reference does
       float* out = d.efc_h + W(s.w, nv * nv);
       if (out != H)

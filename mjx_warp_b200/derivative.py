@@ -114,10 +114,10 @@ def transition_vjp(m: Model, A: torch.Tensor, B: Optional[torch.Tensor], lam: to
 
 
 def ctrl_vjp_supported(m: Model) -> bool:
-  """Whether ctrl_vjp applies to m: dense mass matrix, nv <= 32, no activations, and for
+  """Whether ctrl_vjp applies to m: dense mass matrix, no activations, and for
   implicitfast no velocity-dependent actuator gains or biases."""
   act_on = not (int(m.opt.disableflags) & (1 << 10)) and bool(m.actuator_affine_bias_gain)
-  return (m.nv <= 32 and not m.opt.is_sparse and m.na == 0
+  return (not m.opt.is_sparse and m.na == 0
           and not (int(m.opt.integrator) != 0 and act_on))
 
 
@@ -379,7 +379,7 @@ class Rollout:
     if analytic not in ("full", "qvel_ctrl", "ctrl", "none"):
       raise ValueError(f"analytic must be 'full', 'qvel_ctrl', 'ctrl' or 'none', got {analytic!r}")
     if analytic != "none" and not ctrl_vjp_supported(m):
-      raise NotImplementedError("analytic step VJP: needs a dense mass matrix, nv <= 32, na == 0 "
+      raise NotImplementedError("analytic step VJP: needs a dense mass matrix, na == 0 "
                                 "and, for implicitfast, no affine actuator gains or biases")
     if analytic == "full" and not qpos_vjp_supported(m):
       raise NotImplementedError("analytic qpos adjoint: the model has a feature it does not cover")

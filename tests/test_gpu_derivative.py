@@ -270,6 +270,12 @@ def _vjp_case(case, nworld):
     fn = _lifted_humanoid if case == "lifted" else humanoid_state
     qpos, qvel, ctrl = fn(mjm, nworld, seed=6)
     settle = 10 if case == "standing" else 0
+  elif case == "humanoid_spheres":  # nv = 123: the Hessian outside the warp tile
+    from test_gpu_configs import humanoid_spheres_state
+    mjm = load("humanoid_spheres.xml", integrator=3, timestep=0.005, iterations=30,
+               ls_iterations=30, jacobian=0)
+    qpos, qvel, ctrl, _ = humanoid_spheres_state(mjm, load("humanoid.xml"), nworld, seed=6)
+    settle = 10
   else:
     mjm = load(_JOINTS_XML if case == "joints" else case)
     mjm.opt.iterations, mjm.opt.ls_iterations = 30, 30
@@ -280,14 +286,15 @@ def _vjp_case(case, nworld):
   return mjm, qpos, qvel, ctrl, settle
 
 
-@pytest.mark.parametrize("case", ["lifted", "standing", "sphere_chain.xml", "joints"])
+@pytest.mark.parametrize("case", ["lifted", "standing", "sphere_chain.xml", "joints",
+                                  "humanoid_spheres"])
 def test_step_vjp_matches_differences(case):
   """step_vjp after a step equals (A_q^T lam, A_v^T lam, B^T lam) from central FP64 differences
   of the oracle's step at the same state (A_q, A_v the qpos-tangent and velocity columns of A):
   the humanoid in the air and standing on the floor (implicitfast, contacts and limits), the
   sphere + chain (Euler with eulerdamp, damping, a resting contact), a ball / slide / hinge chain
   with a free body.  qvel_ctrl_vjp and ctrl_vjp give the same velocity and control gradients."""
-  nworld = 8
+  nworld = 4 if case == "humanoid_spheres" else 8
   mjm, qpos, qvel, ctrl, settle = _vjp_case(case, nworld)
   m = mjw.put_model(mjm)
   assert mjw.derivative.qpos_vjp_supported(m)
@@ -308,7 +315,7 @@ def test_step_vjp_matches_differences(case):
   gv2, gu2 = mjw.derivative.qvel_ctrl_vjp(m, d, qvel_prev, lam)
   gu3 = mjw.derivative.ctrl_vjp(m, d, lam)
   torch.cuda.synchronize()
-  if case == "standing":
+  if case in ("standing", "humanoid_spheres"):
     assert int(d.nefc.cpu()[0]) > 0
   assert torch.equal(gu, gu2) and torch.equal(gu, gu3) and torch.equal(gv, gv2)
   gq, gv, gu = gq.cpu().numpy(), gv.cpu().numpy(), gu.cpu().numpy()
