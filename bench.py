@@ -254,6 +254,104 @@ def _grad_rate(mjw, torch, nworld=1024, horizon=32, checkpoint=8, reps=2, center
                                       "p99": float(q[1]) if q[1] is not None else None}}
 
 
+SPHERES_MODEL = os.path.join(ROOT, "tests", "golden", "models", "humanoid_spheres.xml")
+
+
+def _spheres_state(mjm, hum, nworld, seed):
+  """The humanoid's keyframe 0 + U(-0.05, 0.05); k ~ U{0..16} spheres dropped near it from
+  z ~ U(0.1, 0.6), the others parked 100 m away at 10 m height (uneven contact counts)."""
+  rng = np.random.default_rng(seed)
+  qpos = np.zeros((nworld, mjm.nq))
+  qpos[:, :hum.nq] = hum.key_qpos[0] + rng.uniform(-0.05, 0.05, (nworld, hum.nq))
+  qpos[:, 3:7] /= np.linalg.norm(qpos[:, 3:7], axis=1, keepdims=True)
+  nsph = (mjm.nq - hum.nq) // 7
+  k = rng.integers(0, nsph + 1, nworld)
+  for i in range(nsph):
+    a = hum.nq + 7 * i
+    act = i < k
+    qpos[:, a] = np.where(act, rng.uniform(-0.6, 0.6, nworld), 100.0 + 2.0 * i)
+    qpos[:, a + 1] = np.where(act, rng.uniform(-0.6, 0.6, nworld), 100.0)
+    qpos[:, a + 2] = np.where(act, rng.uniform(0.1, 0.6, nworld), 10.0)
+    qpos[:, a + 3] = 1.0
+  return qpos, rng.normal(0.0, 0.01, (nworld, mjm.nv)), rng.uniform(-0.4, 0.4, (nworld, mjm.nu))
+
+
+def _combined(mjw, torch, nworld=32768, horizon=16, checkpoint=4, reps=2):
+  """The combined form of the uneven-contact humanoid: humanoids with 0-16 extra free spheres
+  (nv = 123), a 16-step rollout forward plus the analytic adjoint (d/d ctrl, qpos0, qvel0 of
+  ||root_pos_T - target||^2 + 1e-3 ||ctrl||^2), checkpoints every 4 steps; forward and backward
+  world-steps/s, peak GPU memory of the differentiated rollout, and the plain form's forward."""
+  from mjx_warp_b200 import mjcf
+
+  hum = mjcf.from_xml_path(MODEL)
+  mjm = mjcf.from_xml_path(SPHERES_MODEL)
+  mjm.opt.integrator, mjm.opt.timestep, mjm.opt.jacobian = 3, 0.005, 0
+  mjm.opt.solver, mjm.opt.iterations, mjm.opt.ls_iterations = 2, 10, 10
+  qpos, qvel, ctrl0 = _spheres_state(mjm, hum, nworld, seed=5)
+  m = mjw.put_model(mjm)
+  torch.cuda.synchronize()
+  base = torch.cuda.memory_allocated()
+  torch.cuda.reset_peak_memory_stats()
+  roll = mjw.derivative.Rollout(mjm, m, nworld, checkpoint=checkpoint, nconmax=96, njmax=256)
+  rng = np.random.default_rng(6)
+  ctrl = np.repeat(ctrl0[None], horizon, axis=0) + rng.normal(0.0, 0.05, (horizon, nworld, mjm.nu))
+  q0 = torch.tensor(qpos, dtype=torch.float32, device="cuda")
+  v0 = torch.tensor(qvel, dtype=torch.float32, device="cuda")
+  u0 = torch.tensor(ctrl, dtype=torch.float32, device="cuda")
+  target = q0[:, :3] + torch.tensor([0.05, 0.0, 0.0], device="cuda")
+
+  def once():
+    q, v, u = (t.clone().requires_grad_(True) for t in (q0, v0, u0))
+    e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    e0.record()
+    qT, _ = roll(q, v, u)
+    loss = ((qT[:, :3] - target) ** 2).sum() + 1e-3 * (u ** 2).sum()
+    e1.record()
+    loss.backward()
+    e2.record()
+    torch.cuda.synchronize()
+    ok = torch.isfinite(u.grad).all(2).all(0) & torch.isfinite(q.grad).all(1)
+    return e0.elapsed_time(e1) * 1e-3, e1.elapsed_time(e2) * 1e-3, int(ok.sum())
+
+  once()
+  fwd = bwd = 0.0
+  for _ in range(reps):
+    f, b, nok = once()
+    fwd, bwd = fwd + f / reps, bwd + b / reps
+  peak = torch.cuda.max_memory_allocated() - base
+  status = mjw.world_status(roll.d)
+  # the plain form's forward rollout of the same worlds (no checkpoints, no graph)
+  d = roll.d
+  d.qpos.copy_(q0)
+  d.qvel.copy_(v0)
+  d.qacc_warmstart.zero_()
+  step = lambda: mjw.step(m, d, fused=False)
+  d.ctrl.copy_(u0[0])
+  step()
+  t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+  d.qpos.copy_(q0)
+  d.qvel.copy_(v0)
+  d.qacc_warmstart.zero_()
+  t0.record()
+  for t in range(horizon):
+    d.ctrl.copy_(u0[t])
+    step()
+  t1.record()
+  torch.cuda.synchronize()
+  plain = t0.elapsed_time(t1) * 1e-3
+  return {"workload": "humanoid + 0-16 free spheres per world (nv 123), implicitfast dt=0.005, "
+                      "Newton 10 it / ls 10, dense mass matrix; 16-step rollout + analytic adjoint",
+          "nworld": nworld, "horizon": horizon, "checkpoint": checkpoint,
+          "forward_steps_per_s": nworld * horizon / fwd,
+          "backward_steps_per_s": nworld * horizon / bwd,
+          "grad_steps_per_s": nworld * horizon / (fwd + bwd), "cost_vs_forward": (fwd + bwd) / fwd,
+          "plain_forward_steps_per_s": nworld * horizon / plain,
+          "forward_ms": fwd * 1e3, "backward_ms": bwd * 1e3,
+          "peak_gpu_memory_gb": peak / 1e9, "worlds_with_finite_grads": nok,
+          "worlds_flagged": int((status != 0).sum()),
+          "precision": "FP32 throughout (the 3xTF32 / FP64 precision form is not built)"}
+
+
 def _graph_steps_per_s(torch, step, nworld, steps, barrier, restore):
   g = torch.cuda.CUDAGraph()
   s = torch.cuda.Stream()
@@ -408,6 +506,10 @@ def run_ours(args):
       grad[key] = {k: other[k] for k in ("value", "unit", "cost_vs_forward", "worlds_with_finite_grads")}
       grad[key]["method"] = other["config"]["method"]
 
+  combined = None
+  if rank == 0 and not args.no_combined:
+    combined = _combined(mjw, torch)
+
   launches_per_step = LAUNCHES[args.form]
   total_worlds = nworld * world_size
   value = total_worlds * args.steps / elapsed
@@ -457,6 +559,8 @@ def run_ours(args):
     line["qacc_err"] = accuracy
   if grad is not None:
     line["grad"] = grad
+  if combined is not None:
+    line["combined"] = combined
   if rank == 0 and not args.no_cpu_baseline:
     line["cpu_baseline"] = cpu_baseline(mjm, budget_s=args.cpu_seconds)
   del g
@@ -522,6 +626,7 @@ def main():
   p.add_argument("--no-cpu-baseline", action="store_true")
   p.add_argument("--no-accuracy", action="store_true")
   p.add_argument("--no-grad", action="store_true")
+  p.add_argument("--no-combined", action="store_true")
   args = p.parse_args()
   if args.warmup < 3:
     args.warmup = 3

@@ -265,6 +265,28 @@ def tangent_grad_to_qpos(m: Model, qpos: torch.Tensor, lam: torch.Tensor) -> tor
 
 
 _STATE = ("qpos", "qvel", "act", "qacc_warmstart")
+# Data fields that a step writes before it reads them and that step_vjp does not read: the
+# Data objects of a segment share one copy of each
+_RING_SHARED = ("qLD", "qLDiagInv", "qM_integration", "qfrc_integration", "collision_pair",
+                "collision_worldid", "sap_geom_sort", "sap_projection_lower", "sap_projection_upper",
+                "sap_sort_index", "sap_range", "sap_cumulative_sum")
+_RING_SHARED_EFC = ("h", "quad", "jv", "force", "Ma", "grad", "Mgrad", "search", "mv",
+                    "prev_grad", "prev_Mgrad")
+
+
+def _segment_ring(mjm, nworld: int, nconmax: int, njmax: int, count: int):
+  """`count` Data objects for the steps of one segment, sharing their scratch fields."""
+  ring = [make_data(mjm, nworld, nconmax=nconmax, njmax=njmax)]
+  for _ in range(count - 1):
+    dk = make_data(mjm, nworld, nconmax=nconmax, njmax=njmax)
+    for name in _RING_SHARED:
+      if getattr(ring[0], name, None) is not None:
+        setattr(dk, name, getattr(ring[0], name))
+    for name in _RING_SHARED_EFC:
+      if getattr(ring[0].efc, name, None) is not None:
+        setattr(dk.efc, name, getattr(ring[0].efc, name))
+    ring.append(dk)
+  return ring
 
 
 def _snapshot(d: Data):
@@ -384,10 +406,12 @@ class Rollout:
     if analytic == "full" and not qpos_vjp_supported(m):
       raise NotImplementedError("analytic qpos adjoint: the model has a feature it does not cover")
     self.analytic = analytic
-    self.d = make_data(mjm, nworld, nconmax=nconmax * nworld, njmax=njmax * nworld)
-    # the backward of the analytic adjoint keeps every step of a segment in its own Data
-    self.seg = [make_data(mjm, nworld, nconmax=nconmax * nworld, njmax=njmax * nworld)
-                for _ in range(self.checkpoint)] if analytic == "full" else []
+    # the backward of the analytic adjoint keeps every step of a segment in its own Data (the
+    # forward pass runs in the first of them)
+    self.seg = _segment_ring(mjm, nworld, nconmax * nworld, njmax * nworld,
+                             self.checkpoint) if analytic == "full" else []
+    self.d = self.seg[0] if self.seg else make_data(mjm, nworld, nconmax=nconmax * nworld,
+                                                     njmax=njmax * nworld)
     self.fd = None if analytic == "full" else TransitionFD(
         mjm, m, nworld, eps=eps, centered=centered, nconmax=nconmax, njmax=njmax, fused=fused,
         state_only=analytic == "ctrl", qpos_only=analytic == "qvel_ctrl")
