@@ -249,8 +249,9 @@ int mjb_fd_jacobian(const MjbModel* m, const MjbData* pert, int nworld, float ep
  * contacts held fixed).  Needs the dense mass matrix and na = 0, and for implicitfast no
  * affine actuator gains or biases (else MJB_ERR_UNSUPPORTED); grad_qpos further assumes: ball
  * joints alone on their body, no stiffness on free / ball joints, actuators on hinge / slide
- * joints, planes on bodies welded to the world, zero xfrc_applied.  For nv > 32 the Hessian and its
- * factor are written to d->efc_h. */
+ * joints, planes on bodies welded to the world, zero xfrc_applied.  For nv > 32 with the Newton
+ * solver the factor of the Hessian that the step left in d->efc_h is reused (with CG the Hessian
+ * and its factor are written there). */
 int mjb_step_vjp(const MjbModel* m, const MjbData* d, const float* qvel_prev, const float* lam,
                  float* grad_qpos, float* grad_qvel, float* grad_ctrl, mjbStream stream);
 /* mjb_step_vjp for grad_ctrl alone */

@@ -244,8 +244,8 @@ __device__ void rne_vel_vjp(const MjbModel& m, const MjbData& d, int w, int lane
 // active flags, contacts, qLD_integration, qacc_integration, kinematics, com / rne arrays,
 // actuator arrays) and the post-step qvel; qvel_prev is the pre-step qvel; lam = (lam_q (nv),
 // lam_v (nv)) of the next state.  Any of grad_qpos / grad_qvel / grad_ctrl may be null.  One warp
-// per world (scratch: step_vjp_floats; for nv > 32 H and its factor are written to efc_h), dense
-// qM, na = 0.
+// per world (scratch: step_vjp_floats; for nv > 32 the Newton solver's factor of H in efc_h is
+// reused, and with CG H and its factor are written there), dense qM, na = 0.
 __device__ void step_vjp_world(const MjbModel& m, const MjbData& d, int w, int lane,
                                const float* lam, const float* qvel_prev, float* grad_ctrl,
                                float* grad_qvel, float* grad_qpos, float* tile) {
@@ -365,9 +365,14 @@ __device__ void step_vjp_world(const MjbModel& m, const MjbData& d, int w, int l
     __syncwarp();
     S[lane] = own ? sv : 0.f;
   } else {
+    // the Newton solver (generic path) leaves the factor of H at the final active set in efc_h:
+    // its iterations end with update_gradient, which factors H in place (or keeps the factor
+    // while the active set is unchanged); CG has no H, so it is assembled and factored here
     float* H = d.efc_h + W(w, nv * nv);
-    assemble_hessian(m, d, qM, H, adr, n, tile, lane);
-    chol_any(H, nv, nv, lane, tile);
+    if (m.solver != 2) {
+      assemble_hessian(m, d, qM, H, adr, n, tile, lane);
+      chol_any(H, nv, nv, lane, tile);
+    }
     warp_cho_solve(H, nv, nv, S, WV, lane);
     for (int i = nv + lane; i < VL; i += 32) S[i] = 0.f;
   }

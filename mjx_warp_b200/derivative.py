@@ -270,8 +270,8 @@ _STATE = ("qpos", "qvel", "act", "qacc_warmstart")
 _RING_SHARED = ("qLD", "qLDiagInv", "qM_integration", "qfrc_integration", "collision_pair",
                 "collision_worldid", "sap_geom_sort", "sap_projection_lower", "sap_projection_upper",
                 "sap_sort_index", "sap_range", "sap_cumulative_sum")
-_RING_SHARED_EFC = ("h", "quad", "jv", "force", "Ma", "grad", "Mgrad", "search", "mv",
-                    "prev_grad", "prev_Mgrad")
+_RING_SHARED_EFC = ("quad", "jv", "force", "Ma", "grad", "Mgrad", "search", "mv", "prev_grad",
+                    "prev_Mgrad")
 
 
 def _segment_ring(mjm, nworld: int, nconmax: int, njmax: int, count: int):
