@@ -141,8 +141,8 @@ def _algorithmic_bytes(d, mjm, ncon, nefc):
   return W * (read_state + per_world_out) + contact_bytes + efc_bytes
 
 
-FORMS = {"plain": 0, "chosen": 1, "single": 2}
-LAUNCHES = {"plain": 16, "chosen": 16, "single": 2}  # kernels per step (mjb200.cu run_* paths)
+FORMS = {"plain": 0, "chosen": 1, "single": 2, "precision": 3}
+LAUNCHES = {"plain": 16, "chosen": 16, "single": 2, "precision": 16}  # kernels per step (mjb200.cu run_* paths)
 
 
 def _solver_bytes(mjm, nworld, nefc):

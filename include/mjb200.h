@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define MJB_ABI_VERSION 4
+#define MJB_ABI_VERSION 5
 
 typedef struct CUstream_st* mjbStream; /* == cudaStream_t */
 
@@ -60,6 +60,7 @@ typedef struct MjbModel {
   int32_t integrator, cone, solver, iterations, ls_iterations, disableflags, is_sparse,
       ls_parallel;
   int32_t actuator_affine_bias_gain;
+  int32_t precision;   /* set by MJB_FORM_PRECISION on its own copy; 0 in callers' models */
   float timestep, impratio, tolerance, ls_tolerance, meaninertia;
   float gravity[3];
   /* tree / level tables */
@@ -139,6 +140,9 @@ typedef struct MjbData {
 #define MJB_FORM_PLAIN 0  /* one kernel per reference stage; Hessian refactored every iteration */
 #define MJB_FORM_CHOSEN 1 /* stage kernels to fwd_acceleration + solver reusing its factor + integrator */
 #define MJB_FORM_SINGLE 2 /* the whole step of a world in one warp of one kernel */
+/* MJB_FORM_CHOSEN with the Newton Hessian and mass-matrix Cholesky factor-solves in FP64 and the
+   line-search polynomial coefficients accumulated in FP64 (dense, nv <= 32) */
+#define MJB_FORM_PRECISION 3
 
 typedef struct MjbRunCfg {
   int32_t fused;            /* launch form, MJB_FORM_* */

@@ -20,7 +20,7 @@ LIB_PATH = os.environ.get("MJX_WARP_B200_LIB") or os.path.join(_HERE, "libmjb200
 MODEL_INTS = ("nq", "nv", "na", "nu", "nbody", "njnt", "ngeom", "nsite", "nmocap", "nM", "nlimit",
               "nlevel", "nblock", "npair_cand", "nlsp", "integrator", "cone", "solver",
               "iterations", "ls_iterations", "disableflags", "is_sparse", "ls_parallel",
-              "actuator_affine_bias_gain")
+              "actuator_affine_bias_gain", "precision")
 MODEL_FLOATS = ("timestep", "impratio", "tolerance", "ls_tolerance", "meaninertia")
 MODEL_PTRS = (
   "body_tree", "body_treeadr", "body_childadr", "body_childnum", "body_child", "body_subtreeend",
@@ -173,7 +173,7 @@ def lib() -> ctypes.CDLL:
   L.mjb_autotune.argtypes = [pm, pd, vp, ctypes.POINTER(MjbTune), vp]
   L.mjb_transition_vjp.restype = ctypes.c_int
   L.mjb_transition_vjp.argtypes = [pm, ci, vp, vp, vp, vp, vp, vp]
-  if L.mjb_abi_version() != 4:
+  if L.mjb_abi_version() != 5:
     raise RuntimeError("libmjb200.so ABI version mismatch")
   _lib = L
   return L

@@ -20,14 +20,16 @@ from .types import Data, Model
 
 # launch forms (include/mjb200.h MJB_FORM_*): True / 1 the chosen form, False / 0 the plain
 # one-kernel-per-stage form, 2 the single-kernel form
-_FORMS = {0: _abi.MjbRunCfg(0, 0), 1: _abi.MjbRunCfg(1, 0), 2: _abi.MjbRunCfg(2, 0)}
+_FORMS = {0: _abi.MjbRunCfg(0, 0), 1: _abi.MjbRunCfg(1, 0), 2: _abi.MjbRunCfg(2, 0),
+          3: _abi.MjbRunCfg(3, 0)}
 
 
 def _form(fused) -> "_abi.MjbRunCfg":
   try:
     return _FORMS[int(fused)]
   except (KeyError, TypeError, ValueError):
-    raise ValueError(f"unknown launch form {fused!r} (True/1 chosen, False/0 plain, 2 single)") from None
+    raise ValueError(f"unknown launch form {fused!r} (True/1 chosen, False/0 plain, 2 single, "
+                     "3 precision)") from None
 
 
 def _call(name: str, m: Model, d: Data, *extra) -> None:
@@ -52,7 +54,9 @@ def step(m: Model, d: Data, fused=True) -> None:
   for the solver (keeping the Newton Hessian's factor while the active set is unchanged) and one
   for the integrator; fused=False (or 0) launches one kernel per reference stage and refactors
   the Hessian in every iteration, as the reference does; fused=2 runs the whole step of a world
-  in one warp of a single kernel.
+  in one warp of a single kernel; fused=3 runs the chosen form with the Hessian and mass-matrix
+  Cholesky factor-solves and the line-search coefficient sums in FP64 (the precision form; dense,
+  nv <= 32).
   """
   _integrator_check(m)
   L = _abi.lib()

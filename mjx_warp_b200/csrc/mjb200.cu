@@ -148,13 +148,14 @@ __global__ void __launch_bounds__(128, MJB_MINB) k_step_fused(const __grid_const
 }
 
 // chosen form: the constraint solver with the Hessian factor kept across iterations
+template <bool PREC>
 __global__ void __launch_bounds__(128, MJB_MINB) k_solve(const __grid_constant__ MjbModel m, const __grid_constant__ MjbData d, int smem_per_warp) {
   extern __shared__ __align__(16) float smem[];
   const int lane = threadIdx.x & 31;
   const int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   if (w >= d.nworld) return;
   float* sm = smem_per_warp ? smem + size_t(threadIdx.x >> 5) * smem_per_warp : nullptr;
-  solve(m, d, w, lane, sm, d.efc_h + W(w, m.nv * m.nv), true);
+  solve<PREC>(m, d, w, lane, sm, d.efc_h + W(w, m.nv * m.nv), true);
 }
 
 // The chosen form's solver schedule.  k_order_worlds sorts the worlds by their constraint row
@@ -202,6 +203,7 @@ __global__ void __launch_bounds__(1024) k_order_worlds(const int* nefc, int* ord
   }
 }
 
+template <bool PREC>
 __global__ void __launch_bounds__(128, MJB_MINB) k_solve_queue(const __grid_constant__ MjbModel m, const __grid_constant__ MjbData d, int smem_per_warp) {
   extern __shared__ __align__(16) float smem[];
   const int lane = threadIdx.x & 31;
@@ -212,7 +214,7 @@ __global__ void __launch_bounds__(128, MJB_MINB) k_solve_queue(const __grid_cons
     idx = __shfl_sync(WARP_FULL, idx, 0);
     if (idx >= d.nworld) break;
     const int w = d.world_order[idx];
-    solve(m, d, w, lane, sm, d.efc_h + W(w, m.nv * m.nv), true);
+    solve<PREC>(m, d, w, lane, sm, d.efc_h + W(w, m.nv * m.nv), true);
   }
 }
 
@@ -432,7 +434,7 @@ int launch_stage(const MjbModel* m, const MjbData* d, cudaStream_t s) {
   size_t bytes = 0;
   if (STAGE == S_SOLVE) spw = m->nv <= 32 ? int(solver_smem_floats(m->nv)) : generic_nz_floats(m->nv);
   if (STAGE == S_FACTOR_M || STAGE == S_FWD_ACCELERATION || STAGE == S_EULER || STAGE == S_IMPLICIT)
-    spw = tile_floats(m->nv);
+    spw = tile_floats(m->nv) + (m->precision ? prec_tile_floats(m->nv) : 0);
   if (STAGE == S_SAP) spw = sap_smem_floats(m->ngeom);
   if (spw) {
     bytes = size_t(spw) * warps * sizeof(float);
@@ -597,6 +599,27 @@ int run_forward_plain(const MjbModel* m, const MjbData* d, cudaStream_t s) {
   return d->njmax == 0 ? MJB_OK : launch_stage<S_SOLVE>(m, d, s);
 }
 
+// the chosen form's solver launch: k_order_worlds + the persistent k_solve_queue when the Data has
+// the schedule arrays, else one warp per world (k_solve); PREC selects the precision form's solver
+template <bool PREC>
+void launch_solver(const MjbModel* m, const MjbData* d, const ChosenCfg& cfg, int spw,
+                   cudaStream_t s) {
+  if (d->world_order && d->work_queue && d->world_nefc) {
+    const int qw = cfg.warps;
+    const size_t qbytes = size_t(spw) * qw * sizeof(float);
+    static size_t conf_queue[kSmemDevices];
+    allow_smem(k_solve_queue<PREC>, size_t(spw) * kDefaultWarps * sizeof(float), conf_queue);
+    const int ctas = resident_ctas(k_solve_queue<PREC>, 32 * qw, qbytes);
+    k_order_worlds<<<1, 1024, 0, s>>>(d->world_nefc, d->world_order, d->work_queue, d->nworld);
+    k_solve_queue<PREC><<<std::min(ctas, grid_for(d->nworld, qw)), 32 * qw, qbytes, s>>>(*m, *d, spw);
+  } else {
+    const size_t bytes = size_t(spw) * kDefaultWarps * sizeof(float);
+    static size_t conf_solve[kSmemDevices];
+    allow_smem(k_solve<PREC>, bytes, conf_solve);
+    k_solve<PREC><<<grid_for(d->nworld, kDefaultWarps), 32 * kDefaultWarps, bytes, s>>>(*m, *d, spw);
+  }
+}
+
 // the chosen form's phases: 0 = status reset + the stage kernels up to fwd_acceleration,
 // 1 = k_solve, 2 = k_integrate
 int run_chosen_phase(const MjbModel* m, const MjbData* d, int phase, cudaStream_t s,
@@ -604,29 +627,20 @@ int run_chosen_phase(const MjbModel* m, const MjbData* d, int phase, cudaStream_
   const ChosenCfg cfg = tuned ? *tuned : chosen_cfg(m, d);
   const int warps = kDefaultWarps;
   const int grid = grid_for(d->nworld, warps);
-  const int tpw = tile_floats(m->nv);
+  const int tpw = tile_floats(m->nv) + (m->precision ? prec_tile_floats(m->nv) : 0);
   const size_t tile_bytes = size_t(tpw) * warps * sizeof(float);
-  static size_t conf_solve[kSmemDevices], conf_int[kSmemDevices];
+  static size_t conf_int[kSmemDevices];
   if (phase == 0) {
     reset_counters(d, false, false, false, true, s);
     int rc = run_forward_fork(m, d, s, cfg.lanes);
     if (rc) return rc;
   } else if (phase == 1) {
     if (d->njmax > 0) {
-      const int spw = m->nv <= 32 ? int(solver_smem_floats(m->nv)) : generic_nz_floats(m->nv);
-      if (d->world_order && d->work_queue && d->world_nefc) {
-        const int qw = cfg.warps;
-        const size_t qbytes = size_t(spw) * qw * sizeof(float);
-        static size_t conf_queue[kSmemDevices];
-        allow_smem(k_solve_queue, size_t(spw) * kDefaultWarps * sizeof(float), conf_queue);
-        const int ctas = resident_ctas(k_solve_queue, 32 * qw, qbytes);
-        k_order_worlds<<<1, 1024, 0, s>>>(d->world_nefc, d->world_order, d->work_queue, d->nworld);
-        k_solve_queue<<<std::min(ctas, grid_for(d->nworld, qw)), 32 * qw, qbytes, s>>>(*m, *d, spw);
-      } else {
-        const size_t bytes = size_t(spw) * warps * sizeof(float);
-        allow_smem(k_solve, bytes, conf_solve);
-        k_solve<<<grid, 32 * warps, bytes, s>>>(*m, *d, spw);
-      }
+      const int spw = m->nv <= 32 ? int(solver_smem_floats(m->nv)) +
+                                        (m->precision ? prec_tile_floats(m->nv) : 0)
+                                  : generic_nz_floats(m->nv);
+      if (m->precision) launch_solver<true>(m, d, cfg, spw, s);
+      else launch_solver<false>(m, d, cfg, spw, s);
     }
   } else if (phase == 2) {
     allow_smem(k_integrate, tile_bytes, conf_int);
@@ -682,6 +696,12 @@ int mjb_forward(const MjbModel* m, const MjbData* d, const MjbRunCfg* cfg, mjbSt
   const int form = cfg ? cfg->fused : MJB_FORM_CHOSEN;
   if (form == MJB_FORM_PLAIN) return run_forward_plain(m, d, s);
   if (form == MJB_FORM_SINGLE) return run_fused(m, d, cfg, 0, s);
+  if (form == MJB_FORM_PRECISION) {
+    if (m->nv > 32 || m->is_sparse) return MJB_ERR_UNSUPPORTED;
+    MjbModel mp = *m;
+    mp.precision = 1;
+    return run_chosen(&mp, d, 0, s);
+  }
   if (form != MJB_FORM_CHOSEN) return MJB_ERR_ARG;
   return run_chosen(m, d, 0, s);
 }
@@ -701,6 +721,12 @@ int mjb_step(const MjbModel* m, const MjbData* d, const MjbRunCfg* cfg, mjbStrea
     return launch_stage<S_CHECK>(m, d, s);
   }
   if (form == MJB_FORM_SINGLE) return run_fused(m, d, cfg, 1, s);
+  if (form == MJB_FORM_PRECISION) {
+    if (m->nv > 32 || m->is_sparse) return MJB_ERR_UNSUPPORTED;
+    MjbModel mp = *m;
+    mp.precision = 1;
+    return run_chosen(&mp, d, 1, s);
+  }
   if (form != MJB_FORM_CHOSEN) return MJB_ERR_ARG;
   return run_chosen(m, d, 1, s);
 }

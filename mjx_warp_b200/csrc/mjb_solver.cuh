@@ -516,6 +516,7 @@ struct Small {
   bool factored = false;        // Ls holds the factor of H for the active set factored_mask
   unsigned factored_mask = 0u;
   float *Ms, *Ls, *vs, *F;
+  double* Ld = nullptr;         // precision form: the FP64 factor tile
   const float* J;
   // per-dof registers
   float qacc, Ma, grad, Mgrad, search, mv, qfs, qas, qfc;
@@ -551,10 +552,12 @@ struct Small {
 // otherwise Ls already holds the factor of the same H.  The coefficients come from C
 // (staged rows) or, when C is null, from the rows' active flags and D.  Returns element `lane` of the
 // solution.  Staged Jacobian rows are read as float4 broadcasts.
+template <bool PREC>
 __device__ __noinline__ float newton_direction(const float* Ms, int ld, const float* J, int ldj,
                                                bool staged, const float* C, const int* act,
                                                const float* D, int n, float* Ls, int nv,
-                                               float grad, int lane, bool refactor) {
+                                               float grad, int lane, bool refactor,
+                                               double* Ld = nullptr) {
   const int nq = (nv + 3) >> 2;
   const bool own = lane < nv;
   if (refactor) {
@@ -589,16 +592,33 @@ __device__ __noinline__ float newton_direction(const float* Ms, int ld, const fl
           if (j < nv) h[j] += a * Jr[j];
       }
     }
-    if (own) {  // the whole row (entries above the diagonal are never read)
-      float4* row = reinterpret_cast<float4*>(Ls + lane * ld);
+    if (PREC) {  // precision form: the FP32-assembled row, factored and solved in FP64
+      if (own)
 #pragma unroll
-      for (int q = 0; q < 8; q++)
-        if (q < nq) row[q] = make_float4(h[4 * q], h[4 * q + 1], h[4 * q + 2], h[4 * q + 3]);
+        for (int j = 0; j < 32; j++)
+          if (j < nv) Ld[lane * ld + j] = h[j];
+      __syncwarp();
+      chol_tile_d(Ld, ld, nv, lane);
+    } else {
+      if (own) {  // the whole row (entries above the diagonal are never read)
+        float4* row = reinterpret_cast<float4*>(Ls + lane * ld);
+#pragma unroll
+        for (int q = 0; q < 8; q++)
+          if (q < nq) row[q] = make_float4(h[4 * q], h[4 * q + 1], h[4 * q + 2], h[4 * q + 3]);
+      }
+      __syncwarp();
+      chol_tile(Ls, ld, nv, lane);
     }
-    __syncwarp();
-    chol_tile(Ls, ld, nv, lane);
   }
+  if (PREC) return float(cho_solve_tile_d(Ld, ld, nv, double(grad), lane));
   return cho_solve_tile(Ls, ld, nv, grad, lane);
+}
+
+// Line-search coefficient sums across the warp: base + sum of x, accumulated in FP64 in the
+// precision form.
+__device__ __forceinline__ float ls_sum(float base, float x, bool prec) {
+  if (prec) return float(double(base) + warp_sum_d(double(x)));
+  return base + warp_sum(x);
 }
 
 // solver.py:75-173
@@ -644,6 +664,7 @@ __device__ void small_update_constraint(Small& s) {
 }
 
 // solver.py:176-312
+template <bool PREC>
 __device__ void small_update_gradient(Small& s) {
   const MjbModel& m = s.m;
   const MjbData& d = s.d;
@@ -672,18 +693,20 @@ __device__ void small_update_gradient(Small& s) {
     if (lane < s.n) s.F[lane] = s.ract ? s.rD : 0.f;
     __syncwarp();
   }
-  s.Mgrad = newton_direction(s.Ms, s.ld, s.J, s.ldj, staged, staged ? s.F : nullptr,
+  s.Mgrad = newton_direction<PREC>(s.Ms, s.ld, s.J, s.ldj, staged, staged ? s.F : nullptr,
                              d.efc_active + s.adr, d.efc_D + s.adr, s.n, s.Ls, nv, s.grad, lane,
-                             refactor);
+                             refactor, s.Ld);
   s.factored = true;
   s.factored_mask = mask;
 }
 
 // solver.py:737-869
+template <bool PREC>
 __device__ void small_linesearch(Small& s) {
   const MjbModel& m = s.m;
   const MjbData& d = s.d;
   const int nv = s.nv, lane = s.lane;
+  constexpr bool prec = PREC;
   // f(Jaref, jv, quad0, quad1, quad2) for each of this lane's rows (registers when staged)
   auto rows = [&](auto&& f) {
     if (s.staged) {
@@ -701,9 +724,9 @@ __device__ void small_linesearch(Small& s) {
     float q0 = s.own ? s.gauss / float(nv) : 0.f;
     float q1 = s.own ? s.search * (s.Ma - s.qfs) : 0.f;
     float q2 = s.own ? 0.5f * s.search * s.mv : 0.f;
-    s.qg[0] = warp_sum(q0);
-    s.qg[1] = warp_sum(q1);
-    s.qg[2] = warp_sum(q2);
+    s.qg[0] = ls_sum(0.f, q0, prec);
+    s.qg[1] = ls_sum(0.f, q1, prec);
+    s.qg[2] = ls_sum(0.f, q2, prec);
   }
   s.publish(s.search);
   if (s.staged) {
@@ -745,9 +768,9 @@ __device__ void small_linesearch(Small& s) {
           t2 += q2;
         }
       });
-      t0 = warp_sum(t0) + s.qg[0];
-      t1 = warp_sum(t1) + s.qg[1];
-      t2 = warp_sum(t2) + s.qg[2];
+      t0 = ls_sum(s.qg[0], t0, prec);
+      t1 = ls_sum(s.qg[1], t1, prec);
+      t2 = ls_sum(s.qg[2], t2, prec);
       const float cost = a * a * t2 + a * t1 + t0;
       if (c == 0 || cost < bestc) {
         bestc = cost;
@@ -767,9 +790,9 @@ __device__ void small_linesearch(Small& s) {
         a1 += q1;
         a2 += 2.f * q2;
       });
-      p0[0] = s.qg[0] + warp_sum(a0);
-      p0[1] = s.qg[1] + warp_sum(a1);
-      p0[2] = 2.f * s.qg[2] + warp_sum(a2);
+      p0[0] = ls_sum(s.qg[0], a0, prec);
+      p0[1] = ls_sum(s.qg[1], a1, prec);
+      p0[2] = ls_sum(2.f * s.qg[2], a2, prec);
     }
     auto totals = [&](int na, const float* al, float (*out)[3]) {
       float acc[3][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
@@ -788,9 +811,9 @@ __device__ void small_linesearch(Small& s) {
       for (int t = 0; t < na; t++) {
         float g[3];
         eval_pt3(s.qg, al[t], g);
-        out[t][0] = g[0] + warp_sum(acc[t][0]);
-        out[t][1] = g[1] + warp_sum(acc[t][1]);
-        out[t][2] = g[2] + warp_sum(acc[t][2]);
+        out[t][0] = ls_sum(g[0], acc[t][0], prec);
+        out[t][1] = ls_sum(g[1], acc[t][1], prec);
+        out[t][2] = ls_sum(g[2], acc[t][2], prec);
       }
     };
     float lo_alpha = -safe_div(p0[1], p0[2]);
@@ -854,6 +877,9 @@ __device__ void small_linesearch(Small& s) {
 }
 
 // solver.py:872-1000 for nv <= 32; sm: solver_smem_floats(nv) floats of warp-private scratch
+// PREC: the precision form (FP64 Hessian factor-solve and line-search sums; the double tile at
+// sm + solver_smem_floats(nv))
+template <bool PREC = false>
 __device__ void solve_small(const MjbModel& m, const MjbData& d, int w, int lane, float* sm,
                             bool reuse) {
   const int nv = m.nv;
@@ -864,6 +890,7 @@ __device__ void solve_small(const MjbModel& m, const MjbData& d, int w, int lane
   s.ld = tile_ld(nv);
   s.nq = (nv + 3) >> 2;
   s.Ls = sm;
+  if (PREC) s.Ld = reinterpret_cast<double*>(sm + solver_smem_floats(nv));
   float* Js = sm + tile_floats(nv);
   s.Ms = Js + kSolverRows * s.ld;
   s.vs = s.Ms + tile_floats(nv);
@@ -907,17 +934,17 @@ __device__ void solve_small(const MjbModel& m, const MjbData& d, int w, int lane
   __syncwarp();
   s.Ma = s.mulM(s.qacc);
   small_update_constraint(s);
-  small_update_gradient(s);
+  small_update_gradient<PREC>(s);
   s.search = -s.Mgrad;
   s.search_dot = warp_sum(s.search * s.search);
   bool done = false;
   float beta = 0.f, prev_grad = 0.f, prev_Mgrad = 0.f;
   for (int it = 0; it < m.iterations && !done; it++) {
-    small_linesearch(s);
+    small_linesearch<PREC>(s);
     prev_grad = s.grad;
     prev_Mgrad = s.Mgrad;
     small_update_constraint(s);
-    small_update_gradient(s);
+    small_update_gradient<PREC>(s);
     if (m.solver == 1) {  // Polak-Ribiere (solver.py:918-970)
       const float num = warp_sum(s.own ? s.grad * (s.Mgrad - prev_Mgrad) : 0.f);
       const float den = warp_sum(s.own ? prev_grad * prev_Mgrad : 0.f);
@@ -968,9 +995,10 @@ __device__ void solve_small(const MjbModel& m, const MjbData& d, int w, int lane
 // reuse: keep the Newton Hessian's factor across iterations with an unchanged active set.
 // For nv > 32 or a sparse mass matrix, sm (when given) is the generic solver's scratch of at least
 // generic_nz_floats(nv) floats.
+template <bool PREC = false>
 __device__ __forceinline__ void solve(const MjbModel& m, const MjbData& d, int w, int lane,
                                       float* sm, float* hs, bool reuse = false) {
-  if (m.nv <= 32 && sm && !m.is_sparse) solve_small(m, d, w, lane, sm, reuse);
+  if (m.nv <= 32 && sm && !m.is_sparse) solve_small<PREC>(m, d, w, lane, sm, reuse);
   else solve_generic(m, d, w, lane, hs, (m.nv > 32 || m.is_sparse) ? sm : nullptr, reuse);
 }
 

@@ -570,6 +570,50 @@ __device__ MJB_TILE_FN float cho_solve_tile(const float* L, int ld, int n, float
   return own ? x : 0.f;
 }
 
+// FP64 counterparts of chol_tile / cho_solve_tile for the precision form (MJB_FORM_PRECISION):
+// the same lane-per-row scheme on a tile of doubles (row stride ld doubles), with the pivot from
+// the double square root and division.
+__device__ __noinline__ void chol_tile_d(double* A, int ld, int n, int lane) {
+  for (int k = 0; k < n; k++) {
+    const double* Ai = A + min(k + lane, n - 1) * ld;
+    const double* Ak = A + k * ld;
+    double s0 = 0.0, s1 = 0.0;
+    int m = 0;
+    for (; m + 1 < k; m += 2) {
+      s0 += Ai[m] * Ak[m];
+      s1 += Ai[m + 1] * Ak[m + 1];
+    }
+    if (m < k) s0 += Ai[m] * Ak[m];
+    const double s = Ai[k] - (s0 + s1);
+    const double lkk = sqrt(__shfl_sync(WARP_FULL, s, 0));
+    __syncwarp();
+    if (lane == 0) A[k * ld + k] = lkk;
+    else if (k + lane < n) A[(k + lane) * ld + k] = s / lkk;
+    __syncwarp();
+  }
+}
+__device__ __noinline__ double cho_solve_tile_d(const double* L, int ld, int n, double y, int lane) {
+  const bool own = lane < n;
+  const double* Li = L + min(lane, n - 1) * ld;
+  const double dd = own ? Li[lane] : 1.0;
+  double z = own ? y : 0.0;
+  for (int k = 0; k < n; k++) {
+    const double zk = __shfl_sync(WARP_FULL, z, k) / __shfl_sync(WARP_FULL, dd, k);
+    if (lane == k) z = zk;
+    else if (lane > k && own) z -= Li[k] * zk;
+  }
+  double x = z;
+  for (int k = n - 1; k >= 0; k--) {
+    const double lk = L[k * ld + (lane < k ? lane : 0)];
+    const double xk = __shfl_sync(WARP_FULL, x, k) / __shfl_sync(WARP_FULL, dd, k);
+    if (lane == k) x = xk;
+    else if (lane < k) x -= lk * xk;
+  }
+  return own ? x : 0.0;
+}
+// Floats of per-warp scratch the precision form adds for its double tile.
+__host__ __device__ __forceinline__ int prec_tile_floats(int nv) { return 2 * tile_floats(nv); }
+
 // Copies the lower triangle of an n <= 32 tile to L (leading dimension ld) with zeros above the
 // diagonal, one coalesced row at a time.
 __device__ __forceinline__ void tile_store_lower(const float* T, int tld, int n, float* L, int ld, int lane) {
@@ -769,6 +813,28 @@ __device__ void solve_blocks(const MjbModel& m, const float* L, float* x, const 
     } else {
       warp_cho_solve(L + a * nv + a, nv, n, x + a, y + a, lane);
     }
+  }
+}
+
+// x = (M + scale diag(dadd))^-1 y per tree block, factored and solved in FP64 in the double tile
+// dt (precision form; blocks of n <= 32, dense M with leading dimension nv).
+__device__ void factor_solve_blocks_d(const MjbModel& m, const float* M, const float* dadd,
+                                      float scale, float* x, const float* y, int lane, double* dt) {
+  const int nv = m.nv, ld = tile_ld(nv);
+  for (int blk = 0; blk < m.nblock; blk++) {
+    const int a = m.block_adr[blk], n = m.block_size[blk];
+    for (int r = 0; r < n; r++)
+      if (lane < n) {
+        double v = M[(a + r) * nv + a + lane];
+        if (dadd && lane == r) v += double(scale) * double(dadd[a + r]);
+        dt[r * ld + lane] = v;
+      }
+    __syncwarp();
+    chol_tile_d(dt, ld, n, lane);
+    const double xi = cho_solve_tile_d(dt, ld, n, lane < n ? double(y[a + lane]) : 0.0, lane);
+    __syncwarp();
+    if (lane < n) x[a + lane] = float(xi);
+    __syncwarp();
   }
 }
 
@@ -1077,6 +1143,11 @@ __device__ void fwd_acceleration(const MjbModel& m, const MjbData& d, int w, int
   for (int i = lane; i < nv; i += 32) sm[i] = pas[i] - bias[i] + act[i] + app[i];
   __syncwarp();
   xfrc_accumulate(m, d, w, sm, lane);
+  if (m.precision && tile) {  // FP64 factor-solve in the double tile after the float tile
+    factor_solve_blocks_d(m, d.qM + W(w, nv * nv), nullptr, 0.f, d.qacc_smooth + W(w, nv), sm, lane,
+                          reinterpret_cast<double*>(tile + tile_floats(nv)));
+    return;
+  }
   solve_m_world(m, d, w, d.qacc_smooth + W(w, nv), sm, lane, tile, tile_has_qLD);
 }
 
@@ -1140,7 +1211,11 @@ __device__ void euler(const MjbModel& m, const MjbData& d, int w, int lane, floa
   factor_blocks(m, d.qM + W(w, nv * nv), L, lane, m.dof_damping, m.timestep, tile);
   for (int i = lane; i < nv; i += 32) x[i] = sm[i] + qc[i];
   __syncwarp();
-  solve_blocks(m, L, x, x, lane, tile, true);
+  if (m.precision && tile)  // the float factor stays in qLD_integration; x in FP64
+    factor_solve_blocks_d(m, d.qM + W(w, nv * nv), m.dof_damping, m.timestep, x, x, lane,
+                          reinterpret_cast<double*>(tile + tile_floats(nv)));
+  else
+    solve_blocks(m, L, x, x, lane, tile, true);
   advance(m, d, w, x, lane);
 }
 
@@ -1209,6 +1284,9 @@ __device__ void implicit(const MjbModel& m, const MjbData& d, int w, int lane, f
     factor_blocks(m, Mi, L, lane, nullptr, 0.f, tile);
     solve_blocks(m, L, x, f, lane);
   }
+  if (m.precision && tile)  // the float factor stays in qLD_integration; x again in FP64
+    factor_solve_blocks_d(m, Mi, nullptr, 0.f, x, f, lane,
+                          reinterpret_cast<double*>(tile + tile_floats(nv)));
   advance(m, d, w, x, lane);
 }
 
