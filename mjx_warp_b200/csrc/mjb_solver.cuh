@@ -537,9 +537,10 @@ struct Small {
     vs[lane] = own ? v : 0.f;
     __syncwarp();
   }
+  template <bool ST>
   __device__ __forceinline__ float rowdot(int k) const {
     const float* Jr = J + size_t(k) * ldj;
-    if (staged) return dotq(Jr, vs, nq);
+    if (ST) return dotq(Jr, vs, nq);
     float s = 0.f;
     for (int j = 0; j < nv; j++) s += Jr[j] * vs[j];
     return s;
@@ -552,9 +553,9 @@ struct Small {
 // otherwise Ls already holds the factor of the same H.  The coefficients come from C
 // (staged rows) or, when C is null, from the rows' active flags and D.  Returns element `lane` of the
 // solution.  Staged Jacobian rows are read as float4 broadcasts.
-template <bool PREC>
+template <bool PREC, bool ST>
 __device__ __noinline__ float newton_direction(const float* Ms, int ld, const float* J, int ldj,
-                                               bool staged, const float* C, const int* act,
+                                               const float* C, const int* act,
                                                const float* D, int n, float* Ls, int nv,
                                                float grad, int lane, bool refactor,
                                                double* Ld = nullptr) {
@@ -576,7 +577,7 @@ __device__ __noinline__ float newton_direction(const float* Ms, int ld, const fl
       if (c == 0.f) continue;
       const float* Jr = J + size_t(k) * ldj;
       const float a = own ? c * Jr[lane] : 0.f;
-      if (staged) {  // zero-padded, 16-byte aligned rows
+      if (ST) {  // zero-padded, 16-byte aligned rows
         const float4* J4 = reinterpret_cast<const float4*>(Jr);
 #pragma unroll
         for (int q = 0; q < 8; q++) {
@@ -622,11 +623,12 @@ __device__ __forceinline__ float ls_sum(float base, float x, bool prec) {
 }
 
 // solver.py:75-173
+template <bool ST>
 __device__ void small_update_constraint(Small& s) {
   const MjbData& d = s.d;
   s.prev_cost = s.cost;
   float c = 0.f;
-  if (s.staged) {
+  if (ST) {
     if (s.lane < s.n) {
       const int r = s.adr + s.lane;
       const float Jaref = s.rJaref, D = s.rD;
@@ -664,7 +666,7 @@ __device__ void small_update_constraint(Small& s) {
 }
 
 // solver.py:176-312
-template <bool PREC>
+template <bool PREC, bool ST>
 __device__ void small_update_gradient(Small& s) {
   const MjbModel& m = s.m;
   const MjbData& d = s.d;
@@ -685,7 +687,7 @@ __device__ void small_update_gradient(Small& s) {
   // the previous call is kept (bit-identical) while the set of active rows is unchanged; rows
   // past the first 32 are not tracked, so such worlds refactor every time.  Without s.reuse every
   // call refactors, as the reference does.
-  const bool staged = s.staged;  // unstaged rows keep F in efc_force, which must survive
+  constexpr bool staged = ST;  // unstaged rows keep F in efc_force, which must survive
   const unsigned mask = __ballot_sync(
       WARP_FULL, lane < s.n && (staged ? s.ract != 0 : d.efc_active[s.adr + lane] != 0));
   const bool refactor = !s.reuse || !s.factored || s.n > 32 || mask != s.factored_mask;
@@ -693,7 +695,7 @@ __device__ void small_update_gradient(Small& s) {
     if (lane < s.n) s.F[lane] = s.ract ? s.rD : 0.f;
     __syncwarp();
   }
-  s.Mgrad = newton_direction<PREC>(s.Ms, s.ld, s.J, s.ldj, staged, staged ? s.F : nullptr,
+  s.Mgrad = newton_direction<PREC, ST>(s.Ms, s.ld, s.J, s.ldj, staged ? s.F : nullptr,
                              d.efc_active + s.adr, d.efc_D + s.adr, s.n, s.Ls, nv, s.grad, lane,
                              refactor, s.Ld);
   s.factored = true;
@@ -701,7 +703,7 @@ __device__ void small_update_gradient(Small& s) {
 }
 
 // solver.py:737-869
-template <bool PREC>
+template <bool PREC, bool ST>
 __device__ void small_linesearch(Small& s) {
   const MjbModel& m = s.m;
   const MjbData& d = s.d;
@@ -709,7 +711,7 @@ __device__ void small_linesearch(Small& s) {
   constexpr bool prec = PREC;
   // f(Jaref, jv, quad0, quad1, quad2) for each of this lane's rows (registers when staged)
   auto rows = [&](auto&& f) {
-    if (s.staged) {
+    if (ST) {
       if (lane < s.n) f(s.rJaref, s.rjv, s.rq0, s.rq1, s.rq2);
     } else {
       for (int k = lane; k < s.n; k += 32) {
@@ -729,10 +731,10 @@ __device__ void small_linesearch(Small& s) {
     s.qg[2] = ls_sum(0.f, q2, prec);
   }
   s.publish(s.search);
-  if (s.staged) {
+  if (ST) {
     if (lane < s.n) {
       const int r = s.adr + lane;
-      const float jv = s.rowdot(lane);
+      const float jv = s.template rowdot<ST>(lane);
       const float Jaref = s.rJaref, D = s.rD;
       s.rjv = jv;
       s.rq0 = 0.5f * Jaref * Jaref * D;
@@ -746,7 +748,7 @@ __device__ void small_linesearch(Small& s) {
   } else {
     for (int k = lane; k < s.n; k += 32) {
       const int r = s.adr + k;
-      const float jv = s.rowdot(k);
+      const float jv = s.template rowdot<ST>(k);
       const float Jaref = d.efc_Jaref[r], D = d.efc_D[r];
       d.efc_jv[r] = jv;
       d.efc_quad[3 * r] = 0.5f * Jaref * Jaref * D;
@@ -865,13 +867,91 @@ __device__ void small_linesearch(Small& s) {
     s.qacc += s.alpha * s.search;
     s.Ma += s.alpha * s.mv;
   }
-  if (s.staged) {
+  if (ST) {
     if (lane < s.n) {
       s.rJaref += s.alpha * s.rjv;
       d.efc_Jaref[s.adr + lane] = s.rJaref;
     }
   } else {
     for (int k = lane; k < s.n; k += 32) d.efc_Jaref[s.adr + k] += s.alpha * d.efc_jv[s.adr + k];
+  }
+  __syncwarp();
+}
+
+// The iterations of solve_small once the world's rows are placed; ST: rows staged in shared
+// memory (n <= kSolverRows), a compile-time choice so that each path's code is straight.
+template <bool PREC, bool ST>
+__device__ void solve_small_run(Small& s) {
+  const MjbModel& m = s.m;
+  const MjbData& d = s.d;
+  const int nv = s.nv, lane = s.lane, w = s.w, adr = s.adr, n = s.n;
+  // _create_context (solver.py:26-72)
+  s.cost = __int_as_float(0x7f800000);
+  s.publish(s.qacc);
+  if (ST) {
+    if (lane < n) {
+      s.rD = d.efc_D[adr + lane];
+      s.rJaref = s.template rowdot<ST>(lane) - d.efc_aref[adr + lane];
+      d.efc_Jaref[adr + lane] = s.rJaref;
+    }
+  } else {
+    for (int k = lane; k < n; k += 32) d.efc_Jaref[adr + k] = s.template rowdot<ST>(k) - d.efc_aref[adr + k];
+  }
+  __syncwarp();
+  s.Ma = s.mulM(s.qacc);
+  small_update_constraint<ST>(s);
+  small_update_gradient<PREC, ST>(s);
+  s.search = -s.Mgrad;
+  s.search_dot = warp_sum(s.search * s.search);
+  bool done = false;
+  float beta = 0.f, prev_grad = 0.f, prev_Mgrad = 0.f;
+  for (int it = 0; it < m.iterations && !done; it++) {
+    small_linesearch<PREC, ST>(s);
+    prev_grad = s.grad;
+    prev_Mgrad = s.Mgrad;
+    small_update_constraint<ST>(s);
+    small_update_gradient<PREC, ST>(s);
+    if (m.solver == 1) {  // Polak-Ribiere (solver.py:918-970)
+      const float num = warp_sum(s.own ? s.grad * (s.Mgrad - prev_Mgrad) : 0.f);
+      const float den = warp_sum(s.own ? prev_grad * prev_Mgrad : 0.f);
+      beta = fmaxf(0.f, num / fmaxf(kMinVal, den));
+    }
+    float v = -s.Mgrad;
+    if (m.solver == 1) v += beta * s.search;
+    s.search = s.own ? v : 0.f;
+    s.search_dot = warp_sum(s.search * s.search);
+    const float scale = m.meaninertia * float(max(1, nv));
+    done = (s.prev_cost - s.cost) / scale < m.tolerance || sqrtf(s.grad_dot) / scale < m.tolerance;
+  }
+  if (s.own) {
+    const size_t o = W(w, nv) + lane;
+    d.qacc[o] = s.qacc;
+    d.qacc_warmstart[o] = s.qacc;
+    d.qfrc_constraint[o] = s.qfc;
+    d.efc_Ma[o] = s.Ma;
+    d.efc_grad[o] = s.grad;
+    d.efc_Mgrad[o] = s.Mgrad;
+    d.efc_search[o] = s.search;
+    d.efc_mv[o] = s.mv;
+    if (d.efc_prev_grad) d.efc_prev_grad[o] = prev_grad;
+    if (d.efc_prev_Mgrad) d.efc_prev_Mgrad[o] = prev_Mgrad;
+  }
+  if (lane == 0) {
+    if (d.efc_cost) d.efc_cost[w] = s.cost;
+    if (d.efc_prev_cost) d.efc_prev_cost[w] = s.prev_cost;
+    if (d.efc_gauss) d.efc_gauss[w] = s.gauss;
+    if (d.efc_grad_dot) d.efc_grad_dot[w] = s.grad_dot;
+    if (d.efc_search_dot) d.efc_search_dot[w] = s.search_dot;
+    if (d.efc_gtol) d.efc_gtol[w] = s.gtol;
+    if (d.efc_alpha) d.efc_alpha[w] = s.alpha;
+    if (d.efc_beta) d.efc_beta[w] = beta;
+    if (d.efc_done) d.efc_done[w] = done ? 1 : 0;
+    if (d.efc_solver_niter) d.efc_solver_niter[w] = 0;
+    if (d.efc_quad_gauss) {
+      d.efc_quad_gauss[3 * w] = s.qg[0];
+      d.efc_quad_gauss[3 * w + 1] = s.qg[1];
+      d.efc_quad_gauss[3 * w + 2] = s.qg[2];
+    }
   }
   __syncwarp();
 }
@@ -919,75 +999,8 @@ __device__ void solve_small(const MjbModel& m, const MjbData& d, int w, int lane
   s.gtol = 0.f;
   s.qg[0] = s.qg[1] = s.qg[2] = 0.f;
   __syncwarp();
-  // _create_context (solver.py:26-72)
-  s.cost = __int_as_float(0x7f800000);
-  s.publish(s.qacc);
-  if (s.staged) {
-    if (lane < n) {
-      s.rD = d.efc_D[adr + lane];
-      s.rJaref = s.rowdot(lane) - d.efc_aref[adr + lane];
-      d.efc_Jaref[adr + lane] = s.rJaref;
-    }
-  } else {
-    for (int k = lane; k < n; k += 32) d.efc_Jaref[adr + k] = s.rowdot(k) - d.efc_aref[adr + k];
-  }
-  __syncwarp();
-  s.Ma = s.mulM(s.qacc);
-  small_update_constraint(s);
-  small_update_gradient<PREC>(s);
-  s.search = -s.Mgrad;
-  s.search_dot = warp_sum(s.search * s.search);
-  bool done = false;
-  float beta = 0.f, prev_grad = 0.f, prev_Mgrad = 0.f;
-  for (int it = 0; it < m.iterations && !done; it++) {
-    small_linesearch<PREC>(s);
-    prev_grad = s.grad;
-    prev_Mgrad = s.Mgrad;
-    small_update_constraint(s);
-    small_update_gradient<PREC>(s);
-    if (m.solver == 1) {  // Polak-Ribiere (solver.py:918-970)
-      const float num = warp_sum(s.own ? s.grad * (s.Mgrad - prev_Mgrad) : 0.f);
-      const float den = warp_sum(s.own ? prev_grad * prev_Mgrad : 0.f);
-      beta = fmaxf(0.f, num / fmaxf(kMinVal, den));
-    }
-    float v = -s.Mgrad;
-    if (m.solver == 1) v += beta * s.search;
-    s.search = s.own ? v : 0.f;
-    s.search_dot = warp_sum(s.search * s.search);
-    const float scale = m.meaninertia * float(max(1, nv));
-    done = (s.prev_cost - s.cost) / scale < m.tolerance || sqrtf(s.grad_dot) / scale < m.tolerance;
-  }
-  if (s.own) {
-    const size_t o = W(w, nv) + lane;
-    d.qacc[o] = s.qacc;
-    d.qacc_warmstart[o] = s.qacc;
-    d.qfrc_constraint[o] = s.qfc;
-    d.efc_Ma[o] = s.Ma;
-    d.efc_grad[o] = s.grad;
-    d.efc_Mgrad[o] = s.Mgrad;
-    d.efc_search[o] = s.search;
-    d.efc_mv[o] = s.mv;
-    if (d.efc_prev_grad) d.efc_prev_grad[o] = prev_grad;
-    if (d.efc_prev_Mgrad) d.efc_prev_Mgrad[o] = prev_Mgrad;
-  }
-  if (lane == 0) {
-    if (d.efc_cost) d.efc_cost[w] = s.cost;
-    if (d.efc_prev_cost) d.efc_prev_cost[w] = s.prev_cost;
-    if (d.efc_gauss) d.efc_gauss[w] = s.gauss;
-    if (d.efc_grad_dot) d.efc_grad_dot[w] = s.grad_dot;
-    if (d.efc_search_dot) d.efc_search_dot[w] = s.search_dot;
-    if (d.efc_gtol) d.efc_gtol[w] = s.gtol;
-    if (d.efc_alpha) d.efc_alpha[w] = s.alpha;
-    if (d.efc_beta) d.efc_beta[w] = beta;
-    if (d.efc_done) d.efc_done[w] = done ? 1 : 0;
-    if (d.efc_solver_niter) d.efc_solver_niter[w] = 0;
-    if (d.efc_quad_gauss) {
-      d.efc_quad_gauss[3 * w] = s.qg[0];
-      d.efc_quad_gauss[3 * w + 1] = s.qg[1];
-      d.efc_quad_gauss[3 * w + 2] = s.qg[2];
-    }
-  }
-  __syncwarp();
+  if (s.staged) solve_small_run<PREC, true>(s);
+  else solve_small_run<PREC, false>(s);
 }
 
 // Dispatch: the register / shared-memory solver when nv <= 32 and the caller provides its scratch
