@@ -22,9 +22,10 @@
 #include "mjb_solver.cuh"
 
 // minimum resident CTAs per SM requested for the solver kernels (caps registers per thread at
-// 65536 / (128 * MJB_MINB)); 5 measured fastest: 4 leaves occupancy on the table, 6 spills
+// 65536 / (128 * MJB_MINB)); with the staged / unstaged solver paths compiled apart, 4 (128
+// registers) measured 2 % faster than 5 (96 registers, spilling) on the humanoid at 8192 worlds
 #ifndef MJB_MINB
-#define MJB_MINB 5
+#define MJB_MINB 4
 #endif
 // lanes per world in the chosen form's tree-recursion stage kernels (8, 16 or 32; 16 measured
 // fastest for the humanoid: phase 0 290 us vs 306 at 8 and 323 at 32)
