@@ -666,14 +666,14 @@ __device__ void small_update_constraint(Small& s) {
 }
 
 // solver.py:176-312
-template <bool PREC, bool ST>
+template <bool PREC, bool ST, bool CG>
 __device__ void small_update_gradient(Small& s) {
   const MjbModel& m = s.m;
   const MjbData& d = s.d;
   const int nv = s.nv, lane = s.lane;
   s.grad = s.own ? s.Ma - s.qfs - s.qfc : 0.f;
   s.grad_dot = warp_sum(s.grad * s.grad);
-  if (m.solver == 1) {  // CG: Mgrad = M^-1 grad with the qLD factor
+  if (CG) {  // CG: Mgrad = M^-1 grad with the qLD factor
     float* gg = d.efc_grad + W(s.w, nv);
     float* mg = d.efc_Mgrad + W(s.w, nv);
     if (s.own) gg[lane] = s.grad;
@@ -703,7 +703,7 @@ __device__ void small_update_gradient(Small& s) {
 }
 
 // solver.py:737-869
-template <bool PREC, bool ST>
+template <bool PREC, bool ST, bool LSP>
 __device__ void small_linesearch(Small& s) {
   const MjbModel& m = s.m;
   const MjbData& d = s.d;
@@ -757,7 +757,7 @@ __device__ void small_linesearch(Small& s) {
     }
   }
   __syncwarp();
-  if (m.ls_parallel) {
+  if (LSP) {
     int best = 0;
     float bestc = 0.f;
     for (int c = 0; c < m.nlsp; c++) {
@@ -878,9 +878,10 @@ __device__ void small_linesearch(Small& s) {
   __syncwarp();
 }
 
-// The iterations of solve_small once the world's rows are placed; ST: rows staged in shared
-// memory (n <= kSolverRows), a compile-time choice so that each path's code is straight.
-template <bool PREC, bool ST>
+// The iterations of solve_small once the world's rows are placed.  ST: rows staged in shared
+// memory (n <= kSolverRows); CG: the CG solver (else Newton); LSP: the parallel line search (else
+// the iterative one) -- compile-time choices, so that each path's code is straight.
+template <bool PREC, bool ST, bool CG, bool LSP>
 __device__ void solve_small_run(Small& s) {
   const MjbModel& m = s.m;
   const MjbData& d = s.d;
@@ -900,24 +901,24 @@ __device__ void solve_small_run(Small& s) {
   __syncwarp();
   s.Ma = s.mulM(s.qacc);
   small_update_constraint<ST>(s);
-  small_update_gradient<PREC, ST>(s);
+  small_update_gradient<PREC, ST, CG>(s);
   s.search = -s.Mgrad;
   s.search_dot = warp_sum(s.search * s.search);
   bool done = false;
   float beta = 0.f, prev_grad = 0.f, prev_Mgrad = 0.f;
   for (int it = 0; it < m.iterations && !done; it++) {
-    small_linesearch<PREC, ST>(s);
+    small_linesearch<PREC, ST, LSP>(s);
     prev_grad = s.grad;
     prev_Mgrad = s.Mgrad;
     small_update_constraint<ST>(s);
-    small_update_gradient<PREC, ST>(s);
-    if (m.solver == 1) {  // Polak-Ribiere (solver.py:918-970)
+    small_update_gradient<PREC, ST, CG>(s);
+    if (CG) {  // Polak-Ribiere (solver.py:918-970)
       const float num = warp_sum(s.own ? s.grad * (s.Mgrad - prev_Mgrad) : 0.f);
       const float den = warp_sum(s.own ? prev_grad * prev_Mgrad : 0.f);
       beta = fmaxf(0.f, num / fmaxf(kMinVal, den));
     }
     float v = -s.Mgrad;
-    if (m.solver == 1) v += beta * s.search;
+    if (CG) v += beta * s.search;
     s.search = s.own ? v : 0.f;
     s.search_dot = warp_sum(s.search * s.search);
     const float scale = m.meaninertia * float(max(1, nv));
@@ -999,8 +1000,18 @@ __device__ void solve_small(const MjbModel& m, const MjbData& d, int w, int lane
   s.gtol = 0.f;
   s.qg[0] = s.qg[1] = s.qg[2] = 0.f;
   __syncwarp();
-  if (s.staged) solve_small_run<PREC, true>(s);
-  else solve_small_run<PREC, false>(s);
+  const bool cg = m.solver == 1, lsp = m.ls_parallel != 0;
+  if (s.staged) {
+    if (!cg && !lsp) solve_small_run<PREC, true, false, false>(s);
+    else if (!cg) solve_small_run<PREC, true, false, true>(s);
+    else if (!lsp) solve_small_run<PREC, true, true, false>(s);
+    else solve_small_run<PREC, true, true, true>(s);
+  } else {
+    if (!cg && !lsp) solve_small_run<PREC, false, false, false>(s);
+    else if (!cg) solve_small_run<PREC, false, false, true>(s);
+    else if (!lsp) solve_small_run<PREC, false, true, false>(s);
+    else solve_small_run<PREC, false, true, true>(s);
+  }
 }
 
 // Dispatch: the register / shared-memory solver when nv <= 32 and the caller provides its scratch
