@@ -349,7 +349,7 @@ def _combined(mjw, torch, nworld=32768, horizon=16, checkpoint=4, reps=2):
           "forward_ms": fwd * 1e3, "backward_ms": bwd * 1e3,
           "peak_gpu_memory_gb": peak / 1e9, "worlds_with_finite_grads": nok,
           "worlds_flagged": int((status != 0).sum()),
-          "precision": "FP32 throughout (the 3xTF32 / FP64 precision form is not built)"}
+          "precision": "FP32 throughout (the precision form covers nv <= 32)"}
 
 
 def _graph_steps_per_s(torch, step, nworld, steps, barrier, restore):
