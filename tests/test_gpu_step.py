@@ -240,3 +240,35 @@ def test_autotune_picks_a_setting_and_keeps_results():
     mjw.step(m, d2)
   torch.cuda.synchronize()
   assert torch.equal(d1.qpos, d2.qpos) and torch.equal(d1.qvel, d2.qvel)
+
+
+def test_humanoid_drift_forms_vs_fp64():
+  """Configuration 2's drift comparison: 64 humanoid worlds at the benchmark settings
+  (implicitfast, Newton 3 iterations / ls 4) stepped 1000 times in the plain, chosen and precision
+  forms next to the FP64 oracle; relative qpos error per world at steps 10, 100 and 1000.  The
+  3-iteration step is chaotic (an unconverged iterate's jumps grow), so only early tracking is
+  asserted.  Measured on a B200 (median / p90): step 10 plain and chosen 1.4e-3 / 1.5e-2
+  (identical trajectories), precision 8.2e-4 / 1.7e-2; step 100 about 0.3 / 0.5 for all three;
+  step 1000 about 0.4 / 0.8 -- decorrelated, with or without FP64 factor-solves."""
+  mjm = humanoid()
+  nworld = 64
+  qpos, qvel, ctrl = humanoid_state(mjm, nworld, seed=11)
+  m = mjw.put_model(mjm)
+  o = oracle(mjm, qpos, qvel, ctrl, 64)
+  ds = {f: device_data(mjm, qpos, qvel, ctrl) for f in (0, 1, 3)}
+  marks, done, report = (10, 100, 1000), 0, {}
+  for mark in marks:
+    for f, d in ds.items():
+      for _ in range(mark - done):
+        mjw.step(m, d, fused=f)
+    o.run("step", nstep=mark - done)
+    done = mark
+    torch.cuda.synchronize()
+    ref = o.get("qpos")
+    for f, d in ds.items():
+      e = rel_err(dev(d.qpos), ref)
+      e = np.where(np.isfinite(e), e, np.inf)
+      report[(f, mark)] = (float(np.median(e)), float(np.quantile(e, 0.9)))
+  print("drift (form, step): (median, p90)", report)
+  for f in (0, 1, 3):
+    assert report[(f, 10)][0] < 1e-2, report
