@@ -1115,6 +1115,10 @@ __device__ void xfrc_accumulate(const MjbModel& m, const MjbData& d, int w, floa
   const float* xipos = d.xipos + W(w, 3 * nb);
   const float* sc = d.subtree_com + W(w, 3 * nb);
   const float* xfrc = d.xfrc_applied + W(w, 6 * nb);
+  // a world with no applied body force adds only zeros (for finite states): skip its walk
+  bool any = false;
+  for (int e = lane; e < 6 * nb; e += 32) any |= xfrc[e] != 0.f;
+  if (!__any_sync(WARP_FULL, any)) return;
   for (int i = lane; i < nv; i += 32) {
     const s6 c = ld6(cdof + 6 * i);
     const f3 rot{c.v[0], c.v[1], c.v[2]}, lin{c.v[3], c.v[4], c.v[5]};
