@@ -979,8 +979,7 @@ __device__ void solve_small(const MjbModel& m, const MjbData& d, int w, int lane
   const int ncol = 4 * s.nq;  // staged columns: nv, zero padded to a multiple of 4
   const float* Jg = d.efc_J + size_t(adr) * nv;
   if (n <= kSolverRows) {
-    for (int r = 0; r < n; r++)  // rows zero padded for float4 reads
-      if (lane < ncol) Js[r * s.ld + lane] = lane < nv ? Jg[size_t(r) * nv + lane] : 0.f;
+    copy_rows(Jg, nv, Js, s.ld, n, nv, ncol, lane);  // rows zero padded for float4 reads
     s.J = Js;
     s.ldj = s.ld;
     s.staged = true;
@@ -991,8 +990,7 @@ __device__ void solve_small(const MjbModel& m, const MjbData& d, int w, int lane
     s.F = d.efc_force + adr;  // rows beyond the staged capacity broadcast through global memory
   }
   const float* qMg = d.qM + W(w, nv * nv);
-  for (int i = 0; i < nv; i++)
-    if (lane < ncol) s.Ms[i * s.ld + lane] = lane < nv ? qMg[i * nv + lane] : 0.f;
+  copy_rows(qMg, nv, s.Ms, s.ld, nv, nv, ncol, lane);
   s.qacc = s.own ? d.qacc_warmstart[W(w, nv) + lane] : 0.f;
   s.qfs = s.own ? d.qfrc_smooth[W(w, nv) + lane] : 0.f;
   s.qas = s.own ? d.qacc_smooth[W(w, nv) + lane] : 0.f;

@@ -507,6 +507,23 @@ __host__ __device__ __forceinline__ int tile_floats(int nv) {
   return (nv < 32 ? nv : 32) * tile_ld(nv);
 }
 
+// Copies an nrows x ncols block (ncols <= 32; lane = column) from src (row stride sld) to dst (row
+// stride dld), writing lanes [ncols, pad) as zero.  Eight rows are loaded before they are stored,
+// so the loads overlap: row-by-row copies wait out each load, because dst (shared memory reached
+// through a generic pointer) may alias src as far as the compiler can tell.
+__device__ __forceinline__ void copy_rows(const float* src, int sld, float* dst, int dld, int nrows,
+                                          int ncols, int pad, int lane) {
+  for (int r0 = 0; r0 < nrows; r0 += 8) {
+    float v[8];
+#pragma unroll
+    for (int t = 0; t < 8; t++)
+      v[t] = (r0 + t < nrows && lane < ncols) ? src[size_t(r0 + t) * sld + lane] : 0.f;
+#pragma unroll
+    for (int t = 0; t < 8; t++)
+      if (r0 + t < nrows && lane < pad) dst[size_t(r0 + t) * dld + lane] = v[t];
+  }
+}
+
 // In-place Cholesky of an n x n (n <= 32) SPD tile with row stride ld (lower triangle): the
 // partial sums of chol_lower with float4 row reads; the pivot and its reciprocal come from one
 // rsqrtf (within 2 ulp of the correctly rounded sqrt and reciprocal).
@@ -748,18 +765,21 @@ __device__ void warp_cho_solve(const float* L, int ld, int n, float* x, const fl
 __device__ void factor_blocks(const MjbModel& m, const float* M, float* L, int lane,
                               const float* dadd = nullptr, float scale = 0.f, float* tile = nullptr) {
   const int nv = m.nv;
-  for (int e = lane; e < nv * nv; e += 32) L[e] = 0.f;
-  __syncwarp();
+  // one tiled block covering every dof is written whole by tile_store_lower
+  if (!(tile && m.nblock == 1 && nv <= 32)) {
+    for (int e = lane; e < nv * nv; e += 32) L[e] = 0.f;
+    __syncwarp();
+  }
   for (int blk = 0; blk < m.nblock; blk++) {
     const int a = m.block_adr[blk], n = m.block_size[blk];
     if (tile && n <= 32) {
       const int tld = tile_ld(nv);
-      for (int r = 0; r < n; r++) {  // coalesced row reads of the block
-        if (lane < n) {
-          float v = M[(a + r) * nv + a + lane];
-          if (dadd && lane == r) v += scale * dadd[a + r];
-          tile[r * tld + lane] = v;
-        }
+      copy_rows(M + a * nv + a, nv, tile, tld, n, n, n, lane);  // coalesced row reads of the block
+      __syncwarp();
+      if (dadd && lane < n) {
+        float v = tile[lane * tld + lane];
+        v += scale * dadd[a + lane];
+        tile[lane * tld + lane] = v;
       }
       __syncwarp();
       chol_tile(tile, tld, n, lane);
@@ -797,8 +817,7 @@ __device__ void solve_blocks(const MjbModel& m, const float* L, float* x, const 
       if (tile) {
         const int tld = tile_ld(nv);
         if (!(tile_has_factor && m.nblock == 1)) {
-          for (int r = 0; r < n; r++)
-            if (lane < n) tile[r * tld + lane] = L[(a + r) * nv + a + lane];
+          copy_rows(L + a * nv + a, nv, tile, tld, n, n, n, lane);
           __syncwarp();
         }
         xi = cho_solve_tile(tile, tld, n, yi, lane);
@@ -1254,12 +1273,24 @@ __device__ void implicit(const MjbModel& m, const MjbData& d, int w, int lane, f
   float* L = d.qLD_integration + W(w, nv * nv);
   float* x = d.qacc_integration + W(w, nv);
   for (int i = lane; i < nv; i += 32) f[i] = sm[i] + qc[i];
-  if (tiled)
+  if (tiled && !(m.nblock == 1 && m.block_size[0] == nv))  // else tile_store_lower writes it all
     for (int e = lane; e < nv * nv; e += 32) L[e] = 0.f;
   __syncwarp();
   // qderiv_actuator_fused_kernel, per tree tile: Mi = qM - dt qDeriv, one coalesced row at a time
   for (int blk = 0; blk < m.nblock; blk++) {
     const int a0 = m.block_adr[blk], n = m.block_size[blk];
+    if (tiled && !act_on) {  // damping only: the block's rows loaded into the tile eight at a time
+      const int tld = tile_ld(nv);
+      copy_rows(qM + a0 * nv + a0, nv, tile, tld, n, n, n, lane);
+      __syncwarp();
+      if (passive_on && lane < n) {
+        const int i = a0 + lane;
+        tile[lane * tld + lane] = tile[lane * tld + lane] - (-m.dof_damping[i]) * m.timestep;
+      }
+      __syncwarp();
+      copy_rows(tile, tld, Mi + a0 * nv + a0, nv, n, n, n, lane);
+      __syncwarp();
+    } else
     for (int r = 0; r < n; r++) {
       const int i = a0 + r;
       for (int jj = lane; jj < n; jj += 32) {
