@@ -342,8 +342,7 @@ __device__ void step_vjp_world(const MjbModel& m, const MjbData& d, int w, int l
   if (nv <= 32) {
     const int ld = tile_ld(nv);
     const bool own = lane < nv;
-    for (int r = 0; r < nv; r++)
-      if (lane < 4 * ((nv + 3) >> 2)) tile[r * ld + lane] = lane < nv ? qM[r * nv + lane] : 0.f;
+    copy_rows(qM, nv, tile, ld, nv, nv, 4 * ((nv + 3) >> 2), lane);
     __syncwarp();
     if (own) {
       float h[32];

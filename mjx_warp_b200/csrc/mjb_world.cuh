@@ -634,8 +634,14 @@ __host__ __device__ __forceinline__ int prec_tile_floats(int nv) { return 2 * ti
 // Copies the lower triangle of an n <= 32 tile to L (leading dimension ld) with zeros above the
 // diagonal, one coalesced row at a time.
 __device__ __forceinline__ void tile_store_lower(const float* T, int tld, int n, float* L, int ld, int lane) {
-  for (int r = 0; r < n; r++)
-    if (lane < n) L[r * ld + lane] = lane <= r ? T[r * tld + lane] : 0.f;
+  for (int r0 = 0; r0 < n; r0 += 8) {  // eight rows read before they are written (see copy_rows)
+    float v[8];
+#pragma unroll
+    for (int t = 0; t < 8; t++) v[t] = (r0 + t < n && lane <= r0 + t) ? T[(r0 + t) * tld + lane] : 0.f;
+#pragma unroll
+    for (int t = 0; t < 8; t++)
+      if (r0 + t < n && lane < n) L[(r0 + t) * ld + lane] = v[t];
+  }
 }
 
 // Right-looking blocked Cholesky of the n x n SPD lower triangle of A (row stride ld, shared or
