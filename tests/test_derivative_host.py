@@ -1,0 +1,58 @@
+"""Host-side logic of the derivatives (no GPU): which models the analytic step adjoint covers, and
+the C entry points' argument checks."""
+
+import ctypes
+
+import numpy as np
+import pytest
+
+import mjx_warp_b200 as mjw
+from helpers import load
+from mjx_warp_b200 import _abi
+
+
+def _expected_qpos_support(mjm):
+  """The adjoint's coverage restated from the model's arrays."""
+  if mjm.na or mjm.opt.jacobian == 1:
+    return False
+  jt, jb = np.asarray(mjm.jnt_type), np.asarray(mjm.jnt_bodyid)
+  nj = np.asarray(mjm.body_jntnum)
+  if any(nj[jb[j]] != 1 for j in range(mjm.njnt) if jt[j] == 1):
+    return False
+  if any(mjm.jnt_stiffness[j] != 0 for j in range(mjm.njnt) if jt[j] in (0, 1)):
+    return False
+  tid = np.asarray(mjm.actuator_trnid).reshape(mjm.nu, -1)[:, 0] if mjm.nu else []
+  if any(jt[t] not in (2, 3) for t in tid):
+    return False
+  gb, wb = np.asarray(mjm.geom_bodyid), np.asarray(mjm.body_weldid)
+  return all(wb[gb[g]] == 0 for g in range(mjm.ngeom) if mjm.geom_type[g] == 0)
+
+
+@pytest.mark.parametrize("name", ["humanoid.xml", "sphere_chain.xml", "pendula.xml", "collision.xml"])
+def test_qpos_vjp_support_follows_model_features(name):
+  mjm = load(name)
+  m = mjw.put_model(mjm, device="cpu")
+  assert mjw.derivative.ctrl_vjp_supported(m)
+  assert mjw.derivative.qpos_vjp_supported(m) == _expected_qpos_support(mjm)
+
+
+def test_adjoint_needs_the_dense_mass_matrix():
+  mjm = load("humanoid.xml", jacobian=1)  # sparse
+  m = mjw.put_model(mjm, device="cpu")
+  assert not mjw.derivative.ctrl_vjp_supported(m)
+  assert not mjw.derivative.qpos_vjp_supported(m)
+
+
+def test_humanoid_is_covered():
+  m = mjw.put_model(load("humanoid.xml"), device="cpu")
+  assert mjw.derivative.qpos_vjp_supported(m)
+
+
+def test_step_vjp_entry_rejects_bad_arguments():
+  lib = _abi.lib()
+  assert lib.mjb_step_vjp(None, None, None, None, None, None, None, None) == 1
+  assert lib.mjb_ctrl_vjp(None, None, None, None, None) == 1
+  mv, dv = _abi.MjbModel(), _abi.MjbData()
+  dv.nworld = 0
+  # an empty batch is a no-op whatever the outputs
+  assert lib.mjb_step_vjp(ctypes.byref(mv), ctypes.byref(dv), None, None, None, None, None, None) == 0
