@@ -352,6 +352,67 @@ def _combined(mjw, torch, nworld=32768, horizon=16, checkpoint=4, reps=2):
           "precision": "FP32 throughout (the precision form covers nv <= 32)"}
 
 
+BIN_MODEL = os.path.join(ROOT, "tests", "golden", "models", "bin.xml")
+
+
+def _bin_state(mjm, nworld, seed):
+  """Bin bodies at x, y ~ U(-0.4, 0.4), z ~ U(0.03, 0.35), random orientations: overlapping
+  packings with many contacts (uneven rows per world)."""
+  rng = np.random.default_rng(seed)
+  qpos = np.tile(mjm.qpos0, (nworld, 1))
+  for b in range(mjm.nbody - 1):
+    a = 7 * b
+    qpos[:, a:a + 2] = rng.uniform(-0.4, 0.4, (nworld, 2))
+    qpos[:, a + 2] = rng.uniform(0.03, 0.35, nworld)
+    q = rng.normal(size=(nworld, 4))
+    qpos[:, a + 3:a + 7] = q / np.linalg.norm(q, axis=1, keepdims=True)
+  return qpos, rng.normal(0.0, 0.1, (nworld, mjm.nv)), np.zeros((nworld, 0))
+
+
+def _larger_models(mjw, torch, reps=3):
+  """ms per step (chosen, plain) of the uneven-contact configurations: the bin (nv = 384, 4096
+  worlds, Newton or CG 10 iterations, dense or sparse mass matrix) and the humanoid with 0-16
+  extra spheres (nv = 123, 32768 worlds, implicitfast, Newton 3 iterations)."""
+  from mjx_warp_b200 import mjcf
+
+  def ms(m, mjm, q, v, u, nconmax, njmax, form):
+    W = q.shape[0]
+    d = mjw.make_data(mjm, W, nconmax=nconmax * W, njmax=njmax * W)
+    d.qpos.copy_(torch.as_tensor(q, dtype=torch.float32))
+    d.qvel.copy_(torch.as_tensor(v, dtype=torch.float32))
+    if mjm.nu:
+      d.ctrl.copy_(torch.as_tensor(u, dtype=torch.float32))
+    mjw.step(m, d, fused=form)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+      mjw.step(m, d, fused=form)
+    e1.record()
+    torch.cuda.synchronize()
+    return round(e0.elapsed_time(e1) / reps, 2)
+
+  out = {}
+  for label, jac, solver in (("bin, Newton, dense", 0, 2), ("bin, CG, dense", 0, 1),
+                             ("bin, Newton, sparse", 1, 2), ("bin, CG, sparse", 1, 1)):
+    mjm = mjcf.from_xml_path(BIN_MODEL)
+    mjm.opt.iterations, mjm.opt.ls_iterations, mjm.opt.jacobian, mjm.opt.solver = 10, 10, jac, solver
+    q, v, u = _bin_state(mjm, 4096, seed=3)
+    m = mjw.put_model(mjm)
+    out[label] = {"nworld": 4096, "ms_per_step_chosen": ms(m, mjm, q, v, u, 600, 512, 1),
+                  "ms_per_step_plain": ms(m, mjm, q, v, u, 600, 512, 0)}
+  hum = mjcf.from_xml_path(MODEL)
+  mjm = mjcf.from_xml_path(SPHERES_MODEL)
+  mjm.opt.integrator, mjm.opt.timestep, mjm.opt.jacobian = 3, 0.005, 0
+  mjm.opt.solver, mjm.opt.iterations, mjm.opt.ls_iterations = 2, 3, 4
+  q, v, u = _spheres_state(mjm, hum, 32768, seed=4)
+  m = mjw.put_model(mjm)
+  out["humanoid + 0-16 spheres, Newton 3"] = {
+      "nworld": 32768, "ms_per_step_chosen": ms(m, mjm, q, v, u, 96, 384, 1),
+      "ms_per_step_plain": ms(m, mjm, q, v, u, 96, 384, 0)}
+  return out
+
+
 def _graph_steps_per_s(torch, step, nworld, steps, barrier, restore):
   g = torch.cuda.CUDAGraph()
   s = torch.cuda.Stream()
@@ -627,9 +688,16 @@ def main():
   p.add_argument("--no-accuracy", action="store_true")
   p.add_argument("--no-grad", action="store_true")
   p.add_argument("--no-combined", action="store_true")
+  p.add_argument("--larger-models", action="store_true",
+                 help="print one JSON line of the uneven-contact configurations' step times instead")
   args = p.parse_args()
   if args.warmup < 3:
     args.warmup = 3
+  if args.larger_models:
+    import torch
+    import mjx_warp_b200 as mjw
+    print(json.dumps({"larger_models": _larger_models(mjw, torch)}))
+    return
   if args.impl == "reference":
     run_reference(args)
   else:
