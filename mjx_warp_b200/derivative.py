@@ -312,14 +312,27 @@ class _Rollout(torch.autograd.Function):
     d.act.zero_()
     d.qacc_warmstart.zero_()
     ckpts = []
+    # with the analytic adjoint the last segment runs through the segment's Data, which keep its
+    # steps for the backward pass (it then skips that segment's recomputation)
+    full = r.analytic == "full"
+    last0 = ((T - 1) // r.checkpoint) * r.checkpoint
+    kept_qvel, cur = [], d
     for t in range(T):
       if t % r.checkpoint == 0:
-        ckpts.append(_snapshot(d))
-      d.ctrl.copy_(ctrl[t])
-      step(m, d, fused=r.fused)
-    ctx.r, ctx.ckpts, ctx.qpos0, ctx.qpos_T = r, ckpts, qpos0.detach(), d.qpos.clone()
+        ckpts.append(_snapshot(cur))
+      if full and t >= last0:
+        dk = r.seg[t - last0]
+        if dk is not cur:
+          _restore(dk, _snapshot_view(cur))
+        cur = dk
+        kept_qvel.append(cur.qvel.clone())
+      cur.ctrl.copy_(ctrl[t])
+      step(m, cur, fused=r.fused)
+    r._generation += 1
+    ctx.generation, ctx.kept_qvel = r._generation, kept_qvel
+    ctx.r, ctx.ckpts, ctx.qpos0, ctx.qpos_T = r, ckpts, qpos0.detach(), cur.qpos.clone()
     ctx.save_for_backward(ctrl)
-    return d.qpos.clone(), d.qvel.clone()
+    return cur.qpos.clone(), cur.qvel.clone()
 
   @staticmethod
   def backward(ctx, gq, gv):
@@ -336,13 +349,17 @@ class _Rollout(torch.autograd.Function):
     for seg in reversed(range(len(ctx.ckpts))):
       t0, t1 = seg * r.checkpoint, min(T, (seg + 1) * r.checkpoint)
       if r.analytic == "full":  # one Data per step of the segment: each is stepped once
-        qvel_prev = []
-        for k, t in enumerate(range(t0, t1)):
-          dk = r.seg[k]
-          _restore(dk, ctx.ckpts[seg] if k == 0 else _snapshot_view(r.seg[k - 1]))
-          qvel_prev.append(dk.qvel.clone())
-          dk.ctrl.copy_(ctrl[t])
-          step(m, dk, fused=r.fused)
+        if seg == len(ctx.ckpts) - 1 and ctx.kept_qvel and ctx.generation == r._generation:
+          qvel_prev = ctx.kept_qvel  # the forward pass left this segment's steps in the Data
+        else:
+          r._generation += 1  # the segment's Data stop holding any forward pass's steps
+          qvel_prev = []
+          for k, t in enumerate(range(t0, t1)):
+            dk = r.seg[k]
+            _restore(dk, ctx.ckpts[seg] if k == 0 else _snapshot_view(r.seg[k - 1]))
+            qvel_prev.append(dk.qvel.clone())
+            dk.ctrl.copy_(ctrl[t])
+            step(m, dk, fused=r.fused)
         for k in reversed(range(t1 - t0)):
           gq, gv, grad_ctrl[t0 + k] = step_vjp(m, r.seg[k], qvel_prev[k], lam)
           lam = torch.cat([gq, gv], 1)
@@ -406,6 +423,7 @@ class Rollout:
     if analytic == "full" and not qpos_vjp_supported(m):
       raise NotImplementedError("analytic qpos adjoint: the model has a feature it does not cover")
     self.analytic = analytic
+    self._generation = 0  # bumped whenever the segment's Data are stepped
     # the backward of the analytic adjoint keeps every step of a segment in its own Data (the
     # forward pass runs in the first of them)
     self.seg = _segment_ring(mjm, nworld, nconmax * nworld, njmax * nworld,

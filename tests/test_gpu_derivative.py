@@ -394,3 +394,34 @@ def test_rollout_gradient_standing_vs_fp64_central_fd():
   scale = max(abs(c[1]) for c in checks)
   for g, f in checks:
     assert abs(g - f) <= 1e-2 * abs(f) + 2e-3 * scale, checks
+
+
+def test_rollout_backward_after_another_forward():
+  """The analytic rollout keeps its last segment's steps from the forward pass; a second forward
+  pass through the same Rollout before the first one's backward must not leak into it: the
+  gradients equal those of a lone forward + backward."""
+  mjm = humanoid()
+  nworld, T = 4, 6
+  qpos, qvel, _ = humanoid_state(mjm, nworld, seed=12)
+  rng = np.random.default_rng(13)
+  c1 = rng.uniform(-0.4, 0.4, (T, nworld, mjm.nu))
+  c2 = rng.uniform(-0.4, 0.4, (T, nworld, mjm.nu))
+  m = mjw.put_model(mjm)
+  roll = mjw.derivative.Rollout(mjm, m, nworld, checkpoint=4, analytic="full")
+  q0 = torch.tensor(qpos, dtype=torch.float32, device="cuda")
+  v0 = torch.tensor(qvel, dtype=torch.float32, device="cuda")
+
+  def grads(interleave):
+    u = torch.tensor(c1, dtype=torch.float32, device="cuda", requires_grad=True)
+    q = q0.clone().requires_grad_(True)
+    qT, vT = roll(q, v0, u)
+    if interleave:  # another rollout through the same workspace before the backward
+      roll(q0, v0, torch.tensor(c2, dtype=torch.float32, device="cuda"))
+    ((qT[:, :3] ** 2).sum() + (vT ** 2).sum()).backward()
+    return u.grad.clone(), q.grad.clone()
+
+  ua, qa = grads(False)
+  ub, qb = grads(True)
+  assert torch.isfinite(ua).all() and ua.abs().max() > 0
+  torch.testing.assert_close(ub, ua, rtol=1e-5, atol=1e-7)
+  torch.testing.assert_close(qb, qa, rtol=1e-5, atol=1e-7)
