@@ -366,9 +366,10 @@ __device__ void step_vjp_world(const MjbModel& m, const MjbData& d, int w, int l
   } else {
     // the Newton solver (generic path) leaves the factor of H at the final active set in efc_h:
     // its iterations end with update_gradient, which factors H in place (or keeps the factor
-    // while the active set is unchanged); CG has no H, so it is assembled and factored here
+    // while the active set is unchanged); CG has no H, and without constraint capacity
+    // (njmax = 0) the solver does not run, so there H is assembled and factored here
     float* H = d.efc_h + W(w, nv * nv);
-    if (m.solver != 2) {
+    if (m.solver != 2 || d.njmax == 0) {
       assemble_hessian(m, d, qM, H, adr, n, tile, lane);
       chol_any(H, nv, nv, lane, tile);
     }
