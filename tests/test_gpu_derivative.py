@@ -425,3 +425,34 @@ def test_rollout_backward_after_another_forward():
   assert torch.isfinite(ua).all() and ua.abs().max() > 0
   torch.testing.assert_close(ub, ua, rtol=1e-5, atol=1e-7)
   torch.testing.assert_close(qb, qa, rtol=1e-5, atol=1e-7)
+
+
+def test_step_vjp_without_constraint_capacity():
+  """nv = 123 (the Hessian outside the warp tile): a step without constraint capacity
+  (njmax = 0, the solver does not run) and a step with constraints disabled (the solver runs on
+  no rows) have the same dynamics, so the adjoint -- which reuses the solver's factor only when
+  the solver ran -- must agree between them."""
+  from test_gpu_configs import humanoid_spheres_state
+  nworld = 8
+  out = []
+  for case in ("njmax0", "disabled"):
+    mjm = load("humanoid_spheres.xml", integrator=3, timestep=0.005, iterations=10,
+               ls_iterations=10, jacobian=0)
+    if case == "disabled":
+      mjm.opt.disableflags |= 1  # DSBL_CONSTRAINT
+    qpos, qvel, ctrl, _ = humanoid_spheres_state(mjm, load("humanoid.xml"), nworld, seed=9)
+    m = mjw.put_model(mjm)
+    d = mjw.make_data(mjm, nworld, nconmax=96 * nworld,
+                      njmax=0 if case == "njmax0" else 256 * nworld)
+    d.qpos.copy_(torch.as_tensor(qpos, dtype=torch.float32))
+    d.qvel.copy_(torch.as_tensor(qvel, dtype=torch.float32))
+    d.ctrl.copy_(torch.as_tensor(ctrl, dtype=torch.float32))
+    lam = torch.as_tensor(np.random.default_rng(10).normal(size=(nworld, 2 * mjm.nv)),
+                          dtype=torch.float32, device="cuda")
+    qvel_prev = d.qvel.clone()
+    mjw.step(m, d)
+    out.append([g.clone() for g in mjw.derivative.step_vjp(m, d, qvel_prev, lam)])
+  torch.cuda.synchronize()
+  for a, b in zip(*out):
+    assert torch.isfinite(a).all()
+    torch.testing.assert_close(a, b, rtol=1e-4, atol=1e-5)
