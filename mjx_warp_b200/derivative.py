@@ -302,6 +302,54 @@ def _restore(d: Data, s) -> None:
     getattr(d, k).copy_(v)
 
 
+def _backward_analytic(ctx, r, m, ctrl, lam, grad_ctrl):
+  """The analytic backward over a rollout's segments, last to first: each segment's steps are
+  recomputed once from its checkpoint into a ring of Data (the last segment's are kept from the
+  forward pass when nothing stepped the ring since) and step_vjp runs back through them.  With a
+  second ring and a side stream, the next segment's recomputation runs while the current segment's
+  adjoint steps do."""
+  T = ctrl.shape[0]
+  bounds = lambda sg: (sg * r.checkpoint, min(T, (sg + 1) * r.checkpoint))
+
+  def recompute(sg, ring, qbuf):
+    t0, t1 = bounds(sg)
+    for k, t in enumerate(range(t0, t1)):
+      dk = ring[k]
+      _restore(dk, ctx.ckpts[sg] if k == 0 else _snapshot_view(ring[k - 1]))
+      qbuf[k].copy_(dk.qvel)
+      dk.ctrl.copy_(ctrl[t])
+      step(m, dk, fused=r.fused)
+
+  kept = bool(ctx.kept_qvel) and ctx.generation == r._generation
+  r._generation += 1  # the rings stop holding any forward pass's steps
+  segs = list(reversed(range(len(ctx.ckpts))))
+  overlap = bool(r.seg2)
+  rings = [r.seg, r.seg2] if overlap else [r.seg, r.seg]
+  main = torch.cuda.current_stream()
+  ready = None  # the side stream's recomputation of the segment about to be differentiated
+  for i, sg in enumerate(segs):
+    ring, qbuf = rings[i % 2], r.qbuf[i % 2]
+    if i == 0 and kept:
+      qv = ctx.kept_qvel
+    elif i == 0 or not overlap:
+      recompute(sg, ring, qbuf)
+      qv = qbuf
+    else:
+      main.wait_event(ready)
+      qv = qbuf
+    if overlap and i + 1 < len(segs):  # after the previous segment's adjoint steps, not this one's
+      r.side.wait_stream(main)
+      with torch.cuda.stream(r.side):
+        recompute(segs[i + 1], rings[(i + 1) % 2], r.qbuf[(i + 1) % 2])
+        ready = torch.cuda.Event()
+        ready.record(r.side)
+    t0, t1 = bounds(sg)
+    for k in reversed(range(t1 - t0)):
+      gq, gv, grad_ctrl[t0 + k] = step_vjp(m, ring[k], qv[k], lam)
+      lam = torch.cat([gq, gv], 1)
+  return lam
+
+
 class _Rollout(torch.autograd.Function):
   @staticmethod
   def forward(ctx, qpos0, qvel0, ctrl, r):
@@ -346,24 +394,11 @@ class _Rollout(torch.autograd.Function):
     if gv is not None:
       lam[:, nv:2 * nv] = gv.float()
     grad_ctrl = torch.zeros_like(ctrl)
-    for seg in reversed(range(len(ctx.ckpts))):
+    if r.analytic == "full":
+      lam = _backward_analytic(ctx, r, m, ctrl, lam, grad_ctrl)
+    # the finite-difference paths, segment by segment
+    for seg in ([] if r.analytic == "full" else reversed(range(len(ctx.ckpts)))):
       t0, t1 = seg * r.checkpoint, min(T, (seg + 1) * r.checkpoint)
-      if r.analytic == "full":  # one Data per step of the segment: each is stepped once
-        if seg == len(ctx.ckpts) - 1 and ctx.kept_qvel and ctx.generation == r._generation:
-          qvel_prev = ctx.kept_qvel  # the forward pass left this segment's steps in the Data
-        else:
-          r._generation += 1  # the segment's Data stop holding any forward pass's steps
-          qvel_prev = []
-          for k, t in enumerate(range(t0, t1)):
-            dk = r.seg[k]
-            _restore(dk, ctx.ckpts[seg] if k == 0 else _snapshot_view(r.seg[k - 1]))
-            qvel_prev.append(dk.qvel.clone())
-            dk.ctrl.copy_(ctrl[t])
-            step(m, dk, fused=r.fused)
-        for k in reversed(range(t1 - t0)):
-          gq, gv, grad_ctrl[t0 + k] = step_vjp(m, r.seg[k], qvel_prev[k], lam)
-          lam = torch.cat([gq, gv], 1)
-        continue
       _restore(d, ctx.ckpts[seg])
       states = []
       for t in range(t0, t1):  # recompute the segment's states from its checkpoint
@@ -400,7 +435,9 @@ class Rollout:
   Calling it returns (qpos_T, qvel_T); gradients flow to qpos0 (per qpos coordinate), qvel0 and
   ctrl through finite-difference transition Jacobians (TransitionFD), with the forward states
   checkpointed every `checkpoint` steps and recomputed segment by segment in the backward pass.
-  Each rollout starts from zero act and qacc_warmstart.  `analytic` picks which columns of the
+  Each rollout starts from zero act and qacc_warmstart.  With the analytic adjoint and `overlap`
+  (default: nworld <= 4096) the backward recomputes the next segment on a side stream, into a
+  second ring of Data, while it differentiates the current one.  `analytic` picks which columns of the
   transition Jacobian are not differenced: "full" (the default where qpos_vjp_supported) takes
   every column from step_vjp, "qvel_ctrl" (the default where only ctrl_vjp_supported) takes the
   velocity and control parts from step_vjp and differences the nv qpos columns,
@@ -410,7 +447,7 @@ class Rollout:
 
   def __init__(self, mjm, m: Model, nworld: int, checkpoint: int = 8, eps: float = 1e-3,
                centered: bool = True, nconmax: int = 64, njmax: int = 128, fused=True,
-               analytic: Optional[str] = None):
+               analytic: Optional[str] = None, overlap: Optional[bool] = None):
     self.m, self.checkpoint, self.fused = m, int(checkpoint), fused
     if analytic is None:
       analytic = ("full" if qpos_vjp_supported(m) else
@@ -430,6 +467,15 @@ class Rollout:
                              self.checkpoint) if analytic == "full" else []
     self.d = self.seg[0] if self.seg else make_data(mjm, nworld, nconmax=nconmax * nworld,
                                                      njmax=njmax * nworld)
+    # a second ring lets the backward recompute one segment while it differentiates another:
+    # by default for batches small enough to leave the GPU idle (up to 4096 worlds)
+    if overlap is None:
+      overlap = nworld <= 4096
+    self.seg2 = _segment_ring(mjm, nworld, nconmax * nworld, njmax * nworld,
+                              self.checkpoint) if (analytic == "full" and overlap) else []
+    self.side = torch.cuda.Stream(device=self.d.qpos.device) if self.seg2 else None
+    self.qbuf = [[torch.empty((nworld, m.nv), dtype=torch.float32, device=self.d.qpos.device)
+                  for _ in range(self.checkpoint)] for _ in range(2)] if self.seg else []
     self.fd = None if analytic == "full" else TransitionFD(
         mjm, m, nworld, eps=eps, centered=centered, nconmax=nconmax, njmax=njmax, fused=fused,
         state_only=analytic == "ctrl", qpos_only=analytic == "qvel_ctrl")

@@ -456,3 +456,26 @@ def test_step_vjp_without_constraint_capacity():
   for a, b in zip(*out):
     assert torch.isfinite(a).all()
     torch.testing.assert_close(a, b, rtol=1e-4, atol=1e-5)
+
+
+def test_rollout_overlapped_backward_matches_serial():
+  """The analytic backward recomputing the next segment on a side stream (two rings of Data)
+  gives the same gradients as the serial one, over three segments."""
+  mjm = humanoid()
+  nworld, T = 4, 12
+  qpos, qvel, _ = humanoid_state(mjm, nworld, seed=14)
+  ctrl = np.random.default_rng(15).uniform(-0.4, 0.4, (T, nworld, mjm.nu))
+  m = mjw.put_model(mjm)
+  grads = []
+  for overlap in (False, True):
+    roll = mjw.derivative.Rollout(mjm, m, nworld, checkpoint=4, analytic="full", overlap=overlap)
+    assert bool(roll.seg2) == overlap
+    u = torch.tensor(ctrl, dtype=torch.float32, device="cuda", requires_grad=True)
+    q = torch.tensor(qpos, dtype=torch.float32, device="cuda", requires_grad=True)
+    v = torch.tensor(qvel, dtype=torch.float32, device="cuda", requires_grad=True)
+    qT, vT = roll(q, v, u)
+    ((qT[:, :3] ** 2).sum() + (vT ** 2).sum()).backward()
+    grads.append((u.grad.clone(), q.grad.clone(), v.grad.clone()))
+  for a, b in zip(*grads):
+    assert torch.isfinite(a).all()
+    torch.testing.assert_close(b, a, rtol=1e-5, atol=1e-7)
