@@ -554,7 +554,7 @@ struct Small {
 // (staged rows) or, when C is null, from the rows' active flags and D.  Returns element `lane` of the
 // solution.  Staged Jacobian rows are read as float4 broadcasts.
 template <bool PREC, bool ST>
-__device__ __noinline__ float newton_direction(const float* Ms, int ld, const float* J, int ldj,
+__device__ __forceinline__ float newton_direction(const float* Ms, int ld, const float* J, int ldj,
                                                const float* C, const int* act,
                                                const float* D, int n, float* Ls, int nv,
                                                float grad, int lane, bool refactor,
