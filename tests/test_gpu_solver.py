@@ -1,6 +1,6 @@
 """Constraint solver on the GPU vs the oracle (solver_test.py).
 
-Parity is judged where the problem is well posed: with enough Newton iterations the solve
+Parity is checked where the problem is well posed: with enough Newton iterations the solve
 converges and qacc must agree with the FP64 oracle to 1e-3 relative in every world (the measured
 maximum is ~7e-5).  At the benchmark's 3 iterations the iterate is not converged and depends
 discontinuously on its inputs (FP32 vs FP64 inputs alone move it by up to ~1e-1 in a few worlds),
