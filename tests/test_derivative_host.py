@@ -56,3 +56,24 @@ def test_step_vjp_entry_rejects_bad_arguments():
   dv.nworld = 0
   # an empty batch is a no-op whatever the outputs
   assert lib.mjb_step_vjp(ctypes.byref(mv), ctypes.byref(dv), None, None, None, None, None, None) == 0
+
+
+def test_segment_ring_shares_only_scratch():
+  """The analytic rollout's per-step Data share the fields a step writes before it reads them and
+  the adjoint never reads; everything the adjoint reads stays per step."""
+  from mjx_warp_b200 import derivative
+  mjm = load("humanoid.xml")
+  ring = derivative._segment_ring(mjm, 2, 2 * 48, 2 * 80, 3)
+  a, b = ring[0], ring[2]
+  for name in derivative._RING_SHARED:
+    if getattr(a, name, None) is not None:
+      assert getattr(a, name) is getattr(b, name), name
+  for name in derivative._RING_SHARED_EFC:
+    assert getattr(a.efc, name) is getattr(b.efc, name), name
+  for name in ("qpos", "qvel", "qM", "qLD_integration", "qacc", "qacc_integration", "cdof",
+               "cinert", "cvel", "xpos", "xmat", "geom_xpos", "subtree_com", "actuator_moment"):
+    assert getattr(a, name).data_ptr() != getattr(b, name).data_ptr(), name
+  for name in ("h", "J", "D", "Jaref", "active", "pos", "margin"):
+    assert getattr(a.efc, name).data_ptr() != getattr(b.efc, name).data_ptr(), name
+  for name in ("pos", "frame", "dist", "geom"):
+    assert getattr(a.contact, name).data_ptr() != getattr(b.contact, name).data_ptr(), name
