@@ -267,19 +267,26 @@ int mjb_ctrl_vjp(const MjbModel* m, const MjbData* d, const float* lam, float* g
 int mjb_transition_vjp(const MjbModel* m, int nworld, const float* A, const float* B,
                        const float* lam, float* lam_out, float* grad_ctrl, mjbStream stream);
 
+/* FMA throughput probe (no counterpart in the reference; a measurement aid for the solver's
+ * flop-bound roofline): `blocks` CTAs of 256 threads, each thread running 8 independent FP32
+ * (fp64 = 0) or FP64 FMA chains of `iters` steps, writing one value per thread to sink
+ * (blocks * 256 floats or doubles).  The caller times it: flops = 2 * 8 * iters * blocks * 256. */
+int mjb_fma_probe(int fp64, int blocks, int iters, void* sink, mjbStream stream);
+
 /* Allocation-free variant of mjb_implicit, with no counterpart in the reference.  For callers
  * that may not allocate device memory when they step (a plugin that receives only its operand
  * buffers, a control loop that cannot afford cudaMalloc's synchronisation): the integrator's
- * three per-world work arrays (qM_integration, qLD_integration, qfrc_integration) come from a
- * 64 MiB array compiled into the library instead of from MjbData, so those three fields may be
- * null.  Inputs and outputs are as for mjb_implicit: qM, qfrc_smooth, qfrc_constraint,
- * actuator_moment, ctrl / act are read; qpos, qvel are advanced; qacc_integration is written.
- * Limit: nworld * (2 * nv * nv + nv) * 4 bytes <= mjb_implicit_noalloc_max_bytes() (64 MiB,
- * e.g. 11298 humanoid worlds at nv = 27); larger requests return MJB_ERR_SCRATCH.  The first call
- * on each device resolves the array's device address (cudaGetSymbolAddress), so make one call per
- * device before capturing a CUDA graph.  All calls share the one array: calls that overlap on the
- * GPU (different streams, or graphs replayed concurrently) race on it.  Nothing in it needs to
- * start at zero: every call writes each element before reading it. */
+ * four per-world work arrays (qM_integration, qLD_integration, qfrc_integration and
+ * act_vel_integration) come from a 64 MiB array compiled into the library instead of from
+ * MjbData, so those four fields may be null.  Inputs and outputs are as for mjb_implicit: qM,
+ * qfrc_smooth, qfrc_constraint, actuator_moment, ctrl / act are read; qpos, qvel are advanced;
+ * qacc_integration is written.
+ * Limit: nworld * (2 * nv * nv + nv + nu) * 4 bytes <= mjb_implicit_noalloc_max_bytes() (64 MiB,
+ * e.g. 11140 humanoid worlds at nv = 27, nu = 21); larger requests return MJB_ERR_SCRATCH.  The
+ * first call on each device resolves the array's device address (cudaGetSymbolAddress), so make
+ * one call per device before capturing a CUDA graph.  All calls share the one array: calls that
+ * overlap on the GPU (different streams, or graphs replayed concurrently) race on it.  Nothing in
+ * it needs to start at zero: every call writes each element before reading it. */
 int mjb_implicit_noalloc(const MjbModel* m, const MjbData* d, mjbStream stream);
 size_t mjb_implicit_noalloc_max_bytes(void);
 

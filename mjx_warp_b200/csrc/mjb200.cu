@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <mutex>
 
 #include "mjb_deriv.cuh"
@@ -857,11 +858,12 @@ int mjb_world_status(const MjbData* d, uint32_t* host_out, mjbStream stream) {
 // Some callers cannot allocate device memory at the point where they step the simulation: a
 // host framework that hands a plugin nothing but its operand buffers (an XLA / JAX custom call
 // without a workspace, for instance), or a real-time control loop that must never pay for
-// cudaMalloc's implicit device synchronisation after start-up.  mjb_implicit needs three
-// per-world work arrays (the damped mass matrix, its Cholesky factor and the right-hand side);
-// this variant takes them from a fixed array that lives in the library itself, so the caller only
-// provides the inputs and outputs it already has: qM, qfrc_smooth, qfrc_constraint, the actuator
-// moments and controls (read), qpos and qvel (advanced in place) and qacc_integration (written).
+// cudaMalloc's implicit device synchronisation after start-up.  mjb_implicit needs four
+// per-world work arrays (the damped mass matrix, its Cholesky factor, the right-hand side and the
+// affine actuators' velocity coefficients); this variant takes them from a fixed array that lives
+// in the library itself, so the caller only provides the inputs and outputs it already has: qM,
+// qfrc_smooth, qfrc_constraint, the actuator moments and controls (read), qpos and qvel (advanced
+// in place) and qacc_integration (written).
 namespace {
 
 constexpr size_t kNoallocScratchBytes = size_t(64) << 20;  // 64 MiB, held by every GPU that loads
@@ -869,19 +871,22 @@ constexpr size_t kNoallocScratchBytes = size_t(64) << 20;  // 64 MiB, held by ev
 __device__ __align__(256) float g_noalloc_scratch[kNoallocScratchBytes / sizeof(float)];
 
 constexpr int kMaxDevices = 64;
-float* g_noalloc_ptr[kMaxDevices] = {};
+std::atomic<float*> g_noalloc_ptr[kMaxDevices] = {};
 
 // Device address of the scratch array on the current device, resolved once per device (the name
 // g_noalloc_scratch in host code is only a host-side stand-in and must never be passed to a kernel).
+// Host threads that race on the first call store the same address.
 int noalloc_scratch(float** out) {
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return MJB_ERR_LAUNCH;
-  if (!g_noalloc_ptr[dev]) {
-    void* p = nullptr;
-    if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return MJB_ERR_LAUNCH;
-    g_noalloc_ptr[dev] = static_cast<float*>(p);
+  float* p = g_noalloc_ptr[dev].load(std::memory_order_acquire);
+  if (!p) {
+    void* a = nullptr;
+    if (cudaGetSymbolAddress(&a, g_noalloc_scratch) != cudaSuccess || !a) return MJB_ERR_LAUNCH;
+    p = static_cast<float*>(a);
+    g_noalloc_ptr[dev].store(p, std::memory_order_release);
   }
-  *out = g_noalloc_ptr[dev];
+  *out = p;
   return MJB_OK;
 }
 
@@ -893,15 +898,16 @@ extern "C" int mjb_implicit_noalloc(const MjbModel* m, const MjbData* d, mjbStre
   int rc = check(m, d);
   if (rc || d->nworld == 0) return rc;
   if (m->is_sparse) return MJB_ERR_UNSUPPORTED;
-  const size_t nv = size_t(m->nv);
-  const size_t need = size_t(d->nworld) * (2 * nv * nv + nv) * sizeof(float);
+  const size_t nv = size_t(m->nv), nu = size_t(m->nu), nw = size_t(d->nworld);
+  const size_t need = nw * (2 * nv * nv + nv + nu) * sizeof(float);
   if (need > kNoallocScratchBytes) return MJB_ERR_SCRATCH;
   float* scratch = nullptr;
   if ((rc = noalloc_scratch(&scratch))) return rc;
   MjbData dd = *d;  // same inputs and outputs, work arrays redirected into the static scratch
   dd.qM_integration = scratch;
-  dd.qLD_integration = scratch + size_t(d->nworld) * nv * nv;
-  dd.qfrc_integration = scratch + 2 * size_t(d->nworld) * nv * nv;
+  dd.qLD_integration = scratch + nw * nv * nv;
+  dd.qfrc_integration = scratch + 2 * nw * nv * nv;
+  dd.act_vel_integration = scratch + nw * (2 * nv * nv + nv);
   return launch_stage<S_IMPLICIT>(m, &dd, (cudaStream_t)stream);
 }
 
@@ -1052,5 +1058,37 @@ extern "C" int mjb_transition_vjp(const MjbModel* m, int nworld, const float* A,
   if (nworld == 0) return MJB_OK;
   k_transition_vjp<<<grid_for(nworld, 4), 128, 0, (cudaStream_t)stream>>>(*m, nworld, A, B, lam,
                                                                           lam_out, grad_ctrl);
+  return finish();
+}
+
+// ------------------------------------------------------------------------------------------
+// FMA throughput probe (no counterpart in the reference): the FP32 / FP64 peak that the solver's
+// flop-bound roofline is measured against.  Every thread runs 8 independent FMA chains of `iters`
+// steps; the caller times the launch with CUDA events: flops = 2 * 8 * iters * threads.
+namespace {
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_fma_probe(int iters, T* sink) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  T a[8];
+#pragma unroll
+  for (int c = 0; c < 8; c++) a[c] = T(1) + T(1e-3) * T(c + (t & 7));
+  const T b = T(0.9999), k = T(1e-4);
+  for (int i = 0; i < iters; i++) {
+#pragma unroll
+    for (int c = 0; c < 8; c++) a[c] = a[c] * b + k;
+  }
+  T s = T(0);
+#pragma unroll
+  for (int c = 0; c < 8; c++) s += a[c];
+  sink[t] = s;
+}
+
+}  // namespace
+
+extern "C" int mjb_fma_probe(int fp64, int blocks, int iters, void* sink, mjbStream stream) {
+  if (blocks <= 0 || iters <= 0 || !sink) return MJB_ERR_ARG;
+  if (fp64) k_fma_probe<double><<<blocks, 256, 0, (cudaStream_t)stream>>>(iters, static_cast<double*>(sink));
+  else k_fma_probe<float><<<blocks, 256, 0, (cudaStream_t)stream>>>(iters, static_cast<float*>(sink));
   return finish();
 }

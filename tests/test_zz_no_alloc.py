@@ -1,10 +1,12 @@
 """mjb_implicit_noalloc: the implicitfast integrator for callers that cannot allocate.
 
 A plugin that only receives its operand buffers, or a control loop that may not call cudaMalloc
-once it runs, cannot provide the integrator's three per-world work arrays.  This entry point keeps
-them in a fixed array inside libmjb200.so instead; the test drives it through the C ABI with
-those three MjbData fields set to null and checks that two calls in a row advance the state
-exactly as mjb_implicit (with caller-provided work arrays) does.
+once it runs, cannot provide the integrator's four per-world work arrays.  This entry point keeps
+them in a fixed array inside libmjb200.so instead; the tests drive it through the C ABI with
+those four MjbData fields set to null and check that two calls in a row advance the state
+exactly as mjb_implicit (with caller-provided work arrays) does: on the motor-driven humanoid
+(damping only) and on the pendula with affine position / velocity actuators, which exercise the
+actuator velocity coefficients as well.
 """
 
 import ctypes
@@ -14,7 +16,7 @@ import pytest
 import torch
 
 import mjx_warp_b200 as mjw
-from helpers import device_data, humanoid, humanoid_state
+from helpers import device_data, generic_state, humanoid, humanoid_state, load
 from mjx_warp_b200 import _abi
 
 pytestmark = pytest.mark.gpu
@@ -35,14 +37,41 @@ def _view_without_work_arrays(d):
   v.qM_integration = None
   v.qLD_integration = None
   v.qfrc_integration = None
+  v.act_vel_integration = None
   return v
 
 
-def test_noalloc_matches_implicit_two_calls():
-  lib = _lib()
+def _affine_pendula():
+  """The pendula with affine gains / biases on the velocity (forward_test.py:148-196's setup)."""
+  rng = np.random.default_rng(0)
+  mjm = load("pendula.xml", integrator=3)
+  mjm.actuator_gainprm[:, 2] = rng.normal(scale=10, size=mjm.nu)
+  mjm.actuator_gaintype[3] = 1
+  mjm.actuator_gaintype[6] = 1
+  mjm.actuator_biastype[0:3] = 1
+  mjm.actuator_biastype[4:6] = 1
+  mjm.actuator_biasprm[0:3, 2] = -1
+  mjm.actuator_biasprm[4:6, 2] = -1
+  mjm.actuator_ctrlrange[3:7] = 10.0
+  mjm.actuator_gear[:] = 1.0
+  nworld = 16
+  qpos, _, _ = generic_state(mjm, nworld, 2)
+  qvel = rng.uniform(-0.01, 0.01, (nworld, mjm.nv))
+  ctrl = rng.normal(scale=10, size=(nworld, mjm.nu))
+  return mjm, qpos, qvel, ctrl
+
+
+def _humanoid():
   mjm = humanoid()
-  nworld = 64
-  qpos, qvel, ctrl = humanoid_state(mjm, nworld, seed=21)
+  qpos, qvel, ctrl = humanoid_state(mjm, 64, seed=21)
+  return mjm, qpos, qvel, ctrl
+
+
+@pytest.mark.parametrize("case", ["humanoid", "affine_pendula"])
+def test_noalloc_matches_implicit_two_calls(case):
+  lib = _lib()
+  mjm, qpos, qvel, ctrl = _humanoid() if case == "humanoid" else _affine_pendula()
+  assert case == "humanoid" or mjw.put_model(mjm).actuator_affine_bias_gain
   m = mjw.put_model(mjm)
   ref = device_data(mjm, qpos, qvel, ctrl)
   na = device_data(mjm, qpos, qvel, ctrl)
@@ -67,7 +96,7 @@ def test_noalloc_rejects_oversize_batch():
   m = mjw.put_model(mjm)
   d = mjw.make_data(mjm, nworld=1)
   v = _view_without_work_arrays(d)
-  per_world = (2 * mjm.nv * mjm.nv + mjm.nv) * 4
+  per_world = (2 * mjm.nv * mjm.nv + mjm.nv + mjm.nu) * 4
   v.nworld = lib.mjb_implicit_noalloc_max_bytes() // per_world + 1
   rc = lib.mjb_implicit_noalloc(ctypes.byref(_abi.model_view(m)), ctypes.byref(v), _abi.stream())
   assert rc == 4  # MJB_ERR_SCRATCH
