@@ -156,36 +156,83 @@ def _solver_bytes(mjm, nworld, nefc):
   return 4 * (nworld * per_world + nefc * per_row)
 
 
+def _solver_flops(nv, rows, iters, ls_iters):
+  """Algorithmic flops of one world's Newton solve, counted from the reference algorithm
+  (solver.py:176-312, 737-869): (1 + I) Hessian assemblies and Cholesky factor-solves and I line
+  searches, with R constraint rows, I Newton and L line-search iterations:
+  (1 + I)(F_H + F_chol) + I(2 F_Mv + 2 F_Jv + F_ls), F_H = R nv (nv + 1) (symmetric J'DJ),
+  F_chol = nv^3 / 3 + 2 nv^2, F_Mv = 2 nv^2, F_Jv = 2 R nv, F_ls = 24 L R."""
+  f_h = rows * nv * (nv + 1)
+  f_chol = nv ** 3 / 3.0 + 2.0 * nv * nv
+  return (1 + iters) * (f_h + f_chol) + iters * (4.0 * nv * nv + 4.0 * rows * nv + 24.0 * ls_iters * rows)
+
+
+def _step_flops(mjm, rows, pairs, contacts):
+  """Algorithmic flops of one world-step: smooth dynamics (~600 per body, 60 per geom), collision
+  (20 per broadphase pair, 150 per contact), constraint assembly (R (6 nv + 40)), the mass-matrix
+  and integrator factor-solves (2 (nv^3 / 3 + 2 nv^2)) and the solve."""
+  nv = mjm.nv
+  return (600.0 * (mjm.nbody - 1) + 60.0 * mjm.ngeom + 20.0 * pairs + 150.0 * contacts
+          + rows * (6.0 * nv + 40.0) + 2.0 * (nv ** 3 / 3.0 + 2.0 * nv * nv)
+          + _solver_flops(nv, rows, mjm.opt.iterations, mjm.opt.ls_iterations))
+
+
+def _fma_peaks(torch):
+  """FP32 and FP64 FMA throughput of this GPU (TFLOP/s), best of 3 launches of mjb_fma_probe
+  (8 independent FMA chains per thread, 8 CTAs of 256 threads per SM), CUDA events."""
+  import ctypes
+
+  from mjx_warp_b200 import _abi
+
+  lib = _abi.lib()
+  lib.mjb_fma_probe.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
+                                ctypes.c_void_p]
+  sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+  blocks = 8 * sms
+  out = {}
+  for name, fp64, iters in (("fp32_tflops", 0, 20000), ("fp64_tflops", 1, 4000)):
+    sink = torch.empty(blocks * 256 * 2, dtype=torch.float64, device="cuda")
+    best = 0.0
+    for _ in range(4):
+      a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+      a.record()
+      _abi.check(lib.mjb_fma_probe(fp64, blocks, iters, sink.data_ptr(), _abi.stream()), "fma_probe")
+      b.record()
+      torch.cuda.synchronize()
+      best = max(best, 2.0 * 8 * iters * blocks * 256 / (a.elapsed_time(b) * 1e-3) / 1e12)
+    out[name] = best
+  return out
+
+
 STATE = ("qpos", "qvel", "act", "ctrl", "qacc_warmstart")
 
 
 def _qacc_error(mjm, m, d, mjw, torch, restore, forms, sample=256):
   """qacc of one forward from the bench state (after the warm-up steps), per launch form, against
-  the FP64 CPU restatement with the same solver settings on the first `sample` worlds:
-  per-world ||qacc - qacc_fp64|| / max(||qacc_fp64||, 1)."""
-  from oracle import Oracle
+  the CPU restatement with the same solver settings on the first `sample` worlds (the oracle, used
+  only as the checker): per-world ||qacc - ref|| / max(||ref||, 1) against its FP64 run and its
+  FP32 run (the stand-in for an FP32 implementation of the reference's algorithm), and each world
+  that misses FP64 by more than 1e-4 classified as within 1e-4 of the FP32 restatement,
+  path-dependent (the FP64 iterate at these iteration counts is itself more than 1e-4 from the
+  converged solution, or an FP32 run of the restatement from inputs within one ulp misses too,
+  or FP64 moves by more than 1e-4 under such input perturbations) or unexplained."""
+  import oracle
 
   restore()
   torch.cuda.synchronize()
   s = min(sample, d.nworld)
   host = {k: getattr(d, k)[:s].double().cpu().numpy() for k in ("qpos", "qvel", "ctrl",
                                                                 "qacc_warmstart")}
-  o = Oracle(mjm, s, 64)
-  for k, v in host.items():
-    o.set(k, v)
-  o.run("forward", nthreads=os.cpu_count() or 1)
-  ref = o.get("qacc")
-  finite = np.all(np.isfinite(ref), axis=1)
-  out = {"vs": "FP64 CPU restatement, same solver settings (3 Newton it / ls 4)",
-         "worlds": int(finite.sum())}
+  refs = oracle.qacc_references(mjm, host["qpos"], host["qvel"], host["ctrl"],
+                                host["qacc_warmstart"], nthreads=os.cpu_count() or 1)
+  out = {"vs": f"CPU restatement (FP64 and FP32), same solver settings "
+               f"({mjm.opt.iterations} Newton it / ls {mjm.opt.ls_iterations}), tol 1e-4",
+         "worlds": s}
   for name, f in forms.items():
     restore()
     mjw.forward(m, d, fused=f)
     q = d.qacc[:s].double().cpu().numpy()
-    e = (np.linalg.norm(q - ref, axis=1) / np.maximum(np.linalg.norm(ref, axis=1), 1.0))[finite]
-    e = np.where(np.isfinite(e), e, np.inf)
-    out[name] = {"median": float(np.median(e)), "p90": float(np.quantile(e, 0.9)),
-                 "max": float(e.max()), "frac_le_1e-4": float(np.mean(e <= 1e-4))}
+    out[name] = oracle.classify_qacc(q, refs)
   restore()
   return out
 
@@ -369,6 +416,108 @@ def _bin_state(mjm, nworld, seed):
   return qpos, rng.normal(0.0, 0.1, (nworld, mjm.nv)), np.zeros((nworld, 0))
 
 
+def _bin_config(mjw, torch, nworld=4096, steps=500, plain_steps=10, sample=16):
+  """The uneven-contact bin (48 spheres + 16 capsules in a 5-plane bin, nv = 384, Euler
+  dt = 0.002, Newton 10 iterations / 10 line-search iterations, dense mass matrix): nworld worlds
+  from seeded overlapping packings, the chosen form autotuned (mjw.autotune) and captured as a
+  CUDA graph, replayed for `steps` steps; the plain one-launch-per-stage form launched eagerly
+  from the same state for `plain_steps` steps.  Non-finite / overflow counts after the run, qacc
+  of one forward from the final state against the FP64 restatement on `sample` worlds, and the
+  solver's flop-bound roofline at the measured rows."""
+  from mjx_warp_b200 import mjcf
+  import oracle
+
+  mjm = mjcf.from_xml_path(BIN_MODEL)
+  mjm.opt.iterations, mjm.opt.ls_iterations, mjm.opt.jacobian = 10, 10, 0
+  q, v, _ = _bin_state(mjm, nworld, seed=3)
+  m = mjw.put_model(mjm)
+  d = mjw.make_data(mjm, nworld, nconmax=600 * nworld, njmax=512 * nworld)
+  d.qpos.copy_(torch.as_tensor(q, dtype=torch.float32))
+  d.qvel.copy_(torch.as_tensor(v, dtype=torch.float32))
+  tune = mjw.autotune(m, d)
+  snap = {k: getattr(d, k).clone() for k in ("qpos", "qvel", "qacc_warmstart")}
+
+  def restore():
+    for k, t in snap.items():
+      getattr(d, k).copy_(t)
+
+  restore()
+  g = torch.cuda.CUDAGraph()
+  st = torch.cuda.Stream()
+  st.wait_stream(torch.cuda.current_stream())
+  with torch.cuda.stream(st):
+    with torch.cuda.graph(g, stream=st):
+      mjw.step(m, d)
+  torch.cuda.current_stream().wait_stream(st)
+  restore()
+  torch.cuda.synchronize()
+  e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+  e0.record()
+  for _ in range(steps):
+    g.replay()
+  e1.record()
+  torch.cuda.synchronize()
+  chosen_s = e0.elapsed_time(e1) * 1e-3
+  del g
+  status = mjw.world_status(d)
+  nefc = int(d.world_nefc.sum())
+  rows = d.world_nefc.cpu().numpy()
+  # one phase-timed step from the final state: the solver's share and its roofline
+  a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+  mjw.step_phase(m, d, 0)
+  a.record()
+  mjw.step_phase(m, d, 1)
+  b.record()
+  mjw.step_phase(m, d, 2)
+  torch.cuda.synchronize()
+  solve_s = a.elapsed_time(b) * 1e-3
+  rows_solve = int(d.world_nefc.sum()) / nworld
+  fma = _fma_peaks(torch)
+  flops = _solver_flops(mjm.nv, rows_solve, mjm.opt.iterations, mjm.opt.ls_iterations) * nworld
+  # qacc of one forward from the final state against FP64 on a sample
+  s = min(sample, nworld)
+  host = {k: getattr(d, k)[:s].double().cpu().numpy() for k in ("qpos", "qvel", "qacc_warmstart")}
+  mjw.forward(m, d)
+  qd = d.qacc[:s].double().cpu().numpy()
+  o = oracle.Oracle(mjm, s, 64)
+  for k, t in host.items():
+    o.set(k, t)
+  o.run("forward", nthreads=os.cpu_count() or 1)
+  e = oracle.rel_err(qd, o.get("qacc"))
+  cost_ok = d.efc.cost[:s].cpu().numpy() <= o.scalar("cost") * 1.025 + 1e-3
+  # the plain form, eager, from the same starting state
+  restore()
+  mjw.step(m, d, fused=False)
+  restore()
+  torch.cuda.synchronize()
+  e0.record()
+  for _ in range(plain_steps):
+    mjw.step(m, d, fused=False)
+  e1.record()
+  torch.cuda.synchronize()
+  plain_s = e0.elapsed_time(e1) * 1e-3
+  return {"workload": "bin: 48 spheres + 16 capsules, nv 384, Euler dt 0.002, Newton 10 it / ls 10, "
+                      "dense mass matrix, seeded overlapping packings",
+          "nworld": nworld, "steps": steps, "autotuned": tune,
+          "chosen": {"steps_per_s": nworld * steps / chosen_s, "ms_per_step": chosen_s / steps * 1e3,
+                     "launch": "one captured CUDA graph per step, replayed"},
+          "plain": {"steps_per_s": nworld * plain_steps / plain_s,
+                    "ms_per_step": plain_s / plain_steps * 1e3, "steps": plain_steps,
+                    "launch": "eager, one launch per stage"},
+          "chosen_vs_plain": plain_s / plain_steps / (chosen_s / steps),
+          "status_after": {"nonfinite_worlds": int(np.count_nonzero(status & 0x8)),
+                           "overflow_worlds": int(np.count_nonzero(status & 0x7))},
+          "rows_per_world": {"mean": nefc / nworld, "min": int(rows.min()), "max": int(rows.max())},
+          "qacc_err_vs_fp64": {"worlds": s, "median": float(np.median(e)), "max": float(e.max()),
+                               "frac_le_1e-4": float(np.mean(e <= 1e-4)),
+                               "cost_within_2.5pct": float(np.mean(cost_ok))},
+          "roofline": {"kernel": "k_solve_cta (+ k_order_worlds)", "kernel_ms": solve_s * 1e3,
+                       "flops_per_launch": flops, "achieved_tflops": flops / solve_s / 1e12,
+                       "peak_tflops": fma["fp32_tflops"],
+                       "frac": flops / solve_s / 1e12 / fma["fp32_tflops"], "bound": "fp32",
+                       "rows_per_world": rows_solve}}
+
+
 def _larger_models(mjw, torch, reps=3):
   """ms per step (chosen, plain) of the uneven-contact configurations: the bin (nv = 384, 4096
   worlds, Newton or CG 10 iterations, dense or sparse mass matrix) and the humanoid with 0-16
@@ -499,6 +648,7 @@ def run_ours(args):
   overflow = int(replicas.sum_over_ranks(int(np.count_nonzero(status & 0x7)), device="cuda"))
   ncon = int(d.world_ncon.sum())
   nefc = int(d.world_nefc.sum())
+  npair = int(d.world_npair.sum())
 
   # end to end through the public API: ctrl in from pinned host memory, qpos / qvel back
   ctrl_h = torch.as_tensor(ctrl, dtype=torch.float32).pin_memory()
@@ -570,6 +720,9 @@ def run_ours(args):
   combined = None
   if rank == 0 and not args.no_combined:
     combined = _combined(mjw, torch)
+  bin_cfg = None
+  if rank == 0 and not args.no_bin:
+    bin_cfg = _bin_config(mjw, torch)
 
   launches_per_step = LAUNCHES[args.form]
   total_worlds = nworld * world_size
@@ -584,6 +737,13 @@ def run_ours(args):
     pass
   hbm = float(peaks.get("hbm_gbs", 6650.0))
   achieved = alg / solve_s / 1e9
+  fma = _fma_peaks(torch)
+  rows = nefc_solve / nworld
+  solver_flops = _solver_flops(mjm.nv, rows, mjm.opt.iterations, mjm.opt.ls_iterations) * nworld
+  flop_rate = solver_flops / solve_s / 1e12
+  t_flop, t_hbm = solver_flops / (fma["fp32_tflops"] * 1e12), alg / (hbm * 1e9)
+  flop_bound = t_flop >= t_hbm
+  step_flops = _step_flops(mjm, nefc / nworld, npair / nworld, ncon / nworld) * nworld
   footprint = sum(_bytes_of(t) for t in list(d.arrays().values()) + list(d.contact.arrays().values())
                   + list(d.efc.arrays().values()))
   traffic = None
@@ -603,12 +763,26 @@ def run_ours(args):
     "e2e": {"value": total_worlds * args.steps / e2e_elapsed, "unit": "steps/s",
             "h2d_bytes_per_step": _bytes_of(ctrl_h), "d2h_bytes_per_step": _bytes_of(out_h)},
     "gpu_launches": launches_per_step * args.steps,
-    "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                 "frac": achieved / hbm, "traffic": traffic,
+    "roofline": {"bound": "fp32" if flop_bound else "hbm",
+                 "achieved": flop_rate if flop_bound else achieved,
+                 "peak": fma["fp32_tflops"] if flop_bound else hbm,
+                 "unit": "TFLOP/s" if flop_bound else "GB/s",
+                 "frac": flop_rate / fma["fp32_tflops"] if flop_bound else achieved / hbm,
+                 "traffic": traffic,
                  "kernel": "k_stage<S_SOLVE> (plain)" if args.form == "plain"
                            else "k_solve_queue (+ k_order_worlds)",
                  "kernel_ms": solve_s * 1e3, "kernel_share_of_step": solve_s / (elapsed / args.steps),
-                 "algorithmic_bytes_per_launch": alg, "peak_source": "measured" if peaks else "fallback",
+                 "flops_per_launch": solver_flops, "algorithmic_bytes_per_launch": alg,
+                 "t_min_us": {"fp32": t_flop * 1e6, "hbm": t_hbm * 1e6},
+                 "hbm": {"achieved_gbs": achieved, "peak_gbs": hbm, "frac": achieved / hbm,
+                         "peak_source": "measured (MEASURED_PEAKS.json)" if peaks else "fallback"},
+                 "fp32": {"achieved_tflops": flop_rate, "peak_tflops": fma["fp32_tflops"],
+                          "frac": flop_rate / fma["fp32_tflops"],
+                          "peak_source": "measured in this run (mjb_fma_probe, FFMA)"},
+                 "fp64_peak_tflops": fma["fp64_tflops"],
+                 "rows_per_world": rows,
+                 "step_flops": step_flops,
+                 "step_achieved_tflops": step_flops / (elapsed / args.steps) / 1e12,
                  "step_algorithmic_bytes": step_alg,
                  "step_achieved_gbs": step_alg / (elapsed / args.steps) / 1e9},
     "forms": forms,
@@ -622,8 +796,11 @@ def run_ours(args):
     line["grad"] = grad
   if combined is not None:
     line["combined"] = combined
+  if bin_cfg is not None:
+    line["bin"] = bin_cfg
   if rank == 0 and not args.no_cpu_baseline:
-    line["cpu_baseline"] = cpu_baseline(mjm, budget_s=args.cpu_seconds)
+    line["cpu_baseline"] = cpu_baseline(mjm, args.steps, args.warmup, budget_s=args.cpu_seconds,
+                                        nworld=nworld)
   del g
   if world_size > 1:
     torch.distributed.barrier()
@@ -632,9 +809,11 @@ def run_ours(args):
     print(json.dumps(line), flush=True)
 
 
-def cpu_baseline(mjm, budget_s=10.0, nworld=1024):
-  """The CPU restatement (FP32, OpenMP over worlds, all host threads) on a bounded sample of
-  the same workload: nworld worlds stepped until about budget_s seconds have elapsed."""
+def cpu_baseline(mjm, steps, warmup, budget_s=10.0, nworld=NWORLD, repeats=3):
+  """The CPU restatement (FP32, OpenMP over worlds, all host threads) on the GPU arm's workload:
+  the same nworld worlds from the same seeded states, `warmup` untimed steps, then up to `steps`
+  timed steps (as many as fit in about budget_s / repeats seconds), repeated `repeats` times from
+  the same post-warm-up state; value = the median world-steps/s, with the repeats' spread."""
   from oracle import Oracle
 
   qpos, qvel, ctrl = _state(mjm, 0, nworld)
@@ -643,14 +822,23 @@ def cpu_baseline(mjm, budget_s=10.0, nworld=1024):
   o.set("qvel", qvel)
   o.set("ctrl", ctrl)
   cores = os.cpu_count() or 1
-  o.run("step", nstep=1, nthreads=cores)  # warm-up
-  steps, t0 = 0, time.perf_counter()
-  while time.perf_counter() - t0 < budget_s:
-    o.run("step", nstep=5, nthreads=cores)
-    steps += 5
-  el = time.perf_counter() - t0
-  return {"value": nworld * steps / el, "unit": "steps/s", "cores": cores, "kind": "port",
-          "sample": f"{nworld} worlds x {steps} steps ({el:.1f} s), FP32 CPU restatement"}
+  t0 = time.perf_counter()
+  o.run("step", nstep=max(1, warmup), nthreads=cores)
+  per_step = (time.perf_counter() - t0) / max(1, warmup)
+  k = int(max(1, min(steps, budget_s / repeats / max(per_step, 1e-6))))
+  snap = {f: o.get(f) for f in ("qpos", "qvel", "qacc_warmstart")}
+  rates = []
+  for _ in range(repeats):
+    for f, v in snap.items():
+      o.set(f, v)
+    t0 = time.perf_counter()
+    o.run("step", nstep=k, nthreads=cores)
+    rates.append(nworld * k / (time.perf_counter() - t0))
+  med = statistics.median(rates)
+  return {"value": med, "unit": "steps/s", "cores": cores, "kind": "port",
+          "repeats": rates, "spread": (max(rates) - min(rates)) / med,
+          "sample": (f"{nworld} worlds x {k} steps after {max(1, warmup)} warm-up steps, "
+                     f"{repeats} repeats from the same state (median), FP32 CPU restatement")}
 
 
 def run_reference(args):
@@ -662,7 +850,9 @@ def run_reference(args):
   if rank != 0:
     return
   mjm = _model()
-  cpu = cpu_baseline(mjm, budget_s=max(2.0, 0.02 * (args.steps + args.warmup)), nworld=1024)
+  cpu = cpu_baseline(mjm, args.steps, args.warmup,
+                     budget_s=min(30.0, max(3.0, 0.05 * (args.steps + args.warmup))),
+                     nworld=args.nworld)
   line = {
     "impl": "reference", "metric": METRIC, "value": cpu["value"], "unit": "steps/s",
     "n_gpus": world_size, "steps": args.steps, "warmup": args.warmup,
@@ -688,6 +878,7 @@ def main():
   p.add_argument("--no-accuracy", action="store_true")
   p.add_argument("--no-grad", action="store_true")
   p.add_argument("--no-combined", action="store_true")
+  p.add_argument("--no-bin", action="store_true")
   p.add_argument("--larger-models", action="store_true",
                  help="print one JSON line of the uneven-contact configurations' step times instead")
   args = p.parse_args()

@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define MJB_ABI_VERSION 5
+#define MJB_ABI_VERSION 6
 
 typedef struct CUstream_st* mjbStream; /* == cudaStream_t */
 
@@ -54,6 +54,7 @@ typedef struct MjbModel {
   int32_t nlimit;      /* len(jnt_limited_slide_hinge_adr) */
   int32_t nlevel;      /* BFS levels of the body tree, world included */
   int32_t nblock;      /* dof tree blocks (one per kinematic tree) */
+  int32_t block_max;   /* dofs of the largest tree block (max of block_size) */
   int32_t npair_cand;  /* geom pairs that pass the static filter (broadphase candidates) */
   int32_t nlsp;        /* parallel line-search candidates */
   /* Option (types.py:218-250) */
@@ -140,8 +141,11 @@ typedef struct MjbData {
 #define MJB_FORM_PLAIN 0  /* one kernel per reference stage; Hessian refactored every iteration */
 #define MJB_FORM_CHOSEN 1 /* stage kernels to fwd_acceleration + solver reusing its factor + integrator */
 #define MJB_FORM_SINGLE 2 /* the whole step of a world in one warp of one kernel */
-/* MJB_FORM_CHOSEN with the Newton Hessian and mass-matrix Cholesky factor-solves in FP64 and the
-   line-search polynomial coefficients accumulated in FP64 (dense, nv <= 32) */
+/* MJB_FORM_CHOSEN with the Newton Hessian assembled in split TF32 on the tensor pipe (nv <= 32),
+   the Hessian and mass-matrix Cholesky factor-solves in FP64 and the line-search polynomial
+   coefficients accumulated in FP64.  Dense mass matrix, tree blocks of up to 32 dofs
+   (MJB_ERR_UNSUPPORTED otherwise); for nv > 32 the Hessian's FP64 factor lives in shared memory,
+   which bounds nv at about 160 (MJB_ERR_SCRATCH beyond). */
 #define MJB_FORM_PRECISION 3
 
 typedef struct MjbRunCfg {
@@ -203,22 +207,36 @@ int mjb_xfrc_accumulate(const MjbModel* m, const MjbData* d, float* qfrc, mjbStr
 int mjb_world_status(const MjbData* d, uint32_t* host_out, mjbStream stream);
 
 /* Launch parameters of the chosen form that the autotuner picks (no counterpart in the reference):
- * lanes per world of the tree-recursion stages and warps per CTA of the persistent solver. */
+ * lanes per world of the tree-recursion stages, warps per CTA of the persistent solver (one warp
+ * per world, nv <= 32) and how it assembles the Newton Hessian (FP32 FMAs, or split-TF32
+ * tensor-core products, which the precision form always uses), and warps per world of the CTA
+ * solver of dense models with nv > 32. */
 typedef struct MjbTune {
-  int32_t tree_lanes;    /* 8, 16 or 32 */
-  int32_t solver_warps;  /* 1, 2 or 4 */
-  float ms_per_forward;  /* measured chosen-form forward (fwd_position .. solve) at this setting */
+  int32_t tree_lanes;        /* 8, 16 or 32 */
+  int32_t solver_warps;      /* 1, 2 or 4 */
+  int32_t solver_cta_warps;  /* 2, 4, 8 or 16 warps per world; 0 = one warp per world */
+  int32_t hessian_tc;        /* nv <= 32: 1 = Newton Hessian in split TF32 on the tensor pipe */
+  float ms_per_forward;      /* measured chosen-form forward (fwd_position .. solve) at this setting */
+  float rows_per_world;      /* mean constraint rows per world of the Data it was measured on */
 } MjbTune;
 
 /* Autotuner (no counterpart in the reference): times the chosen form's forward for every
  * tree-lane count and solver CTA width on d's current worlds and keeps the fastest, per device,
  * for models of this nv and Data of this rows-per-world capacity (njmax / nworld); later chosen-
- * form calls with the same key use it (others keep 16 lanes and 4 warps).  warmstart_scratch:
+ * form calls with the same key use it (others keep 16 lanes, 4 warps per solver CTA, FMA
+ * Hessians, and 4 warps per world for dense nv > 32).  out->rows_per_world reports the mean
+ * constraint rows per world of d's worlds (the key cannot hold it: the host does not see the row
+ * counts of a step without synchronising).  warmstart_scratch:
  * nworld * nv floats of caller memory; qacc_warmstart is saved there and restored before every
  * trial and at the end, so d is left as after one chosen-form forward.  Synchronises the stream;
  * out may be null. */
 int mjb_autotune(const MjbModel* m, const MjbData* d, float* warmstart_scratch, MjbTune* out,
                  mjbStream stream);
+/* Sets the chosen form's launch parameters for the same key as mjb_autotune (device, nv, rows-
+ * per-world capacity) without measuring: tree_lanes, solver_warps, solver_cta_warps and
+ * hessian_tc as in MjbTune (the timing fields are ignored).  MJB_ERR_ARG for a value outside
+ * those sets. */
+int mjb_set_tune(const MjbModel* m, const MjbData* d, const MjbTune* tune);
 
 /* Finite-difference transition Jacobians, no counterpart in the reference (whose API has no
  * derivatives); the scheme is MuJoCo's mjd_transitionFD, batched over worlds.  State

@@ -16,6 +16,7 @@ stage functions launch the hand-written sm_100a kernels of libmjb200.so through 
 from . import derivative as derivative
 from . import mjcf as mjcf
 from ._api import autotune as autotune
+from ._api import set_tune as set_tune
 from ._api import benchmark as benchmark
 from ._api import collision as collision
 from ._api import com_pos as com_pos

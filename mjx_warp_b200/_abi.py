@@ -18,7 +18,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.environ.get("MJX_WARP_B200_LIB") or os.path.join(_HERE, "libmjb200.so")
 
 MODEL_INTS = ("nq", "nv", "na", "nu", "nbody", "njnt", "ngeom", "nsite", "nmocap", "nM", "nlimit",
-              "nlevel", "nblock", "npair_cand", "nlsp", "integrator", "cone", "solver",
+              "nlevel", "nblock", "block_max", "npair_cand", "nlsp", "integrator", "cone", "solver",
               "iterations", "ls_iterations", "disableflags", "is_sparse", "ls_parallel",
               "actuator_affine_bias_gain", "precision")
 MODEL_FLOATS = ("timestep", "impratio", "tolerance", "ls_tolerance", "meaninertia")
@@ -115,7 +115,9 @@ class MjbData(ctypes.Structure):
 
 class MjbTune(ctypes.Structure):
   _fields_ = [("tree_lanes", ctypes.c_int32), ("solver_warps", ctypes.c_int32),
-              ("ms_per_forward", ctypes.c_float)]
+              ("solver_cta_warps", ctypes.c_int32), ("hessian_tc", ctypes.c_int32),
+              ("ms_per_forward", ctypes.c_float),
+              ("rows_per_world", ctypes.c_float)]
 
 
 class MjbRunCfg(ctypes.Structure):
@@ -171,9 +173,11 @@ def lib() -> ctypes.CDLL:
   L.mjb_step_vjp.argtypes = [pm, pd, vp, vp, vp, vp, vp, vp]
   L.mjb_autotune.restype = ctypes.c_int
   L.mjb_autotune.argtypes = [pm, pd, vp, ctypes.POINTER(MjbTune), vp]
+  L.mjb_set_tune.restype = ctypes.c_int
+  L.mjb_set_tune.argtypes = [pm, pd, ctypes.POINTER(MjbTune)]
   L.mjb_transition_vjp.restype = ctypes.c_int
   L.mjb_transition_vjp.argtypes = [pm, ci, vp, vp, vp, vp, vp, vp]
-  if L.mjb_abi_version() != 5:
+  if L.mjb_abi_version() != 6:
     raise RuntimeError("libmjb200.so ABI version mismatch")
   _lib = L
   return L
@@ -223,6 +227,10 @@ def model_view(m) -> MjbModel:
   v.nlimit = int(m.jnt_limited_slide_hinge_adr.shape[0])
   v.nlevel = int(m.body_treeadr.shape[0] - 1)
   v.nblock = int(m.block_adr.shape[0])
+  v.block_max = int(m.__dict__.get("_block_max", -1))
+  if v.block_max < 0:
+    v.block_max = int(m.block_size.max().item()) if m.block_size.numel() else 0
+    object.__setattr__(m, "_block_max", v.block_max)
   v.nlsp = int(m.nlsp)
   o = m.opt
   v.integrator, v.cone, v.solver = int(o.integrator), int(o.cone), int(o.solver)

@@ -50,13 +50,14 @@ def _integrator_check(m: Model) -> None:
 def step(m: Model, d: Data, fused=True) -> None:
   """Advance simulation (forward.py:682-695).
 
-  fused=True (or 1) runs the chosen form: one kernel for fwd_position .. fwd_acceleration, one
-  for the solver (keeping the Newton Hessian's factor while the active set is unchanged) and one
-  for the integrator; fused=False (or 0) launches one kernel per reference stage and refactors
+  fused=True (or 1) runs the chosen form: the stage kernels of fwd_position .. fwd_acceleration
+  forked over three streams, the persistent solver (keeping the Newton Hessian's factor while the
+  active set is unchanged; one CTA per world for dense models with nv > 32) and one kernel for
+  the integrator; fused=False (or 0) launches one kernel per reference stage and refactors
   the Hessian in every iteration, as the reference does; fused=2 runs the whole step of a world
   in one warp of a single kernel; fused=3 runs the chosen form with the Hessian and mass-matrix
-  Cholesky factor-solves and the line-search coefficient sums in FP64 (the precision form; dense,
-  nv <= 32).
+  Cholesky factor-solves and the line-search coefficient sums in FP64 (the precision form; dense
+  mass matrix with trees of up to 32 dofs, nv up to about 160).
   """
   _integrator_check(m)
   L = _abi.lib()
@@ -260,8 +261,11 @@ def benchmark(fn: Callable[[Model, Data], None], m: Model, d: Data, nstep: int =
 def autotune(m: Model, d: Data) -> dict:
   """Picks the chosen form's launch parameters for this model and Data (an extension; the
   reference has no autotuner): times the chosen forward for every tree-stage lane count (8, 16,
-  32 lanes per world) and persistent-solver CTA width (1, 2, 4 warps) on d's current worlds and
-  keeps the fastest for later calls with the same nv and rows-per-world capacity on this device.
+  32 lanes per world) and solver CTA shape (for nv <= 32 the persistent one-warp-per-world
+  solver's CTA width, 1, 2, 4 warps, with the Newton Hessian by FMAs or on the tensor pipe; for
+  dense nv > 32 the warps per world of the CTA solver, 2,
+  4, 8, or one warp per world) on d's current worlds and keeps the fastest for later calls with
+  the same nv and rows-per-world capacity on this device; reports the rows per world measured.
   d's qacc_warmstart is saved and restored around the trials; d is left as after one forward.
   Synchronises; call it before capturing a CUDA graph."""
   scratch = torch.empty_like(d.qacc_warmstart)
@@ -270,4 +274,23 @@ def autotune(m: Model, d: Data) -> dict:
                                _abi._ptr(scratch), ctypes.byref(out), _abi.stream())
   _abi.check(rc, "autotune")
   return {"tree_lanes": out.tree_lanes, "solver_warps": out.solver_warps,
-          "ms_per_forward": out.ms_per_forward}
+          "solver_cta_warps": out.solver_cta_warps, "hessian_tc": out.hessian_tc,
+          "ms_per_forward": out.ms_per_forward,
+          "rows_per_world": out.rows_per_world}
+
+
+def set_tune(m: Model, d: Data, tree_lanes: int = 16, solver_warps: int = 4,
+             solver_cta_warps: int = 4, hessian_tc: bool = False) -> None:
+  """Pins the chosen form's launch parameters for this model and Data (an extension, as
+  autotune): lanes per world of the tree-recursion stages (8, 16, 32), warps per CTA of the
+  one-warp-per-world solver (1, 2, 4), its Newton Hessian on the tensor pipe in split TF32
+  (hessian_tc, nv <= 32) and warps per world of the CTA solver of dense models with nv > 32
+  (2, 4, 8, 16, or 0 for one warp per world)."""
+  t = _abi.MjbTune()
+  t.tree_lanes, t.solver_warps, t.solver_cta_warps = tree_lanes, solver_warps, solver_cta_warps
+  t.hessian_tc = int(bool(hessian_tc))
+  rc = _abi.lib().mjb_set_tune(ctypes.byref(_abi.model_view(m)), ctypes.byref(_abi.data_view(d)),
+                               ctypes.byref(t))
+  if rc == 1:
+    raise ValueError(f"set_tune: unsupported setting {tree_lanes}, {solver_warps}, {solver_cta_warps}")
+  _abi.check(rc, "set_tune")

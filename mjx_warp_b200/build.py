@@ -16,7 +16,8 @@ LIB = os.path.join(HERE, "libmjb200.so")
 HEADER = os.path.join(os.path.dirname(HERE), "include", "mjb200.h")
 
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
-              "-Xcompiler", "-fPIC", "-shared", "-cudart", "static"]
+              "-Xcompiler", "-fPIC", "-shared", "-cudart", "static",
+              "-split-compile=0"]  # the optimiser's work spread over all host threads
 
 
 def _sources():

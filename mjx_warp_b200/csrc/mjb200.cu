@@ -21,6 +21,7 @@
 
 #include "mjb_deriv.cuh"
 #include "mjb_solver.cuh"
+#include "mjb_solver_cta.cuh"
 
 // minimum resident CTAs per SM requested for the solver kernels (caps registers per thread at
 // 65536 / (128 * MJB_MINB)); with the staged / unstaged solver paths compiled apart, 4 (128
@@ -43,6 +44,7 @@ enum Stage {
 };
 
 constexpr int kDefaultWarps = 4;
+
 
 // Kernels take the Model / Data views by value as __grid_constant__ parameters: the stages receive
 // them by reference, and without the qualifier every thread would copy both structs (~1.6 KB)
@@ -149,15 +151,17 @@ __global__ void __launch_bounds__(128, MJB_MINB) k_step_fused(const __grid_const
   }
 }
 
-// chosen form: the constraint solver with the Hessian factor kept across iterations
-template <bool PREC>
+// chosen form: the constraint solver with the Hessian factor kept across iterations; TC: the
+// Newton Hessian of up to 32 staged rows assembled on the tensor pipe in split TF32 (hessian_tc;
+// always in the precision form, an autotuner choice in the chosen form)
+template <bool PREC, bool TC>
 __global__ void __launch_bounds__(128, MJB_MINB) k_solve(const __grid_constant__ MjbModel m, const __grid_constant__ MjbData d, int smem_per_warp) {
   extern __shared__ __align__(16) float smem[];
   const int lane = threadIdx.x & 31;
   const int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   if (w >= d.nworld) return;
   float* sm = smem_per_warp ? smem + size_t(threadIdx.x >> 5) * smem_per_warp : nullptr;
-  solve<PREC>(m, d, w, lane, sm, d.efc_h + W(w, m.nv * m.nv), true);
+  solve<PREC, TC>(m, d, w, lane, sm, d.efc_h + W(w, m.nv * m.nv), true);
 }
 
 // The chosen form's solver schedule.  k_order_worlds sorts the worlds by their constraint row
@@ -205,7 +209,7 @@ __global__ void __launch_bounds__(1024) k_order_worlds(const int* nefc, int* ord
   }
 }
 
-template <bool PREC>
+template <bool PREC, bool TC>
 __global__ void __launch_bounds__(128, MJB_MINB) k_solve_queue(const __grid_constant__ MjbModel m, const __grid_constant__ MjbData d, int smem_per_warp) {
   extern __shared__ __align__(16) float smem[];
   const int lane = threadIdx.x & 31;
@@ -216,7 +220,29 @@ __global__ void __launch_bounds__(128, MJB_MINB) k_solve_queue(const __grid_cons
     idx = __shfl_sync(WARP_FULL, idx, 0);
     if (idx >= d.nworld) break;
     const int w = d.world_order[idx];
-    solve<PREC>(m, d, w, lane, sm, d.efc_h + W(w, m.nv * m.nv), true);
+    solve<PREC, TC>(m, d, w, lane, sm, d.efc_h + W(w, m.nv * m.nv), true);
+  }
+}
+
+// chosen form, dense models with nv > 32: one CTA of NW warps per world (mjb_solver_cta.cuh),
+// persistent over the work queue in k_order_worlds' order when the Data has the schedule arrays,
+// else one CTA per world in index order
+template <int NW, bool PREC>
+__global__ void __launch_bounds__(NW * 32, NW >= 16 ? 1 : (NW >= 8 ? 2 : (NW >= 4 ? 4 : 8)))
+    k_solve_cta(const __grid_constant__ MjbModel m, const __grid_constant__ MjbData d) {
+  extern __shared__ __align__(16) float smem[];
+  __shared__ int s_idx;
+  if (!d.work_queue) {
+    if (int(blockIdx.x) < d.nworld) solve_cta<NW, PREC>(m, d, blockIdx.x, smem);
+    return;
+  }
+  for (;;) {
+    if (threadIdx.x == 0) s_idx = atomicAdd(d.work_queue, 1);
+    __syncthreads();
+    const int idx = s_idx;
+    __syncthreads();
+    if (idx >= d.nworld) break;
+    solve_cta<NW, PREC>(m, d, d.world_order[idx], smem);
   }
 }
 
@@ -363,11 +389,153 @@ inline int finish() {
 // implicitfast needs the dense mass matrix (the reference asserts it, forward.py:268)
 inline bool implicit_unsupported(const MjbModel* m) { return m->is_sparse && m->integrator != 0; }
 
+// the precision form: dense mass matrix with tree blocks of up to 32 dofs (the FP64 block
+// factor-solves use a 32-row tile); for nv > 32 the Hessian's FP64 factor must fit in one CTA's
+// shared memory (227 KB: nv up to about 160)
+int precision_supported(const MjbModel* m) {
+  if (m->is_sparse || m->block_max > 32) return MJB_ERR_UNSUPPORTED;
+  if (m->nv > 32 && size_t(cta_solver_smem_floats(m->nv, 8, true)) * sizeof(float) > 227 * 1024)
+    return MJB_ERR_SCRATCH;
+  return MJB_OK;
+}
+
 inline int check(const MjbModel* m, const MjbData* d) {
   if (!m || !d) return MJB_ERR_ARG;
   if (d->nworld <= 0) return d->nworld == 0 ? MJB_OK : MJB_ERR_ARG;
   if (m->cone != 0) return MJB_ERR_UNSUPPORTED;
   return MJB_OK;
+}
+
+// The Data fields each stage reads or writes, given the model's sizes and options: a stage
+// launched with one of them null returns MJB_ERR_ARG instead of faulting on the device.
+// Fields a stage checks for null itself (world_status, the solver's optional per-world outputs,
+// contact_solreffriction, world_order / work_queue) are not required.
+#define MJB_REQ(cond, field) \
+  if ((cond) && !d->field) return MJB_ERR_ARG
+int stage_fields(int stage, const MjbModel* m, const MjbData* d) {
+  const bool nv = m->nv > 0, nq = m->nq > 0, nj = m->njnt > 0, ng = m->ngeom > 0,
+             ns = m->nsite > 0, nu = m->nu > 0, na = m->na > 0;
+  const bool con = d->nconmax > 0, efc = d->njmax > 0;
+  switch (stage) {
+    case S_KINEMATICS:
+      MJB_REQ(nq, qpos); MJB_REQ(true, xpos); MJB_REQ(true, xquat); MJB_REQ(true, xmat);
+      MJB_REQ(true, xipos); MJB_REQ(true, ximat); MJB_REQ(nj, xanchor); MJB_REQ(nj, xaxis);
+      MJB_REQ(ng, geom_xpos); MJB_REQ(ng, geom_xmat); MJB_REQ(ns, site_xpos); MJB_REQ(ns, site_xmat);
+      break;
+    case S_COM_POS:
+      MJB_REQ(true, subtree_com); MJB_REQ(true, cinert); MJB_REQ(nv, cdof); MJB_REQ(true, xipos);
+      MJB_REQ(true, ximat); MJB_REQ(true, xmat); MJB_REQ(nj, xanchor); MJB_REQ(nj, xaxis);
+      break;
+    case S_CRB:
+      MJB_REQ(true, crb); MJB_REQ(true, cinert); MJB_REQ(nv, cdof); MJB_REQ(nv, qM);
+      break;
+    case S_FACTOR_M:
+      MJB_REQ(nv, qM); MJB_REQ(nv, qLD); MJB_REQ(nv && m->is_sparse, qLDiagInv);
+      break;
+    case S_TRANSMISSION:
+      MJB_REQ(nu, actuator_length); MJB_REQ(nu, actuator_moment); MJB_REQ(nu && nq, qpos);
+      break;
+    case S_FWD_VELOCITY:
+      MJB_REQ(nu, actuator_velocity); MJB_REQ(nu, actuator_moment);
+      [[fallthrough]];
+    case S_COM_VEL:
+    case S_PASSIVE:
+    case S_RNE:
+      MJB_REQ(true, cvel); MJB_REQ(nv, cdof_dot); MJB_REQ(nv, cdof); MJB_REQ(nv, qvel);
+      MJB_REQ(nq, qpos); MJB_REQ(nv, qfrc_spring); MJB_REQ(nv, qfrc_damper);
+      MJB_REQ(nv, qfrc_passive); MJB_REQ(true, rne_cacc); MJB_REQ(true, rne_cfrc);
+      MJB_REQ(nv, qfrc_bias); MJB_REQ(true, cinert);
+      break;
+    case S_FWD_ACTUATION:
+      MJB_REQ(nv, qfrc_actuator); MJB_REQ(nu, actuator_force); MJB_REQ(nu, ctrl);
+      MJB_REQ(nu, actuator_length); MJB_REQ(nu, actuator_velocity); MJB_REQ(nu, actuator_moment);
+      MJB_REQ(na, act); MJB_REQ(na, act_dot);
+      break;
+    case S_FWD_ACCELERATION:
+      MJB_REQ(nv, qfrc_smooth); MJB_REQ(nv, qacc_smooth); MJB_REQ(nv, qfrc_applied);
+      MJB_REQ(nv, qfrc_bias); MJB_REQ(nv, qfrc_passive); MJB_REQ(nv, qfrc_actuator);
+      MJB_REQ(nv, qM); MJB_REQ(nv, qLD); MJB_REQ(nv && m->is_sparse, qLDiagInv);
+      MJB_REQ(true, xfrc_applied);
+      break;
+    case S_NXN:
+    case S_SAP:
+      MJB_REQ(con, ncollision); MJB_REQ(con, collision_pair); MJB_REQ(con, collision_worldid);
+      MJB_REQ(true, world_pairadr); MJB_REQ(true, world_npair); MJB_REQ(ng, geom_xpos);
+      MJB_REQ(ng, geom_xmat);
+      break;
+    case S_NARROW:
+      MJB_REQ(con, collision_pair); MJB_REQ(con, ncon); MJB_REQ(true, world_pairadr);
+      MJB_REQ(true, world_npair); MJB_REQ(true, world_conadr); MJB_REQ(true, world_ncon);
+      MJB_REQ(con, contact_dist); MJB_REQ(con, contact_pos); MJB_REQ(con, contact_frame);
+      MJB_REQ(con, contact_geom); MJB_REQ(con, contact_worldid); MJB_REQ(con, contact_dim);
+      MJB_REQ(con, contact_solref); MJB_REQ(con, contact_includemargin);
+      MJB_REQ(con, contact_friction); MJB_REQ(con, contact_solimp);
+      MJB_REQ(ng, geom_xpos); MJB_REQ(ng, geom_xmat);
+      break;
+    case S_MAKE_CONSTRAINT:
+      MJB_REQ(efc, nefc); MJB_REQ(efc, efc_worldid); MJB_REQ(efc, efc_J); MJB_REQ(efc, efc_pos);
+      MJB_REQ(efc, efc_margin); MJB_REQ(efc, efc_D); MJB_REQ(efc, efc_aref);
+      MJB_REQ(true, world_efcadr); MJB_REQ(true, world_nefc); MJB_REQ(true, world_conadr);
+      MJB_REQ(true, world_ncon); MJB_REQ(con, contact_dist); MJB_REQ(con, contact_pos);
+      MJB_REQ(con, contact_frame); MJB_REQ(con, contact_geom); MJB_REQ(con, contact_dim);
+      MJB_REQ(con, contact_solref); MJB_REQ(con, contact_includemargin);
+      MJB_REQ(con, contact_friction); MJB_REQ(con, contact_solimp); MJB_REQ(nv, cdof);
+      MJB_REQ(true, subtree_com); MJB_REQ(nq, qpos); MJB_REQ(nv, qvel);
+      break;
+    case S_SOLVE: {
+      const bool generic = m->nv > 32 || m->is_sparse;
+      MJB_REQ(efc, efc_D); MJB_REQ(efc, efc_J); MJB_REQ(efc, efc_Jaref); MJB_REQ(efc, efc_aref);
+      MJB_REQ(efc, efc_force); MJB_REQ(efc, efc_active); MJB_REQ(efc, efc_jv);
+      MJB_REQ(efc, efc_quad); MJB_REQ(nv, efc_Ma); MJB_REQ(nv, efc_grad); MJB_REQ(nv, efc_Mgrad);
+      MJB_REQ(nv, efc_search); MJB_REQ(nv, efc_mv); MJB_REQ(nv, qfrc_constraint); MJB_REQ(nv, qacc);
+      MJB_REQ(nv, qacc_warmstart); MJB_REQ(nv, qfrc_smooth); MJB_REQ(nv, qacc_smooth);
+      MJB_REQ(nv, qM); MJB_REQ(true, world_efcadr); MJB_REQ(true, world_nefc);
+      MJB_REQ(nv && generic && m->solver == 2, efc_h);
+      MJB_REQ(nv && generic && m->solver == 1, efc_prev_grad);
+      MJB_REQ(nv && generic && m->solver == 1, efc_prev_Mgrad);
+      MJB_REQ(nv && m->solver == 1, qLD); MJB_REQ(nv && m->solver == 1 && m->is_sparse, qLDiagInv);
+      break;
+    }
+    case S_EULER: {
+      const bool damp = !(m->disableflags & DSBL_EULERDAMP);
+      MJB_REQ(nv, qacc); MJB_REQ(nv, qvel); MJB_REQ(nq, qpos);
+      MJB_REQ(nv && damp, qacc_integration); MJB_REQ(nv && damp, qfrc_smooth);
+      MJB_REQ(nv && damp, qfrc_constraint); MJB_REQ(nv && damp, qM);
+      MJB_REQ(nv && damp, qLD_integration);
+      break;
+    }
+    case S_IMPLICIT: {
+      const bool act = !(m->disableflags & DSBL_ACTUATION) && m->actuator_affine_bias_gain;
+      MJB_REQ(nv, qacc); MJB_REQ(nv, qvel); MJB_REQ(nq, qpos); MJB_REQ(nv, qacc_integration);
+      MJB_REQ(nv, qfrc_smooth); MJB_REQ(nv, qfrc_constraint); MJB_REQ(nv, qM);
+      MJB_REQ(nv, qM_integration); MJB_REQ(nv, qLD_integration); MJB_REQ(nv, qfrc_integration);
+      MJB_REQ(act, act_vel_integration); MJB_REQ(act, actuator_moment); MJB_REQ(act, ctrl);
+      break;
+    }
+    case S_QACC_SMOOTH_COPY:
+      MJB_REQ(nv, qacc); MJB_REQ(nv, qacc_smooth);
+      break;
+    default:
+      break;
+  }
+  return MJB_OK;
+}
+#undef MJB_REQ
+
+// the fields of the stages of one phase of a step: 0 = fwd_position .. fwd_acceleration,
+// 1 = the solver (or the qacc_smooth copy without rows), 2 = the integrator
+int phase_fields(const MjbModel* m, const MjbData* d, int phase) {
+  static const int kForward[] = {S_KINEMATICS, S_COM_POS, S_CRB, S_FACTOR_M, S_TRANSMISSION,
+                                 S_FWD_VELOCITY, S_FWD_ACTUATION, S_FWD_ACCELERATION, S_NXN,
+                                 S_NARROW, S_MAKE_CONSTRAINT};
+  int rc;
+  if (phase == 0) {
+    for (int st : kForward)
+      if ((rc = stage_fields(st, m, d))) return rc;
+    return MJB_OK;
+  }
+  if (phase == 1) return stage_fields(d->njmax > 0 ? S_SOLVE : S_QACC_SMOOTH_COPY, m, d);
+  return stage_fields(m->integrator == 0 ? S_EULER : S_IMPLICIT, m, d);
 }
 
 // shared memory per warp (floats) for the solver workspace when nv <= 32, else a factor tile for
@@ -431,6 +599,7 @@ int resident_ctas(K kernel, int threads, size_t smem) {
 
 template <int STAGE>
 int launch_stage(const MjbModel* m, const MjbData* d, cudaStream_t s) {
+  if (int rc = stage_fields(STAGE, m, d)) return rc;
   const int warps = kDefaultWarps;
   int spw = 0;
   size_t bytes = 0;
@@ -474,6 +643,8 @@ int launch_lanes(const MjbModel* m, const MjbData* d, cudaStream_t s, int lanes)
 struct ChosenCfg {
   int lanes = MJB_TREE_LANES;
   int warps = kDefaultWarps;
+  int cta_warps = 4;  // warps per world of the solver for dense nv > 32 (0: one warp per world)
+  int hessian_tc = 0; // nv <= 32: Newton Hessian on the tensor pipe (split TF32) instead of FMAs
 };
 struct TuneEntry {
   int dev, nv, cap;
@@ -603,29 +774,63 @@ int run_forward_plain(const MjbModel* m, const MjbData* d, cudaStream_t s) {
 
 // the chosen form's solver launch: k_order_worlds + the persistent k_solve_queue when the Data has
 // the schedule arrays, else one warp per world (k_solve); PREC selects the precision form's solver
-template <bool PREC>
-void launch_solver(const MjbModel* m, const MjbData* d, const ChosenCfg& cfg, int spw,
-                   cudaStream_t s) {
+template <int NW, bool PREC>
+void launch_solver_cta(const MjbModel* m, const MjbData* d, cudaStream_t s) {
+  const size_t bytes = size_t(cta_solver_smem_floats(m->nv, NW, PREC)) * sizeof(float);
+  static size_t conf[kSmemDevices];
+  allow_smem(k_solve_cta<NW, PREC>, bytes, conf);
+  if (d->world_order && d->work_queue && d->world_nefc) {
+    const int ctas = resident_ctas(k_solve_cta<NW, PREC>, 32 * NW, bytes);
+    k_order_worlds<<<1, 1024, 0, s>>>(d->world_nefc, d->world_order, d->work_queue, d->nworld);
+    k_solve_cta<NW, PREC><<<std::min(ctas, d->nworld), 32 * NW, bytes, s>>>(*m, *d);
+  } else {
+    MjbData dd = *d;
+    dd.work_queue = nullptr;
+    k_solve_cta<NW, PREC><<<d->nworld, 32 * NW, bytes, s>>>(*m, dd);
+  }
+}
+
+template <bool PREC, bool TC>
+void launch_solver_warp(const MjbModel* m, const MjbData* d, const ChosenCfg& cfg, int spw,
+                        cudaStream_t s) {
   if (d->world_order && d->work_queue && d->world_nefc) {
     const int qw = cfg.warps;
     const size_t qbytes = size_t(spw) * qw * sizeof(float);
     static size_t conf_queue[kSmemDevices];
-    allow_smem(k_solve_queue<PREC>, size_t(spw) * kDefaultWarps * sizeof(float), conf_queue);
-    const int ctas = resident_ctas(k_solve_queue<PREC>, 32 * qw, qbytes);
+    allow_smem(k_solve_queue<PREC, TC>, size_t(spw) * kDefaultWarps * sizeof(float), conf_queue);
+    const int ctas = resident_ctas(k_solve_queue<PREC, TC>, 32 * qw, qbytes);
     k_order_worlds<<<1, 1024, 0, s>>>(d->world_nefc, d->world_order, d->work_queue, d->nworld);
-    k_solve_queue<PREC><<<std::min(ctas, grid_for(d->nworld, qw)), 32 * qw, qbytes, s>>>(*m, *d, spw);
+    k_solve_queue<PREC, TC><<<std::min(ctas, grid_for(d->nworld, qw)), 32 * qw, qbytes, s>>>(*m, *d, spw);
   } else {
     const size_t bytes = size_t(spw) * kDefaultWarps * sizeof(float);
     static size_t conf_solve[kSmemDevices];
-    allow_smem(k_solve<PREC>, bytes, conf_solve);
-    k_solve<PREC><<<grid_for(d->nworld, kDefaultWarps), 32 * kDefaultWarps, bytes, s>>>(*m, *d, spw);
+    allow_smem(k_solve<PREC, TC>, bytes, conf_solve);
+    k_solve<PREC, TC><<<grid_for(d->nworld, kDefaultWarps), 32 * kDefaultWarps, bytes, s>>>(*m, *d, spw);
   }
+}
+
+template <bool PREC>
+void launch_solver(const MjbModel* m, const MjbData* d, const ChosenCfg& cfg, int spw,
+                   cudaStream_t s) {
+  // dense nv > 32: the CTA solver (the precision form's FP64 Hessian factor needs it)
+  if (m->nv > 32 && !m->is_sparse && (cfg.cta_warps > 0 || PREC)) {
+    if (cfg.cta_warps == 2) launch_solver_cta<2, PREC>(m, d, s);
+    else if (cfg.cta_warps == 4) launch_solver_cta<4, PREC>(m, d, s);
+    else if (cfg.cta_warps == 16) launch_solver_cta<16, PREC>(m, d, s);
+    else launch_solver_cta<8, PREC>(m, d, s);
+    return;
+  }
+  if (PREC) launch_solver_warp<PREC, true>(m, d, cfg, spw, s);
+  else if (cfg.hessian_tc) launch_solver_warp<PREC, true>(m, d, cfg, spw, s);
+  else launch_solver_warp<PREC, false>(m, d, cfg, spw, s);
 }
 
 // the chosen form's phases: 0 = status reset + the stage kernels up to fwd_acceleration,
 // 1 = k_solve, 2 = k_integrate
 int run_chosen_phase(const MjbModel* m, const MjbData* d, int phase, cudaStream_t s,
                      const ChosenCfg* tuned = nullptr) {
+  if (phase >= 0 && phase <= 2)
+    if (int rc = phase_fields(m, d, phase)) return rc;
   const ChosenCfg cfg = tuned ? *tuned : chosen_cfg(m, d);
   const int warps = kDefaultWarps;
   const int grid = grid_for(d->nworld, warps);
@@ -655,6 +860,8 @@ int run_chosen_phase(const MjbModel* m, const MjbData* d, int phase, cudaStream_
 
 int run_chosen(const MjbModel* m, const MjbData* d, int integrate, cudaStream_t s) {
   int rc;
+  for (int p = 0; p < (integrate ? 3 : 2); p++)  // every phase's fields before the first launch
+    if ((rc = phase_fields(m, d, p))) return rc;
   if ((rc = run_chosen_phase(m, d, 0, s))) return rc;
   if ((rc = run_chosen_phase(m, d, 1, s))) return rc;
   return integrate ? run_chosen_phase(m, d, 2, s) : MJB_OK;
@@ -662,6 +869,8 @@ int run_chosen(const MjbModel* m, const MjbData* d, int integrate, cudaStream_t 
 
 int run_fused(const MjbModel* m, const MjbData* d, const MjbRunCfg* cfg, int integrate,
               cudaStream_t s) {
+  for (int p = 0; p < (integrate ? 3 : 2); p++)
+    if (int rc = phase_fields(m, d, p)) return rc;
   const int warps = (cfg && cfg->worlds_per_block > 0) ? cfg->worlds_per_block : kDefaultWarps;
   if (warps > 4) return MJB_ERR_ARG;  // __launch_bounds__(128)
   reset_counters(d, true, true, true, true, s);
@@ -684,7 +893,7 @@ const char* mjb_error_string(int status) {
   switch (status) {
     case MJB_OK: return "ok";
     case MJB_ERR_ARG: return "invalid argument";
-    case MJB_ERR_UNSUPPORTED: return "unsupported model feature (elliptic cone, or implicitfast with the sparse mass matrix)";
+    case MJB_ERR_UNSUPPORTED: return "unsupported model feature (elliptic cone, implicitfast with the sparse mass matrix, or the precision form with the sparse mass matrix or a tree of over 32 dofs)";
     case MJB_ERR_LAUNCH: return cudaGetErrorString(cudaGetLastError());
     case MJB_ERR_SCRATCH: return "model too large for on-chip scratch";
     default: return "unknown status";
@@ -694,12 +903,14 @@ const char* mjb_error_string(int status) {
 int mjb_forward(const MjbModel* m, const MjbData* d, const MjbRunCfg* cfg, mjbStream stream) {
   int rc = check(m, d);
   if (rc || d->nworld == 0) return rc;
+  for (int p = 0; p < 2; p++)
+    if ((rc = phase_fields(m, d, p))) return rc;
   cudaStream_t s = (cudaStream_t)stream;
   const int form = cfg ? cfg->fused : MJB_FORM_CHOSEN;
   if (form == MJB_FORM_PLAIN) return run_forward_plain(m, d, s);
   if (form == MJB_FORM_SINGLE) return run_fused(m, d, cfg, 0, s);
   if (form == MJB_FORM_PRECISION) {
-    if (m->nv > 32 || m->is_sparse) return MJB_ERR_UNSUPPORTED;
+    if ((rc = precision_supported(m))) return rc;
     MjbModel mp = *m;
     mp.precision = 1;
     return run_chosen(&mp, d, 0, s);
@@ -711,6 +922,8 @@ int mjb_forward(const MjbModel* m, const MjbData* d, const MjbRunCfg* cfg, mjbSt
 int mjb_step(const MjbModel* m, const MjbData* d, const MjbRunCfg* cfg, mjbStream stream) {
   int rc = check(m, d);
   if (rc || d->nworld == 0) return rc;
+  for (int p = 0; p < 3; p++)
+    if ((rc = phase_fields(m, d, p))) return rc;
   if (implicit_unsupported(m)) return MJB_ERR_UNSUPPORTED;
   cudaStream_t s = (cudaStream_t)stream;
   const int form = cfg ? cfg->fused : MJB_FORM_CHOSEN;
@@ -724,7 +937,7 @@ int mjb_step(const MjbModel* m, const MjbData* d, const MjbRunCfg* cfg, mjbStrea
   }
   if (form == MJB_FORM_SINGLE) return run_fused(m, d, cfg, 1, s);
   if (form == MJB_FORM_PRECISION) {
-    if (m->nv > 32 || m->is_sparse) return MJB_ERR_UNSUPPORTED;
+    if ((rc = precision_supported(m))) return rc;
     MjbModel mp = *m;
     mp.precision = 1;
     return run_chosen(&mp, d, 1, s);
@@ -769,6 +982,9 @@ MJB_STAGE_ENTRY(mjb_nxn_broadphase, S_NXN)
 int mjb_fwd_position(const MjbModel* m, const MjbData* d, mjbStream stream) {
   int rc = check(m, d);
   if (rc || d->nworld == 0) return rc;
+  for (int st : {S_KINEMATICS, S_COM_POS, S_CRB, S_FACTOR_M, S_NXN, S_NARROW, S_MAKE_CONSTRAINT,
+                 S_TRANSMISSION})
+    if ((rc = stage_fields(st, m, d))) return rc;
   cudaStream_t s = (cudaStream_t)stream;
   if ((rc = launch_stage<S_KINEMATICS>(m, d, s))) return rc;
   if ((rc = launch_stage<S_COM_POS>(m, d, s))) return rc;
@@ -782,6 +998,7 @@ int mjb_fwd_position(const MjbModel* m, const MjbData* d, mjbStream stream) {
 int mjb_collision(const MjbModel* m, const MjbData* d, mjbStream stream) {
   int rc = check(m, d);
   if (rc || d->nworld == 0) return rc;
+  if ((rc = stage_fields(S_NXN, m, d)) || (rc = stage_fields(S_NARROW, m, d))) return rc;
   cudaStream_t s = (cudaStream_t)stream;
   reset_counters(d, true, true, false, false, s);  // collision_driver.py:533-534
   if ((rc = launch_broadphase(m, d, s))) return rc;
@@ -793,6 +1010,8 @@ MJB_STAGE_ENTRY(mjb_sap_broadphase, S_SAP)
 int mjb_primitive_narrowphase(const MjbModel* m, const MjbData* d, mjbStream stream) {
   int rc = check(m, d);
   if (rc || d->nworld == 0) return rc;
+  if ((rc = stage_fields(S_NARROW, m, d))) return rc;
+  if (!d->collision_worldid || !d->ncollision) return MJB_ERR_ARG;
   cudaStream_t s = (cudaStream_t)stream;
   rebuild_index(d->collision_worldid, d->ncollision, d->nconmax, d->world_pairadr, d->world_npair, d, s);
   return launch_stage<S_NARROW>(m, d, s);
@@ -801,6 +1020,8 @@ int mjb_primitive_narrowphase(const MjbModel* m, const MjbData* d, mjbStream str
 int mjb_make_constraint(const MjbModel* m, const MjbData* d, mjbStream stream) {
   int rc = check(m, d);
   if (rc || d->nworld == 0) return rc;
+  if ((rc = stage_fields(S_MAKE_CONSTRAINT, m, d))) return rc;
+  if (!d->contact_worldid || !d->ncon) return MJB_ERR_ARG;
   cudaStream_t s = (cudaStream_t)stream;
   rebuild_index(d->contact_worldid, d->ncon, d->nconmax, d->world_conadr, d->world_ncon, d, s);
   reset_counters(d, false, false, true, false, s);
@@ -810,6 +1031,8 @@ int mjb_make_constraint(const MjbModel* m, const MjbData* d, mjbStream stream) {
 int mjb_solve(const MjbModel* m, const MjbData* d, mjbStream stream) {
   int rc = check(m, d);
   if (rc || d->nworld == 0) return rc;
+  if ((rc = stage_fields(S_SOLVE, m, d))) return rc;
+  if (d->njmax > 0 && (!d->efc_worldid || !d->nefc)) return MJB_ERR_ARG;
   cudaStream_t s = (cudaStream_t)stream;
   rebuild_index(d->efc_worldid, d->nefc, d->njmax, d->world_efcadr, d->world_nefc, d, s);
   return launch_stage<S_SOLVE>(m, d, s);
@@ -818,7 +1041,8 @@ int mjb_solve(const MjbModel* m, const MjbData* d, mjbStream stream) {
 int mjb_solve_m(const MjbModel* m, const MjbData* d, float* x, const float* y, mjbStream stream) {
   int rc = check(m, d);
   if (rc || d->nworld == 0) return rc;
-  if (!x || !y) return MJB_ERR_ARG;
+  if (!x || !y || (m->nv > 0 && !d->qLD) || (m->is_sparse && m->nv > 0 && !d->qLDiagInv))
+    return MJB_ERR_ARG;
   k_solve_m<<<grid_for(d->nworld, 4), 128, 0, (cudaStream_t)stream>>>(*m, *d, x, y);
   return finish();
 }
@@ -932,15 +1156,24 @@ extern "C" int mjb_autotune(const MjbModel* m, const MjbData* d, float* warmstar
     if (e0) cudaEventDestroy(e0);
     return MJB_ERR_LAUNCH;
   }
-  const int lanes[3] = {8, 16, 32}, widths[3] = {1, 2, 4};
+  // candidates: tree-stage lanes x the solver's CTA shape (warps per CTA of the persistent
+  // one-warp-per-world solver, or, for dense nv > 32, warps per world of the CTA solver)
+  // (for nv <= 32 also the Newton Hessian's assembly: FMAs or the tensor pipe)
+  const int lanes[3] = {8, 16, 32}, widths[6] = {1, 2, 4, 1, 2, 4}, cta[4] = {2, 4, 8, 0};
+  const bool large = m->nv > 32 && !m->is_sparse;
   float best = 0.f;
   ChosenCfg best_cfg;
   bool have = false;
   for (int li = 0; li < 3 && !rc; li++) {
-    for (int wi = 0; wi < 3 && !rc; wi++) {
+    for (int wi = 0; wi < (large ? 4 : 6) && !rc; wi++) {
       ChosenCfg c;
       c.lanes = lanes[li];
-      c.warps = widths[wi];
+      if (large) {
+        c.cta_warps = cta[wi];
+      } else {
+        c.warps = widths[wi];
+        c.hessian_tc = wi >= 3;
+      }
       auto forward = [&]() -> int {
         if (restore() != cudaSuccess) return MJB_ERR_LAUNCH;
         int r = run_chosen_phase(m, d, 0, s, &c);
@@ -967,14 +1200,40 @@ extern "C" int mjb_autotune(const MjbModel* m, const MjbData* d, float* warmstar
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
+  int nefc = 0;  // rows of the last trial's forward (the same worlds in every trial)
+  if (!rc && d->nefc &&
+      cudaMemcpyAsync(&nefc, d->nefc, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess)
+    rc = MJB_ERR_LAUNCH;
   if (!rc && restore() != cudaSuccess) rc = MJB_ERR_LAUNCH;
+  if (!rc && cudaStreamSynchronize(s) != cudaSuccess) rc = MJB_ERR_LAUNCH;
   if (rc) return rc;
   store_cfg(m, d, best_cfg);
   if (out) {
     out->tree_lanes = best_cfg.lanes;
     out->solver_warps = best_cfg.warps;
+    out->solver_cta_warps = best_cfg.cta_warps;
+    out->hessian_tc = best_cfg.hessian_tc;
     out->ms_per_forward = best;
+    out->rows_per_world = float(std::min(nefc, d->njmax)) / float(d->nworld);
   }
+  return MJB_OK;
+}
+
+extern "C" int mjb_set_tune(const MjbModel* m, const MjbData* d, const MjbTune* tune) {
+  int rc = check(m, d);
+  if (rc) return rc;
+  if (!tune) return MJB_ERR_ARG;
+  const int l = tune->tree_lanes, w = tune->solver_warps, c = tune->solver_cta_warps;
+  if ((l != 8 && l != 16 && l != 32) || (w != 1 && w != 2 && w != 4) ||
+      (c != 0 && c != 2 && c != 4 && c != 8 && c != 16) ||
+      (tune->hessian_tc != 0 && tune->hessian_tc != 1))
+    return MJB_ERR_ARG;
+  ChosenCfg cfg;
+  cfg.lanes = l;
+  cfg.warps = w;
+  cfg.cta_warps = c;
+  cfg.hessian_tc = tune->hessian_tc;
+  store_cfg(m, d, cfg);
   return MJB_OK;
 }
 

@@ -11,6 +11,7 @@
 #pragma once
 
 #include "mjb_collide.cuh"
+#include "mjb_tc.cuh"
 
 namespace mjb {
 
@@ -547,21 +548,104 @@ struct Small {
   }
 };
 
+// H = tril(qM) + sum_k c_k J_k^T J_k for nv <= 32 on the tensor pipe, in split TF32 (mjb_tc.cuh):
+// H = qM + A B with A = J^T (nv x na) and B = diag(c) J (na x nv) over the na rows listed in idx
+// (the rows with c != 0), one warp.  The output is computed in the m16n8 tiles that touch the lower
+// triangle, (rows 16 mt .., columns 8 nt ..) = (0, 0), (0, 1) and, for nv > 16, (1, 0) .. (1, 3);
+// the k dimension runs over the listed rows eight at a time.  Ms / Js: qM and the staged rows
+// (stride ld floats, zero padded to 4 ceil(nv / 4) columns); writes rows and columns < nv (and the
+// padding column of an odd nv) of H (stride ldh elements of T), entries above the diagonal too.
+template <typename T>
+__device__ __forceinline__ void hessian_tc(const float* Ms, const float* Js, int ld, const float* c,
+                                           const int* idx, int na, int nv, T* H, int ldh,
+                                           int lane) {
+  const int g = lane >> 2, t = lane & 3;
+  const int ncol = (nv + 3) & ~3;
+  const bool two = nv > 16;
+  constexpr int kMt[6] = {0, 0, 1, 1, 1, 1}, kNt[6] = {0, 1, 0, 1, 2, 3};
+  float acc[6][4];
+#pragma unroll
+  for (int i = 0; i < 6; i++) {
+    const int r0 = 16 * kMt[i] + g, r1 = r0 + 8, cc = 8 * kNt[i] + 2 * t;
+    const float2 z = make_float2(0.f, 0.f);
+    const float2 v0 = (r0 < nv && cc < ncol) ? *reinterpret_cast<const float2*>(Ms + r0 * ld + cc) : z;
+    const float2 v1 = (r1 < nv && cc < ncol) ? *reinterpret_cast<const float2*>(Ms + r1 * ld + cc) : z;
+    acc[i][0] = v0.x;
+    acc[i][1] = v0.y;
+    acc[i][2] = v1.x;
+    acc[i][3] = v1.y;
+  }
+  for (int k0 = 0; k0 < na; k0 += 8) {
+    const int ka = k0 + t, kb = ka + 4;
+    const int ra = ka < na ? idx[ka] : -1, rb = kb < na ? idx[kb] : -1;
+    const float ca = ra >= 0 ? c[ra] : 0.f, cb = rb >= 0 ? c[rb] : 0.f;
+    float ja[4], jb[4];  // J[ra][g + 8 q], J[rb][g + 8 q]
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const int col = g + 8 * q;
+      ja[q] = (ra >= 0 && col < ncol) ? Js[ra * ld + col] : 0.f;
+      jb[q] = (rb >= 0 && col < ncol) ? Js[rb * ld + col] : 0.f;
+    }
+    const FragA a0 = frag_a(ja[0], ja[1], jb[0], jb[1]);  // rows 0..15 of A: dofs g, g + 8
+    FragB b[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) b[q] = frag_b(ca * ja[q], cb * jb[q]);
+    mma_3xtf32(acc[0], a0, b[0]);
+    mma_3xtf32(acc[1], a0, b[1]);
+    if (two) {
+      const FragA a1 = frag_a(ja[2], ja[3], jb[2], jb[3]);  // rows 16..31: dofs g + 16, g + 24
+#pragma unroll
+      for (int q = 0; q < 4; q++) mma_3xtf32(acc[2 + q], a1, b[q]);
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < 6; i++) {
+    if (i >= 2 && !two) break;
+    const int r0 = 16 * kMt[i] + g, r1 = r0 + 8, cc = 8 * kNt[i] + 2 * t;
+    if (cc < nv) {  // cc + 1 < nv, or the padding column of an odd nv (< ldh)
+      if (r0 < nv) {
+        H[r0 * ldh + cc] = T(acc[i][0]);
+        H[r0 * ldh + cc + 1] = T(acc[i][1]);
+      }
+      if (r1 < nv) {
+        H[r1 * ldh + cc] = T(acc[i][2]);
+        H[r1 * ldh + cc + 1] = T(acc[i][3]);
+      }
+    }
+  }
+}
+
 // Newton step direction H^-1 grad for nv <= 32 (solver.py:234-290).  When `refactor` is set,
 // lane i assembles row i of H = tril(qM) + sum_k c_k J_k^T J_k in registers (c_k = D_k for active
 // rows, 0 otherwise; inactive rows are skipped), stores it to the tile Ls and factors it in place;
 // otherwise Ls already holds the factor of the same H.  The coefficients come from C
 // (staged rows) or, when C is null, from the rows' active flags and D.  Returns element `lane` of the
 // solution.  Staged Jacobian rows are read as float4 broadcasts.
-template <bool PREC, bool ST>
+// TC (staged rows only): H is assembled by hessian_tc on the tensor pipe instead; ix is 32 ints
+// of warp scratch for its row list.
+template <bool PREC, bool ST, bool TC = false>
 __device__ __forceinline__ float newton_direction(const float* Ms, int ld, const float* J, int ldj,
                                                const float* C, const int* act,
                                                const float* D, int n, float* Ls, int nv,
                                                float grad, int lane, bool refactor,
-                                               double* Ld = nullptr) {
+                                               double* Ld = nullptr, int* ix = nullptr) {
   const int nq = (nv + 3) >> 2;
   const bool own = lane < nv;
-  if (refactor) {
+  if (TC && ST && refactor) {  // n <= 32: lane k owns row k; list the rows with a nonzero coefficient
+    const bool on = lane < n && C[lane] != 0.f;
+    const unsigned mk = __ballot_sync(WARP_FULL, on);
+    if (on) ix[__popc(mk & ((1u << lane) - 1u))] = lane;
+    __syncwarp();
+    if (PREC) {
+      hessian_tc(Ms, J, ldj, C, ix, __popc(mk), nv, Ld, ld, lane);
+      __syncwarp();
+      chol_tile_d(Ld, ld, nv, lane);
+    } else {
+      hessian_tc(Ms, J, ldj, C, ix, __popc(mk), nv, Ls, ld, lane);
+      __syncwarp();
+      chol_tile(Ls, ld, nv, lane);
+    }
+  } else if (refactor) {
     float h[32];  // row `lane` of qM (columns past nv are zero; entries above the diagonal unused)
     const float4* M4 = reinterpret_cast<const float4*>(Ms + min(lane, nv - 1) * ld);
 #pragma unroll
@@ -666,7 +750,7 @@ __device__ void small_update_constraint(Small& s) {
 }
 
 // solver.py:176-312
-template <bool PREC, bool ST, bool CG>
+template <bool PREC, bool ST, bool CG, bool TC>
 __device__ void small_update_gradient(Small& s) {
   const MjbModel& m = s.m;
   const MjbData& d = s.d;
@@ -695,9 +779,9 @@ __device__ void small_update_gradient(Small& s) {
     if (lane < s.n) s.F[lane] = s.ract ? s.rD : 0.f;
     __syncwarp();
   }
-  s.Mgrad = newton_direction<PREC, ST>(s.Ms, s.ld, s.J, s.ldj, staged ? s.F : nullptr,
+  s.Mgrad = newton_direction<PREC, ST, TC>(s.Ms, s.ld, s.J, s.ldj, staged ? s.F : nullptr,
                              d.efc_active + s.adr, d.efc_D + s.adr, s.n, s.Ls, nv, s.grad, lane,
-                             refactor, s.Ld);
+                             refactor, s.Ld, reinterpret_cast<int*>(s.vs));
   s.factored = true;
   s.factored_mask = mask;
 }
@@ -881,7 +965,7 @@ __device__ void small_linesearch(Small& s) {
 // The iterations of solve_small once the world's rows are placed.  ST: rows staged in shared
 // memory (n <= kSolverRows); CG: the CG solver (else Newton); LSP: the parallel line search (else
 // the iterative one) -- compile-time choices, so that each path's code is straight.
-template <bool PREC, bool ST, bool CG, bool LSP>
+template <bool PREC, bool ST, bool CG, bool LSP, bool TC>
 __device__ void solve_small_run(Small& s) {
   const MjbModel& m = s.m;
   const MjbData& d = s.d;
@@ -901,7 +985,7 @@ __device__ void solve_small_run(Small& s) {
   __syncwarp();
   s.Ma = s.mulM(s.qacc);
   small_update_constraint<ST>(s);
-  small_update_gradient<PREC, ST, CG>(s);
+  small_update_gradient<PREC, ST, CG, TC>(s);
   s.search = -s.Mgrad;
   s.search_dot = warp_sum(s.search * s.search);
   bool done = false;
@@ -911,7 +995,7 @@ __device__ void solve_small_run(Small& s) {
     prev_grad = s.grad;
     prev_Mgrad = s.Mgrad;
     small_update_constraint<ST>(s);
-    small_update_gradient<PREC, ST, CG>(s);
+    small_update_gradient<PREC, ST, CG, TC>(s);
     if (CG) {  // Polak-Ribiere (solver.py:918-970)
       const float num = warp_sum(s.own ? s.grad * (s.Mgrad - prev_Mgrad) : 0.f);
       const float den = warp_sum(s.own ? prev_grad * prev_Mgrad : 0.f);
@@ -960,7 +1044,7 @@ __device__ void solve_small_run(Small& s) {
 // solver.py:872-1000 for nv <= 32; sm: solver_smem_floats(nv) floats of warp-private scratch
 // PREC: the precision form (FP64 Hessian factor-solve and line-search sums; the double tile at
 // sm + solver_smem_floats(nv))
-template <bool PREC = false>
+template <bool PREC = false, bool TC = false>
 __device__ void solve_small(const MjbModel& m, const MjbData& d, int w, int lane, float* sm,
                             bool reuse) {
   const int nv = m.nv;
@@ -1000,15 +1084,15 @@ __device__ void solve_small(const MjbModel& m, const MjbData& d, int w, int lane
   __syncwarp();
   const bool cg = m.solver == 1, lsp = m.ls_parallel != 0;
   if (s.staged) {
-    if (!cg && !lsp) solve_small_run<PREC, true, false, false>(s);
-    else if (!cg) solve_small_run<PREC, true, false, true>(s);
-    else if (!lsp) solve_small_run<PREC, true, true, false>(s);
-    else solve_small_run<PREC, true, true, true>(s);
+    if (!cg && !lsp) solve_small_run<PREC, true, false, false, TC>(s);
+    else if (!cg) solve_small_run<PREC, true, false, true, TC>(s);
+    else if (!lsp) solve_small_run<PREC, true, true, false, TC>(s);
+    else solve_small_run<PREC, true, true, true, TC>(s);
   } else {
-    if (!cg && !lsp) solve_small_run<PREC, false, false, false>(s);
-    else if (!cg) solve_small_run<PREC, false, false, true>(s);
-    else if (!lsp) solve_small_run<PREC, false, true, false>(s);
-    else solve_small_run<PREC, false, true, true>(s);
+    if (!cg && !lsp) solve_small_run<PREC, false, false, false, TC>(s);
+    else if (!cg) solve_small_run<PREC, false, false, true, TC>(s);
+    else if (!lsp) solve_small_run<PREC, false, true, false, TC>(s);
+    else solve_small_run<PREC, false, true, true, TC>(s);
   }
 }
 
@@ -1017,10 +1101,11 @@ __device__ void solve_small(const MjbModel& m, const MjbData& d, int w, int lane
 // reuse: keep the Newton Hessian's factor across iterations with an unchanged active set.
 // For nv > 32 or a sparse mass matrix, sm (when given) is the generic solver's scratch of at least
 // generic_nz_floats(nv) floats.
-template <bool PREC = false>
+// TC: the Newton Hessian of staged rows assembled on the tensor pipe (split TF32, hessian_tc)
+template <bool PREC = false, bool TC = false>
 __device__ __forceinline__ void solve(const MjbModel& m, const MjbData& d, int w, int lane,
                                       float* sm, float* hs, bool reuse = false) {
-  if (m.nv <= 32 && sm && !m.is_sparse) solve_small<PREC>(m, d, w, lane, sm, reuse);
+  if (m.nv <= 32 && sm && !m.is_sparse) solve_small<PREC, TC>(m, d, w, lane, sm, reuse);
   else solve_generic(m, d, w, lane, hs, (m.nv > 32 || m.is_sparse) ? sm : nullptr, reuse);
 }
 

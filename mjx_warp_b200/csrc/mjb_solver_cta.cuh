@@ -1,0 +1,737 @@
+// The chosen form's constraint solver for large dense models (nv > 32): one CTA of NW warps per
+// world (solver.py:26-1000, the same algorithm as solve_generic).
+//
+// A world with hundreds of dofs and constraint rows is too much for one warp: the Newton
+// Hessian's factorisation (nv^3 / 3 multiply-adds) and the row loops (dense nv-wide Jacobian
+// rows) serialise on 32 lanes, and with 16 such warps per SM the per-world matrices (nv^2 floats
+// each) no longer fit in L2.  Here all NW warps of a CTA work on one world: per-row dot products
+// are warp-per-row (coalesced reads of the dense Jacobian rows), per-row scalars thread-per-row,
+// per-dof vectors thread-per-dof, and every per-world sum is a CTA reduction in a fixed order
+// (warp sums, then the warps' partials in warp order), identical in every thread, so control flow
+// stays uniform across the CTA.  The Hessian H = tril(qM) + sum_active D J'J is assembled in efc_h
+// (each warp updates the H rows it owns, row by row in constraint order, so no two warps touch the
+// same entry) and factored by chol_cta: a left-looking blocked Cholesky with 32-column panels
+// whose panel updates A[r, p] -= L[r, :p] L[p, :p]^T run on the tensor pipe in split TF32
+// (mjb_tc.cuh), the 32 x 32 diagonal blocks by chol_tile and the panel rows below by
+// substitution.  One world per CTA keeps each matrix being factored in L2.
+#pragma once
+
+#include "mjb_solver.cuh"
+
+namespace mjb {
+
+// CTA sums of K values: warp sums, then the NW warps' partials added in warp order; every thread
+// returns the totals.  red: K * NW elements of shared memory.
+template <int NW, int K, typename T>
+__device__ __forceinline__ void cta_sum(T (&v)[K], T* red, int warp, int lane) {
+#pragma unroll
+  for (int k = 0; k < K; k++) v[k] = warp_sum_t(v[k]);
+  if (lane == 0) {
+#pragma unroll
+    for (int k = 0; k < K; k++) red[k * NW + warp] = v[k];
+  }
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < K; k++) {
+    T s = red[k * NW];
+#pragma unroll
+    for (int q = 1; q < NW; q++) s += red[k * NW + q];
+    v[k] = s;
+  }
+  __syncthreads();
+}
+
+// the dof tree block [a, a + size) that contains dof i (binary search over block_adr)
+__device__ __forceinline__ void dof_block(const MjbModel& m, int i, int& a, int& size) {
+  int lo = 0, hi = m.nblock - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (m.block_adr[mid] <= i) lo = mid;
+    else hi = mid - 1;
+  }
+  a = m.block_adr[lo];
+  size = m.block_size[lo];
+}
+
+// Left-looking blocked Cholesky of the n x n SPD lower triangle of A (row stride ld, global
+// memory) by a CTA of NW warps: per 32-column panel p, (i) the panel's rows are updated with the
+// finished columns, A[r, p] -= L[r, :p] L[p, :p]^T for every row r >= p, as m16n8k8 tensor-core
+// tiles in split TF32 (16-row m-tiles dealt to the warps, the panel's 32 columns as 4 n-tiles),
+// (ii) warp 0 factors the 32 x 32 diagonal block in the shared tile T (chol_tile) and writes it
+// back with its reciprocal diagonal in T's column 32, (iii) every row below solves
+// L[r, p] = A[r, p] L_pp^-T, one thread per row.  T: 32 x 36 + 32 floats of shared memory.
+template <int NW>
+__device__ __noinline__ void chol_cta(float* A, int ld, int n, float* T, int warp, int lane) {
+  constexpr int TL = 36, kMt = 3;
+  const int g = lane >> 2, t = lane & 3;
+  for (int c0 = 0; c0 < n; c0 += 32) {
+    const int pn = min(32, n - c0);
+    if (c0 > 0) {
+      const int nmt = (n - c0 + 15) >> 4;
+      for (int mt0 = warp; mt0 < nmt; mt0 += NW * kMt) {
+        float acc[kMt][4][4];
+#pragma unroll
+        for (int q = 0; q < kMt; q++)
+#pragma unroll
+          for (int nt = 0; nt < 4; nt++)
+#pragma unroll
+            for (int e = 0; e < 4; e++) acc[q][nt][e] = 0.f;
+#pragma unroll 2
+        for (int k0 = 0; k0 < c0; k0 += 8) {
+          FragB b[4];  // B[k][j] = L[c0 + j][k0 + k], j = 8 nt + g
+#pragma unroll
+          for (int nt = 0; nt < 4; nt++) {
+            const int r = c0 + 8 * nt + g;
+            const float* Ar = A + size_t(r) * ld + k0;
+            b[nt] = r < n ? frag_b(Ar[t], Ar[t + 4]) : frag_b(0.f, 0.f);
+          }
+#pragma unroll
+          for (int q = 0; q < kMt; q++) {
+            const int mt = mt0 + q * NW;
+            if (mt < nmt) {
+              const int r0 = c0 + 16 * mt + g, r1 = r0 + 8;
+              const float* A0 = A + size_t(r0) * ld + k0;
+              const float* A1 = A + size_t(r1) * ld + k0;
+              const FragA a = frag_a(r0 < n ? A0[t] : 0.f, r1 < n ? A1[t] : 0.f,
+                                     r0 < n ? A0[t + 4] : 0.f, r1 < n ? A1[t + 4] : 0.f);
+#pragma unroll
+              for (int nt = 0; nt < 4; nt++) mma_3xtf32(acc[q][nt], a, b[nt]);
+            }
+          }
+        }
+#pragma unroll
+        for (int q = 0; q < kMt; q++) {
+          const int mt = mt0 + q * NW;
+          if (mt >= nmt) break;
+          const int r0 = c0 + 16 * mt + g, r1 = r0 + 8;
+#pragma unroll
+          for (int nt = 0; nt < 4; nt++) {
+            const int cc = c0 + 8 * nt + 2 * t;
+#pragma unroll
+            for (int e = 0; e < 2; e++) {
+              if (cc + e < c0 + pn) {
+                if (r0 < n) A[size_t(r0) * ld + cc + e] -= acc[q][nt][e];
+                if (r1 < n) A[size_t(r1) * ld + cc + e] -= acc[q][nt][2 + e];
+              }
+            }
+          }
+        }
+      }
+    }
+    __syncthreads();
+    if (warp == 0) {  // (ii)
+      for (int r = 0; r < pn; r++)
+        if (lane < pn) T[r * TL + lane] = lane <= r ? A[size_t(c0 + r) * ld + c0 + lane] : 0.f;
+      __syncwarp();
+      chol_tile(T, TL, pn, lane);
+      for (int r = 0; r < pn; r++)
+        if (lane <= r) A[size_t(c0 + r) * ld + c0 + lane] = T[r * TL + lane];
+      if (lane < pn) T[lane * TL + 32] = __frcp_rn(T[lane * TL + lane]);
+    }
+    __syncthreads();
+    for (int i = c0 + pn + int(threadIdx.x); i < n; i += NW * 32) {  // (iii)
+      float* Ai = A + size_t(i) * ld + c0;
+      float x[32];
+#pragma unroll
+      for (int c = 0; c < 32; c++) x[c] = c < pn ? Ai[c] : 0.f;
+#pragma unroll
+      for (int c = 0; c < 32; c++) {
+        if (c < pn) {
+          float v = x[c];
+#pragma unroll
+          for (int q = 0; q < c; q++) v -= x[q] * T[c * TL + q];
+          x[c] = v * T[c * TL + 32];
+        }
+      }
+#pragma unroll
+      for (int c = 0; c < 32; c++)
+        if (c < pn) Ai[c] = x[c];
+    }
+    __syncthreads();
+  }
+}
+
+// x = (L L^T)^-1 y by a CTA of NW warps for the n x n lower factor L in global memory (row stride
+// ld), blocked by 32: forward, each block's partial y_b - L[b, :b] z[:b] is a row-per-warp dot
+// product over the finished part (coalesced row reads, warp sums), then warp 0 solves the 32 x 32
+// diagonal block with its rows in registers; backward, each block's partial
+// z_b - L[b+:, b]^T x[b+:] is accumulated warp-per-row over the rows below (lane j reads the
+// row's entry in column j of the block, coalesced), reduced across the warps in red, then warp 0
+// solves L_bb^T.  z: n floats of shared memory (the intermediate vector); red: 32 NW floats.
+// x and y are in global memory (x may alias y).
+template <int NW>
+__device__ __noinline__ void cho_solve_cta(const float* L, int ld, int n, float* x, const float* y,
+                                           float* z, float* red, int warp, int lane) {
+  for (int c0 = 0; c0 < n; c0 += 32) {  // L z = y
+    const int pn = min(32, n - c0);
+    for (int j = warp; j < pn; j += NW) {
+      const float* Lr = L + size_t(c0 + j) * ld;
+      float a = 0.f;
+      for (int k = lane; k < c0; k += 32) a += Lr[k] * z[k];
+      a = warp_sum(a);
+      if (lane == 0) z[c0 + j] = y[c0 + j] - a;
+    }
+    __syncthreads();
+    if (warp == 0) {
+      float r[32];  // row `lane` of the diagonal block
+      const float* Lr = L + size_t(c0 + min(lane, pn - 1)) * ld + c0;
+#pragma unroll
+      for (int q = 0; q < 32; q++) r[q] = (q < pn && q <= lane && lane < pn) ? Lr[q] : 1.f;
+      float zi = lane < pn ? z[c0 + lane] : 0.f;
+#pragma unroll
+      for (int q = 0; q < 32; q++) {
+        if (q < pn) {
+          const float zq = __shfl_sync(WARP_FULL, zi, q) / __shfl_sync(WARP_FULL, r[q], q);
+          if (lane == q) zi = zq;
+          else if (lane > q && lane < pn) zi -= r[q] * zq;
+        }
+      }
+      if (lane < pn) z[c0 + lane] = zi;
+    }
+    __syncthreads();
+  }
+  const int nb = (n + 31) / 32;
+  for (int b = nb - 1; b >= 0; b--) {  // L^T x = z
+    const int c0 = 32 * b, pn = min(32, n - c0);
+    float acc = 0.f;  // lane j: sum over this warp's rows i below the block of L[i][c0 + j] x[i]
+    for (int i = c0 + pn + warp; i < n; i += NW)
+      if (lane < pn) acc += L[size_t(i) * ld + c0 + lane] * z[i];
+    red[warp * 32 + lane] = acc;
+    __syncthreads();
+    if (warp == 0) {
+      float t = 0.f;
+#pragma unroll
+      for (int q = 0; q < NW; q++) t += red[q * 32 + lane];
+      float xi = lane < pn ? z[c0 + lane] - t : 0.f;
+      // back substitution with L_bb^T: column lane of L_bb is row lane of L_bb^T
+      for (int q = pn - 1; q >= 0; q--) {
+        const float lq = lane < q ? L[size_t(c0 + q) * ld + c0 + lane] : 0.f;
+        const float xq = __shfl_sync(WARP_FULL, xi, q) / L[size_t(c0 + q) * ld + c0 + q];
+        if (lane == q) xi = xq;
+        else if (lane < q) xi -= lq * xq;
+      }
+      if (lane < pn) z[c0 + lane] = xi;
+    }
+    __syncthreads();
+  }
+  for (int i = threadIdx.x; i < n; i += NW * 32) x[i] = z[i];
+  __syncthreads();
+}
+
+// Per-CTA shared memory of the solver (floats): reductions (16 NW, as doubles 32 NW), the
+// diagonal tile (32 x 36 + 32), each warp's row-compaction scratch and the triangular solves'
+// vector (nv); the precision form adds
+// the FP64 Hessian tile (nv rows of cta_ld_d(nv) doubles, 8-byte aligned after the floats).
+__host__ __device__ __forceinline__ int cta_ld_d(int nv) { return nv | 1; }
+__host__ __device__ __forceinline__ int cta_solver_smem_base(int nv, int nw) {
+  return round4i(32 * nw + 32 * 36 + 32 + nw * 2 * round4i(nv) + round4i(nv));
+}
+__host__ __device__ __forceinline__ int cta_solver_smem_floats(int nv, int nw, bool prec = false) {
+  const int base = cta_solver_smem_base(nv, nw);
+  return prec ? base + 2 * (nv * cta_ld_d(nv) + nv + 1) : base;
+}
+
+// FP64 counterpart of chol_cta for the precision form, on an n x n lower triangle held in shared
+// memory (row stride ld doubles): per 32-column panel, (i) every entry (r, j) of the panel's rows
+// r >= p subtracts its dot product over the finished columns, one entry per thread at a time;
+// (ii) warp 0 factors the diagonal block in place (chol_tile_d); (iii) the rows below solve
+// against it, one thread per row.
+template <int NW>
+__device__ __noinline__ void chol_cta_d(double* A, int ld, int n, int warp, int lane) {
+  constexpr int NT = NW * 32;
+  for (int c0 = 0; c0 < n; c0 += 32) {
+    const int pn = min(32, n - c0);
+    if (c0 > 0) {
+      const int cnt = (n - c0) * pn;
+      for (int e = int(threadIdx.x); e < cnt; e += NT) {
+        const int r = c0 + e / pn, j = c0 + e % pn;
+        if (j > r) continue;
+        const double* Ar = A + r * ld;
+        const double* Aj = A + j * ld;
+        double s0 = 0.0, s1 = 0.0;
+        int k = 0;
+        for (; k + 1 < c0; k += 2) {
+          s0 += Ar[k] * Aj[k];
+          s1 += Ar[k + 1] * Aj[k + 1];
+        }
+        if (k < c0) s0 += Ar[k] * Aj[k];
+        A[r * ld + j] -= s0 + s1;
+      }
+      __syncthreads();
+    }
+    if (warp == 0) chol_tile_d(A + c0 * ld + c0, ld, pn, lane);
+    __syncthreads();
+    for (int i = c0 + pn + int(threadIdx.x); i < n; i += NT) {
+      double* Ai = A + i * ld + c0;
+      for (int c = 0; c < pn; c++) {
+        double v = Ai[c];
+        const double* Lc = A + (c0 + c) * ld + c0;
+        for (int q = 0; q < c; q++) v -= Ai[q] * Lc[q];
+        Ai[c] = v / Lc[c];
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// x = (L L^T)^-1 y for the FP64 factor L in shared memory (row stride ld), one warp, in FP64
+// with the intermediate vector in v (n doubles of shared memory); x and y are n floats in
+// global memory (x may alias y).
+__device__ void cho_solve_d_warp(const double* L, int ld, int n, double* v, float* x,
+                                 const float* y, int lane) {
+  for (int i = lane; i < n; i += 32) v[i] = double(y[i]);
+  __syncwarp();
+  for (int k = 0; k < n; k++) {  // L z = y, a column at a time; lanes update the rows below
+    const double zk = v[k] / L[k * ld + k];
+    __syncwarp();
+    if (lane == (k & 31)) v[k] = zk;
+    for (int i = k + 1 + lane; i < n; i += 32) v[i] -= L[i * ld + k] * zk;
+    __syncwarp();
+  }
+  for (int k = n - 1; k >= 0; k--) {  // L^T x = z
+    const double xk = v[k] / L[k * ld + k];
+    __syncwarp();
+    if (lane == (k & 31)) v[k] = xk;
+    for (int i = lane; i < k; i += 32) v[i] -= L[k * ld + i] * xk;
+    __syncwarp();
+  }
+  for (int i = lane; i < n; i += 32) x[i] = float(v[i]);
+  __syncwarp();
+}
+
+template <int NW, bool PREC>
+struct CtaSolver {
+  const MjbModel& m;
+  const MjbData& d;
+  int w, tid, lane, warp, nv, adr, n;
+  float *qacc, *Ma, *grad, *Mgrad, *search, *mv, *qfrc_constraint, *H;
+  const float *qM, *qfrc_smooth, *qacc_smooth;
+  float* red;    // 16 NW floats (or 16 NW doubles over the same space)
+  float* T;      // chol_cta's diagonal tile
+  float* nz;     // this warp's row compaction: round4(nv) ints, then round4(nv) floats
+  float* zv;     // the triangular solves' intermediate vector (nv floats)
+  double* Ld;    // precision form: the Hessian's FP64 factor (nv rows of ldd doubles)
+  double* vd;    // precision form: the FP64 solve's vector (nv doubles)
+  int ldd;
+  bool reuse = true, factored = false, changed = true;
+  float cost, prev_cost, gauss, grad_dot, search_dot, gtol, alpha, beta;
+  float qg[3];
+  static constexpr int NT = NW * 32;
+
+  template <int K>
+  __device__ __forceinline__ void sum(float (&v)[K]) { cta_sum<NW, K, float>(v, red, warp, lane); }
+  // line-search coefficient sums: base + the CTA's sum of x, in FP64 in the precision form
+  template <int K>
+  __device__ __forceinline__ void ls_sums(const float (&base)[K], float (&x)[K]) {
+    if (PREC) {
+      double v[K];
+#pragma unroll
+      for (int k = 0; k < K; k++) v[k] = double(x[k]);
+      cta_sum<NW, K, double>(v, reinterpret_cast<double*>(red), warp, lane);
+#pragma unroll
+      for (int k = 0; k < K; k++) x[k] = float(double(base[k]) + v[k]);
+    } else {
+      sum<K>(x);
+#pragma unroll
+      for (int k = 0; k < K; k++) x[k] = base[k] + x[k];
+    }
+  }
+
+  // res = M vec, the dense mass matrix within each dof tree block (support.py:45-92)
+  __device__ void mul_m(float* res, const float* vec) {
+    for (int i = tid; i < nv; i += NT) {
+      int a, size;
+      dof_block(m, i, a, size);
+      const float* row = qM + size_t(i) * nv;
+      float s = 0.f;
+      for (int j = a; j < a + size; j++) s += row[j] * vec[j];
+      res[i] = s;
+    }
+    __syncthreads();
+  }
+
+  // out[r] = J_r . x - sub[r] for every row (warp per row); sub may be null
+  __device__ void rows_dot(const float* x, float* out, const float* sub) {
+    for (int k = warp; k < n; k += NW) {
+      const float* J = d.efc_J + size_t(adr + k) * nv;
+      float v = 0.f;
+      for (int i = lane; i < nv; i += 32) v += J[i] * x[i];
+      v = warp_sum(v);
+      if (lane == 0) out[adr + k] = sub ? v - sub[adr + k] : v;
+    }
+    __syncthreads();
+  }
+
+  // solver.py:75-173
+  __device__ void update_constraint() {
+    prev_cost = cost;
+    float c[2] = {0.f, 0.f};
+    bool ch = false;
+    for (int k = tid; k < n; k += NT) {
+      const int r = adr + k;
+      const float Jaref = d.efc_Jaref[r], D = d.efc_D[r];
+      const int active = Jaref < 0.f;
+      ch |= d.efc_active[r] != active;
+      d.efc_active[r] = active;
+      if (active) {
+        d.efc_force[r] = -1.f * D * Jaref;
+        c[0] += 0.5f * D * Jaref * Jaref;
+      } else {
+        d.efc_force[r] = 0.f;
+      }
+    }
+    changed = __syncthreads_or(ch) != 0;
+    for (int i = tid; i < nv; i += NT) {
+      float f = 0.f;
+      for (int k = 0; k < n; k++) {
+        const float fk = d.efc_force[adr + k];
+        if (fk != 0.f) f += d.efc_J[size_t(adr + k) * nv + i] * fk;
+      }
+      qfrc_constraint[i] = f;
+      c[1] += 0.5f * (Ma[i] - qfrc_smooth[i]) * (qacc[i] - qacc_smooth[i]);
+    }
+    sum<2>(c);
+    gauss = c[1];
+    cost = c[0] + c[1];
+  }
+
+  // H = tril(qM) + sum over active rows of D J'J in efc_h (update_gradient's Newton Hessian,
+  // solver.py:249-276): warp q owns the H rows i with i % NW == q, and applies each row's outer
+  // product over the row's nonzero columns to those rows in constraint order, so every entry sees
+  // the reference's sequence of additions and no two warps write the same entry.
+  __device__ void assemble_hessian() {
+    for (int i = warp; i < nv; i += NW) {  // the lower triangle of qM, a coalesced row per warp
+      const float* Mi = qM + size_t(i) * nv;
+      float* Hi = H + size_t(i) * nv;
+      for (int j = lane; j <= i; j += 32) Hi[j] = Mi[j];
+    }
+    __syncthreads();
+    int* nzi = reinterpret_cast<int*>(nz);
+    float* nzv = nz + round4i(nv);
+    for (int k = 0; k < n; k++) {
+      const int r = adr + k;
+      if (!d.efc_active[r]) continue;
+      const float D = d.efc_D[r];
+      if (D == 0.f) continue;
+      const float* J = d.efc_J + size_t(r) * nv;
+      int cnt = 0;
+      for (int base = 0; base < nv; base += 32) {
+        const int c = base + lane;
+        const float v = c < nv ? J[c] : 0.f;
+        const unsigned mk = __ballot_sync(WARP_FULL, v != 0.f);
+        if (v != 0.f) {
+          const int p = cnt + __popc(mk & ((1u << lane) - 1u));
+          nzi[p] = c;
+          nzv[p] = v;
+        }
+        cnt += __popc(mk);
+      }
+      __syncwarp();
+      for (int a = 0; a < cnt; a++) {
+        const int i = nzi[a];
+        if (i % NW != warp) continue;
+        float* Hi = H + size_t(i) * nv;
+        const float va = nzv[a];
+        for (int b = lane; b <= a; b += 32) Hi[nzi[b]] += va * nzv[b] * D;
+      }
+      __syncwarp();
+    }
+    __syncthreads();
+  }
+
+  // solver.py:176-312
+  __device__ void update_gradient() {
+    float gd[1] = {0.f};
+    for (int i = tid; i < nv; i += NT) {
+      const float g = Ma[i] - qfrc_smooth[i] - qfrc_constraint[i];
+      grad[i] = g;
+      gd[0] += g * g;
+    }
+    sum<1>(gd);
+    grad_dot = gd[0];
+    if (m.solver == 1) {  // CG: Mgrad = M^-1 grad
+      if (warp == 0) solve_m_world(m, d, w, Mgrad, grad, lane);
+      __syncthreads();
+      return;
+    }
+    if (!(reuse && factored && !changed)) {
+      assemble_hessian();
+      if (PREC) {  // the FP32-assembled H factored in FP64 in shared memory
+        for (int e = tid; e < nv * nv; e += NT) {
+          const int i = e / nv, j = e - i * nv;
+          if (j <= i) Ld[i * ldd + j] = double(H[e]);
+        }
+        __syncthreads();
+        chol_cta_d<NW>(Ld, ldd, nv, warp, lane);
+        for (int e = tid; e < nv * nv; e += NT) {  // efc_h keeps the factor (FP32-rounded)
+          const int i = e / nv, j = e - i * nv;
+          if (j <= i) H[e] = float(Ld[i * ldd + j]);
+        }
+      } else {
+        chol_cta<NW>(H, nv, nv, T, warp, lane);
+      }
+      factored = true;
+    }
+    if (warp == 0) {
+      if (PREC) cho_solve_d_warp(Ld, ldd, nv, vd, Mgrad, grad, lane);
+    }
+    if (!PREC) cho_solve_cta<NW>(H, nv, nv, Mgrad, grad, zv, red, warp, lane);
+    __syncthreads();
+  }
+
+  // solver.py:737-869 with the iterative (:339-664) or parallel (:667-734) line search
+  __device__ void linesearch() {
+    mul_m(mv, search);
+    {
+      float q[3] = {0.f, 0.f, 0.f};
+      for (int i = tid; i < nv; i += NT) {
+        q[0] += gauss / float(nv);
+        q[1] += search[i] * (Ma[i] - qfrc_smooth[i]);
+        q[2] += 0.5f * search[i] * mv[i];
+      }
+      const float z[3] = {0.f, 0.f, 0.f};
+      ls_sums<3>(z, q);
+      qg[0] = q[0];
+      qg[1] = q[1];
+      qg[2] = q[2];
+    }
+    rows_dot(search, d.efc_jv, nullptr);
+    for (int k = tid; k < n; k += NT) {
+      const int r = adr + k;
+      const float jv = d.efc_jv[r], Jaref = d.efc_Jaref[r], D = d.efc_D[r];
+      d.efc_quad[3 * r] = 0.5f * Jaref * Jaref * D;
+      d.efc_quad[3 * r + 1] = jv * Jaref * D;
+      d.efc_quad[3 * r + 2] = 0.5f * jv * jv * D;
+    }
+    __syncthreads();
+    if (m.ls_parallel) {
+      int best = 0;
+      float bestc = 0.f;
+      for (int c = 0; c < m.nlsp; c++) {
+        const float a = m.alpha_candidate[c];
+        float tt[3] = {0.f, 0.f, 0.f};
+        for (int k = tid; k < n; k += NT) {
+          const int r = adr + k;
+          if (d.efc_Jaref[r] + a * d.efc_jv[r] < 0.f) {
+            tt[0] += d.efc_quad[3 * r];
+            tt[1] += d.efc_quad[3 * r + 1];
+            tt[2] += d.efc_quad[3 * r + 2];
+          }
+        }
+        ls_sums<3>(qg, tt);
+        const float cst = a * a * tt[2] + a * tt[1] + tt[0];
+        if (c == 0 || cst < bestc) {
+          bestc = cst;
+          best = c;
+        }
+      }
+      alpha = m.alpha_candidate[best];
+    } else {
+      const float scale = m.meaninertia * float(max(1, nv));
+      gtol = m.tolerance * m.ls_tolerance * sqrtf(search_dot) * scale;
+      float p0[3] = {0.f, 0.f, 0.f};
+      for (int k = tid; k < n; k += NT) {
+        const int r = adr + k;
+        if (d.efc_Jaref[r] >= 0.f) continue;
+        p0[0] += d.efc_quad[3 * r];
+        p0[1] += d.efc_quad[3 * r + 1];
+        p0[2] += 2.f * d.efc_quad[3 * r + 2];
+      }
+      {
+        const float base[3] = {qg[0], qg[1], 2.f * qg[2]};
+        ls_sums<3>(base, p0);
+      }
+      // the total cost polynomial's value and derivatives at up to three step sizes at once
+      auto totals = [&](int na, const float* al, float (*out)[3]) {
+        float acc[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        for (int k = tid; k < n; k += NT) {
+          const int r = adr + k;
+          const float jaref = d.efc_Jaref[r], jv = d.efc_jv[r];
+          const float* q = d.efc_quad + 3 * r;
+          for (int t = 0; t < na; t++) {
+            if (jaref + al[t] * jv < 0.f) {
+              float p[3];
+              eval_pt3(q, al[t], p);
+              acc[3 * t] += p[0];
+              acc[3 * t + 1] += p[1];
+              acc[3 * t + 2] += p[2];
+            }
+          }
+        }
+        float base[9];
+        for (int t = 0; t < 3; t++) {
+          float gq[3] = {0.f, 0.f, 0.f};
+          if (t < na) eval_pt3(qg, al[t], gq);
+          base[3 * t] = gq[0];
+          base[3 * t + 1] = gq[1];
+          base[3 * t + 2] = gq[2];
+        }
+        ls_sums<9>(base, acc);
+        for (int t = 0; t < na; t++) {
+          out[t][0] = acc[3 * t];
+          out[t][1] = acc[3 * t + 1];
+          out[t][2] = acc[3 * t + 2];
+        }
+      };
+      float lo_alpha = -safe_div(p0[1], p0[2]);
+      float lo[3], hi[3], hi_alpha;
+      {
+        float o[1][3];
+        totals(1, &lo_alpha, o);
+        lo[0] = o[0][0]; lo[1] = o[0][1]; lo[2] = o[0][2];
+      }
+      if (lo[1] < p0[1]) {
+        hi[0] = p0[0]; hi[1] = p0[1]; hi[2] = p0[2];
+        hi_alpha = 0.f;
+      } else {
+        hi[0] = lo[0]; hi[1] = lo[1]; hi[2] = lo[2];
+        hi_alpha = lo_alpha;
+        lo[0] = p0[0]; lo[1] = p0[1]; lo[2] = p0[2];
+        lo_alpha = 0.f;
+      }
+      bool done = false;
+      for (int it = 0; it < m.ls_iterations && !done; it++) {
+        float al[3] = {lo_alpha - safe_div(lo[1], lo[2]), hi_alpha - safe_div(hi[1], hi[2]),
+                       0.5f * (lo_alpha + hi_alpha)};
+        float o[3][3];
+        totals(3, al, o);
+        float *lon = o[0], *hin = o[1], *mid = o[2];
+        // _swap (solver.py:537-617)
+        const bool s1 = in_bracket(lo, lon);
+        if (s1) { lo[0] = lon[0]; lo[1] = lon[1]; lo[2] = lon[2]; lo_alpha = al[0]; }
+        const bool s2 = in_bracket(lo, mid);
+        if (s2) { lo[0] = mid[0]; lo[1] = mid[1]; lo[2] = mid[2]; lo_alpha = al[2]; }
+        const bool s3 = in_bracket(lo, hin);
+        if (s3) { lo[0] = hin[0]; lo[1] = hin[1]; lo[2] = hin[2]; lo_alpha = al[1]; }
+        const bool t1 = in_bracket(hi, hin);
+        if (t1) { hi[0] = hin[0]; hi[1] = hin[1]; hi[2] = hin[2]; hi_alpha = al[1]; }
+        const bool t2 = in_bracket(hi, mid);
+        if (t2) { hi[0] = mid[0]; hi[1] = mid[1]; hi[2] = mid[2]; hi_alpha = al[2]; }
+        const bool t3 = in_bracket(hi, lon);
+        if (t3) { hi[0] = lon[0]; hi[1] = lon[1]; hi[2] = lon[2]; hi_alpha = al[0]; }
+        done = (!(s1 || s2 || s3) && !(t1 || t2 || t3)) || (lo[1] < 0.f && lo[1] > -gtol) ||
+               (hi[1] > 0.f && hi[1] < gtol);
+        float a = 0.f;
+        const bool improved = lo[0] < p0[0] || hi[0] < p0[0];
+        const bool lo_better = lo[0] < hi[0];
+        if (improved && lo_better) a = lo_alpha;
+        if (improved && !lo_better) a = hi_alpha;
+        alpha = a;
+      }
+    }
+    // solver.py:816-841
+    for (int i = tid; i < nv; i += NT) {
+      qacc[i] += alpha * search[i];
+      Ma[i] += alpha * mv[i];
+    }
+    for (int k = tid; k < n; k += NT) d.efc_Jaref[adr + k] += alpha * d.efc_jv[adr + k];
+    __syncthreads();
+  }
+
+  // search = -Mgrad (+ beta search for CG); returns search . search
+  __device__ void new_search() {
+    float sd[1] = {0.f};
+    for (int i = tid; i < nv; i += NT) {
+      float v = -Mgrad[i];
+      if (m.solver == 1) v += beta * search[i];
+      search[i] = v;
+      sd[0] += v * v;
+    }
+    sum<1>(sd);
+    search_dot = sd[0];
+  }
+
+  __device__ void run() {
+    const float* ws = d.qacc_warmstart + W(w, nv);
+    for (int i = tid; i < nv; i += NT) qacc[i] = ws[i];
+    __syncthreads();
+    // _create_context (solver.py:26-72)
+    cost = __int_as_float(0x7f800000);
+    search_dot = 0.f;
+    alpha = 0.f;
+    gtol = 0.f;
+    beta = 0.f;
+    qg[0] = qg[1] = qg[2] = 0.f;
+    rows_dot(qacc, d.efc_Jaref, d.efc_aref);
+    mul_m(Ma, qacc);
+    update_constraint();
+    update_gradient();
+    new_search();
+    float* prev_grad = d.efc_prev_grad ? d.efc_prev_grad + W(w, nv) : nullptr;
+    float* prev_Mgrad = d.efc_prev_Mgrad ? d.efc_prev_Mgrad + W(w, nv) : nullptr;
+    bool done = false;
+    for (int it = 0; it < m.iterations && !done; it++) {
+      linesearch();
+      if (m.solver == 1) {
+        for (int i = tid; i < nv; i += NT) {
+          prev_grad[i] = grad[i];
+          prev_Mgrad[i] = Mgrad[i];
+        }
+        __syncthreads();
+      }
+      update_constraint();
+      update_gradient();
+      if (m.solver == 1) {  // Polak-Ribiere (solver.py:918-970)
+        float nd[2] = {0.f, 0.f};
+        for (int i = tid; i < nv; i += NT) {
+          nd[0] += grad[i] * (Mgrad[i] - prev_Mgrad[i]);
+          nd[1] += prev_grad[i] * prev_Mgrad[i];
+        }
+        sum<2>(nd);
+        beta = fmaxf(0.f, nd[0] / fmaxf(kMinVal, nd[1]));
+      }
+      new_search();
+      const float scale = m.meaninertia * float(max(1, nv));
+      done = (prev_cost - cost) / scale < m.tolerance || sqrtf(grad_dot) / scale < m.tolerance;
+    }
+    float* wsw = d.qacc_warmstart + W(w, nv);
+    for (int i = tid; i < nv; i += NT) wsw[i] = qacc[i];
+    if (tid == 0) {
+      if (d.efc_cost) d.efc_cost[w] = cost;
+      if (d.efc_prev_cost) d.efc_prev_cost[w] = prev_cost;
+      if (d.efc_gauss) d.efc_gauss[w] = gauss;
+      if (d.efc_grad_dot) d.efc_grad_dot[w] = grad_dot;
+      if (d.efc_search_dot) d.efc_search_dot[w] = search_dot;
+      if (d.efc_gtol) d.efc_gtol[w] = gtol;
+      if (d.efc_alpha) d.efc_alpha[w] = alpha;
+      if (d.efc_beta) d.efc_beta[w] = beta;
+      if (d.efc_done) d.efc_done[w] = done ? 1 : 0;
+      if (d.efc_solver_niter) d.efc_solver_niter[w] = 0;  // never advanced by the reference
+      if (d.efc_quad_gauss) {
+        d.efc_quad_gauss[3 * w] = qg[0];
+        d.efc_quad_gauss[3 * w + 1] = qg[1];
+        d.efc_quad_gauss[3 * w + 2] = qg[2];
+      }
+    }
+    __syncthreads();
+  }
+};
+
+// One world's solve by the whole CTA; smem: cta_solver_smem_floats(nv, NW) floats
+template <int NW, bool PREC>
+__device__ void solve_cta(const MjbModel& m, const MjbData& d, int w, float* smem) {
+  const int nv = m.nv;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  CtaSolver<NW, PREC> s{m, d, w, tid, lane, warp, nv, d.world_efcadr[w], d.world_nefc[w]};
+  s.qacc = d.qacc + W(w, nv);
+  s.Ma = d.efc_Ma + W(w, nv);
+  s.grad = d.efc_grad + W(w, nv);
+  s.Mgrad = d.efc_Mgrad + W(w, nv);
+  s.search = d.efc_search + W(w, nv);
+  s.mv = d.efc_mv + W(w, nv);
+  s.qfrc_constraint = d.qfrc_constraint + W(w, nv);
+  s.H = d.efc_h + W(w, nv * nv);
+  s.qM = d.qM + W(w, nv * nv);
+  s.qfrc_smooth = d.qfrc_smooth + W(w, nv);
+  s.qacc_smooth = d.qacc_smooth + W(w, nv);
+  s.red = smem;
+  s.T = smem + 32 * NW;
+  s.nz = smem + 32 * NW + 32 * 36 + 32 + warp * 2 * round4i(nv);
+  s.zv = smem + 32 * NW + 32 * 36 + 32 + NW * 2 * round4i(nv);
+  s.ldd = cta_ld_d(nv);
+  s.Ld = PREC ? reinterpret_cast<double*>(smem + cta_solver_smem_base(nv, NW)) : nullptr;
+  s.vd = PREC ? s.Ld + nv * s.ldd : nullptr;
+  s.run();
+}
+
+}  // namespace mjb

@@ -228,3 +228,87 @@ def closest_segments(a0, a1, b0, b1, precision: int = 64):
   lib.oracle_closest_segments(*[a.ctypes.data_as(_D) for a in arrs], pa.ctypes.data_as(_D),
                               pb.ctypes.data_as(_D), precision)
   return pa, pb
+
+
+def qacc_references(mjm, qpos, qvel, ctrl, warmstart, nthreads: int = 0, nperturb: int = 24,
+                    seed: int = 0) -> dict:
+  """qacc of one forward from the same per-world state by the restatement in FP64 and in FP32,
+  plus how far the FP64 iterate is from convergence and how far rounding alone moves it.
+  Returns a dict of per-world arrays: fp64, fp32 (qacc); fp64_unconverged = the FP64 iterate's
+  distance from the converged FP64 solution (100 Newton / 50 line-search iterations); fp64_spread
+  = the largest change of FP64 solves from inputs perturbed by up to one FP32 ulp (relative
+  2^-23, 2 draws); fp32_worst = the largest error against FP64 of any FP32 realisation
+  (unperturbed, or from such perturbed inputs, `nperturb` draws); all as
+  ||x - y|| / max(||y||, 1)."""
+  import copy
+
+  def run(model, prec, inputs):
+    o = Oracle(model, qpos.shape[0], prec)
+    for k, v in inputs.items():
+      o.set(k, v)
+    o.run("forward", nthreads=nthreads)
+    return o.get("qacc")
+
+  base = {"qpos": qpos, "qvel": qvel, "qacc_warmstart": warmstart}
+  if mjm.nu:
+    base["ctrl"] = ctrl
+  ref64 = run(mjm, 64, base)
+  ref32 = run(mjm, 32, base)
+  conv = copy.deepcopy(mjm)
+  conv.opt.iterations, conv.opt.ls_iterations = 100, 50
+  unconverged = rel_err(ref64, run(conv, 64, base))
+  rng = np.random.default_rng(seed)
+  spread = np.zeros(qpos.shape[0])
+  worst32 = rel_err(ref32, ref64)
+  for t in range(nperturb):
+    pert = {k: v * (1.0 + rng.uniform(-1.0, 1.0, v.shape) * 2.0 ** -23) for k, v in base.items()}
+    worst32 = np.maximum(worst32, rel_err(run(mjm, 32, pert), ref64))
+    if t < 2:
+      spread = np.maximum(spread, rel_err(run(mjm, 64, pert), ref64))
+  return {"fp64": ref64, "fp32": ref32, "fp64_unconverged": unconverged, "fp64_spread": spread,
+          "fp32_worst": worst32}
+
+
+def rel_err(a, b) -> np.ndarray:
+  """Per-world ||a - b|| / max(||b||, 1)."""
+  a = np.asarray(a, dtype=np.float64).reshape(a.shape[0], -1)
+  b = np.asarray(b, dtype=np.float64).reshape(b.shape[0], -1)
+  e = np.linalg.norm(a - b, axis=1) / np.maximum(np.linalg.norm(b, axis=1), 1.0)
+  return np.where(np.isfinite(e), e, np.inf)
+
+
+def classify_qacc(q, refs: dict, tol: float = 1e-4) -> dict:
+  """Splits the worlds where q (the device's qacc) misses FP64 by more than tol into: within tol of
+  the FP32 restatement (the same miss as an FP32 implementation of the reference's algorithm
+  makes); path-dependent (at these iteration counts the FP64 iterate is itself more than tol from
+  the converged solution, so which line-search / active-set path the iterations take decides the
+  result, or an FP32 realisation of the restatement from inputs within one ulp also misses, or
+  FP64 moves by more than tol under such perturbations); and unexplained (none of these).
+  refs: qacc_references' dict."""
+  ref64, ref32 = refs["fp64"], refs["fp32"]
+  e64 = rel_err(q, ref64)
+  e32 = rel_err(q, ref32)
+  o32 = rel_err(ref32, ref64)
+  sensitive = ((refs["fp64_unconverged"] > tol) | (refs["fp32_worst"] > tol)
+               | (refs["fp64_spread"] > tol))
+  over = e64 > tol
+  near32 = over & (e32 <= tol)
+  sens = over & ~near32 & sensitive
+  unexplained = over & ~near32 & ~sens
+  return {"worlds": int(len(e64)), "frac_le_tol_vs_fp64": float(np.mean(~over)),
+          "frac_le_tol_vs_fp32_restatement": float(np.mean(e32 <= tol)),
+          "median_vs_fp64": float(np.median(e64)), "max_vs_fp64": float(e64.max()),
+          "median_vs_fp32_restatement": float(np.median(e32)),
+          "over_tol": int(over.sum()), "over_tol_within_tol_of_fp32_restatement": int(near32.sum()),
+          "over_tol_path_dependent": int(sens.sum()), "over_tol_unexplained": int(unexplained.sum()),
+          "fp32_restatement_frac_le_tol_vs_fp64": float(np.mean(o32 <= tol)),
+          "unconverged_worlds": int(np.sum(refs["fp64_unconverged"] > tol)),
+          "path_dependent_worlds": int(np.sum(sensitive)),
+          "frac_le_tol_vs_fp64_in_converged_worlds":
+              float(np.mean(~over[refs["fp64_unconverged"] <= tol]))
+              if np.any(refs["fp64_unconverged"] <= tol) else None,
+          "unexplained_worlds": {int(i): {"vs_fp64": float(e64[i]), "vs_fp32": float(e32[i]),
+                                          "fp32_worst": float(refs["fp32_worst"][i]),
+                                          "fp64_spread": float(refs["fp64_spread"][i]),
+                                          "fp64_unconverged": float(refs["fp64_unconverged"][i])}
+                                 for i in np.nonzero(unexplained)[0][:16]}}

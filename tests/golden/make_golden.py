@@ -1,7 +1,7 @@
 """Regenerates the committed reference fixtures under tests/golden/.
 
-Run once in a checkout that has the reference mounted (default /root/reference):
-  python tests/golden/make_golden.py [reference_root]
+Run once with the root of a reference checkout (the directory holding mujoco_warp/):
+  python tests/golden/make_golden.py <reference_root>
 
 It copies the reference's MJCF test models verbatim (they carry their own licence headers; the
 humanoid is the benchmark model) into tests/golden/models/, and reads the reference's test files
@@ -90,4 +90,6 @@ def main(ref_root):
 
 
 if __name__ == "__main__":
-  main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+  if len(sys.argv) != 2:
+    sys.exit("usage: python tests/golden/make_golden.py <reference_root>")
+  main(sys.argv[1])

@@ -131,3 +131,98 @@ def test_humanoid_spheres_steps_vs_fp64():
   assert np.all(mjw.world_status(d) == 0)
   assert np.quantile(rel_err(dev(d.qvel), o.get("qvel")), 0.9) < 1e-3
   assert np.quantile(rel_err(dev(d.qpos), o.get("qpos")), 0.9) < 1e-4
+
+
+def _bin_forward(mjm, qpos, qvel, ctrl, form, cta_warps=8):
+  nworld = qpos.shape[0]
+  m = mjw.put_model(mjm)
+  d = device_data(mjm, qpos, qvel, ctrl, nconmax=600 * nworld, njmax=512 * nworld)
+  try:
+    if form == 1:
+      mjw.set_tune(m, d, solver_cta_warps=cta_warps)
+    mjw.forward(m, d, fused=form)
+    torch.cuda.synchronize()
+  finally:
+    mjw.set_tune(m, d)
+  return d
+
+
+@pytest.mark.parametrize("cta_warps", [2, 4, 8, 16])
+def test_cta_solver_factor(cta_warps):
+  """The chosen form's Newton Hessian factor for dense nv > 32 (one CTA of 2 / 4 / 8 / 16 warps per
+  world; panel updates on the tensor pipe in split TF32) on the bin (nv = 384): with no solver
+  iterations both forms factor the Hessian of the same active set (the warmstart's), so the
+  chosen form's L must reproduce H = tril(qM) + J_a' D_a J_a and agree with the plain form's
+  FP32 factor, and the Newton directions must agree."""
+  mjm = load("bin.xml", iterations=0, ls_iterations=10, jacobian=MJ_JAC_DENSE)
+  nworld = 6
+  qpos, qvel, ctrl = bin_state(mjm, nworld, seed=5)
+  dc = _bin_forward(mjm, qpos, qvel, ctrl, 1, cta_warps)
+  dp = _bin_forward(mjm, qpos, qvel, ctrl, 0)
+  nv = mjm.nv
+  Lc = np.tril(dc.efc.h.cpu().numpy().astype(np.float64))
+  Lp = np.tril(dp.efc.h.cpu().numpy().astype(np.float64))
+  qM = dc.qM.cpu().numpy().astype(np.float64)
+  n, idx = world_rows(dc, "efc")
+  J = dc.efc.J.cpu().numpy().astype(np.float64)
+  D = dc.efc.D.cpu().numpy().astype(np.float64)
+  act = dc.efc.active.cpu().numpy().astype(bool)
+  start = 0
+  for w in range(nworld):
+    rows = idx[start:start + n[w]]
+    start += n[w]
+    rows = rows[act[rows]]
+    H = np.tril(qM[w]) + np.tril(qM[w], -1).T + J[rows].T @ (D[rows, None] * J[rows])
+    r = np.linalg.norm(Lc[w] @ Lc[w].T - H) / np.linalg.norm(H)
+    assert r < 1e-5, (w, r)
+    assert np.linalg.norm(Lc[w] - Lp[w]) / np.linalg.norm(Lp[w]) < 1e-4, w
+  e = rel_err(dev(dc.efc.Mgrad), dev(dp.efc.Mgrad))
+  assert e.max() < 1e-3, e
+
+
+@pytest.mark.parametrize("cta_warps", [2, 4, 8, 16])
+def test_cta_solver_vs_warp_solver_and_fp64(cta_warps):
+  """The whole Newton solve on the bin with the CTA solver against the plain form's
+  one-warp-per-world solver and the FP64 oracle: the reference's cost acceptance (2.5 %,
+  solver_test.py:127) in every world and the same qacc as the warp solver."""
+  mjm = load("bin.xml", iterations=20, ls_iterations=20, jacobian=MJ_JAC_DENSE)
+  nworld = 8
+  qpos, qvel, ctrl = bin_state(mjm, nworld, seed=1)
+  dc = _bin_forward(mjm, qpos, qvel, ctrl, 1, cta_warps)
+  dp = _bin_forward(mjm, qpos, qvel, ctrl, 0)
+  o = oracle(mjm, qpos, qvel, ctrl, 64)
+  o.run("forward")
+  assert np.all(mjw.world_status(dc) == 0)
+  cg, co = dc.efc.cost.cpu().numpy(), o.scalar("cost")
+  assert np.all(cg <= co + 0.025 * np.abs(co) + 1e-3), (cg, co)
+  assert np.median(rel_err(dev(dc.qacc), o.get("qacc"))) < 1e-2
+  assert np.median(rel_err(dev(dc.qacc), dev(dp.qacc))) < 1e-2
+
+
+def test_precision_form_humanoid_spheres():
+  """The precision form for nv > 32 (the humanoid with 0-16 extra spheres, nv = 123): the CTA
+  solver factors and solves the Newton Hessian in FP64 in shared memory and sums the line-search
+  coefficients in FP64, the mass-matrix factor-solves run in FP64 per tree block; converged qacc
+  within 1e-3 of FP64 in every world and no worse than the FP32 chosen form, and a few steps stay
+  finite and flag-free."""
+  hum = load("humanoid.xml")
+  mjm = load("humanoid_spheres.xml", integrator=3, timestep=0.005, iterations=10, ls_iterations=20,
+             jacobian=MJ_JAC_DENSE)
+  nworld = 16
+  qpos, qvel, ctrl, _ = humanoid_spheres_state(mjm, hum, nworld, seed=7)
+  m = mjw.put_model(mjm)
+  o = oracle(mjm, qpos, qvel, ctrl, 64)
+  o.run("forward")
+  err = {}
+  for form in (1, 3):
+    d = device_data(mjm, qpos, qvel, ctrl, nconmax=96 * nworld, njmax=384 * nworld)
+    mjw.forward(m, d, fused=form)
+    torch.cuda.synchronize()
+    err[form] = rel_err(dev(d.qacc), o.get("qacc"))
+  assert err[3].max() < 1e-3, err[3]
+  assert np.median(err[3]) <= 1.5 * np.median(err[1]) + 1e-7, (np.median(err[3]), np.median(err[1]))
+  for _ in range(3):
+    mjw.step(m, d, fused=3)
+  torch.cuda.synchronize()
+  assert np.all(np.isfinite(d.qpos.cpu().numpy()))
+  assert np.all(mjw.world_status(d) == 0)

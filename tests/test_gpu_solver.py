@@ -75,16 +75,69 @@ def test_cg_and_parallel_linesearch(solver, iterations, ls_iterations, ls_parall
 
 
 def test_benchmark_setting_statistics():
-  """3 Newton iterations (the nworld=8192 benchmark): most worlds agree to 1e-4; the cost is
-  within the reference's 2.5 % acceptance in >= 98 % of worlds."""
+  """3 Newton iterations (the nworld=8192 benchmark) from the keyframe states with no warmstart:
+  most worlds agree to 1e-4 (measured 71 %); the cost is within the reference's 2.5 % acceptance
+  in >= 98 % of worlds."""
   mjm = humanoid(iterations=3, ls_iterations=4)
   _, d, o = _run(mjm, 256, seed=5)
   e = rel_err(dev(d.qacc), o.get("qacc"))
   assert np.median(e) < 1e-4
-  assert np.mean(e < 1e-4) > 0.6
+  assert np.mean(e < 1e-4) > 0.66, np.mean(e < 1e-4)
   cg, co = d.efc.cost.cpu().numpy(), o.scalar("cost")
   ok = cg <= co + 0.025 * np.abs(co) + 1e-3
   assert ok.mean() >= 0.98, ok.mean()
+
+
+@pytest.mark.parametrize("fused", [1, 0])
+def test_benchmark_setting_vs_fp32_restatement(fused):
+  """The benchmark's 3 Newton / 4 line-search iterations from states in contact (after 10 steps):
+  every world whose qacc misses the FP64 restatement by more than 1e-4 is either within 1e-4 of
+  the FP32 restatement (the FP32 implementation of the reference's algorithm misses the same
+  way) or path-dependent: after 3 iterations the FP64 iterate itself is more than 1e-4 from the
+  converged solution there (~30 % of these worlds), so which line-search and active-set path the
+  iterations take decides the result, and rounding picks the path (FP32 runs of the
+  restatement from inputs one ulp apart each miss in ~11 % of worlds, not the same ones).  In
+  the worlds where 3 iterations do converge, the device agrees with FP64 to 1e-4."""
+  import oracle as orc
+
+  mjm = humanoid(iterations=3, ls_iterations=4)
+  qpos, qvel, ctrl = humanoid_state(mjm, 256, seed=12)
+  m = mjw.put_model(mjm)
+  d = device_data(mjm, qpos, qvel, ctrl)
+  for _ in range(10):
+    mjw.step(m, d, fused=fused)
+  torch.cuda.synchronize()
+  host = {k: getattr(d, k).double().cpu().numpy() for k in ("qpos", "qvel", "ctrl", "qacc_warmstart")}
+  refs = orc.qacc_references(mjm, host["qpos"], host["qvel"], host["ctrl"], host["qacc_warmstart"])
+  mjw.forward(m, d, fused=fused)
+  torch.cuda.synchronize()
+  c = orc.classify_qacc(dev(d.qacc), refs)
+  assert c["over_tol_unexplained"] == 0, c
+  assert c["frac_le_tol_vs_fp64"] >= 0.8, c
+  assert c["frac_le_tol_vs_fp64_in_converged_worlds"] >= 0.98, c
+
+
+def test_tensor_core_hessian():
+  """The chosen form with the Newton Hessian assembled on the tensor pipe in split TF32
+  (set_tune(hessian_tc=True)) gives the FMA assembly's converged qacc and FP64's."""
+  mjm = humanoid(iterations=10, ls_iterations=20)
+  qpos, qvel, ctrl = humanoid_state(mjm, 128, seed=3)
+  m = mjw.put_model(mjm)
+  out = []
+  for tc in (False, True):
+    d = device_data(mjm, qpos, qvel, ctrl)
+    try:
+      mjw.set_tune(m, d, hessian_tc=tc)
+      mjw.forward(m, d)
+      torch.cuda.synchronize()
+    finally:
+      mjw.set_tune(m, d)
+    out.append(dev(d.qacc))
+  o = oracle(mjm, qpos, qvel, ctrl, 64)
+  o.run("forward")
+  e = rel_err(out[1], o.get("qacc"))
+  assert e.max() < 1e-3 and np.median(e) < 1e-5, (e.max(), np.median(e))
+  assert np.median(rel_err(out[1], out[0])) < 1e-5
 
 
 def test_solve_standalone_matches_forward():

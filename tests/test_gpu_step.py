@@ -220,26 +220,34 @@ def test_get_data_into_roundtrip():
 
 
 def test_autotune_picks_a_setting_and_keeps_results():
-  """mjb_autotune (an extension) returns one of its candidate settings, restores the warmstart,
-  and the chosen form's steps are bit-identical with and without the tuned setting (lanes per
-  world and solver CTA width change the schedule, not the arithmetic)."""
+  """mjb_autotune (an extension) returns one of its candidate settings and restores the
+  warmstart; the settings that only change the schedule (lanes per world of the tree stages,
+  the solver's CTA width) leave the chosen form's steps bit-identical, for either Hessian
+  assembly."""
   mjm = humanoid()
   nworld = 512
   qpos, qvel, ctrl = humanoid_state(mjm, nworld, seed=9)
   m = mjw.put_model(mjm)
-  d1 = device_data(mjm, qpos, qvel, ctrl)
-  d2 = device_data(mjm, qpos, qvel, ctrl)
-  for _ in range(3):
-    mjw.step(m, d1)
-  ws, q = d2.qacc_warmstart.clone(), d2.qpos.clone()
-  cfg = mjw.autotune(m, d2)
-  assert cfg["tree_lanes"] in (8, 16, 32) and cfg["solver_warps"] in (1, 2, 4)
-  assert cfg["ms_per_forward"] > 0
-  assert torch.equal(d2.qacc_warmstart, ws) and torch.equal(d2.qpos, q)
-  for _ in range(3):
-    mjw.step(m, d2)
-  torch.cuda.synchronize()
-  assert torch.equal(d1.qpos, d2.qpos) and torch.equal(d1.qvel, d2.qvel)
+  d = device_data(mjm, qpos, qvel, ctrl)
+  try:
+    ws, q = d.qacc_warmstart.clone(), d.qpos.clone()
+    cfg = mjw.autotune(m, d)
+    assert cfg["tree_lanes"] in (8, 16, 32) and cfg["solver_warps"] in (1, 2, 4)
+    assert cfg["hessian_tc"] in (0, 1) and cfg["ms_per_forward"] > 0
+    assert cfg["rows_per_world"] > 0
+    assert torch.equal(d.qacc_warmstart, ws) and torch.equal(d.qpos, q)
+    for tc in (False, True):
+      out = []
+      for lanes, warps in ((8, 1), (32, 4)):
+        dd = device_data(mjm, qpos, qvel, ctrl)
+        mjw.set_tune(m, dd, tree_lanes=lanes, solver_warps=warps, hessian_tc=tc)
+        for _ in range(3):
+          mjw.step(m, dd)
+        torch.cuda.synchronize()
+        out.append((dd.qpos.clone(), dd.qvel.clone()))
+      assert torch.equal(out[0][0], out[1][0]) and torch.equal(out[0][1], out[1][1]), tc
+  finally:
+    mjw.set_tune(m, d)
 
 
 def test_humanoid_drift_forms_vs_fp64():

@@ -112,6 +112,7 @@ def test_abi_mirror_matches_header():
   assert [f[0] for f in _abi.MjbModel._fields_] == _header_fields("MjbModel")
   assert [f[0] for f in _abi.MjbData._fields_] == _header_fields("MjbData")
   assert [f[0] for f in _abi.MjbRunCfg._fields_] == _header_fields("MjbRunCfg")
+  assert [f[0] for f in _abi.MjbTune._fields_] == _header_fields("MjbTune")
 
 
 def test_library_exports_every_declared_entry_point():
@@ -122,7 +123,7 @@ def test_library_exports_every_declared_entry_point():
   lib = _abi.lib()
   for n in names:
     assert hasattr(lib, n), n
-  assert lib.mjb_abi_version() == 5
+  assert lib.mjb_abi_version() == 6
   assert lib.mjb_error_string(0) == b"ok"
 
 
@@ -143,3 +144,46 @@ def test_null_arguments_rejected():
   v.nworld = 0
   mv = _abi.MjbModel()
   assert lib.mjb_kinematics(ctypes.byref(mv), ctypes.byref(v), None) == 0
+
+
+def _fake_views(mjm):
+  """MjbModel / MjbData views with the model's sizes and every Data pointer set to a dummy
+  non-null address (never dereferenced: the calls below return before any launch)."""
+  mv = _abi.MjbModel()
+  for n in ("nq", "nv", "na", "nu", "nbody", "njnt", "ngeom", "nsite"):
+    setattr(mv, n, int(getattr(mjm, n)))
+  mv.nblock, mv.block_max = 1, mjm.nv
+  mv.integrator, mv.solver, mv.iterations, mv.ls_iterations = 3, 2, 3, 4
+  mv.actuator_affine_bias_gain = 1
+  dv = _abi.MjbData()
+  dv.nworld, dv.nconmax, dv.njmax = 4, 64, 256
+  for name, _ in _abi.DATA_PTRS:
+    setattr(dv, name, 0x1000)
+  return mv, dv
+
+
+@pytest.mark.parametrize("entry, field", [
+  ("mjb_kinematics", "xpos"), ("mjb_kinematics", "geom_xmat"), ("mjb_com_pos", "cinert"),
+  ("mjb_crb", "qM"), ("mjb_factor_m", "qLD"), ("mjb_transmission", "actuator_moment"),
+  ("mjb_fwd_velocity", "rne_cfrc"), ("mjb_fwd_actuation", "actuator_force"),
+  ("mjb_fwd_acceleration", "qfrc_smooth"), ("mjb_nxn_broadphase", "collision_pair"),
+  ("mjb_primitive_narrowphase", "contact_frame"), ("mjb_make_constraint", "efc_J"),
+  ("mjb_solve", "efc_Jaref"), ("mjb_euler", "qLD_integration"),
+  ("mjb_implicit", "qfrc_integration"), ("mjb_implicit", "act_vel_integration"),
+  ("mjb_forward", "cdof"), ("mjb_forward", "efc_Ma"), ("mjb_step", "qacc_integration"),
+  ("mjb_fwd_position", "subtree_com"), ("mjb_collision", "contact_dist")])
+def test_null_data_field_rejected(entry, field):
+  """An entry point given a null Data field that one of its stages touches returns MJB_ERR_ARG
+  before launching anything, instead of faulting on the device."""
+  mjm = load("humanoid.xml", integrator=3)
+  mv, dv = _fake_views(mjm)
+  if entry == "mjb_euler":
+    mv.integrator = 0
+  setattr(dv, field, None)
+  lib = _abi.lib()
+  fn = getattr(lib, entry)
+  if entry in ("mjb_forward", "mjb_step"):
+    rc = fn(ctypes.byref(mv), ctypes.byref(dv), None, None)
+  else:
+    rc = fn(ctypes.byref(mv), ctypes.byref(dv), None)
+  assert rc == 1, (entry, field, rc)
