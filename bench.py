@@ -1,7 +1,7 @@
 """Benchmark: humanoid batched step, nworld=8192 per GPU, steps/s (one JSON line on rank 0).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--form chosen|plain|single]
+                  [--form chosen|plain|single|precision]
 
 Workload: the reference's humanoid (27 dof, 21 motors) with implicitfast integration, dt=0.005,
 Newton with 3 iterations and 4 line-search iterations, pyramidal condim-3 contacts; seeded
@@ -9,27 +9,36 @@ synthetic initial states (keyframe "squat" + U(-0.05, 0.05), qvel ~ N(0, 0.01),
 ctrl ~ U(-0.4, 0.4)).  A "step" is one mjw.step over all worlds.
 
 value: world-steps/s with the state resident in HBM, one captured CUDA graph of the step replayed
-K times, in the chosen launch form (the stage kernels to fwd_acceleration, the solver's world
-ordering + persistent k_solve_queue, k_integrate); `forms` gives the
-same number for the plain one-kernel-per-stage form (the reference's launch sequence and
-algorithm) and the single-kernel form, measured in the same run.  e2e: the metric through the
-public API (mjw.step) with, every step, the control copied in from pinned host memory and
-qpos / qvel copied back.  roofline: the dominant kernel (the solver) timed with CUDA events
-around its own launch (mjw.step_phase) over K steps.  Multi-GPU: one process per GPU,
-each owning its own 8192 worlds (replicas, weak scaling, no collective on the data path); time is
-the maximum over ranks of CUDA-event time between barriers.
+K times, in the chosen launch form (the stage kernels to fwd_acceleration forked over three
+streams, the solver's world ordering + persistent k_solve_queue, k_integrate); `forms` gives the
+same number for the plain one-kernel-per-stage form, the single-kernel form and the precision
+form, measured in the same run.  e2e: the metric through the public API's host-framework call
+(mjw.step_io) with, every step, the control copied in from pinned host memory and qpos / qvel
+copied back.  roofline: the dominant kernel (the solver) timed with CUDA events around its own
+launch (mjw.step_phase) over K steps, against the FP32 FMA peak measured in the same run
+(mjb_fma_probe) and the measured HBM bandwidth; the bound is whichever takes longer.
+Multi-GPU: one process per GPU, each owning its own 8192 worlds (replicas, weak scaling, no
+collective on the data path); time is the maximum over ranks of CUDA-event time between barriers.
 
 qacc_err (rank 0): one forward from the bench state in every launch form, checked against the
-FP64 CPU restatement (the oracle, used only as the checker) on the first 256 worlds.
+CPU restatement (the oracle, used only as the checker) in FP64 and FP32 on the first 256 worlds,
+each miss over 1e-4 classified (oracle.classify_qacc).
 
-grad (rank 0): grad-steps/s of the differentiation workload — the same humanoid with the Newton
-solve run to convergence (10 iterations), nworld=1024, a 32-step rollout, loss = ||root_pos_T - target||^2 + 1e-3 sum ||ctrl||^2, gradients w.r.t. the
-control sequence (32 x 21), qpos0 and qvel0, checkpoints every 8 steps — through
-mjx_warp_b200.derivative (GPU finite-difference transition Jacobians, centered, eps 1e-3, and
-the reverse recursion); one forward + backward timed with CUDA events after one warm-up.
+grad (rank 0): grad-steps/s of the differentiation workload -- the same humanoid with the Newton
+solve run to convergence (10 iterations), nworld=1024, a 32-step rollout, loss =
+||root_pos_T - target||^2 + 1e-3 sum ||ctrl||^2, gradients w.r.t. the control sequence (32 x 21),
+qpos0 and qvel0, checkpoints every 8 steps, by the analytic adjoint (and, for comparison, with
+finite-difference columns); one forward + backward timed with CUDA events after one warm-up.
 
---impl reference times the reference algorithm's CPU implementation available here — the CPU
-restatement under oracle/, FP32, all host threads — on the same workload.
+combined (rank 0): the humanoid with 0-16 extra spheres (nv = 123), 32768 worlds, a 16-step
+rollout forward + analytic adjoint, in the chosen FP32 form and in the precision form.
+
+bin (rank 0): the uneven-contact bin (nv = 384), 4096 worlds, 500 graph-replayed chosen-form
+steps after autotuning, against the plain form launched eagerly.
+
+cpu_baseline / --impl reference: the reference algorithm's CPU implementation available here --
+the CPU restatement under oracle/, FP32, all host threads -- on the same 8192 worlds and the same
+post-warm-up steps, repeated 3 times.
 """
 
 import argparse
@@ -323,12 +332,17 @@ def _spheres_state(mjm, hum, nworld, seed):
   return qpos, rng.normal(0.0, 0.01, (nworld, mjm.nv)), rng.uniform(-0.4, 0.4, (nworld, mjm.nu))
 
 
-def _combined(mjw, torch, nworld=32768, horizon=16, checkpoint=4, reps=2):
+def _combined(mjw, torch, nworld=32768, horizon=16, checkpoint=4, reps=2, fused=True,
+              plain=True, sample=16):
   """The combined form of the uneven-contact humanoid: humanoids with 0-16 extra free spheres
   (nv = 123), a 16-step rollout forward plus the analytic adjoint (d/d ctrl, qpos0, qvel0 of
-  ||root_pos_T - target||^2 + 1e-3 ||ctrl||^2), checkpoints every 4 steps; forward and backward
-  world-steps/s, peak GPU memory of the differentiated rollout, and the plain form's forward."""
+  ||root_pos_T - target||^2 + 1e-3 ||ctrl||^2), checkpoints every 4 steps, in launch form `fused`
+  (True: the chosen FP32 form; 3: the precision form, FP64 Hessian factor-solves and line-search
+  sums); forward and backward world-steps/s, peak GPU memory of the differentiated rollout, qacc
+  of one forward against the FP64 restatement on `sample` worlds, and (plain=True) the plain
+  form's forward."""
   from mjx_warp_b200 import mjcf
+  import oracle
 
   hum = mjcf.from_xml_path(MODEL)
   mjm = mjcf.from_xml_path(SPHERES_MODEL)
@@ -339,7 +353,8 @@ def _combined(mjw, torch, nworld=32768, horizon=16, checkpoint=4, reps=2):
   torch.cuda.synchronize()
   base = torch.cuda.memory_allocated()
   torch.cuda.reset_peak_memory_stats()
-  roll = mjw.derivative.Rollout(mjm, m, nworld, checkpoint=checkpoint, nconmax=96, njmax=256)
+  roll = mjw.derivative.Rollout(mjm, m, nworld, checkpoint=checkpoint, nconmax=96, njmax=256,
+                                fused=fused)
   rng = np.random.default_rng(6)
   ctrl = np.repeat(ctrl0[None], horizon, axis=0) + rng.normal(0.0, 0.05, (horizon, nworld, mjm.nu))
   q0 = torch.tensor(qpos, dtype=torch.float32, device="cuda")
@@ -367,36 +382,54 @@ def _combined(mjw, torch, nworld=32768, horizon=16, checkpoint=4, reps=2):
     fwd, bwd = fwd + f / reps, bwd + b / reps
   peak = torch.cuda.max_memory_allocated() - base
   status = mjw.world_status(roll.d)
-  # the plain form's forward rollout of the same worlds (no checkpoints, no graph)
   d = roll.d
+  # qacc of one forward from the initial state against FP64 on a sample
   d.qpos.copy_(q0)
   d.qvel.copy_(v0)
-  d.qacc_warmstart.zero_()
-  step = lambda: mjw.step(m, d, fused=False)
   d.ctrl.copy_(u0[0])
-  step()
-  t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-  d.qpos.copy_(q0)
-  d.qvel.copy_(v0)
   d.qacc_warmstart.zero_()
-  t0.record()
-  for t in range(horizon):
-    d.ctrl.copy_(u0[t])
+  mjw.forward(m, d, fused=fused)
+  s = min(sample, nworld)
+  qd = d.qacc[:s].double().cpu().numpy()
+  o = oracle.Oracle(mjm, s, 64)
+  o.set("qpos", qpos[:s])
+  o.set("qvel", qvel[:s])
+  o.set("ctrl", ctrl[0, :s])
+  o.run("forward", nthreads=os.cpu_count() or 1)
+  e = oracle.rel_err(qd, o.get("qacc"))
+  out = {"workload": "humanoid + 0-16 free spheres per world (nv 123), implicitfast dt=0.005, "
+                     "Newton 10 it / ls 10, dense mass matrix; 16-step rollout + analytic adjoint",
+         "form": {True: "chosen", 3: "precision"}.get(fused, str(fused)),
+         "nworld": nworld, "horizon": horizon, "checkpoint": checkpoint,
+         "forward_steps_per_s": nworld * horizon / fwd,
+         "backward_steps_per_s": nworld * horizon / bwd,
+         "grad_steps_per_s": nworld * horizon / (fwd + bwd), "cost_vs_forward": (fwd + bwd) / fwd,
+         "forward_ms": fwd * 1e3, "backward_ms": bwd * 1e3,
+         "peak_gpu_memory_gb": peak / 1e9, "worlds_with_finite_grads": nok,
+         "worlds_flagged": int((status != 0).sum()),
+         "qacc_err_vs_fp64": {"worlds": s, "median": float(np.median(e)), "max": float(e.max()),
+                              "frac_le_1e-4": float(np.mean(e <= 1e-4))}}
+  if plain:  # the plain form's forward rollout of the same worlds (no checkpoints, no graph)
+    step = lambda: mjw.step(m, d, fused=False)
+    d.qpos.copy_(q0)
+    d.qvel.copy_(v0)
+    d.qacc_warmstart.zero_()
+    d.ctrl.copy_(u0[0])
     step()
-  t1.record()
-  torch.cuda.synchronize()
-  plain = t0.elapsed_time(t1) * 1e-3
-  return {"workload": "humanoid + 0-16 free spheres per world (nv 123), implicitfast dt=0.005, "
-                      "Newton 10 it / ls 10, dense mass matrix; 16-step rollout + analytic adjoint",
-          "nworld": nworld, "horizon": horizon, "checkpoint": checkpoint,
-          "forward_steps_per_s": nworld * horizon / fwd,
-          "backward_steps_per_s": nworld * horizon / bwd,
-          "grad_steps_per_s": nworld * horizon / (fwd + bwd), "cost_vs_forward": (fwd + bwd) / fwd,
-          "plain_forward_steps_per_s": nworld * horizon / plain,
-          "forward_ms": fwd * 1e3, "backward_ms": bwd * 1e3,
-          "peak_gpu_memory_gb": peak / 1e9, "worlds_with_finite_grads": nok,
-          "worlds_flagged": int((status != 0).sum()),
-          "precision": "FP32 throughout (the precision form covers nv <= 32)"}
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    d.qpos.copy_(q0)
+    d.qvel.copy_(v0)
+    d.qacc_warmstart.zero_()
+    t0.record()
+    for t in range(horizon):
+      d.ctrl.copy_(u0[t])
+      step()
+    t1.record()
+    torch.cuda.synchronize()
+    out["plain_forward_steps_per_s"] = nworld * horizon / (t0.elapsed_time(t1) * 1e-3)
+  del roll, d
+  torch.cuda.empty_cache()
+  return out
 
 
 BIN_MODEL = os.path.join(ROOT, "tests", "golden", "models", "bin.xml")
@@ -650,21 +683,25 @@ def run_ours(args):
   nefc = int(d.world_nefc.sum())
   npair = int(d.world_npair.sum())
 
-  # end to end through the public API: ctrl in from pinned host memory, qpos / qvel back
+  # end to end through the public API's host-framework call (mjw.step_io: the control copied in,
+  # one step, qpos / qvel copied out), with the control coming from pinned host memory and the
+  # state going back to it every step
   ctrl_h = torch.as_tensor(ctrl, dtype=torch.float32).pin_memory()
-  out_h = torch.empty((nworld, mjm.nq + mjm.nv), dtype=torch.float32).pin_memory()
-  out_d = torch.empty((nworld, mjm.nq + mjm.nv), dtype=torch.float32, device="cuda")
+  ctrl_d = torch.empty_like(d.ctrl)
+  io_out = {"qpos": torch.empty_like(d.qpos), "qvel": torch.empty_like(d.qvel)}
+  qpos_h = torch.empty(d.qpos.shape, dtype=torch.float32).pin_memory()
+  qvel_h = torch.empty(d.qvel.shape, dtype=torch.float32).pin_memory()
   restore()
   barrier()
   e0 = torch.cuda.Event(enable_timing=True)
   e1 = torch.cuda.Event(enable_timing=True)
   e0.record()
   for _ in range(args.steps):
-    d.ctrl.copy_(ctrl_h, non_blocking=True)
-    step()
-    out_d[:, :mjm.nq].copy_(d.qpos)
-    out_d[:, mjm.nq:].copy_(d.qvel)
-    out_h.copy_(out_d, non_blocking=True)
+    ctrl_d.copy_(ctrl_h, non_blocking=True)
+    mjw.step_io(m, d, 1, inputs={"ctrl": ctrl_d}, outputs=("qpos", "qvel"), out=io_out,
+                fused=form)
+    qpos_h.copy_(io_out["qpos"], non_blocking=True)
+    qvel_h.copy_(io_out["qvel"], non_blocking=True)
   e1.record()
   barrier()
   e2e_elapsed = replicas.max_over_ranks(e0.elapsed_time(e1) / 1000.0, device="cuda")
@@ -720,6 +757,7 @@ def run_ours(args):
   combined = None
   if rank == 0 and not args.no_combined:
     combined = _combined(mjw, torch)
+    combined["precision_form"] = _combined(mjw, torch, fused=3, plain=False)
   bin_cfg = None
   if rank == 0 and not args.no_bin:
     bin_cfg = _bin_config(mjw, torch)
@@ -761,7 +799,9 @@ def run_ours(args):
                "l2": f"working set {footprint / 2**20:.0f} MiB per GPU > 126 MB L2, no flush",
                "parallelism": f"replicas x{world_size}"},
     "e2e": {"value": total_worlds * args.steps / e2e_elapsed, "unit": "steps/s",
-            "h2d_bytes_per_step": _bytes_of(ctrl_h), "d2h_bytes_per_step": _bytes_of(out_h)},
+            "h2d_bytes_per_step": _bytes_of(ctrl_h),
+            "d2h_bytes_per_step": _bytes_of(qpos_h) + _bytes_of(qvel_h),
+            "call": "mjw.step_io (mjb_step_io: ctrl in, one step, qpos / qvel out)"},
     "gpu_launches": launches_per_step * args.steps,
     "roofline": {"bound": "fp32" if flop_bound else "hbm",
                  "achieved": flop_rate if flop_bound else achieved,

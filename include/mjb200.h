@@ -166,6 +166,23 @@ int mjb_forward(const MjbModel* m, const MjbData* d, const MjbRunCfg* cfg, mjbSt
    let a caller time the kernels separately or act between forward and integration. */
 int mjb_step_phase(const MjbModel* m, const MjbData* d, int phase, mjbStream stream);
 
+/* The device buffers of a host framework's step call (the JAX FFI pattern of
+ * contrib/jax_unroll.py:40-71 and the notebook's unrolled step): world-major arrays shaped like
+ * the matching Data fields.  Inputs are copied into the Data before the first substep (null: the
+ * Data's own values are kept); outputs are copied out of it after the last substep (null: not
+ * copied). */
+typedef struct MjbStepIO {
+  const float *qpos, *qvel, *ctrl, *qacc_warmstart;
+  float *qpos_out, *qvel_out, *qacc_warmstart_out, *xpos_out, *xmat_out, *subtree_com_out,
+      *cvel_out, *site_xpos_out;
+} MjbStepIO;
+/* Copy in, nstep calls of mjb_step (cfg as there), copy out: every copy is one
+ * cudaMemcpyAsync on the stream, so the call allocates nothing, does not synchronise and can be
+ * captured in a CUDA graph; no counterpart function in the reference, whose callers write these
+ * copies around step themselves. */
+int mjb_step_io(const MjbModel* m, const MjbData* d, const MjbStepIO* io, int nstep,
+                const MjbRunCfg* cfg, mjbStream stream);
+
 /* Pipeline stages (forward.py:408-661). */
 int mjb_fwd_position(const MjbModel* m, const MjbData* d, mjbStream stream);
 int mjb_fwd_velocity(const MjbModel* m, const MjbData* d, mjbStream stream);
@@ -224,7 +241,7 @@ typedef struct MjbTune {
  * tree-lane count and solver CTA width on d's current worlds and keeps the fastest, per device,
  * for models of this nv and Data of this rows-per-world capacity (njmax / nworld); later chosen-
  * form calls with the same key use it (others keep 16 lanes, 4 warps per solver CTA, FMA
- * Hessians, and 4 warps per world for dense nv > 32).  out->rows_per_world reports the mean
+ * Hessians, and for dense models 4 warps per world when nv > 128, one warp per world below).  out->rows_per_world reports the mean
  * constraint rows per world of d's worlds (the key cannot hold it: the host does not see the row
  * counts of a step without synchronising).  warmstart_scratch:
  * nworld * nv floats of caller memory; qacc_warmstart is saved there and restored before every

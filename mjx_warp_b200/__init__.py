@@ -17,6 +17,7 @@ from . import derivative as derivative
 from . import mjcf as mjcf
 from ._api import autotune as autotune
 from ._api import set_tune as set_tune
+from ._api import step_io as step_io
 from ._api import benchmark as benchmark
 from ._api import collision as collision
 from ._api import com_pos as com_pos

@@ -124,6 +124,15 @@ class MjbRunCfg(ctypes.Structure):
   _fields_ = [("fused", ctypes.c_int32), ("worlds_per_block", ctypes.c_int32)]
 
 
+STEP_IO_FIELDS = ("qpos", "qvel", "ctrl", "qacc_warmstart", "qpos_out", "qvel_out",
+                  "qacc_warmstart_out", "xpos_out", "xmat_out", "subtree_com_out", "cvel_out",
+                  "site_xpos_out")
+
+
+class MjbStepIO(ctypes.Structure):
+  _fields_ = [(n, ctypes.c_void_p) for n in STEP_IO_FIELDS]
+
+
 _STAGES = ("kinematics", "com_pos", "crb", "factor_m", "rne", "transmission", "com_vel",
            "passive", "fwd_velocity", "fwd_actuation", "fwd_acceleration", "euler", "implicit",
            "nxn_broadphase", "fwd_position", "collision", "sap_broadphase",
@@ -158,6 +167,9 @@ def lib() -> ctypes.CDLL:
   L.mjb_mul_m.argtypes = [pm, pd, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
   L.mjb_xfrc_accumulate.restype = ctypes.c_int
   L.mjb_xfrc_accumulate.argtypes = [pm, pd, ctypes.c_void_p, ctypes.c_void_p]
+  L.mjb_step_io.restype = ctypes.c_int
+  L.mjb_step_io.argtypes = [pm, pd, ctypes.POINTER(MjbStepIO), ctypes.c_int,
+                            ctypes.POINTER(MjbRunCfg), ctypes.c_void_p]
   L.mjb_step_phase.restype = ctypes.c_int
   L.mjb_step_phase.argtypes = [pm, pd, ctypes.c_int, ctypes.c_void_p]
   L.mjb_world_status.restype = ctypes.c_int

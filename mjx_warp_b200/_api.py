@@ -67,6 +67,51 @@ def step(m: Model, d: Data, fused=True) -> None:
   d.time = d.time + m.opt.timestep
 
 
+_STEP_IO_SHAPES = {"qpos": "nq", "qvel": "nv", "ctrl": "nu", "qacc_warmstart": "nv"}
+_STEP_IO_OUT = {"qpos": (lambda m: (m.nq,)), "qvel": (lambda m: (m.nv,)),
+                "qacc_warmstart": (lambda m: (m.nv,)), "xpos": (lambda m: (m.nbody, 3)),
+                "xmat": (lambda m: (m.nbody, 3, 3)), "subtree_com": (lambda m: (m.nbody, 3)),
+                "cvel": (lambda m: (m.nbody, 6)), "site_xpos": (lambda m: (m.nsite, 3))}
+
+
+def step_io(m: Model, d: Data, nstep: int = 1, inputs: Optional[dict] = None,
+            outputs=("qpos", "qvel"), out: Optional[dict] = None, fused=True) -> dict:
+  """The step call of a host framework (an extension: the reference's callers write these copies
+  around step themselves, e.g. contrib/jax_unroll.py:40-71 and the notebook's unrolled step):
+  copies `inputs` (a dict over qpos, qvel, ctrl, qacc_warmstart of (nworld, n) CUDA tensors)
+  into d, runs `nstep` steps, and copies the `outputs` fields (qpos, qvel, qacc_warmstart, xpos,
+  xmat, subtree_com, cvel, site_xpos) out of d into `out`'s tensors (allocated when not given);
+  returns the output dict.  One C call (mjb_step_io): no allocation besides `out`, no
+  synchronisation, capturable in a CUDA graph.  d.time advances by nstep timesteps."""
+  inputs = inputs or {}
+  io = _abi.MjbStepIO()
+  for k, t in inputs.items():
+    if k not in _STEP_IO_SHAPES:
+      raise ValueError(f"step_io: unknown input {k}")
+    n = getattr(m, _STEP_IO_SHAPES[k])
+    if tuple(t.shape) != (d.nworld, n) or t.dtype != torch.float32:
+      raise ValueError(f"step_io: input {k} must be float32 of shape {(d.nworld, n)}")
+    setattr(io, k, _abi._ptr(t.contiguous()))
+  res = dict(out or {})
+  for k in outputs:
+    if k not in _STEP_IO_OUT:
+      raise ValueError(f"step_io: unknown output {k}")
+    shape = (d.nworld,) + _STEP_IO_OUT[k](m)
+    t = res.get(k)
+    if t is None:
+      t = res[k] = torch.empty(shape, dtype=torch.float32, device=d.qpos.device)
+    elif tuple(t.shape) != shape or t.dtype != torch.float32 or not t.is_contiguous():
+      raise ValueError(f"step_io: output {k} must be a contiguous float32 tensor of shape {shape}")
+    setattr(io, k + "_out", _abi._ptr(t))
+  _integrator_check(m)
+  rc = _abi.lib().mjb_step_io(ctypes.byref(_abi.model_view(m)), ctypes.byref(_abi.data_view(d)),
+                              ctypes.byref(io), int(nstep), ctypes.byref(_form(fused)),
+                              _abi.stream())
+  _abi.check(rc, "step_io")
+  d.time = d.time + nstep * m.opt.timestep
+  return res
+
+
 def step_phase(m: Model, d: Data, phase: int) -> None:
   """One phase of the chosen form's step (not in the reference): 0 = fwd_position ..
   fwd_acceleration, 1 = the constraint solver, 2 = integration.  Phases 0, 1, 2 in order equal

@@ -640,6 +640,7 @@ int launch_lanes(const MjbModel* m, const MjbData* d, cudaStream_t s, int lanes)
 // CTA of the persistent solver.  mjb_autotune measures them per device for a model's nv and a
 // Data's rows-per-world capacity (njmax / nworld, the caller's sizing of its contact density);
 // without a tuned entry the defaults below apply.
+constexpr int kCtaSolverMinNv = 128;
 struct ChosenCfg {
   int lanes = MJB_TREE_LANES;
   int warps = kDefaultWarps;
@@ -663,7 +664,11 @@ ChosenCfg chosen_cfg(const MjbModel* m, const MjbData* d) {
   std::lock_guard<std::mutex> lock(g_tune_mutex);
   for (int i = 0; i < g_ntune; i++)
     if (g_tune[i].dev == dev && g_tune[i].nv == m->nv && g_tune[i].cap == cap) return g_tune[i].cfg;
-  return ChosenCfg{};
+  ChosenCfg c;
+  // untuned: the CTA solver for large trees of dofs (measured faster from the 384-dof bin, slower
+  // for the 123-dof humanoid with spheres), one warp per world below
+  c.cta_warps = m->nv > kCtaSolverMinNv ? 4 : 0;
+  return c;
 }
 
 void store_cfg(const MjbModel* m, const MjbData* d, ChosenCfg cfg) {
@@ -1062,6 +1067,47 @@ int mjb_xfrc_accumulate(const MjbModel* m, const MjbData* d, float* qfrc, mjbStr
   if (!qfrc) return MJB_ERR_ARG;
   k_xfrc<<<grid_for(d->nworld, 4), 128, 0, (cudaStream_t)stream>>>(*m, *d, qfrc);
   return finish();
+}
+
+int mjb_step_io(const MjbModel* m, const MjbData* d, const MjbStepIO* io, int nstep,
+                const MjbRunCfg* cfg, mjbStream stream) {
+  int rc = check(m, d);
+  if (rc) return rc;
+  if (!io || nstep < 0) return MJB_ERR_ARG;
+  if (d->nworld == 0) return MJB_OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  const size_t W = size_t(d->nworld), f = sizeof(float);
+  struct Copy {
+    const void* src;
+    void* dst;
+    size_t bytes;
+  };
+  const Copy in[4] = {{io->qpos, d->qpos, W * m->nq * f}, {io->qvel, d->qvel, W * m->nv * f},
+                      {io->ctrl, d->ctrl, W * m->nu * f},
+                      {io->qacc_warmstart, d->qacc_warmstart, W * m->nv * f}};
+  const Copy out[8] = {{d->qpos, io->qpos_out, W * m->nq * f},
+                       {d->qvel, io->qvel_out, W * m->nv * f},
+                       {d->qacc_warmstart, io->qacc_warmstart_out, W * m->nv * f},
+                       {d->xpos, io->xpos_out, W * m->nbody * 3 * f},
+                       {d->xmat, io->xmat_out, W * m->nbody * 9 * f},
+                       {d->subtree_com, io->subtree_com_out, W * m->nbody * 3 * f},
+                       {d->cvel, io->cvel_out, W * m->nbody * 6 * f},
+                       {d->site_xpos, io->site_xpos_out, W * m->nsite * 3 * f}};
+  for (const Copy& c : in)  // a requested copy into a missing Data field is an error
+    if (c.src && c.bytes && !c.dst) return MJB_ERR_ARG;
+  for (const Copy& c : out)
+    if (c.dst && c.bytes && !c.src) return MJB_ERR_ARG;
+  for (const Copy& c : in)
+    if (c.src && c.bytes &&
+        cudaMemcpyAsync(c.dst, c.src, c.bytes, cudaMemcpyDeviceToDevice, s) != cudaSuccess)
+      return MJB_ERR_LAUNCH;
+  for (int k = 0; k < nstep; k++)
+    if ((rc = mjb_step(m, d, cfg, stream))) return rc;
+  for (const Copy& c : out)
+    if (c.dst && c.bytes &&
+        cudaMemcpyAsync(c.dst, c.src, c.bytes, cudaMemcpyDeviceToDevice, s) != cudaSuccess)
+      return MJB_ERR_LAUNCH;
+  return MJB_OK;
 }
 
 int mjb_world_status(const MjbData* d, uint32_t* host_out, mjbStream stream) {

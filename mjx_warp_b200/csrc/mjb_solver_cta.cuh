@@ -76,7 +76,7 @@ __device__ __noinline__ void chol_cta(float* A, int ld, int n, float* T, int war
           for (int nt = 0; nt < 4; nt++)
 #pragma unroll
             for (int e = 0; e < 4; e++) acc[q][nt][e] = 0.f;
-#pragma unroll 2
+#pragma unroll 4
         for (int k0 = 0; k0 < c0; k0 += 8) {
           FragB b[4];  // B[k][j] = L[c0 + j][k0 + k], j = 8 nt + g
 #pragma unroll
@@ -129,11 +129,23 @@ __device__ __noinline__ void chol_cta(float* A, int ld, int n, float* T, int war
       if (lane < pn) T[lane * TL + 32] = __frcp_rn(T[lane * TL + lane]);
     }
     __syncthreads();
+    const bool vec = (ld & 3) == 0 && pn == 32;  // rows 16-byte aligned: float4 reads and writes
     for (int i = c0 + pn + int(threadIdx.x); i < n; i += NW * 32) {  // (iii)
       float* Ai = A + size_t(i) * ld + c0;
       float x[32];
+      if (vec) {
 #pragma unroll
-      for (int c = 0; c < 32; c++) x[c] = c < pn ? Ai[c] : 0.f;
+        for (int q = 0; q < 8; q++) {
+          const float4 v = reinterpret_cast<const float4*>(Ai)[q];
+          x[4 * q] = v.x;
+          x[4 * q + 1] = v.y;
+          x[4 * q + 2] = v.z;
+          x[4 * q + 3] = v.w;
+        }
+      } else {
+#pragma unroll
+        for (int c = 0; c < 32; c++) x[c] = c < pn ? Ai[c] : 0.f;
+      }
 #pragma unroll
       for (int c = 0; c < 32; c++) {
         if (c < pn) {
@@ -143,9 +155,15 @@ __device__ __noinline__ void chol_cta(float* A, int ld, int n, float* T, int war
           x[c] = v * T[c * TL + 32];
         }
       }
+      if (vec) {
 #pragma unroll
-      for (int c = 0; c < 32; c++)
-        if (c < pn) Ai[c] = x[c];
+        for (int q = 0; q < 8; q++)
+          reinterpret_cast<float4*>(Ai)[q] = make_float4(x[4 * q], x[4 * q + 1], x[4 * q + 2], x[4 * q + 3]);
+      } else {
+#pragma unroll
+        for (int c = 0; c < 32; c++)
+          if (c < pn) Ai[c] = x[c];
+      }
     }
     __syncthreads();
   }
@@ -415,16 +433,23 @@ struct CtaSolver {
       if (D == 0.f) continue;
       const float* J = d.efc_J + size_t(r) * nv;
       int cnt = 0;
-      for (int base = 0; base < nv; base += 32) {
-        const int c = base + lane;
-        const float v = c < nv ? J[c] : 0.f;
-        const unsigned mk = __ballot_sync(WARP_FULL, v != 0.f);
-        if (v != 0.f) {
-          const int p = cnt + __popc(mk & ((1u << lane) - 1u));
-          nzi[p] = c;
-          nzv[p] = v;
+      for (int base = 0; base < nv; base += 256) {  // eight 32-column chunks loaded, then compacted
+        float v[8];
+#pragma unroll
+        for (int q = 0; q < 8; q++) {
+          const int c = base + 32 * q + lane;
+          v[q] = c < nv ? J[c] : 0.f;
         }
-        cnt += __popc(mk);
+#pragma unroll
+        for (int q = 0; q < 8; q++) {
+          const unsigned mk = __ballot_sync(WARP_FULL, v[q] != 0.f);
+          if (v[q] != 0.f) {
+            const int p = cnt + __popc(mk & ((1u << lane) - 1u));
+            nzi[p] = base + 32 * q + lane;
+            nzv[p] = v[q];
+          }
+          cnt += __popc(mk);
+        }
       }
       __syncwarp();
       for (int a = 0; a < cnt; a++) {

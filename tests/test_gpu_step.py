@@ -280,3 +280,51 @@ def test_humanoid_drift_forms_vs_fp64():
   print("drift (form, step): (median, p90)", report)
   for f in (0, 1, 3):
     assert report[(f, 10)][0] < 1e-2, report
+
+
+def test_step_io_matches_copies_around_step():
+  """mjb_step_io, the FFI-style call (copy the inputs in, k substeps, copy the outputs out), gives
+  bit for bit what the same copies written around step give (contrib/jax_unroll.py:40-71's
+  pattern; the notebook's unrolled step also copies the warmstart in), also when the call is
+  captured in a CUDA graph and replayed."""
+  mjm = humanoid()
+  nworld = 64
+  qpos, qvel, ctrl = humanoid_state(mjm, nworld, seed=13)
+  m = mjw.put_model(mjm)
+  q2, v2, c2 = humanoid_state(mjm, nworld, seed=14)
+  q_in = torch.as_tensor(q2, dtype=torch.float32, device="cuda")
+  v_in = torch.as_tensor(v2, dtype=torch.float32, device="cuda")
+  c_in = torch.as_tensor(c2, dtype=torch.float32, device="cuda")
+  w_in = torch.zeros((nworld, mjm.nv), dtype=torch.float32, device="cuda")
+  inputs = {"qpos": q_in, "qvel": v_in, "ctrl": c_in, "qacc_warmstart": w_in}
+  outputs = ("qpos", "qvel", "qacc_warmstart", "xpos", "xmat", "subtree_com", "cvel", "site_xpos")
+  d1 = device_data(mjm, qpos, qvel, ctrl)
+  d1.qpos.copy_(q_in)
+  d1.qvel.copy_(v_in)
+  d1.ctrl.copy_(c_in)
+  for _ in range(4):
+    mjw.step(m, d1)
+  d2 = device_data(mjm, qpos, qvel, ctrl)
+  res = mjw.step_io(m, d2, nstep=4, inputs=inputs, outputs=outputs)
+  torch.cuda.synchronize()
+  for k in outputs:
+    assert torch.equal(res[k], getattr(d1, k).reshape(res[k].shape)), k
+  assert abs(d2.time - d1.time) < 1e-9
+  # captured: the same call replayed from the same inputs
+  d3 = device_data(mjm, qpos, qvel, ctrl)
+  out = {k: torch.empty_like(v) for k, v in res.items()}
+  mjw.step_io(m, d3, nstep=4, inputs=inputs, outputs=outputs, out=out)  # warm-up, uncaptured
+  g = torch.cuda.CUDAGraph()
+  s = torch.cuda.Stream()
+  s.wait_stream(torch.cuda.current_stream())
+  with torch.cuda.stream(s):
+    with torch.cuda.graph(g, stream=s):
+      mjw.step_io(m, d3, nstep=4, inputs=inputs, outputs=outputs, out=out)
+  torch.cuda.current_stream().wait_stream(s)
+  for t in out.values():
+    t.zero_()
+  g.replay()
+  torch.cuda.synchronize()
+  for k in outputs:
+    assert torch.equal(out[k], res[k]), k
+  del g

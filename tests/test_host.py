@@ -187,3 +187,18 @@ def test_null_data_field_rejected(entry, field):
   else:
     rc = fn(ctypes.byref(mv), ctypes.byref(dv), None)
   assert rc == 1, (entry, field, rc)
+
+
+def test_step_io_rejects_mismatched_buffers():
+  """step_io checks its buffers' shapes and types on the host before any device call."""
+  mjm = load("pendula.xml")
+  m = mjw.put_model(mjm, device="cpu")
+  d = mjw.make_data(mjm, nworld=2, device="cpu")
+  with pytest.raises(ValueError):
+    mjw.step_io(m, d, inputs={"qpos": torch.zeros((3, mjm.nq))})
+  with pytest.raises(ValueError):
+    mjw.step_io(m, d, inputs={"qvel": torch.zeros((2, mjm.nv), dtype=torch.float64)})
+  with pytest.raises(ValueError):
+    mjw.step_io(m, d, outputs=("qacc",))
+  with pytest.raises(ValueError):
+    mjw.step_io(m, d, outputs=("xpos",), out={"xpos": torch.zeros((2, 3))})
