@@ -551,6 +551,28 @@ def _bin_config(mjw, torch, nworld=4096, steps=500, plain_steps=10, sample=16):
                        "rows_per_world": rows_solve}}
 
 
+def _profile_case_bin(mjw, torch, nworld=512, cta_warps=2):
+  """A small case of the bin for a profiler capture of the CTA solver: nworld worlds of
+  _bin_config's bin from the same seeded packings, the CTA width pinned, one step then one
+  forward (the capture's launch)."""
+  from mjx_warp_b200 import mjcf
+
+  mjm = mjcf.from_xml_path(BIN_MODEL)
+  mjm.opt.iterations, mjm.opt.ls_iterations, mjm.opt.jacobian = 10, 10, 0
+  q, v, _ = _bin_state(mjm, nworld, seed=3)
+  m = mjw.put_model(mjm)
+  d = mjw.make_data(mjm, nworld, nconmax=600 * nworld, njmax=512 * nworld)
+  d.qpos.copy_(torch.as_tensor(q, dtype=torch.float32))
+  d.qvel.copy_(torch.as_tensor(v, dtype=torch.float32))
+  mjw.set_tune(m, d, solver_cta_warps=cta_warps)
+  mjw.step(m, d)
+  mjw.forward(m, d)
+  torch.cuda.synchronize()
+  return {"profile_case": "bin", "nworld": nworld, "cta_warps": cta_warps,
+          "rows_per_world": float(d.world_nefc.float().mean()),
+          "device_gb": torch.cuda.max_memory_allocated() / 1e9}
+
+
 def _larger_models(mjw, torch, reps=3):
   """ms per step (chosen, plain) of the uneven-contact configurations: the bin (nv = 384, 4096
   worlds, Newton or CG 10 iterations, dense or sparse mass matrix) and the humanoid with 0-16
@@ -919,11 +941,19 @@ def main():
   p.add_argument("--no-grad", action="store_true")
   p.add_argument("--no-combined", action="store_true")
   p.add_argument("--no-bin", action="store_true")
+  p.add_argument("--profile-case", choices=["bin"],
+                 help="run one small case for a profiler capture (bin: 512 worlds, the CTA solver's "
+                      "launch is the forward's) and print one JSON line instead of the bench")
   p.add_argument("--larger-models", action="store_true",
                  help="print one JSON line of the uneven-contact configurations' step times instead")
   args = p.parse_args()
   if args.warmup < 3:
     args.warmup = 3
+  if args.profile_case:
+    import torch
+    import mjx_warp_b200 as mjw
+    print(json.dumps(_profile_case_bin(mjw, torch, nworld=min(args.nworld, 512))))
+    return
   if args.larger_models:
     import torch
     import mjx_warp_b200 as mjw
