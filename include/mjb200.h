@@ -145,7 +145,7 @@ typedef struct MjbData {
    the Hessian and mass-matrix Cholesky factor-solves in FP64 and the line-search polynomial
    coefficients accumulated in FP64.  Dense mass matrix, tree blocks of up to 32 dofs
    (MJB_ERR_UNSUPPORTED otherwise); for nv > 32 the Hessian's FP64 factor lives in shared memory,
-   which bounds nv at about 160 (MJB_ERR_SCRATCH beyond). */
+   which bounds nv at about 230 (MJB_ERR_SCRATCH beyond). */
 #define MJB_FORM_PRECISION 3
 
 typedef struct MjbRunCfg {

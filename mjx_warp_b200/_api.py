@@ -57,7 +57,7 @@ def step(m: Model, d: Data, fused=True) -> None:
   the Hessian in every iteration, as the reference does; fused=2 runs the whole step of a world
   in one warp of a single kernel; fused=3 runs the chosen form with the Hessian and mass-matrix
   Cholesky factor-solves and the line-search coefficient sums in FP64 (the precision form; dense
-  mass matrix with trees of up to 32 dofs, nv up to about 160).
+  mass matrix with trees of up to 32 dofs, nv up to about 230).
   """
   _integrator_check(m)
   L = _abi.lib()

@@ -229,11 +229,11 @@ __global__ void __launch_bounds__(128, MJB_MINB) k_solve_queue(const __grid_cons
 // else one CTA per world in index order
 template <int NW, bool PREC>
 __global__ void __launch_bounds__(NW * 32, NW >= 16 ? 1 : (NW >= 8 ? 2 : (NW >= 4 ? 4 : 8)))
-    k_solve_cta(const __grid_constant__ MjbModel m, const __grid_constant__ MjbData d) {
+    k_solve_cta(const __grid_constant__ MjbModel m, const __grid_constant__ MjbData d, int tc) {
   extern __shared__ __align__(16) float smem[];
   __shared__ int s_idx;
   if (!d.work_queue) {
-    if (int(blockIdx.x) < d.nworld) solve_cta<NW, PREC>(m, d, blockIdx.x, smem);
+    if (int(blockIdx.x) < d.nworld) solve_cta<NW, PREC>(m, d, blockIdx.x, smem, tc != 0);
     return;
   }
   for (;;) {
@@ -242,7 +242,7 @@ __global__ void __launch_bounds__(NW * 32, NW >= 16 ? 1 : (NW >= 8 ? 2 : (NW >= 
     const int idx = s_idx;
     __syncthreads();
     if (idx >= d.nworld) break;
-    solve_cta<NW, PREC>(m, d, d.world_order[idx], smem);
+    solve_cta<NW, PREC>(m, d, d.world_order[idx], smem, tc != 0);
   }
 }
 
@@ -390,11 +390,11 @@ inline int finish() {
 inline bool implicit_unsupported(const MjbModel* m) { return m->is_sparse && m->integrator != 0; }
 
 // the precision form: dense mass matrix with tree blocks of up to 32 dofs (the FP64 block
-// factor-solves use a 32-row tile); for nv > 32 the Hessian's FP64 factor must fit in one CTA's
-// shared memory (227 KB: nv up to about 160)
+// factor-solves use a 32-row tile); for nv > 32 the Hessian's packed FP64 factor must fit in one
+// CTA's shared memory (227 KB: nv up to about 230)
 int precision_supported(const MjbModel* m) {
   if (m->is_sparse || m->block_max > 32) return MJB_ERR_UNSUPPORTED;
-  if (m->nv > 32 && size_t(cta_solver_smem_floats(m->nv, 8, true)) * sizeof(float) > 227 * 1024)
+  if (m->nv > 32 && size_t(cta_solver_smem_floats(m->nv, 16, true)) * sizeof(float) > 227 * 1024)
     return MJB_ERR_SCRATCH;
   return MJB_OK;
 }
@@ -780,18 +780,18 @@ int run_forward_plain(const MjbModel* m, const MjbData* d, cudaStream_t s) {
 // the chosen form's solver launch: k_order_worlds + the persistent k_solve_queue when the Data has
 // the schedule arrays, else one warp per world (k_solve); PREC selects the precision form's solver
 template <int NW, bool PREC>
-void launch_solver_cta(const MjbModel* m, const MjbData* d, cudaStream_t s) {
+void launch_solver_cta(const MjbModel* m, const MjbData* d, int tc, cudaStream_t s) {
   const size_t bytes = size_t(cta_solver_smem_floats(m->nv, NW, PREC)) * sizeof(float);
   static size_t conf[kSmemDevices];
   allow_smem(k_solve_cta<NW, PREC>, bytes, conf);
   if (d->world_order && d->work_queue && d->world_nefc) {
     const int ctas = resident_ctas(k_solve_cta<NW, PREC>, 32 * NW, bytes);
     k_order_worlds<<<1, 1024, 0, s>>>(d->world_nefc, d->world_order, d->work_queue, d->nworld);
-    k_solve_cta<NW, PREC><<<std::min(ctas, d->nworld), 32 * NW, bytes, s>>>(*m, *d);
+    k_solve_cta<NW, PREC><<<std::min(ctas, d->nworld), 32 * NW, bytes, s>>>(*m, *d, tc);
   } else {
     MjbData dd = *d;
     dd.work_queue = nullptr;
-    k_solve_cta<NW, PREC><<<d->nworld, 32 * NW, bytes, s>>>(*m, dd);
+    k_solve_cta<NW, PREC><<<d->nworld, 32 * NW, bytes, s>>>(*m, dd, tc);
   }
 }
 
@@ -819,10 +819,12 @@ void launch_solver(const MjbModel* m, const MjbData* d, const ChosenCfg& cfg, in
                    cudaStream_t s) {
   // dense nv > 32: the CTA solver (the precision form's FP64 Hessian factor needs it)
   if (m->nv > 32 && !m->is_sparse && (cfg.cta_warps > 0 || PREC)) {
-    if (cfg.cta_warps == 2) launch_solver_cta<2, PREC>(m, d, s);
-    else if (cfg.cta_warps == 4) launch_solver_cta<4, PREC>(m, d, s);
-    else if (cfg.cta_warps == 16) launch_solver_cta<16, PREC>(m, d, s);
-    else launch_solver_cta<8, PREC>(m, d, s);
+    const int tc = cfg.hessian_tc;
+    const int nw = cfg.cta_warps > 0 ? cfg.cta_warps : 4;  // the precision form's default: 4
+    if (nw == 2) launch_solver_cta<2, PREC>(m, d, tc, s);
+    else if (nw == 4) launch_solver_cta<4, PREC>(m, d, tc, s);
+    else if (nw == 16) launch_solver_cta<16, PREC>(m, d, tc, s);
+    else launch_solver_cta<8, PREC>(m, d, tc, s);
     return;
   }
   if (PREC) launch_solver_warp<PREC, true>(m, d, cfg, spw, s);
@@ -1203,13 +1205,38 @@ extern "C" int mjb_autotune(const MjbModel* m, const MjbData* d, float* warmstar
     return MJB_ERR_LAUNCH;
   }
   // candidates: tree-stage lanes x the solver's CTA shape (warps per CTA of the persistent
-  // one-warp-per-world solver, or, for dense nv > 32, warps per world of the CTA solver)
-  // (for nv <= 32 also the Newton Hessian's assembly: FMAs or the tensor pipe)
+  // one-warp-per-world solver, or, for dense nv > 32, warps per world of the CTA solver); for
+  // nv <= 32 also the Newton Hessian's assembly (FMAs or the tensor pipe), for nv > 32 the
+  // tensor-core assembly tried once more on the best CTA shape
   const int lanes[3] = {8, 16, 32}, widths[6] = {1, 2, 4, 1, 2, 4}, cta[4] = {2, 4, 8, 0};
   const bool large = m->nv > 32 && !m->is_sparse;
   float best = 0.f;
   ChosenCfg best_cfg;
   bool have = false;
+  auto trial = [&](const ChosenCfg& c) -> int {
+    auto forward = [&]() -> int {
+      if (restore() != cudaSuccess) return MJB_ERR_LAUNCH;
+      int r = run_chosen_phase(m, d, 0, s, &c);
+      return r ? r : run_chosen_phase(m, d, 1, s, &c);
+    };
+    int r = forward();  // warm-up
+    if (r) return r;
+    constexpr int kReps = 3;
+    if (cudaEventRecord(e0, s) != cudaSuccess) return MJB_ERR_LAUNCH;
+    for (int k = 0; k < kReps && !r; k++) r = forward();
+    if (r) return r;
+    float ms = 0.f;
+    if (cudaEventRecord(e1, s) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+        cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess)
+      return MJB_ERR_LAUNCH;
+    ms /= kReps;
+    if (!have || ms < best) {
+      best = ms;
+      best_cfg = c;
+      have = true;
+    }
+    return MJB_OK;
+  };
   for (int li = 0; li < 3 && !rc; li++) {
     for (int wi = 0; wi < (large ? 4 : 6) && !rc; wi++) {
       ChosenCfg c;
@@ -1220,29 +1247,13 @@ extern "C" int mjb_autotune(const MjbModel* m, const MjbData* d, float* warmstar
         c.warps = widths[wi];
         c.hessian_tc = wi >= 3;
       }
-      auto forward = [&]() -> int {
-        if (restore() != cudaSuccess) return MJB_ERR_LAUNCH;
-        int r = run_chosen_phase(m, d, 0, s, &c);
-        return r ? r : run_chosen_phase(m, d, 1, s, &c);
-      };
-      if ((rc = forward())) break;  // warm-up
-      constexpr int kReps = 3;
-      if (cudaEventRecord(e0, s) != cudaSuccess) { rc = MJB_ERR_LAUNCH; break; }
-      for (int r = 0; r < kReps && !rc; r++) rc = forward();
-      if (rc) break;
-      float ms = 0.f;
-      if (cudaEventRecord(e1, s) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
-          cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) {
-        rc = MJB_ERR_LAUNCH;
-        break;
-      }
-      ms /= kReps;
-      if (!have || ms < best) {
-        best = ms;
-        best_cfg = c;
-        have = true;
-      }
+      rc = trial(c);
     }
+  }
+  if (!rc && large && best_cfg.cta_warps > 0) {
+    ChosenCfg c = best_cfg;
+    c.hessian_tc = 1;
+    rc = trial(c);
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);

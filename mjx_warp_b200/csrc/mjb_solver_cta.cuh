@@ -10,7 +10,8 @@
 // (warp sums, then the warps' partials in warp order), identical in every thread, so control flow
 // stays uniform across the CTA.  The Hessian H = tril(qM) + sum_active D J'J is assembled in efc_h
 // (each warp updates the H rows it owns, row by row in constraint order, so no two warps touch the
-// same entry) and factored by chol_cta: a left-looking blocked Cholesky with 32-column panels
+// same entry; or, selected by the autotuner and always in the precision form, as split-TF32
+// tensor-core tiles, assemble_hessian_tc) and factored by chol_cta: a left-looking blocked Cholesky with 32-column panels
 // whose panel updates A[r, p] -= L[r, :p] L[p, :p]^T run on the tensor pipe in split TF32
 // (mjb_tc.cuh), the 32 x 32 diagonal blocks by chol_tile and the panel rows below by
 // substitution.  One world per CTA keeps each matrix being factored in L2.
@@ -238,79 +239,109 @@ __device__ __noinline__ void cho_solve_cta(const float* L, int ld, int n, float*
 
 // Per-CTA shared memory of the solver (floats): reductions (16 NW, as doubles 32 NW), the
 // diagonal tile (32 x 36 + 32), each warp's row-compaction scratch and the triangular solves'
-// vector (nv); the precision form adds
-// the FP64 Hessian tile (nv rows of cta_ld_d(nv) doubles, 8-byte aligned after the floats).
-__host__ __device__ __forceinline__ int cta_ld_d(int nv) { return nv | 1; }
+// vector (nv); the precision form adds the FP64 Hessian factor, its lower triangle packed row by row (row i at i (i + 1) / 2), then
+// the FP64 solve's vector and the factor's reciprocal diagonal (nv doubles each), 8-byte aligned
+// after the floats.
+__host__ __device__ __forceinline__ int tri(int i) { return i * (i + 1) / 2; }
 __host__ __device__ __forceinline__ int cta_solver_smem_base(int nv, int nw) {
   return round4i(32 * nw + 32 * 36 + 32 + nw * 2 * round4i(nv) + round4i(nv));
 }
 __host__ __device__ __forceinline__ int cta_solver_smem_floats(int nv, int nw, bool prec = false) {
   const int base = cta_solver_smem_base(nv, nw);
-  return prec ? base + 2 * (nv * cta_ld_d(nv) + nv + 1) : base;
+  return prec ? base + 2 * (tri(nv) + 2 * nv + 1) : base;
 }
 
-// FP64 counterpart of chol_cta for the precision form, on an n x n lower triangle held in shared
-// memory (row stride ld doubles): per 32-column panel, (i) every entry (r, j) of the panel's rows
-// r >= p subtracts its dot product over the finished columns, one entry per thread at a time;
-// (ii) warp 0 factors the diagonal block in place (chol_tile_d); (iii) the rows below solve
-// against it, one thread per row.
+// FP64 counterpart of chol_cta for the precision form, on the packed lower triangle P of an
+// n x n SPD matrix in shared memory: per 32-column panel, (i) every entry (r, j) of the panel's
+// rows r >= p subtracts its dot product over the finished columns (4 x 1 strips of entries per
+// thread, so each loaded L[j][k] serves four rows); (ii) warp 0 factors the diagonal block in
+// place, lane per row, with the pivot's reciprocal kept in rd; (iii) the rows below solve
+// against it, one thread per row, multiplying by rd.
 template <int NW>
-__device__ __noinline__ void chol_cta_d(double* A, int ld, int n, int warp, int lane) {
+__device__ __noinline__ void chol_cta_d(double* P, double* rd, int n, int warp, int lane) {
   constexpr int NT = NW * 32;
   for (int c0 = 0; c0 < n; c0 += 32) {
     const int pn = min(32, n - c0);
     if (c0 > 0) {
-      const int cnt = (n - c0) * pn;
-      for (int e = int(threadIdx.x); e < cnt; e += NT) {
-        const int r = c0 + e / pn, j = c0 + e % pn;
-        if (j > r) continue;
-        const double* Ar = A + r * ld;
-        const double* Aj = A + j * ld;
-        double s0 = 0.0, s1 = 0.0;
-        int k = 0;
-        for (; k + 1 < c0; k += 2) {
-          s0 += Ar[k] * Aj[k];
-          s1 += Ar[k + 1] * Aj[k + 1];
+      const int nr4 = (n - c0 + 3) / 4;  // strips of four rows
+      for (int e = int(threadIdx.x); e < nr4 * pn; e += NT) {
+        const int r = c0 + 4 * (e / pn), j = c0 + e % pn;
+        const double* Lj = P + tri(j);
+        double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+        const double* R0 = P + tri(r);
+        const double* R1 = P + tri(min(r + 1, n - 1));
+        const double* R2 = P + tri(min(r + 2, n - 1));
+        const double* R3 = P + tri(min(r + 3, n - 1));
+        for (int k = 0; k < c0; k++) {
+          const double l = Lj[k];
+          s0 += R0[k] * l;
+          s1 += R1[k] * l;
+          s2 += R2[k] * l;
+          s3 += R3[k] * l;
         }
-        if (k < c0) s0 += Ar[k] * Aj[k];
-        A[r * ld + j] -= s0 + s1;
+        if (j <= r) P[tri(r) + j] -= s0;
+        if (r + 1 < n && j <= r + 1) P[tri(r + 1) + j] -= s1;
+        if (r + 2 < n && j <= r + 2) P[tri(r + 2) + j] -= s2;
+        if (r + 3 < n && j <= r + 3) P[tri(r + 3) + j] -= s3;
       }
       __syncthreads();
     }
-    if (warp == 0) chol_tile_d(A + c0 * ld + c0, ld, pn, lane);
+    if (warp == 0) {  // (ii): column k of the block, lanes over its rows (left-looking)
+      for (int k = 0; k < pn; k++) {
+        const int i = c0 + k + lane;
+        const double* Lk = P + tri(c0 + k) + c0;
+        double s = 0.0;
+        if (k + lane < pn) {
+          const double* Li = P + tri(i) + c0;
+          s = Li[k];
+          for (int q = 0; q < k; q++) s -= Li[q] * Lk[q];
+        }
+        const double lkk = sqrt(__shfl_sync(WARP_FULL, s, 0));
+        const double inv = 1.0 / lkk;
+        __syncwarp();
+        if (lane == 0) {
+          P[tri(c0 + k) + c0 + k] = lkk;
+          rd[c0 + k] = inv;
+        } else if (k + lane < pn) {
+          P[tri(i) + c0 + k] = s * inv;
+        }
+        __syncwarp();
+      }
+    }
     __syncthreads();
-    for (int i = c0 + pn + int(threadIdx.x); i < n; i += NT) {
-      double* Ai = A + i * ld + c0;
+    for (int i = c0 + pn + int(threadIdx.x); i < n; i += NT) {  // (iii)
+      double* Ai = P + tri(i) + c0;
       for (int c = 0; c < pn; c++) {
         double v = Ai[c];
-        const double* Lc = A + (c0 + c) * ld + c0;
+        const double* Lc = P + tri(c0 + c) + c0;
         for (int q = 0; q < c; q++) v -= Ai[q] * Lc[q];
-        Ai[c] = v / Lc[c];
+        Ai[c] = v * rd[c0 + c];
       }
     }
     __syncthreads();
   }
 }
 
-// x = (L L^T)^-1 y for the FP64 factor L in shared memory (row stride ld), one warp, in FP64
-// with the intermediate vector in v (n doubles of shared memory); x and y are n floats in
-// global memory (x may alias y).
-__device__ void cho_solve_d_warp(const double* L, int ld, int n, double* v, float* x,
+// x = (L L^T)^-1 y for the packed FP64 factor in shared memory, one warp, in FP64 with the
+// intermediate vector in v (n doubles of shared memory) and the reciprocal diagonal rd; x and y
+// are n floats in global memory (x may alias y).
+__device__ void cho_solve_d_warp(const double* P, const double* rd, int n, double* v, float* x,
                                  const float* y, int lane) {
   for (int i = lane; i < n; i += 32) v[i] = double(y[i]);
   __syncwarp();
   for (int k = 0; k < n; k++) {  // L z = y, a column at a time; lanes update the rows below
-    const double zk = v[k] / L[k * ld + k];
+    const double zk = v[k] * rd[k];
     __syncwarp();
     if (lane == (k & 31)) v[k] = zk;
-    for (int i = k + 1 + lane; i < n; i += 32) v[i] -= L[i * ld + k] * zk;
+    for (int i = k + 1 + lane; i < n; i += 32) v[i] -= P[tri(i) + k] * zk;
     __syncwarp();
   }
-  for (int k = n - 1; k >= 0; k--) {  // L^T x = z
-    const double xk = v[k] / L[k * ld + k];
+  for (int k = n - 1; k >= 0; k--) {  // L^T x = z: row k of L is column k of L^T
+    const double xk = v[k] * rd[k];
     __syncwarp();
     if (lane == (k & 31)) v[k] = xk;
-    for (int i = lane; i < k; i += 32) v[i] -= L[k * ld + i] * xk;
+    const double* Lk = P + tri(k);
+    for (int i = lane; i < k; i += 32) v[i] -= Lk[i] * xk;
     __syncwarp();
   }
   for (int i = lane; i < n; i += 32) x[i] = float(v[i]);
@@ -328,10 +359,11 @@ struct CtaSolver {
   float* T;      // chol_cta's diagonal tile
   float* nz;     // this warp's row compaction: round4(nv) ints, then round4(nv) floats
   float* zv;     // the triangular solves' intermediate vector (nv floats)
-  double* Ld;    // precision form: the Hessian's FP64 factor (nv rows of ldd doubles)
+  double* Ld;    // precision form: the Hessian's FP64 factor, lower triangle packed by rows
   double* vd;    // precision form: the FP64 solve's vector (nv doubles)
-  int ldd;
+  double* rdg;   // precision form: the factor's reciprocal diagonal (nv doubles)
   bool reuse = true, factored = false, changed = true;
+  bool tc = false;  // FP32 form: the Hessian assembled on the tensor pipe (assemble_hessian_tc)
   float cost, prev_cost, gauss, grad_dot, search_dot, gtol, alpha, beta;
   float qg[3];
   static constexpr int NT = NW * 32;
@@ -464,6 +496,64 @@ struct CtaSolver {
     __syncthreads();
   }
 
+  // H = tril(qM) + sum over active rows of D J'J on the tensor pipe in split TF32 (mjb_tc.cuh):
+  // H = qM + A B with A = J^T (nv x n) and B = diag(c) J (n x nv), c = D on active rows and 0
+  // elsewhere; warp q takes the 16-row m-tiles mt = q, q + NW, ... and, four at a time, the m16n8
+  // tiles of that row band that touch the lower triangle; the k dimension runs over the world's
+  // rows eight at a time, the accumulators start from qM; writes the lower triangle of Hout (row
+  // stride ldh elements: efc_h; or, PACKED, the precision form's packed FP64 triangle).
+  template <typename TH, bool PACKED = false>
+  __device__ void assemble_hessian_tc(TH* Hout, int ldh) {
+    const int g = lane >> 2, t = lane & 3;
+    const int nmt = (nv + 15) >> 4, ncol8 = (nv + 7) >> 3;
+    const float* J = d.efc_J + size_t(adr) * nv;
+    for (int mt = warp; mt < nmt; mt += NW) {
+      const int r0 = 16 * mt + g, r1 = r0 + 8;
+      const int nnt = min((16 * mt + 15) / 8 + 1, ncol8);
+      for (int nt0 = 0; nt0 < nnt; nt0 += 4) {
+        float acc[4][4];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+          const int c = 8 * (nt0 + q) + 2 * t;
+          acc[q][0] = (r0 < nv && c < nv) ? qM[size_t(r0) * nv + c] : 0.f;
+          acc[q][1] = (r0 < nv && c + 1 < nv) ? qM[size_t(r0) * nv + c + 1] : 0.f;
+          acc[q][2] = (r1 < nv && c < nv) ? qM[size_t(r1) * nv + c] : 0.f;
+          acc[q][3] = (r1 < nv && c + 1 < nv) ? qM[size_t(r1) * nv + c + 1] : 0.f;
+        }
+        for (int k0 = 0; k0 < n; k0 += 8) {
+          const int ka = k0 + t, kb = ka + 4;
+          const bool va = ka < n, vb = kb < n;
+          const float ca = (va && d.efc_active[adr + ka]) ? d.efc_D[adr + ka] : 0.f;
+          const float cb = (vb && d.efc_active[adr + kb]) ? d.efc_D[adr + kb] : 0.f;
+          const float* Ja = J + size_t(va ? ka : 0) * nv;
+          const float* Jb = J + size_t(vb ? kb : 0) * nv;
+          const FragA a = frag_a((va && r0 < nv) ? Ja[r0] : 0.f, (va && r1 < nv) ? Ja[r1] : 0.f,
+                                 (vb && r0 < nv) ? Jb[r0] : 0.f, (vb && r1 < nv) ? Jb[r1] : 0.f);
+#pragma unroll
+          for (int q = 0; q < 4; q++) {
+            const int c = 8 * (nt0 + q) + g;
+            if (nt0 + q < nnt) {
+              const FragB b = frag_b((va && c < nv) ? ca * Ja[c] : 0.f, (vb && c < nv) ? cb * Jb[c] : 0.f);
+              mma_3xtf32(acc[q], a, b);
+            }
+          }
+        }
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+          const int c = 8 * (nt0 + q) + 2 * t;
+#pragma unroll
+          for (int e = 0; e < 2; e++) {
+            if (r0 < nv && c + e <= r0)
+              Hout[(PACKED ? size_t(tri(r0)) : size_t(r0) * ldh) + c + e] = TH(acc[q][e]);
+            if (r1 < nv && c + e <= r1)
+              Hout[(PACKED ? size_t(tri(r1)) : size_t(r1) * ldh) + c + e] = TH(acc[q][2 + e]);
+          }
+        }
+      }
+    }
+    __syncthreads();
+  }
+
   // solver.py:176-312
   __device__ void update_gradient() {
     float gd[1] = {0.f};
@@ -480,25 +570,22 @@ struct CtaSolver {
       return;
     }
     if (!(reuse && factored && !changed)) {
-      assemble_hessian();
-      if (PREC) {  // the FP32-assembled H factored in FP64 in shared memory
-        for (int e = tid; e < nv * nv; e += NT) {
-          const int i = e / nv, j = e - i * nv;
-          if (j <= i) Ld[i * ldd + j] = double(H[e]);
-        }
-        __syncthreads();
-        chol_cta_d<NW>(Ld, ldd, nv, warp, lane);
+      if (PREC) {  // H in split TF32 straight into the FP64 tile, factored there in FP64
+        assemble_hessian_tc<double, true>(Ld, 0);
+        chol_cta_d<NW>(Ld, rdg, nv, warp, lane);
         for (int e = tid; e < nv * nv; e += NT) {  // efc_h keeps the factor (FP32-rounded)
           const int i = e / nv, j = e - i * nv;
-          if (j <= i) H[e] = float(Ld[i * ldd + j]);
+          if (j <= i) H[e] = float(Ld[tri(i) + j]);
         }
       } else {
+        if (tc) assemble_hessian_tc(H, nv);
+        else assemble_hessian();
         chol_cta<NW>(H, nv, nv, T, warp, lane);
       }
       factored = true;
     }
     if (warp == 0) {
-      if (PREC) cho_solve_d_warp(Ld, ldd, nv, vd, Mgrad, grad, lane);
+      if (PREC) cho_solve_d_warp(Ld, rdg, nv, vd, Mgrad, grad, lane);
     }
     if (!PREC) cho_solve_cta<NW>(H, nv, nv, Mgrad, grad, zv, red, warp, lane);
     __syncthreads();
@@ -734,7 +821,7 @@ struct CtaSolver {
 
 // One world's solve by the whole CTA; smem: cta_solver_smem_floats(nv, NW) floats
 template <int NW, bool PREC>
-__device__ void solve_cta(const MjbModel& m, const MjbData& d, int w, float* smem) {
+__device__ void solve_cta(const MjbModel& m, const MjbData& d, int w, float* smem, bool tc) {
   const int nv = m.nv;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   CtaSolver<NW, PREC> s{m, d, w, tid, lane, warp, nv, d.world_efcadr[w], d.world_nefc[w]};
@@ -753,9 +840,10 @@ __device__ void solve_cta(const MjbModel& m, const MjbData& d, int w, float* sme
   s.T = smem + 32 * NW;
   s.nz = smem + 32 * NW + 32 * 36 + 32 + warp * 2 * round4i(nv);
   s.zv = smem + 32 * NW + 32 * 36 + 32 + NW * 2 * round4i(nv);
-  s.ldd = cta_ld_d(nv);
   s.Ld = PREC ? reinterpret_cast<double*>(smem + cta_solver_smem_base(nv, NW)) : nullptr;
-  s.vd = PREC ? s.Ld + nv * s.ldd : nullptr;
+  s.vd = PREC ? s.Ld + tri(nv) : nullptr;
+  s.rdg = PREC ? s.vd + nv : nullptr;
+  s.tc = tc;
   s.run();
 }
 

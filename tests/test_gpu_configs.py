@@ -133,13 +133,13 @@ def test_humanoid_spheres_steps_vs_fp64():
   assert np.quantile(rel_err(dev(d.qpos), o.get("qpos")), 0.9) < 1e-4
 
 
-def _bin_forward(mjm, qpos, qvel, ctrl, form, cta_warps=8):
+def _bin_forward(mjm, qpos, qvel, ctrl, form, cta_warps=8, tc=False):
   nworld = qpos.shape[0]
   m = mjw.put_model(mjm)
   d = device_data(mjm, qpos, qvel, ctrl, nconmax=600 * nworld, njmax=512 * nworld)
   try:
     if form == 1:
-      mjw.set_tune(m, d, solver_cta_warps=cta_warps)
+      mjw.set_tune(m, d, solver_cta_warps=cta_warps, hessian_tc=tc)
     mjw.forward(m, d, fused=form)
     torch.cuda.synchronize()
   finally:
@@ -147,17 +147,19 @@ def _bin_forward(mjm, qpos, qvel, ctrl, form, cta_warps=8):
   return d
 
 
-@pytest.mark.parametrize("cta_warps", [2, 4, 8, 16])
-def test_cta_solver_factor(cta_warps):
+@pytest.mark.parametrize("cta_warps, tc", [(2, False), (4, False), (8, False), (16, False),
+                                           (2, True), (4, True)])
+def test_cta_solver_factor(cta_warps, tc):
   """The chosen form's Newton Hessian factor for dense nv > 32 (one CTA of 2 / 4 / 8 / 16 warps per
-  world; panel updates on the tensor pipe in split TF32) on the bin (nv = 384): with no solver
+  world; panel updates on the tensor pipe in split TF32; tc: the Hessian itself assembled there
+  too) on the bin (nv = 384): with no solver
   iterations both forms factor the Hessian of the same active set (the warmstart's), so the
   chosen form's L must reproduce H = tril(qM) + J_a' D_a J_a and agree with the plain form's
   FP32 factor, and the Newton directions must agree."""
   mjm = load("bin.xml", iterations=0, ls_iterations=10, jacobian=MJ_JAC_DENSE)
   nworld = 6
   qpos, qvel, ctrl = bin_state(mjm, nworld, seed=5)
-  dc = _bin_forward(mjm, qpos, qvel, ctrl, 1, cta_warps)
+  dc = _bin_forward(mjm, qpos, qvel, ctrl, 1, cta_warps, tc)
   dp = _bin_forward(mjm, qpos, qvel, ctrl, 0)
   nv = mjm.nv
   Lc = np.tril(dc.efc.h.cpu().numpy().astype(np.float64))
@@ -180,15 +182,16 @@ def test_cta_solver_factor(cta_warps):
   assert e.max() < 1e-3, e
 
 
-@pytest.mark.parametrize("cta_warps", [2, 4, 8, 16])
-def test_cta_solver_vs_warp_solver_and_fp64(cta_warps):
+@pytest.mark.parametrize("cta_warps, tc", [(2, False), (4, False), (8, False), (16, False),
+                                           (4, True)])
+def test_cta_solver_vs_warp_solver_and_fp64(cta_warps, tc):
   """The whole Newton solve on the bin with the CTA solver against the plain form's
   one-warp-per-world solver and the FP64 oracle: the reference's cost acceptance (2.5 %,
   solver_test.py:127) in every world and the same qacc as the warp solver."""
   mjm = load("bin.xml", iterations=20, ls_iterations=20, jacobian=MJ_JAC_DENSE)
   nworld = 8
   qpos, qvel, ctrl = bin_state(mjm, nworld, seed=1)
-  dc = _bin_forward(mjm, qpos, qvel, ctrl, 1, cta_warps)
+  dc = _bin_forward(mjm, qpos, qvel, ctrl, 1, cta_warps, tc)
   dp = _bin_forward(mjm, qpos, qvel, ctrl, 0)
   o = oracle(mjm, qpos, qvel, ctrl, 64)
   o.run("forward")
