@@ -202,3 +202,22 @@ def test_step_io_rejects_mismatched_buffers():
     mjw.step_io(m, d, outputs=("qacc",))
   with pytest.raises(ValueError):
     mjw.step_io(m, d, outputs=("xpos",), out={"xpos": torch.zeros((2, 3))})
+
+
+def test_step_io_c_abi_argument_checks():
+  """mjb_step_io returns MJB_ERR_ARG for a null io, a negative step count, or a requested copy
+  into or out of a Data field that is null, before any copy or launch."""
+  mjm = load("humanoid.xml", integrator=3)
+  mv, dv = _fake_views(mjm)
+  lib = _abi.lib()
+  io = _abi.MjbStepIO()
+  assert lib.mjb_step_io(ctypes.byref(mv), ctypes.byref(dv), None, 1, None, None) == 1
+  assert lib.mjb_step_io(ctypes.byref(mv), ctypes.byref(dv), ctypes.byref(io), -1, None, None) == 1
+  dv.ctrl = None
+  io.ctrl = 0x2000
+  assert lib.mjb_step_io(ctypes.byref(mv), ctypes.byref(dv), ctypes.byref(io), 1, None, None) == 1
+  io.ctrl = None
+  dv.site_xpos = None
+  io.site_xpos_out = 0x2000
+  mv.nsite = 1
+  assert lib.mjb_step_io(ctypes.byref(mv), ctypes.byref(dv), ctypes.byref(io), 1, None, None) == 1
