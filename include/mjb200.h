@@ -227,7 +227,7 @@ int mjb_world_status(const MjbData* d, uint32_t* host_out, mjbStream stream);
  * lanes per world of the tree-recursion stages, warps per CTA of the persistent solver (one warp
  * per world, nv <= 32) and how it assembles the Newton Hessian (FP32 FMAs, or split-TF32
  * tensor-core products, which the precision form always uses), and warps per world of the CTA
- * solver of dense models with nv > 32. */
+ * solver of models with nv > 32. */
 typedef struct MjbTune {
   int32_t tree_lanes;        /* 8, 16 or 32 */
   int32_t solver_warps;      /* 1, 2 or 4 */
@@ -241,7 +241,7 @@ typedef struct MjbTune {
  * tree-lane count and solver CTA width on d's current worlds and keeps the fastest, per device,
  * for models of this nv and Data of this rows-per-world capacity (njmax / nworld); later chosen-
  * form calls with the same key use it (others keep 16 lanes, 4 warps per solver CTA, FMA
- * Hessians, and for dense models 4 warps per world when nv > 128, one warp per world below).  out->rows_per_world reports the mean
+ * Hessians, and 4 warps per world when nv > 128, one warp per world below).  out->rows_per_world reports the mean
  * constraint rows per world of d's worlds (the key cannot hold it: the host does not see the row
  * counts of a step without synchronising).  warmstart_scratch:
  * nworld * nv floats of caller memory; qacc_warmstart is saved there and restored before every

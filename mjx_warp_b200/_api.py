@@ -52,7 +52,7 @@ def step(m: Model, d: Data, fused=True) -> None:
 
   fused=True (or 1) runs the chosen form: the stage kernels of fwd_position .. fwd_acceleration
   forked over three streams, the persistent solver (keeping the Newton Hessian's factor while the
-  active set is unchanged; one CTA per world for dense models with nv > 32) and one kernel for
+  active set is unchanged; one CTA per world for models with nv > 128) and one kernel for
   the integrator; fused=False (or 0) launches one kernel per reference stage and refactors
   the Hessian in every iteration, as the reference does; fused=2 runs the whole step of a world
   in one warp of a single kernel; fused=3 runs the chosen form with the Hessian and mass-matrix
@@ -308,7 +308,7 @@ def autotune(m: Model, d: Data) -> dict:
   reference has no autotuner): times the chosen forward for every tree-stage lane count (8, 16,
   32 lanes per world) and solver CTA shape (for nv <= 32 the persistent one-warp-per-world
   solver's CTA width, 1, 2, 4 warps, with the Newton Hessian by FMAs or on the tensor pipe; for
-  dense nv > 32 the warps per world of the CTA solver, 2,
+  nv > 32 the warps per world of the CTA solver, 2,
   4, 8, or one warp per world) on d's current worlds and keeps the fastest for later calls with
   the same nv and rows-per-world capacity on this device; reports the rows per world measured.
   d's qacc_warmstart is saved and restored around the trials; d is left as after one forward.
@@ -329,7 +329,7 @@ def set_tune(m: Model, d: Data, tree_lanes: int = 16, solver_warps: int = 4,
   """Pins the chosen form's launch parameters for this model and Data (an extension, as
   autotune): lanes per world of the tree-recursion stages (8, 16, 32), warps per CTA of the
   one-warp-per-world solver (1, 2, 4), its Newton Hessian on the tensor pipe in split TF32
-  (hessian_tc, nv <= 32) and warps per world of the CTA solver of dense models with nv > 32
+  (hessian_tc, nv <= 32) and warps per world of the CTA solver of models with nv > 32
   (2, 4, 8, 16, or 0 for one warp per world)."""
   t = _abi.MjbTune()
   t.tree_lanes, t.solver_warps, t.solver_cta_warps = tree_lanes, solver_warps, solver_cta_warps

@@ -224,7 +224,7 @@ __global__ void __launch_bounds__(128, MJB_MINB) k_solve_queue(const __grid_cons
   }
 }
 
-// chosen form, dense models with nv > 32: one CTA of NW warps per world (mjb_solver_cta.cuh),
+// chosen form, models with nv > 32: one CTA of NW warps per world (mjb_solver_cta.cuh),
 // persistent over the work queue in k_order_worlds' order when the Data has the schedule arrays,
 // else one CTA per world in index order
 template <int NW, bool PREC>
@@ -644,7 +644,7 @@ constexpr int kCtaSolverMinNv = 128;
 struct ChosenCfg {
   int lanes = MJB_TREE_LANES;
   int warps = kDefaultWarps;
-  int cta_warps = 4;  // warps per world of the solver for dense nv > 32 (0: one warp per world)
+  int cta_warps = 4;  // warps per world of the solver for nv > 32 (0: one warp per world)
   int hessian_tc = 0; // nv <= 32: Newton Hessian on the tensor pipe (split TF32) instead of FMAs
 };
 struct TuneEntry {
@@ -817,8 +817,8 @@ void launch_solver_warp(const MjbModel* m, const MjbData* d, const ChosenCfg& cf
 template <bool PREC>
 void launch_solver(const MjbModel* m, const MjbData* d, const ChosenCfg& cfg, int spw,
                    cudaStream_t s) {
-  // dense nv > 32: the CTA solver (the precision form's FP64 Hessian factor needs it)
-  if (m->nv > 32 && !m->is_sparse && (cfg.cta_warps > 0 || PREC)) {
+  // nv > 32: the CTA solver (the precision form's FP64 Hessian factor needs it)
+  if (m->nv > 32 && (cfg.cta_warps > 0 || PREC)) {
     const int tc = cfg.hessian_tc;
     const int nw = cfg.cta_warps > 0 ? cfg.cta_warps : 4;  // the precision form's default: 4
     if (nw == 2) launch_solver_cta<2, PREC>(m, d, tc, s);
@@ -1205,11 +1205,11 @@ extern "C" int mjb_autotune(const MjbModel* m, const MjbData* d, float* warmstar
     return MJB_ERR_LAUNCH;
   }
   // candidates: tree-stage lanes x the solver's CTA shape (warps per CTA of the persistent
-  // one-warp-per-world solver, or, for dense nv > 32, warps per world of the CTA solver); for
+  // one-warp-per-world solver, or, for nv > 32, warps per world of the CTA solver); for
   // nv <= 32 also the Newton Hessian's assembly (FMAs or the tensor pipe), for nv > 32 the
   // tensor-core assembly tried once more on the best CTA shape
   const int lanes[3] = {8, 16, 32}, widths[6] = {1, 2, 4, 1, 2, 4}, cta[4] = {2, 4, 8, 0};
-  const bool large = m->nv > 32 && !m->is_sparse;
+  const bool large = m->nv > 32;
   float best = 0.f;
   ChosenCfg best_cfg;
   bool have = false;

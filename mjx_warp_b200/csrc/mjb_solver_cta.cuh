@@ -1,5 +1,5 @@
-// The chosen form's constraint solver for large dense models (nv > 32): one CTA of NW warps per
-// world (solver.py:26-1000, the same algorithm as solve_generic).
+// The chosen form's constraint solver for large models (nv > 32, dense or sparse mass matrix): one
+// CTA of NW warps per world (solver.py:26-1000, the same algorithm as solve_generic).
 //
 // A world with hundreds of dofs and constraint rows is too much for one warp: the Newton
 // Hessian's factorisation (nv^3 / 3 multiply-adds) and the row loops (dense nv-wide Jacobian
@@ -387,8 +387,24 @@ struct CtaSolver {
     }
   }
 
-  // res = M vec, the dense mass matrix within each dof tree block (support.py:45-92)
+  // res = M vec (support.py:35-137): the dense mass matrix within each dof tree block, or the
+  // sparse one's diagonal-plus-ancestor products, one tree per thread
   __device__ void mul_m(float* res, const float* vec) {
+    if (m.is_sparse) {
+      for (int blk = tid; blk < m.nblock; blk += NT) {
+        const int a = m.block_adr[blk], size = m.block_size[blk];
+        for (int i = a; i < a + size; i++) res[i] = qM[m.dof_Madr[i]] * vec[i];
+        for (int i = a; i < a + size; i++) {
+          int Mij = m.dof_Madr[i] + 1;
+          for (int j = m.dof_parentid[i]; j >= 0; j = m.dof_parentid[j], Mij++) {
+            res[i] += qM[Mij] * vec[j];
+            res[j] += qM[Mij] * vec[i];
+          }
+        }
+      }
+      __syncthreads();
+      return;
+    }
     for (int i = tid; i < nv; i += NT) {
       int a, size;
       dof_block(m, i, a, size);
@@ -449,13 +465,37 @@ struct CtaSolver {
   // solver.py:249-276): warp q owns the H rows i with i % NW == q, and applies each row's outer
   // product over the row's nonzero columns to those rows in constraint order, so every entry sees
   // the reference's sequence of additions and no two warps write the same entry.
-  __device__ void assemble_hessian() {
-    for (int i = warp; i < nv; i += NW) {  // the lower triangle of qM, a coalesced row per warp
-      const float* Mi = qM + size_t(i) * nv;
-      float* Hi = H + size_t(i) * nv;
-      for (int j = lane; j <= i; j += 32) Hi[j] = Mi[j];
+  // the lower triangle of the mass matrix into Out (row stride ldh, or packed by rows): the
+  // dense qM a coalesced row per warp; the sparse one zeros, then each dof's row of its
+  // ancestors (smooth.py:264-279's layout), one dof per thread
+  template <typename TH, bool PACKED = false>
+  __device__ void lower_mass(TH* Out, int ldh) {
+    auto at = [&](int i) { return PACKED ? size_t(tri(i)) : size_t(i) * ldh; };
+    if (!m.is_sparse) {
+      for (int i = warp; i < nv; i += NW) {
+        const float* Mi = qM + size_t(i) * nv;
+        TH* Hi = Out + at(i);
+        for (int j = lane; j <= i; j += 32) Hi[j] = TH(Mi[j]);
+      }
+      __syncthreads();
+      return;
+    }
+    for (int i = warp; i < nv; i += NW) {
+      TH* Hi = Out + at(i);
+      for (int j = lane; j <= i; j += 32) Hi[j] = TH(0);
     }
     __syncthreads();
+    for (int i = tid; i < nv; i += NT) {
+      int a = m.dof_Madr[i];
+      TH* Hi = Out + at(i);
+      Hi[i] = TH(qM[a]);
+      for (int j = m.dof_parentid[i]; j >= 0; j = m.dof_parentid[j]) Hi[j] = TH(qM[++a]);
+    }
+    __syncthreads();
+  }
+
+  __device__ void assemble_hessian() {
+    lower_mass<float>(H, nv);
     int* nzi = reinterpret_cast<int*>(nz);
     float* nzv = nz + round4i(nv);
     for (int k = 0; k < n; k++) {
@@ -507,6 +547,15 @@ struct CtaSolver {
     const int g = lane >> 2, t = lane & 3;
     const int nmt = (nv + 15) >> 4, ncol8 = (nv + 7) >> 3;
     const float* J = d.efc_J + size_t(adr) * nv;
+    // the accumulators start from the mass matrix: read from qM when dense; the sparse layout is
+    // first expanded into Hout's lower triangle and read back from there
+    const bool sparse = m.is_sparse;
+    if (sparse) lower_mass<TH, PACKED>(Hout, ldh);
+    auto mass = [&](int r, int c) -> float {
+      if (r >= nv || c >= nv) return 0.f;
+      if (!sparse) return qM[size_t(r) * nv + c];
+      return c <= r ? float(Hout[(PACKED ? size_t(tri(r)) : size_t(r) * ldh) + c]) : 0.f;
+    };
     for (int mt = warp; mt < nmt; mt += NW) {
       const int r0 = 16 * mt + g, r1 = r0 + 8;
       const int nnt = min((16 * mt + 15) / 8 + 1, ncol8);
@@ -515,10 +564,10 @@ struct CtaSolver {
 #pragma unroll
         for (int q = 0; q < 4; q++) {
           const int c = 8 * (nt0 + q) + 2 * t;
-          acc[q][0] = (r0 < nv && c < nv) ? qM[size_t(r0) * nv + c] : 0.f;
-          acc[q][1] = (r0 < nv && c + 1 < nv) ? qM[size_t(r0) * nv + c + 1] : 0.f;
-          acc[q][2] = (r1 < nv && c < nv) ? qM[size_t(r1) * nv + c] : 0.f;
-          acc[q][3] = (r1 < nv && c + 1 < nv) ? qM[size_t(r1) * nv + c + 1] : 0.f;
+          acc[q][0] = mass(r0, c);
+          acc[q][1] = mass(r0, c + 1);
+          acc[q][2] = mass(r1, c);
+          acc[q][3] = mass(r1, c + 1);
         }
         for (int k0 = 0; k0 < n; k0 += 8) {
           const int ka = k0 + t, kb = ka + 4;
@@ -833,7 +882,7 @@ __device__ void solve_cta(const MjbModel& m, const MjbData& d, int w, float* sme
   s.mv = d.efc_mv + W(w, nv);
   s.qfrc_constraint = d.qfrc_constraint + W(w, nv);
   s.H = d.efc_h + W(w, nv * nv);
-  s.qM = d.qM + W(w, nv * nv);
+  s.qM = d.qM + (m.is_sparse ? W(w, m.nM) : W(w, nv * nv));
   s.qfrc_smooth = d.qfrc_smooth + W(w, nv);
   s.qacc_smooth = d.qacc_smooth + W(w, nv);
   s.red = smem;

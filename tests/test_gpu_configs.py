@@ -229,3 +229,25 @@ def test_precision_form_humanoid_spheres():
   torch.cuda.synchronize()
   assert np.all(np.isfinite(d.qpos.cpu().numpy()))
   assert np.all(mjw.world_status(d) == 0)
+
+
+def test_cta_solver_sparse_mass_matrix():
+  """The CTA solver with the sparse mass matrix (the reference's automatic choice for nv >= 60):
+  the bin's Newton solve against the dense CTA solve and the FP64 oracle (the reference's cost
+  acceptance, solver_test.py:127), with the FMA and the tensor-core Hessian assembly."""
+  from mjx_warp_b200.types import MJ_JAC_SPARSE
+
+  nworld = 8
+  mjd = load("bin.xml", iterations=20, ls_iterations=20, jacobian=MJ_JAC_DENSE)
+  mjs = load("bin.xml", iterations=20, ls_iterations=20, jacobian=MJ_JAC_SPARSE)
+  qpos, qvel, ctrl = bin_state(mjd, nworld, seed=1)
+  dd = _bin_forward(mjd, qpos, qvel, ctrl, 1, 2)
+  o = oracle(mjd, qpos, qvel, ctrl, 64)
+  o.run("forward")
+  co = o.scalar("cost")
+  for tc in (False, True):
+    ds = _bin_forward(mjs, qpos, qvel, ctrl, 1, 2, tc)
+    assert np.all(mjw.world_status(ds) == 0)
+    cg = ds.efc.cost.cpu().numpy()
+    assert np.all(cg <= co + 0.025 * np.abs(co) + 1e-3), (tc, cg, co)
+    assert np.median(rel_err(dev(ds.qacc), dev(dd.qacc))) < 1e-2, tc
