@@ -11,10 +11,10 @@
 // stays uniform across the CTA.  The Hessian H = tril(qM) + sum_active D J'J is assembled in efc_h
 // (each warp updates the H rows it owns, row by row in constraint order, so no two warps touch the
 // same entry; or, selected by the autotuner and always in the precision form, as split-TF32
-// tensor-core tiles, assemble_hessian_tc) and factored by chol_cta: a left-looking blocked Cholesky with 32-column panels
-// whose panel updates A[r, p] -= L[r, :p] L[p, :p]^T run on the tensor pipe in split TF32
-// (mjb_tc.cuh), the 32 x 32 diagonal blocks by chol_tile and the panel rows below by
-// substitution.  One world per CTA keeps each matrix being factored in L2.
+// tensor-core tiles, assemble_hessian_tc) and factored by chol_cta: a left-looking blocked
+// Cholesky with 32-column panels whose panel updates A[r, p] -= L[r, :p] L[p, :p]^T run on the
+// tensor pipe in split TF32 (mjb_tc.cuh), the 32 x 32 diagonal blocks by chol_tile and the panel
+// rows below by substitution.  The precision form factors and solves in FP64 in shared memory.
 #pragma once
 
 #include "mjb_solver.cuh"
@@ -110,9 +110,10 @@ __device__ __noinline__ void chol_cta(float* A, int ld, int n, float* T, int war
             const int cc = c0 + 8 * nt + 2 * t;
 #pragma unroll
             for (int e = 0; e < 2; e++) {
-              if (cc + e < c0 + pn) {
-                if (r0 < n) A[size_t(r0) * ld + cc + e] -= acc[q][nt][e];
-                if (r1 < n) A[size_t(r1) * ld + cc + e] -= acc[q][nt][2 + e];
+              if (cc + e < c0 + pn) {  // lower triangle only (the diagonal block's upper part
+                                       // is not part of the factor)
+                if (r0 < n && cc + e <= r0) A[size_t(r0) * ld + cc + e] -= acc[q][nt][e];
+                if (r1 < n && cc + e <= r1) A[size_t(r1) * ld + cc + e] -= acc[q][nt][2 + e];
               }
             }
           }
@@ -239,9 +240,9 @@ __device__ __noinline__ void cho_solve_cta(const float* L, int ld, int n, float*
 
 // Per-CTA shared memory of the solver (floats): reductions (16 NW, as doubles 32 NW), the
 // diagonal tile (32 x 36 + 32), each warp's row-compaction scratch and the triangular solves'
-// vector (nv); the precision form adds the FP64 Hessian factor, its lower triangle packed row by row (row i at i (i + 1) / 2), then
-// the FP64 solve's vector and the factor's reciprocal diagonal (nv doubles each), 8-byte aligned
-// after the floats.
+// vector (nv); the precision form adds the FP64 Hessian factor, its lower triangle packed row by
+// row (row i at i (i + 1) / 2), then the FP64 solve's vector and the factor's reciprocal
+// diagonal (nv doubles each), 16-byte aligned after the floats.
 __host__ __device__ __forceinline__ int tri(int i) { return i * (i + 1) / 2; }
 __host__ __device__ __forceinline__ int cta_solver_smem_base(int nv, int nw) {
   return round4i(32 * nw + 32 * 36 + 32 + nw * 2 * round4i(nv) + round4i(nv));
@@ -355,7 +356,7 @@ struct CtaSolver {
   int w, tid, lane, warp, nv, adr, n;
   float *qacc, *Ma, *grad, *Mgrad, *search, *mv, *qfrc_constraint, *H;
   const float *qM, *qfrc_smooth, *qacc_smooth;
-  float* red;    // 16 NW floats (or 16 NW doubles over the same space)
+  float* red;    // 32 NW floats (cta sums of up to 9 values, as floats or doubles; the solves)
   float* T;      // chol_cta's diagonal tile
   float* nz;     // this warp's row compaction: round4(nv) ints, then round4(nv) floats
   float* zv;     // the triangular solves' intermediate vector (nv floats)
