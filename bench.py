@@ -246,6 +246,34 @@ def _qacc_error(mjm, m, d, mjw, torch, restore, forms, sample=256):
   return out
 
 
+def _stability(mjm, mjw, torch, nworld=1024, nstep=200):
+  """Worlds that go non-finite within nstep steps of the benchmark configuration from the seeded
+  initial states: the device (chosen form) against the CPU restatement in FP32 and in FP64 on the
+  same worlds.  The 3-iteration implicitfast humanoid loses a few worlds in every arithmetic."""
+  import oracle
+
+  qpos, qvel, ctrl = _state(mjm, 0, nworld)
+  m = mjw.put_model(mjm)
+  d = mjw.make_data(mjm, nworld=nworld, nconmax=48 * nworld, njmax=80 * nworld)
+  d.qpos.copy_(torch.as_tensor(qpos, dtype=torch.float32))
+  d.qvel.copy_(torch.as_tensor(qvel, dtype=torch.float32))
+  d.ctrl.copy_(torch.as_tensor(ctrl, dtype=torch.float32))
+  for _ in range(nstep):
+    mjw.step(m, d)
+  torch.cuda.synchronize()
+  out = {"worlds": nworld, "steps": nstep,
+         "device": int(np.count_nonzero(mjw.world_status(d) & 0x8))}
+  for prec in (32, 64):
+    o = oracle.Oracle(mjm, nworld, prec)
+    o.set("qpos", qpos)
+    o.set("qvel", qvel)
+    o.set("ctrl", ctrl)
+    o.run("step", nstep=nstep, nthreads=os.cpu_count() or 1)
+    q, v = o.get("qpos"), o.get("qvel")
+    out[f"fp{prec}_restatement"] = int((~(np.isfinite(q).all(1) & np.isfinite(v).all(1))).sum())
+  return out
+
+
 def _grad_rate(mjw, torch, nworld=1024, horizon=32, checkpoint=8, reps=2, centered=True,
                analytic=None):
   """grad-steps/s of a differentiated rollout (see the module docstring).  The Newton solve runs
@@ -790,8 +818,10 @@ def run_ours(args):
     forms[name] = {"value": nworld * world_size * args.steps / el, "ms_per_step": el / args.steps * 1e3}
 
   accuracy = None
+  stability = None
   if rank == 0 and not args.no_accuracy:
     accuracy = _qacc_error(mjm, m, d, mjw, torch, restore, FORMS)
+    stability = _stability(mjm, mjw, torch)
   grad = None
   if rank == 0 and not args.no_grad:
     grad = _grad_rate(mjw, torch)
@@ -880,6 +910,8 @@ def run_ours(args):
   }
   if accuracy is not None:
     line["qacc_err"] = accuracy
+  if stability is not None:
+    line["status"]["nonfinite_within_200_steps"] = stability
   if grad is not None:
     line["grad"] = grad
   if combined is not None:

@@ -328,3 +328,15 @@ def test_step_io_matches_copies_around_step():
   for k in outputs:
     assert torch.equal(out[k], res[k]), k
   del g
+
+
+def test_benchmark_configuration_stability_vs_restatement():
+  """The benchmark configuration (implicitfast, Newton 3 / ls 4) loses a few worlds to
+  non-finite states within 200 steps in every arithmetic: the CPU restatement loses 2 (FP32) and
+  7 (FP64) of these 1024 seeded worlds.  The device's count stays of the same order."""
+  import bench
+
+  mjm = bench._model()
+  out = bench._stability(mjm, mjw, torch, nworld=1024, nstep=200)
+  worst = max(out["fp32_restatement"], out["fp64_restatement"])
+  assert out["device"] <= 3 * worst + 8, out
