@@ -15,9 +15,10 @@ SRC_DIR = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libmjb200.so")
 HEADER = os.path.join(os.path.dirname(HERE), "include", "mjb200.h")
 
+# No -split-compile: its partitioning of the module changes the generated code from one build of
+# the same kernels to the next (one such build ran the small-model solver 17 % slower).
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
-              "-Xcompiler", "-fPIC", "-shared", "-cudart", "static",
-              "-split-compile=0"]  # the optimiser's work spread over all host threads
+              "-Xcompiler", "-fPIC", "-shared", "-cudart", "static"]
 
 
 def _sources():

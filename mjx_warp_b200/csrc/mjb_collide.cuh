@@ -439,17 +439,25 @@ __device__ __forceinline__ ContactOut make_out(const MjbModel& m, const MjbData&
   return o;
 }
 
-// collision_primitive.py:271-274 over this world's pairs
+// Pairs whose contact count (at most 4: plane-box) a lane keeps from the counting pass, 3 bits
+// each in one 64-bit register: the first kCountChunks chunks of 32 pairs (672 pairs per world).
+// The write pass evaluates only those pairs that make contacts; pairs beyond are counted again.
+constexpr int kCountChunks = 21;
+
+// collision_primitive.py:271-274 over this world's pairs.  The world's contacts take one
+// contiguous block: a counting pass sizes it, a write pass fills it in pair order.
 __device__ void primitive_narrowphase(const MjbModel& m, const MjbData& d, int w, int lane) {
   const int pa = d.world_pairadr[w], np = d.world_npair[w];
   int total = 0;
-  for (int base = 0; base < np; base += 32) {
+  unsigned long long counts = 0;
+  for (int base = 0, chunk = 0; base < np; base += 32, chunk++) {
     int c = 0;
     if (base + lane < np) {
       ContactOut o = make_out(m, d, w, pa + base + lane);
       narrow_pair(o);
       c = o.count;
     }
+    if (chunk < kCountChunks) counts |= (unsigned long long)c << (3 * chunk);
     total += warp_sum_i(c);
   }
   const int adr = reserve(d.ncon, total, d.nconmax, d.world_status ? d.world_status + w : nullptr,
@@ -457,18 +465,19 @@ __device__ void primitive_narrowphase(const MjbModel& m, const MjbData& d, int w
   if (adr < 0) total = 0;
   if (total > 0) {
     int run = 0;
-    for (int base = 0; base < np; base += 32) {
-      ContactOut o;
+    for (int base = 0, chunk = 0; base < np; base += 32, chunk++) {
       int c = 0;
-      if (base + lane < np) {
-        o = make_out(m, d, w, pa + base + lane);
+      if (chunk < kCountChunks) {
+        c = (int)((counts >> (3 * chunk)) & 7ull);
+      } else if (base + lane < np) {
+        ContactOut o = make_out(m, d, w, pa + base + lane);
         narrow_pair(o);
         c = o.count;
       }
       int tot;
       const int off = warp_excl_scan(c, lane, &tot);
       if (c > 0) {
-        o.count = 0;
+        ContactOut o = make_out(m, d, w, pa + base + lane);
         o.next = adr + run + off;
         narrow_pair(o);
       }

@@ -105,19 +105,26 @@ def _scatter(mjm, nworld, seed, half=0.45, zmax=0.4):
   return qpos, np.zeros((nworld, mjm.nv)), np.zeros((nworld, 0))
 
 
-@pytest.mark.parametrize("name", ["bin.xml", "spheres120"])
+@pytest.mark.parametrize("name", ["bin.xml", "spheres120", "spheres240"])
 def test_sap_pair_lists_bit_exact(name):
   """Sweep-and-prune (collision_driver.py:350-455) on the device vs the oracle's restatement given
   the device's geom poses: identical pair lists, in the same sweep order, in every world.
   bin.xml (69 geoms, walls off the origin) calls sap_broadphase directly; the 123-geom model goes
   through collision(), which selects sweep-and-prune for ngeom > 100 as the reference does, and
-  its contacts are compared too.  (Both models are large enough for the reference's automatic
+  its contacts are compared too; with 240 spheres every world has more candidate pairs than the
+  narrowphase keeps contact counts for between its counting and write passes (672), so the pairs
+  past them are counted twice.  (These models are large enough for the reference's automatic
   sparse mass matrix; jacobian = 0 selects the dense one the kernels implement.)"""
-  mjm = load("bin.xml", jacobian=0) if name == "bin.xml" else load(_spheres_xml(120), jacobian=0)
+  nsphere = 240 if name == "spheres240" else 120
+  mjm = load("bin.xml", jacobian=0) if name == "bin.xml" else load(_spheres_xml(nsphere), jacobian=0)
   nworld = 64
-  qpos, qvel, ctrl = _scatter(mjm, nworld, seed=5)
+  if name == "spheres240":  # packed into a 0.6 x 0.6 x 0.3 box: 876-979 pairs per world
+    qpos, qvel, ctrl = _scatter(mjm, nworld, seed=5, half=0.3, zmax=0.3)
+  else:
+    qpos, qvel, ctrl = _scatter(mjm, nworld, seed=5)
   m = mjw.put_model(mjm)
-  d = device_data(mjm, qpos, qvel, ctrl, nconmax=4096 * nworld // 8, njmax=64 * nworld)
+  nconmax = (1024 if name == "spheres240" else 512) * nworld
+  d = device_data(mjm, qpos, qvel, ctrl, nconmax=nconmax, njmax=64 * nworld)
   mjw.kinematics(m, d)
   if name == "bin.xml":
     mjw.sap_broadphase(m, d)
@@ -133,6 +140,8 @@ def test_sap_pair_lists_bit_exact(name):
   cnt, opairs = o.rows("pair")
   n, pairs = _device_rows(d, "pair", d.collision_pair, 2)
   assert cnt.sum() > nworld
+  if name == "spheres240":
+    assert cnt.min() > 672
   np.testing.assert_array_equal(n, cnt)
   np.testing.assert_array_equal(pairs, opairs.astype(np.int32))
   if name != "bin.xml":
