@@ -526,31 +526,49 @@ __device__ __forceinline__ void copy_rows(const float* src, int sld, float* dst,
 
 // In-place Cholesky of an n x n (n <= 32) SPD tile with row stride ld (lower triangle): the
 // partial sums of chol_lower with float4 row reads; the pivot and its reciprocal come from one
-// rsqrtf (within 2 ulp of the correctly rounded sqrt and reciprocal).
+// rsqrtf (within 2 ulp of the correctly rounded sqrt and reciprocal).  Lane i works on row i,
+// two columns per step: one pass over the row's finished columns feeds both columns' partial sums
+// (its loads shared), the first column's new entry L[i][k] completes the second's with the entry
+// L[k+1][k] shuffled from lane k + 1, and one __syncwarp() publishes both columns.  Every sum is
+// formed in the order of the one-column form (k is even, so column k + 1 has the same float4
+// chunks as column k and one more term in its tail), so the factor is the same bit for bit.
 __device__ MJB_TILE_FN void chol_tile(float* A, int ld, int n, int lane) {
-  for (int k = 0; k < n; k++) {
-    const float* Ai = A + min(k + lane, n - 1) * ld;  // lanes past the last row reuse it
+  float* Ar = A + min(lane, n - 1) * ld;  // lanes past the last row repeat it
+  for (int k = 0; k < n; k += 2) {
+    const bool two = k + 1 < n;
     const float* Ak = A + k * ld;
-    float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f;
+    const float* Ak1 = two ? Ak + ld : Ak;
+    float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f, t0 = 0.f, t1 = 0.f, t2 = 0.f, t3 = 0.f;
     int m = 0;
 #pragma unroll 4
     for (; m + 3 < k; m += 4) {
-      const float4 a = *reinterpret_cast<const float4*>(Ai + m);
+      const float4 a = *reinterpret_cast<const float4*>(Ar + m);
       const float4 b = *reinterpret_cast<const float4*>(Ak + m);
+      const float4 c = *reinterpret_cast<const float4*>(Ak1 + m);
       s0 += a.x * b.x;
       s1 += a.y * b.y;
       s2 += a.z * b.z;
       s3 += a.w * b.w;
+      t0 += a.x * c.x;
+      t1 += a.y * c.y;
+      t2 += a.z * c.z;
+      t3 += a.w * c.w;
     }
-    for (; m < k; m++) s0 += Ai[m] * Ak[m];
-    const float s = Ai[k] - ((s0 + s1) + (s2 + s3));
-    // pivot from one reciprocal square root: 1 / L_kk = rsqrt(s_k), L_kk = s_k * rsqrt(s_k)
-    const float sk = __shfl_sync(WARP_FULL, s, 0);
-    const float inv = rsqrtf(sk);
-    const float lkk = sk * inv;
-    __syncwarp();
-    if (lane == 0) A[k * ld + k] = lkk;
-    else if (k + lane < n) A[(k + lane) * ld + k] = s * inv;
+    for (; m < k; m++) {
+      const float a = Ar[m];
+      s0 += a * Ak[m];
+      t0 += a * Ak1[m];
+    }
+    const float si = Ar[k] - ((s0 + s1) + (s2 + s3));
+    const float inv = rsqrtf(__shfl_sync(WARP_FULL, si, k));
+    const float lik = si * inv;  // L[i][k]; on lane k the pivot L[k][k]
+    if (lane >= k && lane < n) Ar[k] = lik;
+    if (two) {
+      t0 += lik * __shfl_sync(WARP_FULL, lik, k + 1);  // the term L[i][k] L[k+1][k]
+      const float ti = Ar[k + 1] - ((t0 + t1) + (t2 + t3));
+      const float inv1 = rsqrtf(__shfl_sync(WARP_FULL, ti, k + 1));
+      if (lane > k && lane < n) Ar[k + 1] = ti * inv1;
+    }
     __syncwarp();
   }
 }
@@ -569,10 +587,10 @@ __device__ MJB_TILE_FN float cho_solve_tile(const float* L, int ld, int n, float
 #pragma unroll
     for (int t = 0; t < 4; t++) {
       const int k = 4 * q + t;
-      if (k < n) {
-        const float zk = __shfl_sync(WARP_FULL, z, k) * __shfl_sync(WARP_FULL, invd, k);
-        if (lane == k) z = zk;
-        else if (lane > k && own) z -= lq[t] * zk;
+      if (k < n) {  // lane k scales its entry, one shuffle broadcasts it
+        if (lane == k) z *= invd;
+        const float zk = __shfl_sync(WARP_FULL, z, k);
+        if (lane > k && own) z -= lq[t] * zk;
       }
     }
   }
@@ -580,9 +598,9 @@ __device__ MJB_TILE_FN float cho_solve_tile(const float* L, int ld, int n, float
 #pragma unroll 4
   for (int k = n - 1; k >= 0; k--) {
     const float lk = L[k * ld + (lane < k ? lane : 0)];
-    const float xk = __shfl_sync(WARP_FULL, x, k) * __shfl_sync(WARP_FULL, invd, k);
-    if (lane == k) x = xk;
-    else if (lane < k) x -= lk * xk;
+    if (lane == k) x *= invd;
+    const float xk = __shfl_sync(WARP_FULL, x, k);
+    if (lane < k) x -= lk * xk;
   }
   return own ? x : 0.f;
 }
@@ -590,22 +608,33 @@ __device__ MJB_TILE_FN float cho_solve_tile(const float* L, int ld, int n, float
 // FP64 counterparts of chol_tile / cho_solve_tile for the precision form (MJB_FORM_PRECISION):
 // the same lane-per-row scheme on a tile of doubles (row stride ld doubles), with the pivot from
 // the double square root and division.
+// chol_tile_d takes two columns per step as chol_tile does (k even: both columns' pairs of
+// partial sums cover [0, k), column k + 1 adds L[i][k] L[k+1][k] as its tail term).
 __device__ __noinline__ void chol_tile_d(double* A, int ld, int n, int lane) {
-  for (int k = 0; k < n; k++) {
-    const double* Ai = A + min(k + lane, n - 1) * ld;
+  double* Ar = A + min(lane, n - 1) * ld;  // lane i on row i; lanes past the last row repeat it
+  for (int k = 0; k < n; k += 2) {
+    const bool two = k + 1 < n;
     const double* Ak = A + k * ld;
-    double s0 = 0.0, s1 = 0.0;
-    int m = 0;
-    for (; m + 1 < k; m += 2) {
-      s0 += Ai[m] * Ak[m];
-      s1 += Ai[m + 1] * Ak[m + 1];
+    const double* Ak1 = two ? Ak + ld : Ak;
+    double s0 = 0.0, s1 = 0.0, t0 = 0.0, t1 = 0.0;
+    for (int m = 0; m + 1 < k; m += 2) {
+      const double a0 = Ar[m], a1 = Ar[m + 1];
+      s0 += a0 * Ak[m];
+      s1 += a1 * Ak[m + 1];
+      t0 += a0 * Ak1[m];
+      t1 += a1 * Ak1[m + 1];
     }
-    if (m < k) s0 += Ai[m] * Ak[m];
-    const double s = Ai[k] - (s0 + s1);
-    const double lkk = sqrt(__shfl_sync(WARP_FULL, s, 0));
-    __syncwarp();
-    if (lane == 0) A[k * ld + k] = lkk;
-    else if (k + lane < n) A[(k + lane) * ld + k] = s / lkk;
+    const double si = Ar[k] - (s0 + s1);
+    const double lkk = sqrt(__shfl_sync(WARP_FULL, si, k));
+    const double lik = lane == k ? lkk : si / lkk;
+    if (lane >= k && lane < n) Ar[k] = lik;
+    if (two) {
+      t0 += lik * __shfl_sync(WARP_FULL, lik, k + 1);
+      const double ti = Ar[k + 1] - (t0 + t1);
+      const double l1 = sqrt(__shfl_sync(WARP_FULL, ti, k + 1));
+      if (lane == k + 1) Ar[k + 1] = l1;
+      else if (lane > k + 1 && lane < n) Ar[k + 1] = ti / l1;
+    }
     __syncwarp();
   }
 }
