@@ -174,38 +174,69 @@ constexpr int kOrderBuckets = 256;
 // Worlds with the same bucket in a warp are counted and placed with one shared-memory atomic per
 // bucket (the lanes of a bucket found by __match_any_sync), so the few buckets a model's row
 // counts fall into do not serialise thousands of atomics.
+// Each thread loads kOrderLoads of its worlds' row counts before it counts or places any of them
+// (one load latency per kOrderLoads worlds), and the descending exclusive scan of the buckets is
+// a warp scan over eight buckets per lane.
+constexpr int kOrderLoads = 8;
+__device__ __forceinline__ int order_bucket(const int* nefc, int w, int nworld) {
+  return w < nworld ? min(max(nefc[w], 0), kOrderBuckets - 1) : -1;
+}
 __global__ void __launch_bounds__(1024) k_order_worlds(const int* nefc, int* order, int* queue,
                                                       int nworld) {
   __shared__ int cnt[kOrderBuckets];
   const int lane = threadIdx.x & 31;
   const unsigned below = (1u << lane) - 1u;
-  const int span = (nworld + blockDim.x - 1) / blockDim.x * blockDim.x;  // warp-uniform trip count
+  const int chunk = kOrderLoads * blockDim.x;  // worlds per pass of the whole block (warp-uniform)
   for (int b = threadIdx.x; b < kOrderBuckets; b += blockDim.x) cnt[b] = 0;
   __syncthreads();
-  for (int w = threadIdx.x; w < span; w += blockDim.x) {
-    const int b = w < nworld ? min(max(nefc[w], 0), kOrderBuckets - 1) : -1;
-    const unsigned peers = __match_any_sync(WARP_FULL, b);
-    if (b >= 0 && (peers & below) == 0) atomicAdd(&cnt[b], __popc(peers));
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    int run = 0;
-    for (int b = kOrderBuckets - 1; b >= 0; b--) {
-      const int c = cnt[b];
-      cnt[b] = run;
-      run += c;
+  for (int w0 = 0; w0 < nworld; w0 += chunk) {
+    int bk[kOrderLoads];
+#pragma unroll
+    for (int j = 0; j < kOrderLoads; j++) bk[j] = order_bucket(nefc, w0 + j * blockDim.x + threadIdx.x, nworld);
+#pragma unroll
+    for (int j = 0; j < kOrderLoads; j++) {
+      const unsigned peers = __match_any_sync(WARP_FULL, bk[j]);
+      if (bk[j] >= 0 && (peers & below) == 0) atomicAdd(&cnt[bk[j]], __popc(peers));
     }
-    *queue = 0;
   }
   __syncthreads();
-  for (int w = threadIdx.x; w < span; w += blockDim.x) {
-    const int b = w < nworld ? min(max(nefc[w], 0), kOrderBuckets - 1) : -1;
-    const unsigned peers = __match_any_sync(WARP_FULL, b);
-    const int leader = __ffs(peers) - 1;
-    int base = 0;
-    if (b >= 0 && lane == leader) base = atomicAdd(&cnt[b], __popc(peers));
-    base = __shfl_sync(WARP_FULL, base, leader);
-    if (b >= 0) order[base + __popc(peers & below)] = w;
+  static_assert(kOrderBuckets == 32 * 8, "eight buckets per lane of the scanning warp");
+  if (threadIdx.x < 32) {  // lane l: buckets 255 - 8 l .. 248 - 8 l (largest row counts first)
+    int c[8], sum = 0;
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+      c[j] = cnt[kOrderBuckets - 1 - 8 * lane - j];
+      sum += c[j];
+    }
+    int incl = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(WARP_FULL, incl, o);
+      if (lane >= o) incl += t;
+    }
+    int run = incl - sum;
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+      cnt[kOrderBuckets - 1 - 8 * lane - j] = run;
+      run += c[j];
+    }
+    if (lane == 0) *queue = 0;
+  }
+  __syncthreads();
+  for (int w0 = 0; w0 < nworld; w0 += chunk) {
+    int bk[kOrderLoads];
+#pragma unroll
+    for (int j = 0; j < kOrderLoads; j++) bk[j] = order_bucket(nefc, w0 + j * blockDim.x + threadIdx.x, nworld);
+#pragma unroll
+    for (int j = 0; j < kOrderLoads; j++) {
+      const int b = bk[j];
+      const unsigned peers = __match_any_sync(WARP_FULL, b);
+      const int leader = __ffs(peers) - 1;
+      int base = 0;
+      if (b >= 0 && lane == leader) base = atomicAdd(&cnt[b], __popc(peers));
+      base = __shfl_sync(WARP_FULL, base, leader);
+      if (b >= 0) order[base + __popc(peers & below)] = w0 + j * blockDim.x + threadIdx.x;
+    }
   }
 }
 

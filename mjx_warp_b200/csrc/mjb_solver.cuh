@@ -656,22 +656,56 @@ __device__ __forceinline__ float newton_direction(const float* Ms, int ld, const
       h[4 * q + 2] = v.z;
       h[4 * q + 3] = v.w;
     }
-    for (int k = 0; k < n; k++) {
-      const float c = C ? C[k] : (act[k] ? D[k] : 0.f);
-      if (c == 0.f) continue;
-      const float* Jr = J + size_t(k) * ldj;
-      const float a = own ? c * Jr[lane] : 0.f;
-      if (ST) {  // zero-padded, 16-byte aligned rows
-        const float4* J4 = reinterpret_cast<const float4*>(Jr);
+    if (ST) {
+      // staged rows (n <= 32, zero-padded, 16-byte aligned): the rows with c != 0 taken from a
+      // ballot mask in increasing order, two per pass (each h[j] still adds the rows' terms in
+      // row order)
+      unsigned mk = __ballot_sync(WARP_FULL, lane < n && C[lane] != 0.f);
+      while (mk) {
+        const int k0 = __ffs(mk) - 1;
+        mk &= mk - 1u;
+        const float* J0 = J + k0 * ldj;
+        const float a0 = own ? C[k0] * J0[lane] : 0.f;
+        const float4* A4 = reinterpret_cast<const float4*>(J0);
+        if (mk) {
+          const int k1 = __ffs(mk) - 1;
+          mk &= mk - 1u;
+          const float* J1 = J + k1 * ldj;
+          const float a1 = own ? C[k1] * J1[lane] : 0.f;
+          const float4* B4 = reinterpret_cast<const float4*>(J1);
 #pragma unroll
-        for (int q = 0; q < 8; q++) {
-          const float4 v = q < nq ? J4[q] : make_float4(0.f, 0.f, 0.f, 0.f);
-          h[4 * q] += a * v.x;
-          h[4 * q + 1] += a * v.y;
-          h[4 * q + 2] += a * v.z;
-          h[4 * q + 3] += a * v.w;
+          for (int q = 0; q < 8; q++) {
+            if (q < nq) {
+              const float4 u = A4[q], v = B4[q];
+              h[4 * q] += a0 * u.x;
+              h[4 * q + 1] += a0 * u.y;
+              h[4 * q + 2] += a0 * u.z;
+              h[4 * q + 3] += a0 * u.w;
+              h[4 * q] += a1 * v.x;
+              h[4 * q + 1] += a1 * v.y;
+              h[4 * q + 2] += a1 * v.z;
+              h[4 * q + 3] += a1 * v.w;
+            }
+          }
+        } else {
+#pragma unroll
+          for (int q = 0; q < 8; q++) {
+            if (q < nq) {
+              const float4 u = A4[q];
+              h[4 * q] += a0 * u.x;
+              h[4 * q + 1] += a0 * u.y;
+              h[4 * q + 2] += a0 * u.z;
+              h[4 * q + 3] += a0 * u.w;
+            }
+          }
         }
-      } else {
+      }
+    } else {
+      for (int k = 0; k < n; k++) {
+        const float c = C ? C[k] : (act[k] ? D[k] : 0.f);
+        if (c == 0.f) continue;
+        const float* Jr = J + size_t(k) * ldj;
+        const float a = own ? c * Jr[lane] : 0.f;
 #pragma unroll
         for (int j = 0; j < 32; j++)
           if (j < nv) h[j] += a * Jr[j];
