@@ -527,47 +527,43 @@ __device__ __forceinline__ void copy_rows(const float* src, int sld, float* dst,
 // In-place Cholesky of an n x n (n <= 32) SPD tile with row stride ld (lower triangle): the
 // partial sums of chol_lower with float4 row reads; the pivot and its reciprocal come from one
 // rsqrtf (within 2 ulp of the correctly rounded sqrt and reciprocal).  Lane i works on row i,
-// two columns per step: one pass over the row's finished columns feeds both columns' partial sums
-// (its loads shared), the first column's new entry L[i][k] completes the second's with the entry
-// L[k+1][k] shuffled from lane k + 1, and one __syncwarp() publishes both columns.  Every sum is
-// formed in the order of the one-column form (k is even, so column k + 1 has the same float4
-// chunks as column k and one more term in its tail), so the factor is the same bit for bit.
+// four columns per step: one pass over the row's finished columns (whole float4 chunks, k being a
+// multiple of 4) feeds the four columns' partial sums, its row loads shared; then column k + j
+// adds the terms L[i][k + t] L[k + j][k + t], t < j, with L[k + j][k + t] shuffled from lane k + j,
+// and one __syncwarp() publishes the four columns.  Every sum is formed in the order of the
+// one-column form (the same float4 chunks, then the remaining terms in column order into the first
+// partial sum), so the factor is the same bit for bit.
 __device__ MJB_TILE_FN void chol_tile(float* A, int ld, int n, int lane) {
   float* Ar = A + min(lane, n - 1) * ld;  // lanes past the last row repeat it
-  for (int k = 0; k < n; k += 2) {
-    const bool two = k + 1 < n;
-    const float* Ak = A + k * ld;
-    const float* Ak1 = two ? Ak + ld : Ak;
-    float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f, t0 = 0.f, t1 = 0.f, t2 = 0.f, t3 = 0.f;
-    int m = 0;
-#pragma unroll 4
-    for (; m + 3 < k; m += 4) {
+  for (int k = 0; k < n; k += 4) {
+    const int nb = min(4, n - k);  // columns of this step
+    const float* Ak[4];
+#pragma unroll
+    for (int j = 0; j < 4; j++) Ak[j] = A + (k + (j < nb ? j : 0)) * ld;
+    float s[4][4];
+#pragma unroll
+    for (int j = 0; j < 4; j++) s[j][0] = s[j][1] = s[j][2] = s[j][3] = 0.f;
+    for (int m = 0; m < k; m += 4) {
       const float4 a = *reinterpret_cast<const float4*>(Ar + m);
-      const float4 b = *reinterpret_cast<const float4*>(Ak + m);
-      const float4 c = *reinterpret_cast<const float4*>(Ak1 + m);
-      s0 += a.x * b.x;
-      s1 += a.y * b.y;
-      s2 += a.z * b.z;
-      s3 += a.w * b.w;
-      t0 += a.x * c.x;
-      t1 += a.y * c.y;
-      t2 += a.z * c.z;
-      t3 += a.w * c.w;
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        const float4 b = *reinterpret_cast<const float4*>(Ak[j] + m);
+        s[j][0] += a.x * b.x;
+        s[j][1] += a.y * b.y;
+        s[j][2] += a.z * b.z;
+        s[j][3] += a.w * b.w;
+      }
     }
-    for (; m < k; m++) {
-      const float a = Ar[m];
-      s0 += a * Ak[m];
-      t0 += a * Ak1[m];
-    }
-    const float si = Ar[k] - ((s0 + s1) + (s2 + s3));
-    const float inv = rsqrtf(__shfl_sync(WARP_FULL, si, k));
-    const float lik = si * inv;  // L[i][k]; on lane k the pivot L[k][k]
-    if (lane >= k && lane < n) Ar[k] = lik;
-    if (two) {
-      t0 += lik * __shfl_sync(WARP_FULL, lik, k + 1);  // the term L[i][k] L[k+1][k]
-      const float ti = Ar[k + 1] - ((t0 + t1) + (t2 + t3));
-      const float inv1 = rsqrtf(__shfl_sync(WARP_FULL, ti, k + 1));
-      if (lane > k && lane < n) Ar[k + 1] = ti * inv1;
+    float l[4] = {0.f, 0.f, 0.f, 0.f};  // L[i][k + j]; on lane k + j the pivot
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      if (j < nb) {
+#pragma unroll
+        for (int t = 0; t < j; t++) s[j][0] += l[t] * __shfl_sync(WARP_FULL, l[t], k + j);
+        const float x = Ar[k + j] - ((s[j][0] + s[j][1]) + (s[j][2] + s[j][3]));
+        l[j] = x * rsqrtf(__shfl_sync(WARP_FULL, x, k + j));
+        if (lane >= k + j && lane < n) Ar[k + j] = l[j];
+      }
     }
     __syncwarp();
   }
