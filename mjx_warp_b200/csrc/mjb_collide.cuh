@@ -56,9 +56,11 @@ __device__ void nxn_broadphase(const MjbModel& m, const MjbData& d, int w, int l
   const float* gxmat = d.geom_xmat + W(w, 9 * m.ngeom);
   const int np = m.npair_cand;
   int count = 0;
-  for (int base = 0; base < np; base += 32) {
+  unsigned passed = 0u;  // the lane's test results for the first 32 chunks, kept for the write pass
+  for (int base = 0, chunk = 0; base < np; base += 32, chunk++) {
     const int e = base + lane;
     const bool pass = e < np && nxn_bound(m, gxpos, gxmat, m.pair_cand[2 * e], m.pair_cand[2 * e + 1]);
+    if (pass && chunk < 32) passed |= 1u << chunk;
     count += __popc(__ballot_sync(WARP_FULL, pass));
   }
   const int adr = reserve(d.ncollision, count, d.nconmax, d.world_status ? d.world_status + w : nullptr,
@@ -66,14 +68,14 @@ __device__ void nxn_broadphase(const MjbModel& m, const MjbData& d, int w, int l
   if (adr < 0) count = 0;
   if (count > 0) {
     int run = 0;
-    for (int base = 0; base < np; base += 32) {
+    for (int base = 0, chunk = 0; base < np; base += 32, chunk++) {
       const int e = base + lane;
       int g1 = 0, g2 = 0;
       bool pass = false;
       if (e < np) {
         g1 = m.pair_cand[2 * e];
         g2 = m.pair_cand[2 * e + 1];
-        pass = nxn_bound(m, gxpos, gxmat, g1, g2);
+        pass = chunk < 32 ? ((passed >> chunk) & 1u) != 0u : nxn_bound(m, gxpos, gxmat, g1, g2);
       }
       const unsigned mask = __ballot_sync(WARP_FULL, pass);
       if (pass) {

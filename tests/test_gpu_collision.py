@@ -152,6 +152,38 @@ def test_sap_pair_lists_bit_exact(name):
     np.testing.assert_array_equal(geoms, o.rows("contact_geom")[1].astype(np.int32))
 
 
+def test_nxn_many_candidates_bit_exact():
+  """nxn_broadphase with more candidate pairs than the 32 chunks of 32 whose test results the
+  kernel keeps for its write pass (63 geoms: 1950 candidates), the rest tested again: the same
+  pair lists as the oracle, in the same order, in every world, and the same contacts."""
+  mjm = load(_spheres_xml(60), jacobian=0)
+  assert mjm.ngeom <= 100
+  nworld = 32
+  qpos, qvel, ctrl = _scatter(mjm, nworld, seed=9, half=0.25, zmax=0.3)
+  m = mjw.put_model(mjm)
+  from mjx_warp_b200.io import pair_candidates
+  assert pair_candidates(m).shape[0] > 32 * 32
+  d = device_data(mjm, qpos, qvel, ctrl, nconmax=1024 * nworld, njmax=64 * nworld)
+  mjw.kinematics(m, d)
+  mjw.collision(m, d)
+  torch.cuda.synchronize()
+  assert np.all(mjw.world_status(d) == 0)
+  o = oracle(mjm, qpos, qvel, ctrl, 32)
+  o.set("geom_xpos", dev(d.geom_xpos))
+  o.set("geom_xmat", dev(d.geom_xmat))
+  o.run("nxn_broadphase")
+  cnt, opairs = o.rows("pair")
+  n, pairs = _device_rows(d, "pair", d.collision_pair, 2)
+  assert cnt.sum() > nworld
+  np.testing.assert_array_equal(n, cnt)
+  np.testing.assert_array_equal(pairs, opairs.astype(np.int32))
+  o.run("narrowphase")
+  ccnt, _ = o.rows("contact_dist")
+  nc, geoms = _device_rows(d, "contact", d.contact.geom, 2)
+  np.testing.assert_array_equal(nc, ccnt)
+  np.testing.assert_array_equal(geoms, o.rows("contact_geom")[1].astype(np.int32))
+
+
 @pytest.mark.parametrize("name", ["humanoid.xml", "collision.xml"])
 def test_pair_sets_bit_exact(name):
   """Given the device's geom poses, the oracle's FP32 nxn test selects the identical pair list,
