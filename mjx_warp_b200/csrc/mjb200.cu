@@ -29,6 +29,12 @@
 #ifndef MJB_MINB
 #define MJB_MINB 4
 #endif
+// the same for the chosen form's FP32 persistent solver (k_solve_queue<false, false>): 5 CTAs
+// per SM (96 registers, with spills) measured 0.271 -> 0.258 ms on the humanoid at 8192 worlds,
+// while the plain form's solver and the precision solver were slower at 5
+#ifndef MJB_MINB_QUEUE
+#define MJB_MINB_QUEUE 5
+#endif
 // lanes per world in the chosen form's tree-recursion stage kernels (8, 16 or 32; 16 measured
 // fastest for the humanoid: phase 0 290 us vs 306 at 8 and 323 at 32)
 #ifndef MJB_TREE_LANES
@@ -241,7 +247,7 @@ __global__ void __launch_bounds__(1024) k_order_worlds(const int* nefc, int* ord
 }
 
 template <bool PREC, bool TC>
-__global__ void __launch_bounds__(128, MJB_MINB) k_solve_queue(const __grid_constant__ MjbModel m, const __grid_constant__ MjbData d, int smem_per_warp) {
+__global__ void __launch_bounds__(128, (PREC || TC) ? MJB_MINB : MJB_MINB_QUEUE) k_solve_queue(const __grid_constant__ MjbModel m, const __grid_constant__ MjbData d, int smem_per_warp) {
   extern __shared__ __align__(16) float smem[];
   const int lane = threadIdx.x & 31;
   float* sm = smem_per_warp ? smem + size_t(threadIdx.x >> 5) * smem_per_warp : nullptr;
