@@ -35,6 +35,13 @@
 #ifndef MJB_MINB_QUEUE
 #define MJB_MINB_QUEUE 5
 #endif
+// minimum resident CTAs per SM of the other stage kernels and of the integrator (64 registers)
+#ifndef MJB_MINB_STAGE
+#define MJB_MINB_STAGE 8
+#endif
+#ifndef MJB_MINB_INT
+#define MJB_MINB_INT 8
+#endif
 // lanes per world in the chosen form's tree-recursion stage kernels (8, 16 or 32; 16 measured
 // fastest for the humanoid: phase 0 290 us vs 306 at 8 and 323 at 32)
 #ifndef MJB_TREE_LANES
@@ -74,7 +81,7 @@ __device__ __forceinline__ void copy_qacc_smooth(const MjbModel& m, const MjbDat
 
 // the solver needs up to 128 registers; every other stage is held to 64 for occupancy
 template <int STAGE>
-__global__ void __launch_bounds__(128, STAGE == S_SOLVE ? MJB_MINB : 8)
+__global__ void __launch_bounds__(128, STAGE == S_SOLVE ? MJB_MINB : MJB_MINB_STAGE)
     k_stage(const __grid_constant__ MjbModel m, const __grid_constant__ MjbData d, int smem_per_warp) {
   extern __shared__ __align__(16) float smem[];
   const int lane = threadIdx.x & 31;
@@ -110,7 +117,7 @@ __global__ void __launch_bounds__(128, STAGE == S_SOLVE ? MJB_MINB : 8)
 // keeps the world's lanes busy instead of leaving most of a warp idle, so the warp instructions
 // per world drop by up to 32 / L.  The stages' arithmetic does not depend on L.
 template <int STAGE, int L>
-__global__ void __launch_bounds__(128, 8)
+__global__ void __launch_bounds__(128, MJB_MINB_STAGE)
     k_stage_lanes(const __grid_constant__ MjbModel m, const __grid_constant__ MjbData d) {
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const int w = int(t / L), lane = int(t % L);
@@ -284,7 +291,7 @@ __global__ void __launch_bounds__(NW * 32, NW >= 16 ? 1 : (NW >= 8 ? 2 : (NW >= 
 }
 
 // chosen form: integration (forward.py:165-405) and the finiteness check
-__global__ void __launch_bounds__(128, 8) k_integrate(const __grid_constant__ MjbModel m, const __grid_constant__ MjbData d, int tile_per_warp) {
+__global__ void __launch_bounds__(128, MJB_MINB_INT) k_integrate(const __grid_constant__ MjbModel m, const __grid_constant__ MjbData d, int tile_per_warp) {
   extern __shared__ __align__(16) float smem[];
   const int lane = threadIdx.x & 31;
   const int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
