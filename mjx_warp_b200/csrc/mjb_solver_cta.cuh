@@ -77,27 +77,55 @@ __device__ __noinline__ void chol_cta(float* A, int ld, int n, float* T, int war
           for (int nt = 0; nt < 4; nt++)
 #pragma unroll
             for (int e = 0; e < 4; e++) acc[q][nt][e] = 0.f;
-#pragma unroll 4
-        for (int k0 = 0; k0 < c0; k0 += 8) {
-          FragB b[4];  // B[k][j] = L[c0 + j][k0 + k], j = 8 nt + g
+        // raw loads of chunk k0 + 8 are issued before chunk k0's splits and products
+        float rb[4][2], ra[kMt][4];
+        auto load = [&](int k0, float (&xb)[4][2], float (&xa)[kMt][4]) {
 #pragma unroll
-          for (int nt = 0; nt < 4; nt++) {
+          for (int nt = 0; nt < 4; nt++) {  // B[k][j] = L[c0 + j][k0 + k], j = 8 nt + g
             const int r = c0 + 8 * nt + g;
             const float* Ar = A + size_t(r) * ld + k0;
-            b[nt] = r < n ? frag_b(Ar[t], Ar[t + 4]) : frag_b(0.f, 0.f);
+            xb[nt][0] = r < n ? Ar[t] : 0.f;
+            xb[nt][1] = r < n ? Ar[t + 4] : 0.f;
           }
 #pragma unroll
           for (int q = 0; q < kMt; q++) {
             const int mt = mt0 + q * NW;
+            const int r0 = c0 + 16 * mt + g, r1 = r0 + 8;
+            const bool ok0 = mt < nmt && r0 < n, ok1 = mt < nmt && r1 < n;
+            const float* A0 = A + size_t(r0) * ld + k0;
+            const float* A1 = A + size_t(r1) * ld + k0;
+            xa[q][0] = ok0 ? A0[t] : 0.f;
+            xa[q][1] = ok1 ? A1[t] : 0.f;
+            xa[q][2] = ok0 ? A0[t + 4] : 0.f;
+            xa[q][3] = ok1 ? A1[t + 4] : 0.f;
+          }
+        };
+        load(0, rb, ra);
+        for (int k0 = 0; k0 < c0; k0 += 8) {
+          float nb[4][2], na[kMt][4];
+          if (k0 + 8 < c0) load(k0 + 8, nb, na);
+          FragB b[4];
+#pragma unroll
+          for (int nt = 0; nt < 4; nt++) b[nt] = frag_b(rb[nt][0], rb[nt][1]);
+#pragma unroll
+          for (int q = 0; q < kMt; q++) {
+            const int mt = mt0 + q * NW;
             if (mt < nmt) {
-              const int r0 = c0 + 16 * mt + g, r1 = r0 + 8;
-              const float* A0 = A + size_t(r0) * ld + k0;
-              const float* A1 = A + size_t(r1) * ld + k0;
-              const FragA a = frag_a(r0 < n ? A0[t] : 0.f, r1 < n ? A1[t] : 0.f,
-                                     r0 < n ? A0[t + 4] : 0.f, r1 < n ? A1[t + 4] : 0.f);
+              const FragA a = frag_a(ra[q][0], ra[q][1], ra[q][2], ra[q][3]);
 #pragma unroll
               for (int nt = 0; nt < 4; nt++) mma_3xtf32(acc[q][nt], a, b[nt]);
             }
+          }
+          if (k0 + 8 < c0) {
+#pragma unroll
+            for (int nt = 0; nt < 4; nt++) {
+              rb[nt][0] = nb[nt][0];
+              rb[nt][1] = nb[nt][1];
+            }
+#pragma unroll
+            for (int q = 0; q < kMt; q++)
+#pragma unroll
+              for (int e = 0; e < 4; e++) ra[q][e] = na[q][e];
           }
         }
 #pragma unroll
