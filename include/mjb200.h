@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define MJB_ABI_VERSION 6
+#define MJB_ABI_VERSION 7
 
 typedef struct CUstream_st* mjbStream; /* == cudaStream_t */
 
@@ -233,12 +233,15 @@ typedef struct MjbTune {
   int32_t solver_warps;      /* 1, 2 or 4 */
   int32_t solver_cta_warps;  /* 2, 4, 8 or 16 warps per world; 0 = one warp per world */
   int32_t hessian_tc;        /* nv <= 32: 1 = Newton Hessian in split TF32 on the tensor pipe */
+  int32_t solver_ctas_per_sm; /* nv <= 32, FMA Hessian: resident CTAs per SM of the persistent
+                                 solver, 4 (128 registers) or 5 (96); 0 in mjb_set_tune = 5 */
   float ms_per_forward;      /* measured chosen-form forward (fwd_position .. solve) at this setting */
   float rows_per_world;      /* mean constraint rows per world of the Data it was measured on */
 } MjbTune;
 
 /* Autotuner (no counterpart in the reference): times the chosen form's forward for every
- * tree-lane count and solver CTA width on d's current worlds and keeps the fastest, per device,
+ * tree-lane count and solver CTA width (and, for nv <= 32, the persistent solver's resident CTAs
+ * per SM on the best of those) on d's current worlds and keeps the fastest, per device,
  * for models of this nv and Data of this rows-per-world capacity (njmax / nworld); later chosen-
  * form calls with the same key use it (others keep 16 lanes, 4 warps per solver CTA, FMA
  * Hessians, and 4 warps per world when nv > 128, one warp per world below).  out->rows_per_world reports the mean
@@ -250,8 +253,8 @@ typedef struct MjbTune {
 int mjb_autotune(const MjbModel* m, const MjbData* d, float* warmstart_scratch, MjbTune* out,
                  mjbStream stream);
 /* Sets the chosen form's launch parameters for the same key as mjb_autotune (device, nv, rows-
- * per-world capacity) without measuring: tree_lanes, solver_warps, solver_cta_warps and
- * hessian_tc as in MjbTune (the timing fields are ignored).  MJB_ERR_ARG for a value outside
+ * per-world capacity) without measuring: tree_lanes, solver_warps, solver_cta_warps, hessian_tc
+ * and solver_ctas_per_sm as in MjbTune (the timing fields are ignored).  MJB_ERR_ARG for a value outside
  * those sets. */
 int mjb_set_tune(const MjbModel* m, const MjbData* d, const MjbTune* tune);
 

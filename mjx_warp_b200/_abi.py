@@ -116,7 +116,7 @@ class MjbData(ctypes.Structure):
 class MjbTune(ctypes.Structure):
   _fields_ = [("tree_lanes", ctypes.c_int32), ("solver_warps", ctypes.c_int32),
               ("solver_cta_warps", ctypes.c_int32), ("hessian_tc", ctypes.c_int32),
-              ("ms_per_forward", ctypes.c_float),
+              ("solver_ctas_per_sm", ctypes.c_int32), ("ms_per_forward", ctypes.c_float),
               ("rows_per_world", ctypes.c_float)]
 
 
@@ -189,7 +189,7 @@ def lib() -> ctypes.CDLL:
   L.mjb_set_tune.argtypes = [pm, pd, ctypes.POINTER(MjbTune)]
   L.mjb_transition_vjp.restype = ctypes.c_int
   L.mjb_transition_vjp.argtypes = [pm, ci, vp, vp, vp, vp, vp, vp]
-  if L.mjb_abi_version() != 6:
+  if L.mjb_abi_version() != 7:
     raise RuntimeError("libmjb200.so ABI version mismatch")
   _lib = L
   return L

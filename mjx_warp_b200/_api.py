@@ -307,7 +307,8 @@ def autotune(m: Model, d: Data) -> dict:
   """Picks the chosen form's launch parameters for this model and Data (an extension; the
   reference has no autotuner): times the chosen forward for every tree-stage lane count (8, 16,
   32 lanes per world) and solver CTA shape (for nv <= 32 the persistent one-warp-per-world
-  solver's CTA width, 1, 2, 4 warps, with the Newton Hessian by FMAs or on the tensor pipe; for
+  solver's CTA width, 1, 2, 4 warps, with the Newton Hessian by FMAs or on the tensor pipe, then
+  4 or 5 resident CTAs per SM for the best FMA setting; for
   nv > 32 the warps per world of the CTA solver, 2,
   4, 8, or one warp per world) on d's current worlds and keeps the fastest for later calls with
   the same nv and rows-per-world capacity on this device; reports the rows per world measured.
@@ -320,20 +321,23 @@ def autotune(m: Model, d: Data) -> dict:
   _abi.check(rc, "autotune")
   return {"tree_lanes": out.tree_lanes, "solver_warps": out.solver_warps,
           "solver_cta_warps": out.solver_cta_warps, "hessian_tc": out.hessian_tc,
-          "ms_per_forward": out.ms_per_forward,
+          "solver_ctas_per_sm": out.solver_ctas_per_sm, "ms_per_forward": out.ms_per_forward,
           "rows_per_world": out.rows_per_world}
 
 
 def set_tune(m: Model, d: Data, tree_lanes: int = 16, solver_warps: int = 4,
-             solver_cta_warps: int = 4, hessian_tc: bool = False) -> None:
+             solver_cta_warps: int = 4, hessian_tc: bool = False,
+             solver_ctas_per_sm: int = 0) -> None:
   """Pins the chosen form's launch parameters for this model and Data (an extension, as
   autotune): lanes per world of the tree-recursion stages (8, 16, 32), warps per CTA of the
   one-warp-per-world solver (1, 2, 4), its Newton Hessian on the tensor pipe in split TF32
-  (hessian_tc, nv <= 32) and warps per world of the CTA solver of models with nv > 32
+  (hessian_tc, nv <= 32), its resident CTAs per SM with the FMA Hessian (solver_ctas_per_sm: 4
+  or 5, 0 for the default 5) and warps per world of the CTA solver of models with nv > 32
   (2, 4, 8, 16, or 0 for one warp per world)."""
   t = _abi.MjbTune()
   t.tree_lanes, t.solver_warps, t.solver_cta_warps = tree_lanes, solver_warps, solver_cta_warps
   t.hessian_tc = int(bool(hessian_tc))
+  t.solver_ctas_per_sm = solver_ctas_per_sm
   rc = _abi.lib().mjb_set_tune(ctypes.byref(_abi.model_view(m)), ctypes.byref(_abi.data_view(d)),
                                ctypes.byref(t))
   if rc == 1:

@@ -29,9 +29,11 @@
 #ifndef MJB_MINB
 #define MJB_MINB 4
 #endif
-// the same for the chosen form's FP32 persistent solver (k_solve_queue<false, false>): 5 CTAs
-// per SM (96 registers, with spills) measured 0.271 -> 0.258 ms on the humanoid at 8192 worlds,
-// while the plain form's solver and the precision solver were slower at 5
+// the default for the chosen form's FP32 persistent solver (k_solve_queue<false, false, *>),
+// which is compiled for 4 and for 5 (MjbTune.solver_ctas_per_sm): on the humanoid at 8192 worlds
+// 5 CTAs per SM (96 registers, with spills) measured 0.256 against 0.241 ms early in a run and
+// 0.381 against 0.352 ms once the worlds lie on the floor; the plain form's solver and the
+// precision solver were slower at 5
 #ifndef MJB_MINB_QUEUE
 #define MJB_MINB_QUEUE 5
 #endif
@@ -253,8 +255,8 @@ __global__ void __launch_bounds__(1024) k_order_worlds(const int* nefc, int* ord
   }
 }
 
-template <bool PREC, bool TC>
-__global__ void __launch_bounds__(128, (PREC || TC) ? MJB_MINB : MJB_MINB_QUEUE) k_solve_queue(const __grid_constant__ MjbModel m, const __grid_constant__ MjbData d, int smem_per_warp) {
+template <bool PREC, bool TC, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_solve_queue(const __grid_constant__ MjbModel m, const __grid_constant__ MjbData d, int smem_per_warp) {
   extern __shared__ __align__(16) float smem[];
   const int lane = threadIdx.x & 31;
   float* sm = smem_per_warp ? smem + size_t(threadIdx.x >> 5) * smem_per_warp : nullptr;
@@ -690,6 +692,7 @@ struct ChosenCfg {
   int warps = kDefaultWarps;
   int cta_warps = 4;  // warps per world of the solver for nv > 32 (0: one warp per world)
   int hessian_tc = 0; // nv <= 32: Newton Hessian on the tensor pipe (split TF32) instead of FMAs
+  int solver_ctas = MJB_MINB_QUEUE;  // CTAs per SM of the FP32 FMA-Hessian persistent solver (4, 5)
 };
 struct TuneEntry {
   int dev, nv, cap;
@@ -839,17 +842,26 @@ void launch_solver_cta(const MjbModel* m, const MjbData* d, int tc, cudaStream_t
   }
 }
 
+template <bool PREC, bool TC, int MINB>
+void launch_solver_queue(const MjbModel* m, const MjbData* d, int qw, int spw, cudaStream_t s) {
+  const size_t qbytes = size_t(spw) * qw * sizeof(float);
+  static size_t conf_queue[kSmemDevices];
+  allow_smem(k_solve_queue<PREC, TC, MINB>, size_t(spw) * kDefaultWarps * sizeof(float), conf_queue);
+  const int ctas = resident_ctas(k_solve_queue<PREC, TC, MINB>, 32 * qw, qbytes);
+  k_order_worlds<<<1, 1024, 0, s>>>(d->world_nefc, d->world_order, d->work_queue, d->nworld);
+  k_solve_queue<PREC, TC, MINB><<<std::min(ctas, grid_for(d->nworld, qw)), 32 * qw, qbytes, s>>>(*m, *d, spw);
+}
+
 template <bool PREC, bool TC>
 void launch_solver_warp(const MjbModel* m, const MjbData* d, const ChosenCfg& cfg, int spw,
                         cudaStream_t s) {
   if (d->world_order && d->work_queue && d->world_nefc) {
-    const int qw = cfg.warps;
-    const size_t qbytes = size_t(spw) * qw * sizeof(float);
-    static size_t conf_queue[kSmemDevices];
-    allow_smem(k_solve_queue<PREC, TC>, size_t(spw) * kDefaultWarps * sizeof(float), conf_queue);
-    const int ctas = resident_ctas(k_solve_queue<PREC, TC>, 32 * qw, qbytes);
-    k_order_worlds<<<1, 1024, 0, s>>>(d->world_nefc, d->world_order, d->work_queue, d->nworld);
-    k_solve_queue<PREC, TC><<<std::min(ctas, grid_for(d->nworld, qw)), 32 * qw, qbytes, s>>>(*m, *d, spw);
+    if constexpr (PREC || TC) {
+      launch_solver_queue<PREC, TC, MJB_MINB>(m, d, cfg.warps, spw, s);
+    } else {
+      if (cfg.solver_ctas == 4) launch_solver_queue<PREC, TC, 4>(m, d, cfg.warps, spw, s);
+      else launch_solver_queue<PREC, TC, 5>(m, d, cfg.warps, spw, s);
+    }
   } else {
     const size_t bytes = size_t(spw) * kDefaultWarps * sizeof(float);
     static size_t conf_solve[kSmemDevices];
@@ -1299,6 +1311,11 @@ extern "C" int mjb_autotune(const MjbModel* m, const MjbData* d, float* warmstar
     c.hessian_tc = 1;
     rc = trial(c);
   }
+  if (!rc && !large && !best_cfg.hessian_tc) {  // the persistent solver's other occupancy
+    ChosenCfg c = best_cfg;
+    c.solver_ctas = best_cfg.solver_ctas == 4 ? 5 : 4;
+    rc = trial(c);
+  }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   int nefc = 0;  // rows of the last trial's forward (the same worlds in every trial)
@@ -1314,6 +1331,7 @@ extern "C" int mjb_autotune(const MjbModel* m, const MjbData* d, float* warmstar
     out->solver_warps = best_cfg.warps;
     out->solver_cta_warps = best_cfg.cta_warps;
     out->hessian_tc = best_cfg.hessian_tc;
+    out->solver_ctas_per_sm = best_cfg.solver_ctas;
     out->ms_per_forward = best;
     out->rows_per_world = float(std::min(nefc, d->njmax)) / float(d->nworld);
   }
@@ -1325,15 +1343,17 @@ extern "C" int mjb_set_tune(const MjbModel* m, const MjbData* d, const MjbTune* 
   if (rc) return rc;
   if (!tune) return MJB_ERR_ARG;
   const int l = tune->tree_lanes, w = tune->solver_warps, c = tune->solver_cta_warps;
+  const int o = tune->solver_ctas_per_sm;
   if ((l != 8 && l != 16 && l != 32) || (w != 1 && w != 2 && w != 4) ||
       (c != 0 && c != 2 && c != 4 && c != 8 && c != 16) ||
-      (tune->hessian_tc != 0 && tune->hessian_tc != 1))
+      (tune->hessian_tc != 0 && tune->hessian_tc != 1) || (o != 0 && o != 4 && o != 5))
     return MJB_ERR_ARG;
   ChosenCfg cfg;
   cfg.lanes = l;
   cfg.warps = w;
   cfg.cta_warps = c;
   cfg.hessian_tc = tune->hessian_tc;
+  if (o) cfg.solver_ctas = o;
   store_cfg(m, d, cfg);
   return MJB_OK;
 }

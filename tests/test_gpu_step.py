@@ -234,13 +234,15 @@ def test_autotune_picks_a_setting_and_keeps_results():
     cfg = mjw.autotune(m, d)
     assert cfg["tree_lanes"] in (8, 16, 32) and cfg["solver_warps"] in (1, 2, 4)
     assert cfg["hessian_tc"] in (0, 1) and cfg["ms_per_forward"] > 0
+    assert cfg["solver_ctas_per_sm"] in (4, 5)
     assert cfg["rows_per_world"] > 0
     assert torch.equal(d.qacc_warmstart, ws) and torch.equal(d.qpos, q)
     for tc in (False, True):
       out = []
-      for lanes, warps in ((8, 1), (32, 4)):
+      for lanes, warps, ctas in ((8, 1, 4), (32, 4, 5)):
         dd = device_data(mjm, qpos, qvel, ctrl)
-        mjw.set_tune(m, dd, tree_lanes=lanes, solver_warps=warps, hessian_tc=tc)
+        mjw.set_tune(m, dd, tree_lanes=lanes, solver_warps=warps, hessian_tc=tc,
+                     solver_ctas_per_sm=ctas)
         for _ in range(3):
           mjw.step(m, dd)
         torch.cuda.synchronize()

@@ -123,7 +123,7 @@ def test_library_exports_every_declared_entry_point():
   lib = _abi.lib()
   for n in names:
     assert hasattr(lib, n), n
-  assert lib.mjb_abi_version() == 6
+  assert lib.mjb_abi_version() == 7
   assert lib.mjb_error_string(0) == b"ok"
 
 
