@@ -602,8 +602,8 @@ __device__ MJB_TILE_FN float cho_solve_tile(const float* L, int ld, int n, float
 }
 
 // FP64 counterparts of chol_tile / cho_solve_tile for the precision form (MJB_FORM_PRECISION):
-// the same lane-per-row scheme on a tile of doubles (row stride ld doubles), with the pivot from
-// the double square root and division.
+// the same lane-per-row scheme on a tile of doubles (row stride ld doubles), the pivot and its
+// reciprocal from one double rsqrt (L_kk = s_k rsqrt(s_k), L_ik = s_i rsqrt(s_k)) as in chol_tile.
 // chol_tile_d takes two columns per step as chol_tile does (k even: both columns' pairs of
 // partial sums cover [0, k), column k + 1 adds L[i][k] L[k+1][k] as its tail term).
 __device__ __noinline__ void chol_tile_d(double* A, int ld, int n, int lane) {
@@ -621,35 +621,35 @@ __device__ __noinline__ void chol_tile_d(double* A, int ld, int n, int lane) {
       t1 += a1 * Ak1[m + 1];
     }
     const double si = Ar[k] - (s0 + s1);
-    const double lkk = sqrt(__shfl_sync(WARP_FULL, si, k));
-    const double lik = lane == k ? lkk : si / lkk;
+    const double lik = si * rsqrt(__shfl_sync(WARP_FULL, si, k));  // on lane k the pivot
     if (lane >= k && lane < n) Ar[k] = lik;
     if (two) {
       t0 += lik * __shfl_sync(WARP_FULL, lik, k + 1);
       const double ti = Ar[k + 1] - (t0 + t1);
-      const double l1 = sqrt(__shfl_sync(WARP_FULL, ti, k + 1));
-      if (lane == k + 1) Ar[k + 1] = l1;
-      else if (lane > k + 1 && lane < n) Ar[k + 1] = ti / l1;
+      const double li1 = ti * rsqrt(__shfl_sync(WARP_FULL, ti, k + 1));
+      if (lane > k && lane < n) Ar[k + 1] = li1;
     }
     __syncwarp();
   }
 }
+// The substitutions multiply by each lane's reciprocal pivot, formed once (one FP64 division per
+// lane instead of one per step of each pass); lane k scales its entry, one shuffle broadcasts it.
 __device__ __noinline__ double cho_solve_tile_d(const double* L, int ld, int n, double y, int lane) {
   const bool own = lane < n;
   const double* Li = L + min(lane, n - 1) * ld;
-  const double dd = own ? Li[lane] : 1.0;
+  const double invd = own ? 1.0 / Li[lane] : 0.0;
   double z = own ? y : 0.0;
   for (int k = 0; k < n; k++) {
-    const double zk = __shfl_sync(WARP_FULL, z, k) / __shfl_sync(WARP_FULL, dd, k);
-    if (lane == k) z = zk;
-    else if (lane > k && own) z -= Li[k] * zk;
+    if (lane == k) z *= invd;
+    const double zk = __shfl_sync(WARP_FULL, z, k);
+    if (lane > k && own) z -= Li[k] * zk;
   }
   double x = z;
   for (int k = n - 1; k >= 0; k--) {
     const double lk = L[k * ld + (lane < k ? lane : 0)];
-    const double xk = __shfl_sync(WARP_FULL, x, k) / __shfl_sync(WARP_FULL, dd, k);
-    if (lane == k) x = xk;
-    else if (lane < k) x -= lk * xk;
+    if (lane == k) x *= invd;
+    const double xk = __shfl_sync(WARP_FULL, x, k);
+    if (lane < k) x -= lk * xk;
   }
   return own ? x : 0.0;
 }
