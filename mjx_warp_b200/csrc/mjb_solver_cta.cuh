@@ -325,8 +325,9 @@ __device__ __noinline__ void chol_cta_d(double* P, double* rd, int n, int warp, 
           s = Li[k];
           for (int q = 0; q < k; q++) s -= Li[q] * Lk[q];
         }
-        const double lkk = sqrt(__shfl_sync(WARP_FULL, s, 0));
-        const double inv = 1.0 / lkk;
+        const double sk = __shfl_sync(WARP_FULL, s, 0);
+        const double inv = rsqrt(sk);  // the pivot's reciprocal; L_kk = s_k rsqrt(s_k)
+        const double lkk = sk * inv;
         __syncwarp();
         if (lane == 0) {
           P[tri(c0 + k) + c0 + k] = lkk;
