@@ -604,30 +604,39 @@ __device__ MJB_TILE_FN float cho_solve_tile(const float* L, int ld, int n, float
 // FP64 counterparts of chol_tile / cho_solve_tile for the precision form (MJB_FORM_PRECISION):
 // the same lane-per-row scheme on a tile of doubles (row stride ld doubles), the pivot and its
 // reciprocal from one double rsqrt (L_kk = s_k rsqrt(s_k), L_ik = s_i rsqrt(s_k)) as in chol_tile.
-// chol_tile_d takes two columns per step as chol_tile does (k even: both columns' pairs of
-// partial sums cover [0, k), column k + 1 adds L[i][k] L[k+1][k] as its tail term).
+// chol_tile_d takes four columns per step as chol_tile does: one pass over the row's finished
+// columns (pairs of partial sums, k a multiple of 4) feeds the four columns, then column k + j
+// adds the terms of columns k .. k + j - 1 as the one-column form orders them (the pair
+// (k, k + 1) into the two partial sums, column k + 2 as the tail term).
 __device__ __noinline__ void chol_tile_d(double* A, int ld, int n, int lane) {
   double* Ar = A + min(lane, n - 1) * ld;  // lane i on row i; lanes past the last row repeat it
-  for (int k = 0; k < n; k += 2) {
-    const bool two = k + 1 < n;
-    const double* Ak = A + k * ld;
-    const double* Ak1 = two ? Ak + ld : Ak;
-    double s0 = 0.0, s1 = 0.0, t0 = 0.0, t1 = 0.0;
-    for (int m = 0; m + 1 < k; m += 2) {
+  for (int k = 0; k < n; k += 4) {
+    const int nb = min(4, n - k);
+    const double* Ak[4];
+#pragma unroll
+    for (int j = 0; j < 4; j++) Ak[j] = A + (k + (j < nb ? j : 0)) * ld;
+    double s[4][2];
+#pragma unroll
+    for (int j = 0; j < 4; j++) s[j][0] = s[j][1] = 0.0;
+    for (int m = 0; m < k; m += 2) {
       const double a0 = Ar[m], a1 = Ar[m + 1];
-      s0 += a0 * Ak[m];
-      s1 += a1 * Ak[m + 1];
-      t0 += a0 * Ak1[m];
-      t1 += a1 * Ak1[m + 1];
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        s[j][0] += a0 * Ak[j][m];
+        s[j][1] += a1 * Ak[j][m + 1];
+      }
     }
-    const double si = Ar[k] - (s0 + s1);
-    const double lik = si * rsqrt(__shfl_sync(WARP_FULL, si, k));  // on lane k the pivot
-    if (lane >= k && lane < n) Ar[k] = lik;
-    if (two) {
-      t0 += lik * __shfl_sync(WARP_FULL, lik, k + 1);
-      const double ti = Ar[k + 1] - (t0 + t1);
-      const double li1 = ti * rsqrt(__shfl_sync(WARP_FULL, ti, k + 1));
-      if (lane > k && lane < n) Ar[k + 1] = li1;
+    double l[4] = {0.0, 0.0, 0.0, 0.0};  // L[i][k + j]; on lane k + j the pivot
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      if (j < nb) {
+        if (j >= 1) s[j][0] += l[0] * __shfl_sync(WARP_FULL, l[0], k + j);
+        if (j >= 2) s[j][1] += l[1] * __shfl_sync(WARP_FULL, l[1], k + j);
+        if (j >= 3) s[j][0] += l[2] * __shfl_sync(WARP_FULL, l[2], k + j);
+        const double x = Ar[k + j] - (s[j][0] + s[j][1]);
+        l[j] = x * rsqrt(__shfl_sync(WARP_FULL, x, k + j));
+        if (lane >= k + j && lane < n) Ar[k + j] = l[j];
+      }
     }
     __syncwarp();
   }
