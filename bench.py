@@ -746,6 +746,16 @@ def run_ours(args):
   qvel_h = torch.empty(d.qvel.shape, dtype=torch.float32).pin_memory()
   copy = torch.cuda.Stream()
   main = torch.cuda.current_stream()
+  # one captured CUDA graph of the step_io call per buffer pair, as a framework that calls it every
+  # step would use it (the call is graph-capturable; the transfers stay outside, on the copy stream)
+  io_graphs = []
+  for b in range(2):
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+      mjw.step_io(m, d, 1, inputs={"ctrl": ctrl_d[b]}, outputs=("qpos", "qvel"), out=io_out[b],
+                  fused=form)
+    io_graphs.append(g)
+  torch.cuda.synchronize()
   up = [torch.cuda.Event() for _ in range(2)]      # control t uploaded
   done = [torch.cuda.Event() for _ in range(2)]    # step t's outputs written / its control read
   down = [torch.cuda.Event() for _ in range(2)]    # outputs t downloaded
@@ -768,8 +778,7 @@ def run_ours(args):
     main.wait_event(up[b])
     if t >= 2:
       main.wait_event(down[b])  # step t - 2's outputs left this buffer
-    mjw.step_io(m, d, 1, inputs={"ctrl": ctrl_d[b]}, outputs=("qpos", "qvel"), out=io_out[b],
-                fused=form)
+    io_graphs[b].replay()
     done[b].record(main)
     with torch.cuda.stream(copy):
       copy.wait_event(done[b])
@@ -780,6 +789,7 @@ def run_ours(args):
   e1.record()
   barrier()
   e2e_elapsed = replicas.max_over_ranks(e0.elapsed_time(e1) / 1000.0, device="cuda")
+  del io_graphs
 
   # the dominant kernel (the solver) timed around its own launch, same stream, K steps
   solve_ms = []
@@ -878,7 +888,8 @@ def run_ours(args):
     "e2e": {"value": total_worlds * args.steps / e2e_elapsed, "unit": "steps/s",
             "h2d_bytes_per_step": _bytes_of(ctrl_h),
             "d2h_bytes_per_step": _bytes_of(qpos_h) + _bytes_of(qvel_h),
-            "call": "mjw.step_io (mjb_step_io: ctrl in, one step, qpos / qvel out); transfers "
+            "call": "mjw.step_io (mjb_step_io: ctrl in, one step, qpos / qvel out), one captured "
+                    "CUDA graph of the call per buffer, replayed every step; transfers "
                     "double-buffered on a copy stream, overlapping the neighbouring steps"},
     "gpu_launches": launches_per_step * args.steps,
     "roofline": {"bound": "fp32" if flop_bound else "hbm",
