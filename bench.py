@@ -13,8 +13,8 @@ K times, in the chosen launch form (the stage kernels to fwd_acceleration forked
 streams, the solver's world ordering + persistent k_solve_queue, k_integrate); `forms` gives the
 same number for the plain one-kernel-per-stage form, the single-kernel form and the precision
 form, measured in the same run.  e2e: the metric through the public API's host-framework call
-(mjw.step_io) with, every step, the control copied in from pinned host memory and qpos / qvel
-copied back.  roofline: the dominant kernel (the solver) timed with CUDA events around its own
+(mjw.step_io, captured once per buffer in a CUDA graph and replayed) with, every step, the control
+copied in from pinned host memory and qpos / qvel copied back.  roofline: the dominant kernel (the solver) timed with CUDA events around its own
 launch (mjw.step_phase) over K steps, against the FP32 FMA peak measured in the same run
 (mjb_fma_probe) and the measured HBM bandwidth; the bound is whichever takes longer.
 Multi-GPU: one process per GPU, each owning its own 8192 worlds (replicas, weak scaling, no
