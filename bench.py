@@ -572,7 +572,7 @@ def _bin_config(mjw, torch, nworld=4096, steps=500, plain_steps=10, sample=16):
           "qacc_err_vs_fp64": {"worlds": s, "median": float(np.median(e)), "max": float(e.max()),
                                "frac_le_1e-4": float(np.mean(e <= 1e-4)),
                                "cost_within_2.5pct": float(np.mean(cost_ok))},
-          "roofline": {"kernel": "k_solve_cta (+ k_order_worlds)", "kernel_ms": solve_s * 1e3,
+          "roofline": {"kernel": "k_solve_cta", "kernel_ms": solve_s * 1e3,
                        "flops_per_launch": flops, "achieved_tflops": flops / solve_s / 1e12,
                        "peak_tflops": fma["fp32_tflops"],
                        "frac": flops / solve_s / 1e12 / fma["fp32_tflops"], "bound": "fp32",
@@ -899,7 +899,7 @@ def run_ours(args):
                  "frac": flop_rate / fma["fp32_tflops"] if flop_bound else achieved / hbm,
                  "traffic": traffic,
                  "kernel": "k_stage<S_SOLVE> (plain)" if args.form == "plain"
-                           else "k_solve_queue (+ k_order_worlds)",
+                           else "k_solve_queue",
                  "kernel_ms": solve_s * 1e3, "kernel_share_of_step": solve_s / (elapsed / args.steps),
                  "flops_per_launch": solver_flops, "algorithmic_bytes_per_launch": alg,
                  "t_min_us": {"fp32": t_flop * 1e6, "hbm": t_hbm * 1e6},

@@ -161,9 +161,11 @@ int mjb_step(const MjbModel* m, const MjbData* d, const MjbRunCfg* cfg, mjbStrea
 /* forward (forward.py:664-679). */
 int mjb_forward(const MjbModel* m, const MjbData* d, const MjbRunCfg* cfg, mjbStream stream);
 /* One phase of MJB_FORM_CHOSEN's step (no counterpart in the reference, whose step is one call):
-   0 = counter reset + fwd_position .. fwd_acceleration, 1 = the constraint solver, 2 = Euler /
+   0 = counter reset + fwd_position .. fwd_acceleration (and the ordering of the worlds by their
+   constraint rows for phase 1's persistent solver), 1 = the constraint solver, 2 = Euler /
    implicitfast integration + the finiteness check.  Phases 0, 1, 2 in order equal mjb_step; they
-   let a caller time the kernels separately or act between forward and integration. */
+   let a caller time the kernels separately or act between forward and integration.  Phase 1
+   reads phase 0's ordering: run it once after each phase 0. */
 int mjb_step_phase(const MjbModel* m, const MjbData* d, int phase, mjbStream stream);
 
 /* The device buffers of a host framework's step call (the JAX FFI pattern of

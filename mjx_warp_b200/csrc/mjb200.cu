@@ -746,6 +746,13 @@ void rebuild_index(const int* worldid, const int* counter, int cap, int* adr, in
   k_index_fix<<<grid_for(d->nworld, 4), 128, 0, s>>>(worldid, adr, cnt, d->world_status, d->nworld);
 }
 
+// the chosen form's world ordering for its persistent solvers (k_order_worlds), launched in
+// phase 0 once the rows are made, so that it overlaps the other forward chains' tails
+inline void order_worlds(const MjbData* d, cudaStream_t s) {
+  if (d->njmax > 0 && d->world_order && d->work_queue && d->world_nefc)
+    k_order_worlds<<<1, 1024, 0, s>>>(d->world_nefc, d->world_order, d->work_queue, d->nworld);
+}
+
 int run_forward_plain_nosolve(const MjbModel* m, const MjbData* d, cudaStream_t s) {
   int rc;
   if ((rc = launch_stage<S_KINEMATICS>(m, d, s))) return rc;
@@ -781,8 +788,11 @@ StageFork g_fork[kSmemDevices];
 
 int run_forward_fork(const MjbModel* m, const MjbData* d, cudaStream_t s, int lanes) {
   int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kSmemDevices)
-    return run_forward_plain_nosolve(m, d, s);
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kSmemDevices) {
+    const int rc = run_forward_plain_nosolve(m, d, s);
+    if (!rc) order_worlds(d, s);
+    return rc;
+  }
   std::lock_guard<std::mutex> lock(g_fork_mutex);
   StageFork& f = g_fork[dev];
   if (!f.ready) {
@@ -807,6 +817,7 @@ int run_forward_fork(const MjbModel* m, const MjbData* d, cudaStream_t s, int la
   int rc2 = launch_broadphase(m, d, s);
   if (!rc2) rc2 = launch_stage<S_NARROW>(m, d, s);
   if (!rc2) rc2 = launch_stage<S_MAKE_CONSTRAINT>(m, d, s);
+  if (!rc2) order_worlds(d, s);
   // join even after a failed launch, so a capture is never left with unjoined streams
   if (cudaEventRecord(f.ev[1], f.aux[0]) != cudaSuccess) return MJB_ERR_LAUNCH;
   if (cudaEventRecord(f.ev[2], f.aux[1]) != cudaSuccess) return MJB_ERR_LAUNCH;
@@ -832,8 +843,7 @@ void launch_solver_cta(const MjbModel* m, const MjbData* d, int tc, cudaStream_t
   static size_t conf[kSmemDevices];
   allow_smem(k_solve_cta<NW, PREC>, bytes, conf);
   if (d->world_order && d->work_queue && d->world_nefc) {
-    const int ctas = resident_ctas(k_solve_cta<NW, PREC>, 32 * NW, bytes);
-    k_order_worlds<<<1, 1024, 0, s>>>(d->world_nefc, d->world_order, d->work_queue, d->nworld);
+    const int ctas = resident_ctas(k_solve_cta<NW, PREC>, 32 * NW, bytes);  // ordered in phase 0
     k_solve_cta<NW, PREC><<<std::min(ctas, d->nworld), 32 * NW, bytes, s>>>(*m, *d, tc);
   } else {
     MjbData dd = *d;
@@ -847,8 +857,7 @@ void launch_solver_queue(const MjbModel* m, const MjbData* d, int qw, int spw, c
   const size_t qbytes = size_t(spw) * qw * sizeof(float);
   static size_t conf_queue[kSmemDevices];
   allow_smem(k_solve_queue<PREC, TC, MINB>, size_t(spw) * kDefaultWarps * sizeof(float), conf_queue);
-  const int ctas = resident_ctas(k_solve_queue<PREC, TC, MINB>, 32 * qw, qbytes);
-  k_order_worlds<<<1, 1024, 0, s>>>(d->world_nefc, d->world_order, d->work_queue, d->nworld);
+  const int ctas = resident_ctas(k_solve_queue<PREC, TC, MINB>, 32 * qw, qbytes);  // ordered in phase 0
   k_solve_queue<PREC, TC, MINB><<<std::min(ctas, grid_for(d->nworld, qw)), 32 * qw, qbytes, s>>>(*m, *d, spw);
 }
 
